@@ -1,0 +1,113 @@
+"""In-tree build of the native libraries, for sm_100a (B200):
+
+  qoraholo_b200/libqhk.so        CUDA kernels and the C ABI (include/qoraholo_b200.h)
+  qoraholo_b200/libqoraholo.so   the C++20 host API (include/qoraholo/*.hpp) over the C ABI
+  qoraholo_b200/_core*.so        pybind11 bindings with the reference's Python signatures
+
+nvcc cross-compiles without a GPU. Objects go to qoraholo_b200/_build/; a library is rebuilt
+when any of its sources or headers is newer. Usage: python -m qoraholo_b200._build [--force]
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import sysconfig
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+INCLUDE = ROOT / "include"
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++20", "-O3", *ARCH, "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler",
+              "-fPIC,-ffp-contract=off", f"-I{INCLUDE}", f"-I{CSRC}"]
+CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", f"-I{INCLUDE}", f"-I{CSRC}"]
+
+LIB_QHK = PKG / "libqhk.so"
+LIB_HOST = PKG / "libqoraholo.so"
+
+
+def _newest(paths):
+    return max((p.stat().st_mtime for p in paths if p.exists()), default=0.0)
+
+
+def _headers():
+    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list(INCLUDE.rglob("*.h*"))
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build failed: {' '.join(map(str, cmd))}\n{r.stdout}\n{r.stderr}")
+    return r
+
+
+def _compile_many(jobs):
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        list(ex.map(_run, jobs))
+
+
+def build_qhk(force=False) -> Path:
+    sources = sorted(CSRC.glob("*.cu"))
+    BUILD.mkdir(exist_ok=True)
+    hdr_time = _newest(_headers())
+    jobs, objs = [], []
+    for src in sources:
+        obj = BUILD / (src.stem + ".o")
+        objs.append(obj)
+        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_time):
+            jobs.append([NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+    _compile_many(jobs)
+    if force or jobs or not LIB_QHK.exists() or LIB_QHK.stat().st_mtime < _newest(objs):
+        _run([NVCC, *ARCH, "-shared", "-o", str(LIB_QHK), *map(str, objs)])
+    return LIB_QHK
+
+
+def build_host(force=False) -> Path | None:
+    host_dir = CSRC / "host"
+    sources = sorted(host_dir.glob("*.cpp")) if host_dir.exists() else []
+    if not sources:
+        return None
+    BUILD.mkdir(exist_ok=True)
+    hdr_time = max(_newest(_headers()), _newest(host_dir.glob("*.hpp")))
+    jobs, objs = [], []
+    for src in sources:
+        obj = BUILD / ("host_" + src.stem + ".o")
+        objs.append(obj)
+        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_time):
+            jobs.append(["g++", *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
+    _compile_many(jobs)
+    if force or jobs or not LIB_HOST.exists() or LIB_HOST.stat().st_mtime < max(_newest(objs), LIB_QHK.stat().st_mtime):
+        _run(["g++", "-shared", "-o", str(LIB_HOST), *map(str, objs), f"-L{PKG}", "-lqhk", "-Wl,-rpath,$ORIGIN"])
+    return LIB_HOST
+
+
+def build_bindings(force=False) -> Path | None:
+    src = CSRC / "bindings.cpp"
+    if not src.exists():
+        return None
+    import pybind11
+
+    suffix = sysconfig.get_config_var("EXT_SUFFIX")
+    out = PKG / f"_core{suffix}"
+    deps = [src, LIB_HOST, *(_headers())]
+    if force or not out.exists() or out.stat().st_mtime < _newest(deps):
+        _run(["g++", *CXX_FLAGS, "-shared", f"-I{pybind11.get_include()}", f"-I{sysconfig.get_paths()['include']}",
+              str(src), "-o", str(out), f"-L{PKG}", "-lqoraholo", "-lqhk", "-Wl,-rpath,$ORIGIN"])
+    return out
+
+
+def build(force=False):
+    build_qhk(force)
+    build_host(force)
+    build_bindings(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)
+    print("built", LIB_QHK)

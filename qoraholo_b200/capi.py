@@ -1,0 +1,175 @@
+"""ctypes binding of the C ABI in include/qoraholo_b200.h (libqhk.so).
+
+This is the device-level interface: plans and kernels take device pointers (ints; e.g. a torch
+tensor's ``data_ptr()``) and a CUDA stream handle. The reference-compatible numpy API lives in
+``qoraholo_b200`` (``__init__.py``) on top of the C++ host layer. Loading fails loudly if the
+library has not been built (``python -m qoraholo_b200._build``); there is no fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libqhk.so"
+
+OK, INVALID_ARGUMENT, CUDA_ERROR, LOGIC_ERROR, OUT_OF_MEMORY, TIMEOUT, INTERNAL = range(7)
+SOLVERS = {"gp": 0, "tv": 1}
+TRANSFORMS = {"r2c": 0, "c2c": 1}
+MAPPINGS = {"gather": 0, "scatter": 1}
+
+_lib = None
+
+
+class QhkError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+class Geometry(C.Structure):
+    _fields_ = [("wavelength", C.c_float), ("n_medium", C.c_float), ("na", C.c_float), ("pixel", C.c_float)]
+
+
+class OdtOptions(C.Structure):
+    _fields_ = [("nz", C.c_int), ("iterations", C.c_int), ("solver", C.c_int), ("gp_transform", C.c_int),
+                ("tv_weight", C.c_float), ("tv_inner", C.c_int), ("mapping", C.c_int)]
+
+
+_VP = C.c_void_p
+_I = C.c_int
+_F = C.c_float
+_PROTOS = {
+    "qhk_last_error": (C.c_char_p, []),
+    "qhk_device_present": (_I, []),
+    "qhk_odt_create": (_I, [C.POINTER(_VP), _I, _I, _VP, C.POINTER(Geometry), C.POINTER(OdtOptions)]),
+    "qhk_odt_run": (_I, [_VP, _VP, _VP, _VP]),
+    "qhk_odt_filled": (_I, [_VP, _VP, C.POINTER(C.c_double)]),
+    "qhk_odt_shape": (_I, [_VP, C.POINTER(_I), C.POINTER(_I)]),
+    "qhk_odt_device_bytes": (C.c_size_t, [_VP]),
+    "qhk_odt_destroy": (_I, [_VP]),
+    "qhk_reconstruct": (_I, [_VP, _I, _I, _VP, C.POINTER(Geometry), C.POINTER(OdtOptions), _VP,
+                             C.POINTER(C.c_double)]),
+    "qhk_ewald_map": (_I, [_VP, _I, _I, _I, _VP, C.POINTER(Geometry), _I, _VP, _VP, _VP, _VP]),
+    "qhk_tv_prox": (_I, [_VP, _VP, _VP, _I, _I, _I, _F, _I, _VP]),
+    "qhk_fft2d": (_I, [_VP, _I, _I, _I, _F, _VP]),
+    "qhk_rfft3": (_I, [_VP, _VP, _I, _I, _I, _VP]),
+    "qhk_irfft3": (_I, [_VP, _VP, _I, _I, _I, _F, _VP]),
+}
+
+
+def lib():
+    """The loaded libqhk.so with argument types declared."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m qoraholo_b200._build`")
+        _lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(_lib, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+def check(code):
+    if code != OK:
+        msg = lib().qhk_last_error().decode()
+        if code == INVALID_ARGUMENT:
+            raise ValueError(msg)
+        raise QhkError(code, msg)
+
+
+def geometry(g) -> Geometry:
+    w, nm, na, px = (float(v) for v in (g if not hasattr(g, "wavelength") else (g.wavelength, g.n_medium, g.na, g.pixel)))
+    return Geometry(w, nm, na, px)
+
+
+def odt_options(nz=0, iterations=0, solver="gp", gp_transform="r2c", tv_weight=1e-2, tv_inner=10,
+                mapping="gather") -> OdtOptions:
+    return OdtOptions(int(nz), int(iterations), SOLVERS[solver], TRANSFORMS[gp_transform], float(tv_weight),
+                      int(tv_inner), MAPPINGS[mapping])
+
+
+def host_ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_VP)
+
+
+def device_present() -> bool:
+    return bool(lib().qhk_device_present())
+
+
+class OdtPlan:
+    """Device-resident solver for one geometry (qhk_odt_*): fields -> index, no allocation per run."""
+
+    def __init__(self, n, count, illuminations, geom, **options):
+        self._il = np.ascontiguousarray(np.reshape(illuminations, (-1, 2)), np.float32)
+        self._h = _VP()
+        check(lib().qhk_odt_create(C.byref(self._h), int(n), int(count), host_ptr(self._il), C.byref(geometry(geom)),
+                                   C.byref(odt_options(**options))))
+        nz, nn = _I(), _I()
+        check(lib().qhk_odt_shape(self._h, C.byref(nz), C.byref(nn)))
+        self.shape = (nz.value, nn.value, nn.value)
+
+    def run(self, d_fields: int, d_index: int, stream: int = 0):
+        check(lib().qhk_odt_run(self._h, _VP(d_fields), _VP(d_index), _VP(stream)))
+
+    def filled(self, stream: int = 0) -> float:
+        v = C.c_double()
+        check(lib().qhk_odt_filled(self._h, _VP(stream), C.byref(v)))
+        return v.value
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().qhk_odt_device_bytes(self._h))
+
+    def close(self):
+        if self._h:
+            check(lib().qhk_odt_destroy(self._h))
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def reconstruct(fields, illuminations, geom, **options):
+    """qhk_reconstruct: host complex64 fields (count, n, n) -> (ri, filled)."""
+    f = np.ascontiguousarray(fields, np.complex64)
+    il = np.ascontiguousarray(np.reshape(illuminations, (-1, 2)), np.float32)
+    count, n = f.shape[0], f.shape[2]
+    nz = options.get("nz", 0) or n
+    out = np.zeros((nz, n, n), np.float32)
+    filled = C.c_double()
+    check(lib().qhk_reconstruct(host_ptr(f), count, n, host_ptr(il), C.byref(geometry(geom)),
+                                C.byref(odt_options(**options)), host_ptr(out), C.byref(filled)))
+    return out, filled.value
+
+
+def ewald_map(d_spectra, count, n, nz, illuminations, geom, half, d_data, d_hits, d_filled, stream=0):
+    il = np.ascontiguousarray(np.reshape(illuminations, (-1, 2)), np.float32)
+    check(lib().qhk_ewald_map(_VP(d_spectra), count, n, nz, host_ptr(il), C.byref(geometry(geom)), int(half),
+                              _VP(d_data), _VP(d_hits), _VP(d_filled), _VP(stream)))
+
+
+def tv_prox(d_b, d_x, d_dual, nz, ny, nx, lam, inner, stream=0):
+    check(lib().qhk_tv_prox(_VP(d_b), _VP(d_x), _VP(d_dual), nz, ny, nx, float(lam), int(inner), _VP(stream)))
+
+
+def fft2d(d_data, count, n, forward=True, scale=1.0, stream=0):
+    check(lib().qhk_fft2d(_VP(d_data), count, n, int(forward), float(scale), _VP(stream)))
+
+
+def rfft3(d_x, d_half, nz, ny, nx, stream=0):
+    check(lib().qhk_rfft3(_VP(d_x), _VP(d_half), nz, ny, nx, _VP(stream)))
+
+
+def irfft3(d_half, d_x, nz, ny, nx, scale=1.0, stream=0):
+    check(lib().qhk_irfft3(_VP(d_half), _VP(d_x), nz, ny, nx, float(scale), _VP(stream)))

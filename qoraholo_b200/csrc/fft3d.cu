@@ -1,0 +1,491 @@
+// FFT passes over HBM-resident volumes and image stacks, built on the shared-memory engine
+// (fft_engine.cuh). One kernel launch is one pass over the data along one axis: a CTA stages a
+// tile of lines, transforms it on chip and writes it back, with the pointwise step that precedes
+// or follows the transform folded into the load or the store:
+//   * axis passes along y or z of (outer, pos, inner) data, tiles of COLS contiguous columns;
+//     the z pass of the Gerchberg-Papoulis / FISTA loop runs forward transform, k-space restore
+//     and inverse transform in one launch (the restore touches every voxel exactly there);
+//   * real rows <-> half spectra by a half-length complex FFT (two real samples per complex
+//     value) with the split / merge step in shared memory;
+//   * complex rows, with the clamp of the complex GP loop between its inverse and forward row
+//     transforms, or the refractive index as the epilogue of the last inverse.
+#include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+
+#include "qhk_internal.hpp"
+
+namespace qhk {
+
+int sm_count() {
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  int n = 0;
+  check(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+  return n;
+}
+
+FftLen make_fft_len(int n) {
+  require(n >= 1, "fft: length must be positive");
+  FftLen L;
+  L.n = n;
+  int m = n;
+  const auto push = [&](int r) {
+    if (L.passes >= kMaxPasses) fail(kInternal, "fft: too many passes");
+    L.radix[L.passes++] = r;
+    m /= r;
+  };
+  while (m % 8 == 0) push(8);
+  if (m % 4 == 0) push(4);
+  if (m % 2 == 0) push(2);
+  while (m % 3 == 0) push(3);
+  while (m % 5 == 0) push(5);
+  for (int p = 7; m > 1; p += 2) {
+    while (m % p == 0) push(p);
+  }
+  return L;
+}
+
+namespace {
+
+struct TwiddleEntry {
+  FftLen len;
+  DevBuf<float2> table;
+};
+
+std::mutex g_tw_mutex;
+std::map<std::pair<int, int>, std::unique_ptr<TwiddleEntry>> g_tw;
+
+// Sets the dynamic shared memory limit of a kernel once per (device, kernel).
+std::mutex g_attr_mutex;
+std::set<std::pair<int, const void*>> g_attr_done;
+
+template <class K>
+void allow_smem(K kernel, std::size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
+  if (g_attr_done.count(key)) return;
+  check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+        "cudaFuncSetAttribute");
+  g_attr_done.insert(key);
+}
+
+constexpr int kThreads = 256;
+
+// ---- axis passes ------------------------------------------------------------------------------
+
+template <bool Fwd, int Mode, int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_axis(float2* __restrict__ data, std::size_t so, std::size_t sp, int ni, FftLen L, float scale,
+           const float2* __restrict__ aux_a, const std::uint8_t* __restrict__ aux_h) {
+  extern __shared__ float2 sm[];
+  const int n = L.n;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(n) * COLS;
+  const int c0 = static_cast<int>(blockIdx.x) * COLS;
+  const int cols = min(COLS, ni - c0);
+  const std::size_t base = static_cast<std::size_t>(blockIdx.y) * so + c0;
+  const int tid = static_cast<int>(threadIdx.x);
+  const int nth = static_cast<int>(blockDim.x);
+  constexpr int kFrom = static_cast<int>(AxisMode::from_data);
+  constexpr int kHalf = static_cast<int>(AxisMode::restore_half);
+  constexpr int kMask = static_cast<int>(AxisMode::restore_mask);
+
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int pos = idx / COLS;
+    const int col = idx - pos * COLS;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (col < cols) {
+      const std::size_t g = base + pos * sp + col;
+      v = Mode == kFrom ? cscale(aux_a[g], scale) : data[g];
+    }
+    A[idx] = v;
+  }
+  __syncthreads();
+
+  float2* res;
+  if constexpr (Mode == kHalf || Mode == kMask) {
+    res = smem_fft<true>(A, B, COLS, COLS, L, tid, nth);
+    float2* other = res == A ? B : A;
+    for (int idx = tid; idx < n * COLS; idx += nth) {
+      const int pos = idx / COLS;
+      const int col = idx - pos * COLS;
+      if (col >= cols) continue;
+      const std::size_t g = base + pos * sp + col;
+      float2 v = res[idx];
+      if constexpr (Mode == kHalf) {
+        const float2 a = aux_a[g];
+        const float b = 1.0f - 0.5f * static_cast<float>(aux_h[g]);
+        v = make_float2((a.x + b * v.x) * scale, (a.y + b * v.y) * scale);
+      } else {
+        if (aux_h[g]) v = aux_a[g];
+      }
+      res[idx] = v;
+    }
+    __syncthreads();
+    res = smem_fft<false>(res, other, COLS, COLS, L, tid, nth);
+  } else {
+    res = smem_fft<Fwd>(A, B, COLS, COLS, L, tid, nth);
+  }
+
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int pos = idx / COLS;
+    const int col = idx - pos * COLS;
+    if (col >= cols) continue;
+    float2 v = res[idx];
+    if (Mode == static_cast<int>(AxisMode::plain) && scale != 1.0f) v = cscale(v, scale);
+    data[base + pos * sp + col] = v;
+  }
+}
+
+template <bool Fwd, int Mode, int COLS>
+void launch_axis(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, float scale,
+                 const AxisAux& aux, cudaStream_t s) {
+  const FftLen& L = fft_len(n);
+  const std::size_t smem = 2 * static_cast<std::size_t>(n) * COLS * sizeof(float2);
+  auto kernel = k_axis<Fwd, Mode, COLS>;
+  allow_smem(kernel, smem);
+  const dim3 grid((ni + COLS - 1) / COLS, n_outer);
+  kernel<<<grid, kThreads, smem, s>>>(data, so, sp, ni, L, scale, aux.a, aux.hits);
+  check_launch("fft axis pass");
+}
+
+template <int Mode, int COLS>
+void axis_dispatch_dir(bool forward, float2* data, int n_outer, std::size_t so, int n, std::size_t sp,
+                       int ni, float scale, const AxisAux& aux, cudaStream_t s) {
+  if (forward) {
+    launch_axis<true, Mode, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+  } else {
+    launch_axis<false, Mode, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+  }
+}
+
+template <int COLS>
+void axis_dispatch(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
+                   AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
+  switch (mode) {
+    case AxisMode::plain:
+      axis_dispatch_dir<0, COLS>(forward, data, n_outer, so, n, sp, ni, scale, aux, s);
+      break;
+    case AxisMode::restore_half:
+      launch_axis<true, 1, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+      break;
+    case AxisMode::restore_mask:
+      launch_axis<true, 2, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+      break;
+    case AxisMode::from_data:
+      launch_axis<false, 3, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+      break;
+  }
+}
+
+// ---- real rows <-> half spectra -----------------------------------------------------------------
+
+template <bool Clamp, int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_rows_r2c(const float* __restrict__ x, float2* __restrict__ e, std::size_t rows, int nx, FftLen Lm,
+               const float2* __restrict__ twn) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  const int M = Lm.n;
+  const int h = M + 1;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(h) * cp;
+  const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
+  const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
+  const int tid = static_cast<int>(threadIdx.x);
+  const int nth = static_cast<int>(blockDim.x);
+
+  for (int idx = tid; idx < M * COLS; idx += nth) {
+    const int row = idx / M;
+    const int m = idx - row * M;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (row < nr) {
+      v = *reinterpret_cast<const float2*>(x + (r0 + row) * nx + 2 * m);
+      if (Clamp) v = make_float2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
+    }
+    A[m * cp + row] = v;
+  }
+  __syncthreads();
+  const float2* res = smem_fft<true>(A, B, cp, COLS, Lm, tid, nth);
+
+  for (int idx = tid; idx < h * COLS; idx += nth) {
+    const int row = idx / h;
+    const int k = idx - row * h;
+    if (row >= nr) continue;
+    const float2 zk = res[(k == M ? 0 : k) * cp + row];
+    const float2 zm = res[(k == 0 ? 0 : M - k) * cp + row];
+    const float2 ev = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
+    const float2 od = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
+    const float2 w = __ldg(twn + k);
+    e[(r0 + row) * h + k] = cadd(ev, cmul(w, od));
+  }
+}
+
+template <int Mode, int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_rows_c2r(const float2* __restrict__ e, float* __restrict__ x, std::size_t rows, int nx, FftLen Lm,
+               const float2* __restrict__ twn, float nm2, float inv_k02) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  const int M = Lm.n;
+  const int h = M + 1;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(h) * cp;
+  const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
+  const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
+  const int tid = static_cast<int>(threadIdx.x);
+  const int nth = static_cast<int>(blockDim.x);
+
+  for (int idx = tid; idx < h * COLS; idx += nth) {
+    const int row = idx / h;
+    const int k = idx - row * h;
+    A[k * cp + row] = row < nr ? e[(r0 + row) * h + k] : make_float2(0.0f, 0.0f);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < M * COLS; idx += nth) {
+    const int k = idx / COLS;
+    const int row = idx - k * COLS;
+    float2 xk = A[k * cp + row];
+    float2 xm = A[(M - k) * cp + row];
+    if (k == 0) {  // a real signal has real bins 0 and M; their imaginary parts drop out
+      xk.y = 0.0f;
+      xm.y = 0.0f;
+    }
+    const float2 sv = make_float2(xk.x + xm.x, xk.y - xm.y);  // xk + conj(xm)
+    const float2 d = make_float2(xk.x - xm.x, xk.y + xm.y);   // xk - conj(xm)
+    const float2 w = __ldg(twn + k);
+    const float2 t = cmulc(d, w);                              // d * e^{+2 pi i k / nx}
+    B[k * cp + row] = make_float2(sv.x - t.y, sv.y + t.x);     // sv + i t
+  }
+  __syncthreads();
+  const float2* res = smem_fft<false>(B, A, cp, COLS, Lm, tid, nth);
+
+  for (int idx = tid; idx < M * COLS; idx += nth) {
+    const int row = idx / M;
+    const int m = idx - row * M;
+    if (row >= nr) continue;
+    float2 z = res[m * cp + row];
+    if (Mode == static_cast<int>(C2rMode::index)) {
+      z = make_float2(index_from_potential(z.x, 0.0f, nm2, inv_k02), index_from_potential(z.y, 0.0f, nm2, inv_k02));
+    }
+    *reinterpret_cast<float2*>(x + (r0 + row) * nx + 2 * m) = z;
+  }
+}
+
+// ---- complex rows -----------------------------------------------------------------------------------
+
+template <bool Fwd, int Mode, int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_rows_c2c(float2* __restrict__ data, std::size_t rows, FftLen L, float scale, float* __restrict__ index,
+               float nm2, float inv_k02) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  const int n = L.n;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(n) * cp;
+  const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
+  const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
+  const int tid = static_cast<int>(threadIdx.x);
+  const int nth = static_cast<int>(blockDim.x);
+
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int row = idx / n;
+    const int pos = idx - row * n;
+    A[pos * cp + row] = row < nr ? data[(r0 + row) * n + pos] : make_float2(0.0f, 0.0f);
+  }
+  __syncthreads();
+  float2* res;
+  if constexpr (Mode == static_cast<int>(RowMode::plain)) {
+    res = smem_fft<Fwd>(A, B, cp, COLS, L, tid, nth);
+  } else {
+    res = smem_fft<false>(A, B, cp, COLS, L, tid, nth);
+    if constexpr (Mode == static_cast<int>(RowMode::inv_clamp_fwd)) {
+      float2* other = res == A ? B : A;
+      for (int idx = tid; idx < n * COLS; idx += nth) {
+        const int pos = idx / COLS;
+        const int row = idx - pos * COLS;
+        const float2 v = res[pos * cp + row];
+        res[pos * cp + row] = make_float2(fmaxf(v.x * scale, 0.0f), 0.0f);
+      }
+      __syncthreads();
+      res = smem_fft<true>(res, other, cp, COLS, L, tid, nth);
+    }
+  }
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int row = idx / n;
+    const int pos = idx - row * n;
+    if (row >= nr) continue;
+    const float2 v = res[pos * cp + row];
+    if constexpr (Mode == static_cast<int>(RowMode::inv_index)) {
+      index[(r0 + row) * n + pos] = index_from_potential(v.x * scale, v.y * scale, nm2, inv_k02);
+    } else if constexpr (Mode == static_cast<int>(RowMode::plain)) {
+      data[(r0 + row) * n + pos] = scale != 1.0f ? cscale(v, scale) : v;
+    } else {
+      data[(r0 + row) * n + pos] = v;
+    }
+  }
+}
+
+// Rows per CTA: as many as fit a 64 KiB double buffer, at most 16.
+int rows_per_cta(int n) {
+  int c = 16;
+  while (c > 1 && 2 * static_cast<std::size_t>(n + 1) * (c + 1) * sizeof(float2) > 64 * 1024) c /= 2;
+  return c;
+}
+
+template <int COLS>
+void launch_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, cudaStream_t s) {
+  const int M = nx / 2;
+  const FftLen& Lm = fft_len(M);
+  const FftLen& Ln = fft_len(nx);
+  const std::size_t smem = 2 * static_cast<std::size_t>(M + 1) * (COLS + 1) * sizeof(float2);
+  const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
+  if (clamp) {
+    allow_smem(k_rows_r2c<true, COLS>, smem);
+    k_rows_r2c<true, COLS><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
+  } else {
+    allow_smem(k_rows_r2c<false, COLS>, smem);
+    k_rows_r2c<false, COLS><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
+  }
+  check_launch("rows r2c");
+}
+
+template <int COLS>
+void launch_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
+                cudaStream_t s) {
+  const int M = nx / 2;
+  const FftLen& Lm = fft_len(M);
+  const FftLen& Ln = fft_len(nx);
+  const std::size_t smem = 2 * static_cast<std::size_t>(M + 1) * (COLS + 1) * sizeof(float2);
+  const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
+  if (mode == C2rMode::index) {
+    allow_smem(k_rows_c2r<1, COLS>, smem);
+    k_rows_c2r<1, COLS><<<grid, kThreads, smem, s>>>(e, x, rows, nx, Lm, Ln.tw, nm2, inv_k02);
+  } else {
+    allow_smem(k_rows_c2r<0, COLS>, smem);
+    k_rows_c2r<0, COLS><<<grid, kThreads, smem, s>>>(e, x, rows, nx, Lm, Ln.tw, nm2, inv_k02);
+  }
+  check_launch("rows c2r");
+}
+
+template <bool Fwd, int Mode, int COLS>
+void launch_c2c_rows(float2* data, std::size_t rows, int nx, float scale, float* index, float nm2,
+                     float inv_k02, cudaStream_t s) {
+  const FftLen& L = fft_len(nx);
+  const std::size_t smem = 2 * static_cast<std::size_t>(nx) * (COLS + 1) * sizeof(float2);
+  auto kernel = k_rows_c2c<Fwd, Mode, COLS>;
+  allow_smem(kernel, smem);
+  const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
+  kernel<<<grid, kThreads, smem, s>>>(data, rows, L, scale, index, nm2, inv_k02);
+  check_launch("rows c2c");
+}
+
+template <int COLS>
+void c2c_rows_dispatch(float2* data, std::size_t rows, int nx, bool forward, RowMode mode, float scale,
+                       float* index, float nm2, float inv_k02, cudaStream_t s) {
+  switch (mode) {
+    case RowMode::plain:
+      if (forward) {
+        launch_c2c_rows<true, 0, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+      } else {
+        launch_c2c_rows<false, 0, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+      }
+      break;
+    case RowMode::inv_clamp_fwd:
+      launch_c2c_rows<false, 1, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+      break;
+    case RowMode::inv_index:
+      launch_c2c_rows<false, 2, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+      break;
+  }
+}
+
+}  // namespace
+
+const FftLen& fft_len(int n) {
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(g_tw_mutex);
+  auto& slot = g_tw[{dev, n}];
+  if (!slot) {
+    auto entry = std::make_unique<TwiddleEntry>();
+    entry->len = make_fft_len(n);
+    std::vector<float2> host(n);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int k = 0; k < n; ++k) {
+      const double a = two_pi * static_cast<double>(k) / static_cast<double>(n);
+      host[k] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
+    }
+    entry->table.reset(n);
+    check(cudaMemcpy(entry->table.get(), host.data(), n * sizeof(float2), cudaMemcpyHostToDevice),
+          "upload twiddles");
+    entry->len.tw = entry->table.get();
+    slot = std::move(entry);
+  }
+  return slot->len;
+}
+
+void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
+               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
+  require(n_outer >= 1 && n_outer <= 65535, "fft: too many lines in the outer dimension");
+  require(static_cast<std::size_t>(n) * 2 * sizeof(float2) <= 200 * 1024, "fft: transform length too large");
+  const auto fits = [&](int cols) { return 2 * static_cast<std::size_t>(n) * cols * sizeof(float2) <= 72 * 1024; };
+  if (fits(16)) {
+    axis_dispatch<16>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
+  } else if (fits(8)) {
+    axis_dispatch<8>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
+  } else if (fits(4)) {
+    axis_dispatch<4>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
+  } else {
+    axis_dispatch<1>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
+  }
+}
+
+void rows_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, cudaStream_t s) {
+  require(nx >= 2 && nx % 2 == 0, "rfft: row length must be even");
+  switch (rows_per_cta(nx / 2)) {
+    case 16: launch_r2c<16>(x, e, rows, nx, clamp, s); break;
+    case 8: launch_r2c<8>(x, e, rows, nx, clamp, s); break;
+    case 4: launch_r2c<4>(x, e, rows, nx, clamp, s); break;
+    case 2: launch_r2c<2>(x, e, rows, nx, clamp, s); break;
+    default: launch_r2c<1>(x, e, rows, nx, clamp, s); break;
+  }
+}
+
+void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
+              cudaStream_t s) {
+  require(nx >= 2 && nx % 2 == 0, "irfft: row length must be even");
+  switch (rows_per_cta(nx / 2)) {
+    case 16: launch_c2r<16>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    case 8: launch_c2r<8>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    case 4: launch_c2r<4>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    case 2: launch_c2r<2>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    default: launch_c2r<1>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+  }
+}
+
+void rows_c2c(float2* data, std::size_t rows, int nx, bool forward, RowMode mode, float scale, float* index,
+              float nm2, float inv_k02, cudaStream_t s) {
+  switch (rows_per_cta(nx)) {
+    case 16: c2c_rows_dispatch<16>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    case 8: c2c_rows_dispatch<8>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    case 4: c2c_rows_dispatch<4>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    case 2: c2c_rows_dispatch<2>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    default: c2c_rows_dispatch<1>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+  }
+}
+
+void fft2d(float2* data, int count, int n, bool forward, float scale, cudaStream_t s) {
+  rows_c2c(data, static_cast<std::size_t>(count) * n, n, forward, RowMode::plain, 1.0f, nullptr, 0, 0, s);
+  axis_pass(data, count, static_cast<std::size_t>(n) * n, n, static_cast<std::size_t>(n), n, forward,
+            AxisMode::plain, scale, AxisAux{}, s);
+}
+
+}  // namespace qhk

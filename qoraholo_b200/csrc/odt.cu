@@ -1,0 +1,333 @@
+// Rytov fields -> refractive index on the device: 2D FFT of the fields, Ewald-sphere mapping into
+// 3D k-space, and the missing-cone solver (Gerchberg-Papoulis on half or full spectra, FISTA-TV).
+// Replaces the reference's OdtSolver (src/cuda/odt.cu:170-349; CPU form src/cpu/odt.cpp:124-242).
+//
+// Mapping. Each voxel of k-space receives the sum, in illumination order, of the spectrum values
+// whose Ewald target it is, divided by their count. A thread owns K consecutive axial bins of one
+// lateral column and walks all illuminations, recomputing the target bin with the reference's
+// float operations (qhk_math.cuh: ewald_target), and accumulates the hits that fall in its bins
+// in registers. Every voxel therefore has exactly one writer, sums in the CPU's order and needs
+// no atomics; indices and hit counts are bit-identical to the CPU's, and so are the sums given the
+// same spectra. For the real (R2C) solvers the same thread also walks the mirrored column -k and
+// writes the half-spectrum data a = (P(k) + conj P(-k)) / 2 and hits = M(k) + M(-k) directly
+// (src/common.hpp:72-87), so neither the full complex potential nor the weights are ever stored.
+// The filled-voxel count is an integer reduction.
+#include <algorithm>
+#include <cmath>
+#include <numbers>
+#include <vector>
+
+#include "odt.hpp"
+
+namespace qhk {
+
+namespace {
+
+constexpr int kMapK = 8;  // axial bins per thread
+
+__device__ __forceinline__ void accumulate(float (&re)[kMapK], float (&im)[kMapK], float (&w)[kMapK], int slot,
+                                           float vr, float vi) {
+#pragma unroll
+  for (int i = 0; i < kMapK; ++i) {
+    if (slot == i) {
+      re[i] = __fadd_rn(re[i], vr);
+      im[i] = __fadd_rn(im[i], vi);
+      w[i] = __fadd_rn(w[i], 1.0f);
+    }
+  }
+}
+
+// Mapped value of spectrum s at axial bin kz: parity(kz) * (0, -gain nu_z) * s, as the host
+// computes it: (0*sr - f*si, 0*si + f*sr) with f = -gain*nu_z, then the sign.
+__device__ __forceinline__ void mapped(const Grid& g, float nuz, int kz, float2 s, float& vr, float& vi) {
+  const float f = __fmul_rn(-g.gain, nuz);
+  const float p = parity(kz);
+  vr = __fmul_rn(p, -__fmul_rn(f, s.y));
+  vi = __fmul_rn(p, __fmul_rn(f, s.x));
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(256)
+    k_map_half(const float2* __restrict__ spectra, const float4* __restrict__ illum, int count, Grid g,
+               float2* __restrict__ a, std::uint8_t* __restrict__ hits, unsigned long long* __restrict__ filled) {
+  const int n = g.n, nz = g.nz, h = n / 2 + 1;
+  const int chunks = (nz + kMapK - 1) / kMapK;
+  const std::size_t total = static_cast<std::size_t>(chunks) * n * h;
+  const std::size_t t = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x;
+  unsigned long long cnt = 0;
+  if (t < total) {
+    const int kx = static_cast<int>(t % h);
+    const std::size_t rest = t / h;
+    const int ky = static_cast<int>(rest % n);
+    const int k0 = static_cast<int>(rest / n) * kMapK;
+    const int myk = negative_bin(ky, n);
+    const int mkx = negative_bin(kx, n);
+    const std::size_t plane = static_cast<std::size_t>(n) * n;
+    float pre[kMapK] = {}, pim[kMapK] = {}, pw[kMapK] = {};
+    float nre[kMapK] = {}, nim[kMapK] = {}, nw[kMapK] = {};
+    for (int ai = 0; ai < count; ++ai) {
+      const float4 il = __ldg(illum + ai);
+      int kz;
+      float nuz;
+      if (ewald_target(g, ky, kx, il.x, il.y, il.z, kz, nuz) && kz >= k0 && kz < k0 + kMapK) {
+        float vr, vi;
+        mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(ky) * n + kx], vr, vi);
+        accumulate(pre, pim, pw, kz - k0, vr, vi);
+      }
+      if (ewald_target(g, myk, mkx, il.x, il.y, il.z, kz, nuz)) {
+        const int km = negative_bin(kz, nz);
+        if (km >= k0 && km < k0 + kMapK) {
+          float vr, vi;
+          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(myk) * n + mkx], vr, vi);
+          accumulate(nre, nim, nw, km - k0, vr, vi);
+        }
+      }
+    }
+    const bool mirror_is_full_only = kx >= 1 && kx <= n / 2 - 1;
+#pragma unroll
+    for (int i = 0; i < kMapK; ++i) {
+      const int kz = k0 + i;
+      if (kz >= nz) break;
+      float pr = pre[i], pi = pim[i], mr = nre[i], mi = nim[i];
+      if (pw[i] > 0.0f) {
+        pr = __fdiv_rn(pr, pw[i]);
+        pi = __fdiv_rn(pi, pw[i]);
+      }
+      if (nw[i] > 0.0f) {
+        mr = __fdiv_rn(mr, nw[i]);
+        mi = __fdiv_rn(mi, nw[i]);
+      }
+      const std::size_t o = (static_cast<std::size_t>(kz) * n + ky) * h + kx;
+      a[o] = make_float2(__fmul_rn(0.5f, __fadd_rn(pr, mr)), __fmul_rn(0.5f, __fsub_rn(pi, mi)));
+      hits[o] = static_cast<std::uint8_t>((pw[i] > 0.0f) + (nw[i] > 0.0f));
+      cnt += (pw[i] > 0.0f) + (mirror_is_full_only && nw[i] > 0.0f);
+    }
+  }
+  cnt = warp_sum(cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(filled, cnt);
+}
+
+// Full complex potential (normalised) and the measured mask, for the complex solver and the plain
+// Rytov reconstruction. `measured` (optional) receives a second copy of the potential.
+__global__ void __launch_bounds__(256)
+    k_map_full(const float2* __restrict__ spectra, const float4* __restrict__ illum, int count, Grid g,
+               float2* __restrict__ pot, float2* __restrict__ measured, std::uint8_t* __restrict__ mask,
+               unsigned long long* __restrict__ filled) {
+  const int n = g.n, nz = g.nz;
+  const int chunks = (nz + kMapK - 1) / kMapK;
+  const std::size_t total = static_cast<std::size_t>(chunks) * n * n;
+  const std::size_t t = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x;
+  unsigned long long cnt = 0;
+  if (t < total) {
+    const int kx = static_cast<int>(t % n);
+    const std::size_t rest = t / n;
+    const int ky = static_cast<int>(rest % n);
+    const int k0 = static_cast<int>(rest / n) * kMapK;
+    const std::size_t plane = static_cast<std::size_t>(n) * n;
+    float pre[kMapK] = {}, pim[kMapK] = {}, pw[kMapK] = {};
+    for (int ai = 0; ai < count; ++ai) {
+      const float4 il = __ldg(illum + ai);
+      int kz;
+      float nuz;
+      if (ewald_target(g, ky, kx, il.x, il.y, il.z, kz, nuz) && kz >= k0 && kz < k0 + kMapK) {
+        float vr, vi;
+        mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(ky) * n + kx], vr, vi);
+        accumulate(pre, pim, pw, kz - k0, vr, vi);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kMapK; ++i) {
+      const int kz = k0 + i;
+      if (kz >= nz) break;
+      float pr = pre[i], pi = pim[i];
+      if (pw[i] > 0.0f) {
+        pr = __fdiv_rn(pr, pw[i]);
+        pi = __fdiv_rn(pi, pw[i]);
+      }
+      const std::size_t o = (static_cast<std::size_t>(kz) * n + ky) * n + kx;
+      pot[o] = make_float2(pr, pi);
+      if (measured) measured[o] = make_float2(pr, pi);
+      mask[o] = pw[i] > 0.0f;
+      cnt += pw[i] > 0.0f;
+    }
+  }
+  cnt = warp_sum(cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(filled, cnt);
+}
+
+}  // namespace
+
+void map_half(const float2* spectra, const float4* illum, int count, const Grid& g, float2* a, std::uint8_t* hits,
+              unsigned long long* filled, cudaStream_t s) {
+  const int chunks = (g.nz + kMapK - 1) / kMapK;
+  const std::size_t threads = static_cast<std::size_t>(chunks) * g.n * (g.n / 2 + 1);
+  k_map_half<<<blocks_for(threads, 256), 256, 0, s>>>(spectra, illum, count, g, a, hits, filled);
+  check_launch("ewald mapping");
+}
+
+void map_full(const float2* spectra, const float4* illum, int count, const Grid& g, float2* pot, float2* measured,
+              std::uint8_t* mask, unsigned long long* filled, cudaStream_t s) {
+  const int chunks = (g.nz + kMapK - 1) / kMapK;
+  const std::size_t threads = static_cast<std::size_t>(chunks) * g.n * g.n;
+  k_map_full<<<blocks_for(threads, 256), 256, 0, s>>>(spectra, illum, count, g, pot, measured, mask, filled);
+  check_launch("ewald mapping");
+}
+
+std::vector<float4> illumination_table(const Grid& g, const float* illum_fyfx, int count) {
+  std::vector<float4> il(count);
+  for (int a = 0; a < count; ++a) {
+    const float fy = illum_fyfx[2 * a];
+    const float fx = illum_fyfx[2 * a + 1];
+    il[a] = make_float4(fy, fx, std::sqrt(g.fm2 - fy * fy - fx * fx), 0.0f);
+  }
+  return il;
+}
+
+Grid make_grid(int n, int nz, float wavelength, float n_medium, float na, float pixel) {
+  const float fm = n_medium / wavelength;
+  const float fna = na / wavelength;
+  return Grid{n,
+              nz,
+              1.0f / (static_cast<float>(n) * pixel),
+              1.0f / (static_cast<float>(nz) * pixel),
+              fm * fm,
+              fna * fna,
+              4.0f * std::numbers::pi_v<float> / pixel};
+}
+
+OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
+  const Grid& g = cfg_.grid;
+  const int n = g.n, nz = g.nz, h = n / 2 + 1;
+  require(n >= 4 && n % 2 == 0 && nz >= 2 && nz % 2 == 0, "odt: invalid grid");
+  require(cfg_.count >= 1, "odt: need at least one field");
+  real_ = cfg_.iterations > 0 && (cfg_.tv || cfg_.r2c);
+  half_ = static_cast<std::size_t>(nz) * n * h;
+  vol_ = static_cast<std::size_t>(nz) * n * n;
+  const std::vector<float4> il = illumination_table(g, illum_fyfx, cfg_.count);
+  illum_.reset(cfg_.count);
+  check(cudaMemcpy(illum_.get(), il.data(), il.size() * sizeof(float4), cudaMemcpyHostToDevice), "upload illuminations");
+  filled_.reset(1);
+  if (real_) {
+    a_.reset(half_);
+    hits_.reset(half_);
+    e_.reset(half_);
+    x_.reset(vol_);
+    if (cfg_.tv) {
+      xprev_.reset(vol_);
+      dual_.reset(9 * vol_);
+      for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) tv_.v[i][c] = dual_.get() + (3 * i + c) * vol_;
+    }
+  } else {
+    pot_.reset(vol_);
+    mask_.reset(vol_);
+    if (cfg_.iterations > 0) measured_.reset(vol_);
+  }
+}
+
+std::size_t OdtPlan::device_bytes() const {
+  return illum_.bytes() + filled_.bytes() + a_.bytes() + hits_.bytes() + e_.bytes() + x_.bytes() + xprev_.bytes() +
+         dual_.bytes() + pot_.bytes() + mask_.bytes() + measured_.bytes();
+}
+
+void OdtPlan::mark(StageClock* clock, int m, cudaStream_t s) const {
+  if (clock) clock->mark(first_mark_ + m, s);
+}
+
+void OdtPlan::run(float2* fields, float* index, cudaStream_t s, StageClock* clock) {
+  const Grid& g = cfg_.grid;
+  const int n = g.n, nz = g.nz, h = n / 2 + 1;
+  const std::size_t nh = static_cast<std::size_t>(n) * h;
+  const std::size_t nn = static_cast<std::size_t>(n) * n;
+  const float inv = 1.0f / (static_cast<float>(nz) * static_cast<float>(n) * static_cast<float>(n));
+
+  fft2d(fields, cfg_.count, n, true, 1.0f, s);
+  mark(clock, kMarkFft2, s);
+  check(cudaMemsetAsync(filled_.get(), 0, sizeof(unsigned long long), s), "cudaMemset");
+  mark(clock, kMarkClear, s);
+  if (real_) {
+    map_half(fields, illum_.get(), cfg_.count, g, a_.get(), hits_.get(), filled_.get(), s);
+  } else {
+    map_full(fields, illum_.get(), cfg_.count, g, pot_.get(), measured_.get(), mask_.get(), filled_.get(), s);
+  }
+  mark(clock, kMarkMapping, s);
+  mark(clock, kMarkNormalize, s);
+
+  if (real_) {
+    solve_real(index, inv, s);
+  } else {
+    solve_complex(index, inv, s);
+  }
+  mark(clock, kMarkSolve, s);
+  mark(clock, kMarkFinish, s);
+}
+
+// Half-spectrum loops (src/cpu/odt.cpp:76-120). x = irfft3(a) inv first; the k-space step is the
+// z pass (forward, restore, inverse); FISTA-TV then runs the proximal step on the C2R output.
+void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
+  const Grid& g = cfg_.grid;
+  const int n = g.n, nz = g.nz, h = n / 2 + 1;
+  const std::size_t nh = static_cast<std::size_t>(n) * h;
+  const std::size_t rows = static_cast<std::size_t>(nz) * n;
+  float2* e = e_.get();
+  const AxisAux aux{a_.get(), hits_.get()};
+  // E = a * inv, inverse along z, then y, then C2R along x.
+  axis_pass(e, n, h, nz, nh, h, false, AxisMode::from_data, inv, aux, s);
+  axis_pass(e, nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+  rows_c2r(e, x_.get(), rows, n, C2rMode::store, cfg_.nm2, cfg_.inv_k02, s);
+  const auto kspace_step = [&](const float* in, bool clamp, float* out, C2rMode mode) {
+    rows_r2c(in, e, rows, n, clamp, s);
+    axis_pass(e, nz, nh, n, h, h, true, AxisMode::plain, 1.0f, AxisAux{}, s);
+    axis_pass(e, n, h, nz, nh, h, true, AxisMode::restore_half, inv, aux, s);
+    axis_pass(e, nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+    rows_c2r(e, out, rows, n, mode, cfg_.nm2, cfg_.inv_k02, s);
+  };
+  if (!cfg_.tv) {
+    for (int it = 0; it < cfg_.iterations; ++it) {
+      const bool last = it == cfg_.iterations - 1;
+      kspace_step(x_.get(), true, last ? index : x_.get(), last ? C2rMode::index : C2rMode::store);
+    }
+    return;
+  }
+  // FISTA-TV: y lives in x_ (it is also b, the C2R output), x_prev in xprev_, the dual in dual_.
+  const std::size_t vbytes = vol_ * sizeof(float);
+  check(cudaMemcpyAsync(xprev_.get(), x_.get(), vbytes, cudaMemcpyDeviceToDevice, s), "copy x");
+  check(cudaMemsetAsync(dual_.get(), 0, 3 * vbytes, s), "cudaMemset");
+  tv_.p_index = 0;
+  float t = 1.0f;
+  for (int it = 0; it < cfg_.iterations; ++it) {
+    const bool last = it == cfg_.iterations - 1;
+    kspace_step(x_.get(), false, x_.get(), C2rMode::store);
+    const float tn = fista_t(t);
+    const float m = (t - 1.0f) / tn;
+    tv_prox(x_.get(), tv_, nz, n, n, cfg_.lambda, cfg_.tv_inner, last ? TvFinal::index : TvFinal::momentum, m,
+            xprev_.get(), last ? index : x_.get(), cfg_.nm2, cfg_.inv_k02, s);
+    t = tn;
+  }
+}
+
+// Full complex spectra (src/cpu/odt.cpp:208-240): plain Rytov ODT, or GP with the C2C transforms.
+void OdtPlan::solve_complex(float* index, float inv, cudaStream_t s) {
+  const Grid& g = cfg_.grid;
+  const int n = g.n, nz = g.nz;
+  const std::size_t nn = static_cast<std::size_t>(n) * n;
+  const std::size_t rows = static_cast<std::size_t>(nz) * n;
+  float2* p = pot_.get();
+  const AxisAux aux{measured_.get(), mask_.get()};
+  axis_pass(p, n, n, nz, nn, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+  axis_pass(p, nz, nn, n, n, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+  for (int it = 0; it < cfg_.iterations; ++it) {
+    rows_c2c(p, rows, n, false, RowMode::inv_clamp_fwd, inv, nullptr, 0, 0, s);
+    axis_pass(p, nz, nn, n, n, n, true, AxisMode::plain, 1.0f, AxisAux{}, s);
+    axis_pass(p, n, n, nz, nn, n, true, AxisMode::restore_mask, 1.0f, aux, s);
+    axis_pass(p, nz, nn, n, n, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+  }
+  rows_c2c(p, rows, n, false, RowMode::inv_index, inv, index, cfg_.nm2, cfg_.inv_k02, s);
+}
+
+}  // namespace qhk

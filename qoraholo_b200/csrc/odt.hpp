@@ -1,0 +1,95 @@
+// ODT solver plan of the CUDA backend (odt.cu): holds the device buffers for one geometry and
+// runs fields -> index on a stream.
+#pragma once
+
+#include <vector>
+
+#include "qhk_internal.hpp"
+
+namespace qhk {
+
+// Events recorded at stage boundaries on one stream, read after the stream has finished.
+class StageClock {
+ public:
+  explicit StageClock(int marks) : events_(marks) {}
+  void mark(int i, cudaStream_t s) { events_.at(i).record(s); }
+  [[nodiscard]] double ms(int from, int to) const { return events_.at(to).since(events_.at(from)); }
+  [[nodiscard]] cudaEvent_t event(int i) const { return events_.at(i).get(); }
+
+ private:
+  std::vector<Event> events_;
+};
+
+Grid make_grid(int n, int nz, float wavelength, float n_medium, float na, float pixel);
+
+// Per-illumination (fy, fx, fiz, 0), fiz = sqrt(fm2 - fy^2 - fx^2) in float as the host computes it.
+std::vector<float4> illumination_table(const Grid& g, const float* illum_fyfx, int count);
+
+// Ewald mapping of `count` spectra (count, n, n): half-spectrum data and hit counts (nz, n, n/2+1)
+// for the real solvers, or the full normalised potential and mask (nz, n, n) for the complex one
+// (`measured`, optional, gets a copy). `filled` is incremented by the number of voxels with data.
+void map_half(const float2* spectra, const float4* illum, int count, const Grid& g, float2* a, std::uint8_t* hits,
+              unsigned long long* filled, cudaStream_t s);
+void map_full(const float2* spectra, const float4* illum, int count, const Grid& g, float2* pot, float2* measured,
+              std::uint8_t* mask, unsigned long long* filled, cudaStream_t s);
+
+struct OdtConfig {
+  Grid grid{};
+  int count = 0;       // fields (illuminations)
+  int iterations = 0;  // missing-cone iterations; 0: plain Rytov ODT
+  bool tv = false;     // FISTA-TV instead of Gerchberg-Papoulis
+  bool r2c = true;     // GP on half spectra (the TV solver always is)
+  float lambda = 0;    // TV weight times k0^2
+  int tv_inner = 10;
+  float nm2 = 0;       // n_medium^2
+  float inv_k02 = 0;   // 1 / k0^2
+};
+
+class OdtPlan {
+ public:
+  // Stage marks recorded by run() when a clock is given, in this order.
+  enum Mark { kMarkFft2, kMarkClear, kMarkMapping, kMarkNormalize, kMarkSolve, kMarkFinish, kMarks };
+
+  // illum_fyfx: count (fy, fx) pairs on the host.
+  OdtPlan(const OdtConfig& cfg, const float* illum_fyfx);
+
+  // fields: (count, n, n) Rytov fields on the device, overwritten by their spectra. index: (nz, n,
+  // n) output on the device. Clock marks are `first + Mark`.
+  void run(float2* fields, float* index, cudaStream_t s, StageClock* clock = nullptr);
+  void run_marked(float2* fields, float* index, cudaStream_t s, StageClock* clock, int first) {
+    first_mark_ = first;
+    run(fields, index, s, clock);
+    first_mark_ = 0;
+  }
+
+  // Voxels that received data in the last run, on the device.
+  [[nodiscard]] const unsigned long long* filled() const { return filled_.get(); }
+  [[nodiscard]] std::size_t volume() const { return vol_; }
+  [[nodiscard]] std::size_t device_bytes() const;
+  [[nodiscard]] const OdtConfig& config() const { return cfg_; }
+
+ private:
+  void mark(StageClock* clock, int m, cudaStream_t s) const;
+  void solve_real(float* index, float inv, cudaStream_t s);
+  void solve_complex(float* index, float inv, cudaStream_t s);
+
+  OdtConfig cfg_;
+  bool real_ = false;
+  std::size_t half_ = 0;
+  std::size_t vol_ = 0;
+  int first_mark_ = 0;
+  DevBuf<float4> illum_;
+  DevBuf<unsigned long long> filled_;
+  DevBuf<float2> a_;
+  DevBuf<std::uint8_t> hits_;
+  DevBuf<float2> e_;
+  DevBuf<float> x_;
+  DevBuf<float> xprev_;
+  DevBuf<float> dual_;
+  TvBuffers tv_;
+  DevBuf<float2> pot_;
+  DevBuf<std::uint8_t> mask_;
+  DevBuf<float2> measured_;
+};
+
+}  // namespace qhk

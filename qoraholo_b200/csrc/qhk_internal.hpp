@@ -1,0 +1,82 @@
+// Internal interfaces shared by the CUDA translation units of the backend. The public boundary is
+// the C ABI in include/qoraholo_b200.h (capi.cu); these declarations are not exported.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "fft_engine.cuh"
+#include "qhk_math.cuh"
+#include "qhk_util.cuh"
+
+namespace qhk {
+
+// Cached transform description (radices + device twiddle table) of length n on the current
+// device. Thread safe; tables live until the process exits.
+const FftLen& fft_len(int n);
+
+// ---- FFT passes (fft3d.cu) ------------------------------------------------------------------
+// Data viewed as [outer][pos][inner], element (o, p, i) at o * so + p * sp + i, inner contiguous.
+// Transforms along pos for every (o, i) with i < ni.
+enum class AxisMode : int {
+  plain,          // transform, times scale
+  restore_half,   // forward, e = a + (1 - hits / 2) e, times scale, inverse (GP/FISTA k-space step)
+  restore_mask,   // forward, e = mask ? measured : e, inverse (complex GP k-space step)
+  from_data,      // loads aux (a) times scale instead of data, inverse transform
+};
+struct AxisAux {
+  const float2* a = nullptr;        // half-spectrum data, or measured spectrum
+  const std::uint8_t* hits = nullptr;  // hits (0..2) or mask (0/1)
+};
+void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
+               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s);
+
+// Rows of real length nx <-> half spectra of nx / 2 + 1 bins (rows dense, row pitches nx and
+// nx / 2 + 1). R2C optionally clamps its input at 0 (Gerchberg-Papoulis). C2R writes the real
+// rows, or the refractive index of the potential (last iteration).
+void rows_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, cudaStream_t s);
+enum class C2rMode : int { store, index };
+void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
+              cudaStream_t s);
+
+// Complex rows of length nx (dense). Modes for the complex Gerchberg-Papoulis loop.
+enum class RowMode : int {
+  plain,            // transform (forward or inverse), times scale
+  inv_clamp_fwd,    // inverse times scale, (max(re, 0), 0), forward
+  inv_index,        // inverse times scale, refractive index of (re, im) into `index`
+};
+void rows_c2c(float2* data, std::size_t rows, int nx, bool forward, RowMode mode, float scale, float* index,
+              float nm2, float inv_k02, cudaStream_t s);
+
+// 2D FFT of `count` images of n x n (dense), in place.
+void fft2d(float2* data, int count, int n, bool forward, float scale, cudaStream_t s);
+
+// ---- TV proximal step (tv.cu) -----------------------------------------------------------------
+// Three triplets of dual volumes (z, y, x components). The dual p lives in v[p_index]; an FGP
+// step reads the previous dual r from one triplet and writes the next r to another, and the
+// first step of a call moves p to a free triplet (neighbouring CTAs still read the old p as r),
+// so the three rotate and p_index is updated by tv_prox.
+struct TvBuffers {
+  float* v[3][3] = {};
+  int p_index = 0;
+};
+enum class TvFinal : int {
+  plain,     // out = argmin
+  momentum,  // x = argmin; y = x + m (x - xprev); xprev <- x; out <- y
+  index,     // out = refractive index of argmin
+};
+// `inner` FGP steps on the dual started from p, then the final primal. b and all volumes are dense
+// (nz, ny, nx). For `momentum` the primal goes to xprev (in place) and the extrapolated point to out
+// (which may alias b).
+void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, int inner,
+             TvFinal final_mode, float momentum, float* xprev, float* out, float nm2, float inv_k02,
+             cudaStream_t s);
+
+// t_{k+1} of FISTA and FGP, 0.5 (1 + sqrt(1 + 4 t^2)) in float (host).
+float fista_t(float t);
+
+}  // namespace qhk

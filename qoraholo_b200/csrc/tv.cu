@@ -1,0 +1,393 @@
+// Total-variation proximal step by FGP on the dual (Beck & Teboulle 2009), the dominant cost of
+// the FISTA-TV reconstruction (it follows the reference's tv_prox, src/cuda/tv.cu:256-293, and
+// its CPU form src/cpu/tv.cpp:7-44, with the per-voxel math of src/common.hpp:107-153).
+//
+// One FGP step is one kernel. A CTA owns TY full rows (all x) of a y-slab and marches along z
+// through `zchunk` planes. Shared memory holds the input dual r for two planes (rows y0-1 ..
+// y0+TY, three components) and the primal point z = max(b - lambda L(r), 0) for two planes (rows
+// y0 .. y0+TY): z of plane k+1 is computed once from the ring and reused as plane k of the next
+// step, so z is never written to HBM, and each r value is read from HBM once (the one-row halos
+// come from L2). Per step the HBM traffic is b, r_in (3), p (3) read and p (3), r_out (3) written
+// -- 13 volumes; the first step reads p as r (10 volumes) and the last writes no r (10 volumes).
+//
+// All arithmetic uses the round-to-nearest intrinsics in the reference's operation order, so the
+// device iterates are bit-identical to the CPU's.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <set>
+
+#include "qhk_internal.hpp"
+
+namespace qhk {
+
+namespace {
+
+struct FgpArgs {
+  const float* b;
+  const float* rin[3];
+  const float* pin[3];
+  float* pout[3];
+  float* rout[3];
+  int nz, ny, nx;
+  int zchunk;
+  float lambda, step, momentum;
+};
+
+template <int VEC>
+struct Vec;
+template <>
+struct Vec<4> {
+  using T = float4;
+  __device__ static void load(const float* p, float* v) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  }
+  __device__ static void store(float* p, const float* v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+template <>
+struct Vec<1> {
+  __device__ static void load(const float* p, float* v) { v[0] = *p; }
+  __device__ static void store(float* p, const float* v) { *p = v[0]; }
+};
+
+template <int VEC, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(1024) k_fgp(FgpArgs A) {
+  extern __shared__ float sm[];
+  const int nx = A.nx, ny = A.ny, nz = A.nz;
+  const int TY = static_cast<int>(blockDim.y);
+  const int tx = static_cast<int>(threadIdx.x);
+  const int ty = static_cast<int>(threadIdx.y);
+  const int x0 = tx * VEC;
+  const int y0 = static_cast<int>(blockIdx.x) * TY;
+  const int z0 = static_cast<int>(blockIdx.y) * A.zchunk;
+  if (z0 >= nz) return;
+  const int z1 = min(z0 + A.zchunk, nz);
+  const int ring_rows = TY + 2;
+  const std::size_t plane_sz = static_cast<std::size_t>(3) * ring_rows * nx;
+  float* R0 = sm;
+  float* R1 = sm + plane_sz;
+  float* Z0 = sm + 2 * plane_sz;
+  float* Z1 = Z0 + static_cast<std::size_t>(TY + 1) * nx;
+  float* Bs = Z1 + static_cast<std::size_t>(TY + 1) * nx;
+  const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
+
+  // r of plane z (rows y0-1 .. y0+TY), zeros outside the volume.
+  const auto load_r = [&](float* R, int z) {
+    for (int rc = ty; rc < 3 * ring_rows; rc += TY) {
+      const int c = rc / ring_rows;
+      const int rr = rc - c * ring_rows;
+      const int y = y0 - 1 + rr;
+      float v[VEC];
+      if (z >= 0 && z < nz && y >= 0 && y < ny) {
+        Vec<VEC>::load(A.rin[c] + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0, v);
+      } else {
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) v[i] = 0.0f;
+      }
+      Vec<VEC>::store(R + (static_cast<std::size_t>(c) * ring_rows + rr) * nx + x0, v);
+    }
+  };
+  const auto load_b = [&](int z) {
+    for (int rr = ty; rr < TY + 1; rr += TY) {
+      const int y = y0 + rr;
+      float v[VEC];
+      if (y < ny) {
+        Vec<VEC>::load(A.b + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0, v);
+      } else {
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) v[i] = 0.0f;
+      }
+      Vec<VEC>::store(Bs + static_cast<std::size_t>(rr) * nx + x0, v);
+    }
+  };
+  // z on plane z (rows y0 .. y0+TY) from r of that plane (Rc) and of the plane below (Rb).
+  const auto primal = [&](float* Z, int z, const float* Rc, const float* Rb) {
+    for (int rr = ty; rr < TY + 1; rr += TY) {
+      const int y = y0 + rr;
+      const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+      const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+      const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+      const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr) * nx;
+      const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+      float out[VEC];
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) {
+        const int x = x0 + i;
+        float zv = 0.0f;
+        if (y < ny) {
+          float s = 0.0f;
+          if (z < nz - 1) s = __fadd_rn(s, rz[x]);
+          if (z > 0) s = __fsub_rn(s, rzb[x]);
+          if (y < ny - 1) s = __fadd_rn(s, ry[x]);
+          if (y > 0) s = __fsub_rn(s, rym[x]);
+          if (x < nx - 1) s = __fadd_rn(s, rx[x]);
+          if (x > 0) s = __fsub_rn(s, rx[x - 1]);
+          zv = tv_primal(Bs[static_cast<std::size_t>(rr) * nx + x], A.lambda, s);
+        }
+        out[i] = zv;
+      }
+      Vec<VEC>::store(Z + static_cast<std::size_t>(rr) * nx + x0, out);
+    }
+  };
+
+  load_r(R0, z0);
+  load_r(R1, z0 - 1);
+  load_b(z0);
+  __syncthreads();
+  primal(Z0, z0, R0, R1);
+  __syncthreads();
+
+  const int y = y0 + ty;
+  for (int z = z0; z < z1; ++z) {
+    const bool next = z + 1 < nz;
+    if (next) {
+      load_r(R1, z + 1);
+      load_b(z + 1);
+    }
+    const std::size_t at = static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0;
+    float pv[3][VEC];
+    if (!FIRST && y < ny) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Vec<VEC>::load(A.pin[c] + at, pv[c]);
+    }
+    __syncthreads();
+    if (next) primal(Z1, z + 1, R1, R0);
+    __syncthreads();
+    if (y < ny) {
+      float rv[3][VEC];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Vec<VEC>::load(R0 + (static_cast<std::size_t>(c) * ring_rows + ty + 1) * nx + x0, rv[c]);
+        if (FIRST) {
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) pv[c][i] = rv[c][i];
+        }
+      }
+      const float* zc = Z0 + static_cast<std::size_t>(ty) * nx;
+      const float* zy = Z0 + static_cast<std::size_t>(ty + 1) * nx;
+      const float* zz = Z1 + static_cast<std::size_t>(ty) * nx;
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) {
+        const int x = x0 + i;
+        const float c = zc[x];
+        float g[3];
+        g[0] = z < nz - 1 ? __fsub_rn(c, zz[x]) : 0.0f;
+        g[1] = y < ny - 1 ? __fsub_rn(c, zy[x]) : 0.0f;
+        g[2] = x < nx - 1 ? __fsub_rn(c, zc[x + 1]) : 0.0f;
+        float p[3] = {pv[0][i], pv[1][i], pv[2][i]};
+        float r[3] = {rv[0][i], rv[1][i], rv[2][i]};
+        tv_dual_step(g, A.step, A.momentum, p, r);
+#pragma unroll
+        for (int c2 = 0; c2 < 3; ++c2) {
+          pv[c2][i] = p[c2];
+          rv[c2][i] = r[c2];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Vec<VEC>::store(A.pout[c] + at, pv[c]);
+        if (!LAST) Vec<VEC>::store(A.rout[c] + at, rv[c]);
+      }
+    }
+    __syncthreads();
+    float* t = R0;
+    R0 = R1;
+    R1 = t;
+    t = Z0;
+    Z0 = Z1;
+    Z1 = t;
+  }
+}
+
+// Final primal point x = max(b - lambda L(p), 0), VEC voxels of one row per thread, and its use.
+template <int VEC, int Mode>
+__global__ void __launch_bounds__(256)
+    k_tv_final(const float* b, const float* pz, const float* py, const float* px, int nz, int ny, int nx,
+               float lambda, float momentum, float* xprev, float* out, float nm2, float inv_k02) {
+  const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
+  const std::size_t total = nxy * nz / VEC;
+  for (std::size_t t = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const std::size_t i0 = t * VEC;
+    const int x0 = static_cast<int>(i0 % nx);
+    const int y = static_cast<int>((i0 / nx) % ny);
+    const int z = static_cast<int>(i0 / nxy);
+    float bv[VEC], cz[VEC], cy[VEC], cx[VEC], bz[VEC], by[VEC];
+    Vec<VEC>::load(b + i0, bv);
+    Vec<VEC>::load(pz + i0, cz);
+    Vec<VEC>::load(py + i0, cy);
+    Vec<VEC>::load(px + i0, cx);
+    if (z > 0) Vec<VEC>::load(pz + i0 - nxy, bz);
+    if (y > 0) Vec<VEC>::load(py + i0 - nx, by);
+    const float left = x0 > 0 ? px[i0 - 1] : 0.0f;
+    float xv[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const int x = x0 + i;
+      float s = 0.0f;
+      if (z < nz - 1) s = __fadd_rn(s, cz[i]);
+      if (z > 0) s = __fsub_rn(s, bz[i]);
+      if (y < ny - 1) s = __fadd_rn(s, cy[i]);
+      if (y > 0) s = __fsub_rn(s, by[i]);
+      if (x < nx - 1) s = __fadd_rn(s, cx[i]);
+      if (x > 0) s = __fsub_rn(s, i == 0 ? left : cx[i > 0 ? i - 1 : 0]);
+      xv[i] = tv_primal(bv[i], lambda, s);
+    }
+    if constexpr (Mode == static_cast<int>(TvFinal::plain)) {
+      Vec<VEC>::store(out + i0, xv);
+    } else if constexpr (Mode == static_cast<int>(TvFinal::momentum)) {
+      float pv[VEC], yv[VEC];
+      Vec<VEC>::load(xprev + i0, pv);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) yv[i] = __fadd_rn(xv[i], __fmul_rn(momentum, __fsub_rn(xv[i], pv[i])));
+      Vec<VEC>::store(xprev + i0, xv);
+      Vec<VEC>::store(out + i0, yv);
+    } else {
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) xv[i] = index_from_potential(xv[i], 0.0f, nm2, inv_k02);
+      Vec<VEC>::store(out + i0, xv);
+    }
+  }
+}
+
+// Rows per CTA and planes per CTA for an (nz, ny, nx) volume.
+struct FgpShape {
+  int ty;
+  int zchunk;
+  std::size_t smem;
+};
+
+FgpShape fgp_shape(int nz, int ny, int nx, int vec) {
+  const int tx = nx / vec;
+  int ty = 4;
+  const auto smem_of = [&](int t) {
+    return (2 * static_cast<std::size_t>(3) * (t + 2) + 3 * static_cast<std::size_t>(t + 1)) * nx * sizeof(float);
+  };
+  while (ty > 1 && (tx * ty > 1024 || smem_of(ty) > 110 * 1024)) --ty;
+  require(tx * ty <= 1024 && smem_of(ty) <= 220 * 1024, "tv: volume rows too long for the FGP kernel");
+  // About two resident CTAs' worth of work per SM slot, at least 8 planes per CTA.
+  const int ytiles = (ny + ty - 1) / ty;
+  const int per_sm = std::max(1, std::min(static_cast<int>((200 * 1024) / smem_of(ty)), 2048 / (tx * ty)));
+  const int slots = sm_count() * per_sm;
+  int chunks = std::max(1, (slots + ytiles - 1) / ytiles);
+  int zchunk = std::max(8, (nz + chunks - 1) / chunks);
+  zchunk = std::min(zchunk, nz);
+  return {ty, zchunk, smem_of(ty)};
+}
+
+std::mutex g_fgp_mutex;
+std::set<std::pair<int, const void*>> g_fgp_attr;
+
+template <class K>
+void fgp_allow(K kernel) {
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(g_fgp_mutex);
+  const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
+  if (g_fgp_attr.count(key)) return;
+  check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+        "cudaFuncSetAttribute");
+  g_fgp_attr.insert(key);
+}
+
+template <int VEC, bool FIRST, bool LAST>
+void launch_fgp(const FgpArgs& a, const FgpShape& sh, cudaStream_t s) {
+  auto kernel = k_fgp<VEC, FIRST, LAST>;
+  fgp_allow(kernel);
+  const dim3 block(a.nx / VEC, sh.ty);
+  const dim3 grid((a.ny + sh.ty - 1) / sh.ty, (a.nz + sh.zchunk - 1) / sh.zchunk);
+  kernel<<<grid, block, sh.smem, s>>>(a);
+  check_launch("fgp step");
+}
+
+template <int VEC>
+void launch_fgp_any(bool first, bool last, const FgpArgs& a, const FgpShape& sh, cudaStream_t s) {
+  if (first && last) {
+    launch_fgp<VEC, true, true>(a, sh, s);
+  } else if (first) {
+    launch_fgp<VEC, true, false>(a, sh, s);
+  } else if (last) {
+    launch_fgp<VEC, false, true>(a, sh, s);
+  } else {
+    launch_fgp<VEC, false, false>(a, sh, s);
+  }
+}
+
+template <int VEC>
+void launch_final(TvFinal mode, const float* b, float* const p[3], int nz, int ny, int nx, float lambda,
+                  float momentum, float* xprev, float* out, float nm2, float inv_k02, cudaStream_t s) {
+  const std::size_t total = static_cast<std::size_t>(nz) * ny * nx / VEC;
+  const unsigned grid = static_cast<unsigned>(std::min<std::size_t>((total + 255) / 256, 148u * 16u));
+  switch (mode) {
+    case TvFinal::plain:
+      k_tv_final<VEC, 0><<<grid, 256, 0, s>>>(b, p[0], p[1], p[2], nz, ny, nx, lambda, momentum, xprev, out, nm2,
+                                               inv_k02);
+      break;
+    case TvFinal::momentum:
+      k_tv_final<VEC, 1><<<grid, 256, 0, s>>>(b, p[0], p[1], p[2], nz, ny, nx, lambda, momentum, xprev, out, nm2,
+                                               inv_k02);
+      break;
+    case TvFinal::index:
+      k_tv_final<VEC, 2><<<grid, 256, 0, s>>>(b, p[0], p[1], p[2], nz, ny, nx, lambda, momentum, xprev, out, nm2,
+                                               inv_k02);
+      break;
+  }
+  check_launch("tv final primal");
+}
+
+}  // namespace
+
+float fista_t(float t) { return 0.5f * (1.0f + std::sqrt(1.0f + 4.0f * t * t)); }
+
+void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, int inner, TvFinal final_mode,
+             float momentum, float* xprev, float* out, float nm2, float inv_k02, cudaStream_t s) {
+  require(nz >= 1 && ny >= 1 && nx >= 1, "tv: empty volume");
+  // float4 rows need nx % 4 == 0 and 16-byte aligned volumes.
+  bool aligned = nx % 4 == 0 && reinterpret_cast<std::uintptr_t>(b) % 16 == 0 &&
+                 reinterpret_cast<std::uintptr_t>(out) % 16 == 0 &&
+                 (xprev == nullptr || reinterpret_cast<std::uintptr_t>(xprev) % 16 == 0);
+  for (int i = 0; i < 3; ++i)
+    for (int c = 0; c < 3; ++c) aligned = aligned && reinterpret_cast<std::uintptr_t>(t.v[i][c]) % 16 == 0;
+  const int vec = aligned ? 4 : 1;
+  const FgpShape sh = fgp_shape(nz, ny, nx, vec);
+  const float step = 1.0f / (12.0f * lambda);
+  float tk = 1.0f;
+  const int ip = t.p_index;
+  const int ia = (ip + 1) % 3;
+  int cur_r = ip;
+  for (int k = 0; k < inner; ++k) {
+    const float tn = fista_t(tk);
+    const float m = (tk - 1.0f) / tn;
+    FgpArgs a{};
+    a.b = b;
+    a.nz = nz, a.ny = ny, a.nx = nx;
+    a.zchunk = sh.zchunk;
+    a.lambda = lambda, a.step = step, a.momentum = m;
+    const int rout = k == 0 ? (ip + 2) % 3 : 3 - ia - cur_r;
+    for (int c = 0; c < 3; ++c) {
+      a.rin[c] = t.v[cur_r][c];
+      a.pin[c] = t.v[k == 0 ? ip : ia][c];
+      a.pout[c] = t.v[ia][c];
+      a.rout[c] = t.v[rout][c];
+    }
+    if (vec == 4) {
+      launch_fgp_any<4>(k == 0, k == inner - 1, a, sh, s);
+    } else {
+      launch_fgp_any<1>(k == 0, k == inner - 1, a, sh, s);
+    }
+    cur_r = rout;
+    tk = tn;
+  }
+  if (inner > 0) t.p_index = ia;
+  float* const* p = t.v[t.p_index];
+  if (vec == 4) {
+    launch_final<4>(final_mode, b, p, nz, ny, nx, lambda, momentum, xprev, out, nm2, inv_k02, s);
+  } else {
+    launch_final<1>(final_mode, b, p, nz, ny, nx, lambda, momentum, xprev, out, nm2, inv_k02, s);
+  }
+}
+
+}  // namespace qhk

@@ -1,0 +1,159 @@
+"""CUDA kernels through the C ABI (libqhk.so) against the oracle and the reference's golden
+fixtures: FFTs, the FGP proximal step (bit-identical), the Ewald mapping (bit-identical indices,
+counts and sums), and the ODT solvers (1e-4 relative, the reference's CPU/CUDA bar,
+tests/test_cuda.cpp:74-115)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import contrast_err, dev, golden, host, rel_err
+from oracle import qh_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GEOM = np.array([0.532, 1.337, 1.2, 0.2], np.float32)
+CELL = np.array([[0.0, 0.4, -0.3, 2.5, 1.36], [0.0, 0.4, -0.3, 1.0, 1.38]], np.float32)
+
+
+@pytest.fixture(scope="module")
+def qhk(cuda):
+    from qoraholo_b200 import capi
+
+    assert capi.device_present()
+    return capi
+
+
+@pytest.mark.parametrize("n", [4, 6, 12, 30, 60, 62, 64, 96, 128, 192, 256, 384, 512, 1024])
+def test_fft2d_matches_numpy(cuda, qhk, n):
+    rng = np.random.default_rng(n)
+    count = 3 if n <= 512 else 1
+    a = (rng.standard_normal((count, n, n)) + 1j * rng.standard_normal((count, n, n))).astype(np.complex64)
+    t = dev(cuda, a)
+    qhk.fft2d(t.data_ptr(), count, n, True, 1.0)
+    ref = np.fft.fft2(a.astype(np.complex128))
+    assert rel_err(host(t), ref) < 2e-6
+    qhk.fft2d(t.data_ptr(), count, n, False, 1.0 / (n * n))
+    assert rel_err(host(t), a) < 2e-6
+
+
+@pytest.mark.parametrize("shape", [(4, 6, 8), (16, 12, 20), (32, 32, 32), (34, 32, 32), (62, 60, 60), (24, 48, 62)])
+def test_rfft3_and_irfft3_match_numpy(cuda, qhk, shape):
+    nz, ny, nx = shape
+    rng = np.random.default_rng(sum(shape))
+    x = rng.standard_normal(shape).astype(np.float32)
+    half = cuda.zeros((nz, ny, nx // 2 + 1), dtype=cuda.complex64, device="cuda")
+    tx = dev(cuda, x)
+    qhk.rfft3(tx.data_ptr(), half.data_ptr(), nz, ny, nx)
+    ref = np.fft.rfftn(x.astype(np.float64))
+    assert rel_err(host(half), ref) < 2e-6
+    out = cuda.zeros(shape, dtype=cuda.float32, device="cuda")
+    qhk.irfft3(half.data_ptr(), out.data_ptr(), nz, ny, nx, 1.0 / x.size)
+    assert rel_err(host(out), x) < 2e-6
+
+
+def test_tv_prox_bit_identical_to_reference(cuda, qhk):
+    g = golden("tv_prox")
+    nz, ny, nx = g["b"].shape
+    b = dev(cuda, g["b"])
+    x = cuda.zeros_like(b)
+    dual = dev(cuda, g["p0"].copy())
+    qhk.tv_prox(b.data_ptr(), x.data_ptr(), dual.data_ptr(), nz, ny, nx, float(g["lam"]), int(g["inner"]))
+    assert np.array_equal(host(x), g["x"])
+    assert np.array_equal(host(dual), g["p"])
+
+
+@pytest.mark.parametrize("shape,inner", [((24, 20, 36), 7), ((10, 12, 30), 5), ((9, 7, 8), 1), ((8, 8, 8), 0),
+                                         ((40, 33, 64), 10)])
+def test_tv_prox_bit_identical_to_oracle(cuda, qhk, shape, inner):
+    rng = np.random.default_rng(inner + shape[0])
+    b = rng.uniform(-0.2, 1.0, shape).astype(np.float32)
+    p0 = (rng.uniform(-0.6, 0.6, (3,) + shape) * (rng.uniform(size=(3,) + shape) > 0.3)).astype(np.float32)
+    lam = 0.04
+    p = [p0[a].copy() for a in range(3)]
+    x_ref = O.tv_prox(b, p, lam, inner)
+    tb, tx, td = dev(cuda, b), cuda.zeros(shape, dtype=cuda.float32, device="cuda"), dev(cuda, p0.copy())
+    qhk.tv_prox(tb.data_ptr(), tx.data_ptr(), td.data_ptr(), *shape, lam, inner)
+    assert np.array_equal(host(tx), x_ref)
+    assert np.array_equal(host(td), np.stack(p))
+
+
+@pytest.mark.parametrize("n,nz,count", [(32, 32, 13), (48, 40, 25), (64, 64, 49), (30, 34, 7)])
+def test_ewald_mapping_bit_identical(cuda, qhk, n, nz, count):
+    geom = GEOM.copy()
+    geom[3] = 0.25
+    il = O.circular_scan(count, 0.9, geom)
+    rng = np.random.default_rng(n + count)
+    spectra = (rng.standard_normal((count, n, n)) + 1j * rng.standard_normal((count, n, n))).astype(np.complex64)
+    g = O.make_grid(n, nz, geom)
+    pre, pim, w = O.ewald_map(spectra, il, g)
+    filled = w > 0
+    pre = np.where(filled, pre / np.where(filled, w, 1), pre).astype(np.float32)
+    pim = np.where(filled, pim / np.where(filled, w, 1), pim).astype(np.float32)
+    a_ref, hits_ref = O.hermitian_half(pre, pim, w)
+    ts = dev(cuda, spectra)
+    h = n // 2 + 1
+    a = cuda.zeros((nz, n, h), dtype=cuda.complex64, device="cuda")
+    hits = cuda.zeros((nz, n, h), dtype=cuda.uint8, device="cuda")
+    cnt = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    qhk.ewald_map(ts.data_ptr(), count, n, nz, il, geom, 1, a.data_ptr(), hits.data_ptr(), cnt.data_ptr())
+    assert np.array_equal(host(hits), hits_ref)
+    assert np.array_equal(host(a).view(np.uint64), a_ref.view(np.uint64)) or np.array_equal(host(a), a_ref)
+    assert int(host(cnt)[0]) == int(np.count_nonzero(filled))
+    full = cuda.zeros((nz, n, n), dtype=cuda.complex64, device="cuda")
+    mask = cuda.zeros((nz, n, n), dtype=cuda.uint8, device="cuda")
+    cnt.zero_()
+    qhk.ewald_map(ts.data_ptr(), count, n, nz, il, geom, 0, full.data_ptr(), mask.data_ptr(), cnt.data_ptr())
+    assert np.array_equal(host(mask), filled.astype(np.uint8))
+    assert np.array_equal(host(full), (pre + 1j * pim).astype(np.complex64))
+    assert int(host(cnt)[0]) == int(np.count_nonzero(filled))
+
+
+CASES = {"plain": {}, "gp_r2c": dict(iterations=5), "gp_c2c": dict(iterations=5, gp_transform="c2c"),
+         "tv": dict(iterations=5, solver="tv"), "tv_nz34": dict(iterations=3, solver="tv", nz=34)}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_reconstruct_matches_reference_fixture(qhk, case):
+    g = golden("reconstruct")
+    ri, filled = qhk.reconstruct(g["fields"], g["illum"], g["geom"], **CASES[case])
+    assert contrast_err(ri, g[case], float(g["geom"][1])) < 1e-4
+    assert filled == float(g[case + "_filled"])  # EXPECT_DOUBLE_EQ(filled), tests/test_cuda.cpp:98
+
+
+@pytest.mark.parametrize("kw", [dict(iterations=5), dict(iterations=5, mapping="scatter"),
+                                dict(iterations=5, gp_transform="c2c"), dict(iterations=10, solver="tv")])
+def test_reconstruct_matches_oracle_at_64(qhk, kw):
+    # Cuda.ReconstructionMatchesCpu / TvMatchesCpu (tests/test_cuda.cpp:74-115): 25 angles, 64^3.
+    il = O.circular_scan(25, 0.9, GEOM)
+    fields = O.rytov(O.forward_fields(CELL, il, GEOM, 64, "rytov"))
+    okw = {k: v for k, v in kw.items() if k != "mapping"}
+    a, fa = O.reconstruct(fields, il, GEOM, **okw)
+    b, fb = qhk.reconstruct(fields, il, GEOM, **kw)
+    assert contrast_err(b, a, GEOM[1]) < 1e-4
+    assert fa == fb
+
+
+def test_tv_odd_shape_partial_tiles(qhk):
+    # Cuda.TvKernelVariantsAgree (tests/test_cuda.cpp:120-137): 60 x 60 x 62 leaves partial tiles.
+    il = O.circular_scan(25, 0.9, GEOM)
+    fields = O.rytov(O.forward_fields(CELL, il, GEOM, 60, "rytov"))
+    a, fa = O.reconstruct(fields, il, GEOM, nz=62, iterations=5, solver="tv")
+    b, fb = qhk.reconstruct(fields, il, GEOM, nz=62, iterations=5, solver="tv")
+    assert contrast_err(b, a, GEOM[1]) < 1e-4 and fa == fb
+
+
+def test_odt_plan_runs_are_deterministic(cuda, qhk):
+    il = O.circular_scan(13, 0.9, GEOM)
+    fields = O.rytov(O.forward_fields(CELL, il, GEOM, 48, "rytov"))
+    plan = qhk.OdtPlan(48, 13, il, GEOM, iterations=4, solver="tv", tv_inner=5)
+    out = []
+    for _ in range(2):
+        f = dev(cuda, fields)
+        idx = cuda.zeros(plan.shape, dtype=cuda.float32, device="cuda")
+        plan.run(f.data_ptr(), idx.data_ptr())
+        out.append(host(idx))
+    assert np.array_equal(out[0], out[1])
+    assert plan.device_bytes > 0
+    assert 0 < plan.filled() < 1
