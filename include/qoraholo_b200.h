@@ -105,12 +105,107 @@ int qhk_ewald_map(const void* d_spectra, int count, int n, int nz, const float* 
 int qhk_tv_prox(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int nx, float lambda, int inner,
                 void* stream);
 
+/* The same proximal step with no allocation: d_dual holds 9 volumes -- the dual p (3 volumes, warm
+ * start, updated in place) followed by 6 volumes of scratch. Asynchronous on `stream`. */
+int qhk_tv_prox_device(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int nx, float lambda, int inner,
+                       void* stream);
+
+/* Number of kernels this library has launched since it was loaded (for launch accounting). */
+uint64_t qhk_kernel_launches(void);
+
 /* ---- FFTs on the device (the transforms the reference ran through cuFFT, src/cuda/util.cuh:137-174).
  * Unnormalised; results times `scale`. */
 int qhk_fft2d(void* d_data, int count, int n, int forward, float scale, void* stream);
 /* Real (nz, ny, nx) -> half spectrum (nz, ny, nx/2+1), and back (d_half is overwritten). */
 int qhk_rfft3(const float* d_x, void* d_half, int nz, int ny, int nx, void* stream);
 int qhk_irfft3(void* d_half, float* d_x, int nz, int ny, int nx, float scale, void* stream);
+
+/* ---- Field retrieval: replaces cuda::extract_fields / FieldStage (src/cuda/field.cu:121-135,
+ * src/cuda/stages.cuh:19-47). Host in / host out. holo: (count, n, n) float32; the crop follows
+ * crop_plan (src/api.cpp:52-60): centre (cy, cx) pixels from DC rounded to integers, radius <= 0
+ * means |centre| / 3, output_size 0 means n. out: (count, m, m) complex64, m the output side. */
+int qhk_extract_fields(const float* holo, int count, int n, float cy, float cx, float radius, int output_size,
+                       void* out);
+
+/* sample / background pixel by pixel (field_ratio, src/cpu/field.cpp:62-74; host-only in the reference).
+ * sample: (count, ny, nx) complex64, background: bcount == 1 or bcount == count images. Host in / out. */
+int qhk_field_ratio(const void* sample, int count, int ny, int nx, const void* background, int bcount, void* out);
+
+/* Peak of the +1 sideband of hologram `holo` (n x n, host): find_sideband (src/cpu/field.cpp:25-60),
+ * integer peak and the Jacobsen / Candan sub-pixel refinement. dc_exclusion <= 0 means n / 8. */
+int qhk_find_sideband(const float* holo, int n, float dc_exclusion, int* iy, int* ix, float* y, float* x,
+                      float* magnitude);
+
+/* ---- Unwrap and Rytov: replaces cuda::unwrap / cuda::rytov / Unwrapper (src/cuda/unwrap.cu:156-263).
+ * Host in / host out, (count, ny, nx) with even sides. */
+int qhk_unwrap(const float* wrapped, int count, int ny, int nx, float* out);
+int qhk_rytov(const void* ratio, int count, int ny, int nx, void* out);
+
+/* ---- Pipeline: replaces cuda::make_pipeline and Pipeline::Impl (src/backends.hpp:75-89,
+ * src/cuda/pipeline.cu:12-161). Validation of the Pipeline constructor (src/pipeline.cpp:72-91). */
+typedef struct qhk_pipeline_options {
+  int count;          /* holograms per stack */
+  int hologram_size;  /* side N */
+  float center_y;     /* reference carrier, pixels from DC */
+  float center_x;
+  float radius;       /* crop radius; <= 0: |centre| / 3 */
+  int output_size;    /* field side m; 0: N */
+  int upload_chunks;  /* 1 .. count */
+  qhk_odt_options odt;
+} qhk_pipeline_options;
+
+/* qoraholo::PipelineTimings (include/qoraholo/pipeline.hpp:31-43), milliseconds. */
+typedef struct qhk_pipeline_timings {
+  double upload, fields, rytov, fft2, clear, mapping, normalize, solve, finish, download, total;
+} qhk_pipeline_timings;
+
+typedef struct qhk_pipeline qhk_pipeline;
+int qhk_pipeline_create(qhk_pipeline** pipeline, const qhk_pipeline_options* options, const float* illum_fyfx,
+                        const qhk_geometry* geometry);
+/* Background holograms (count, N, N), host. Their fields stay on the device. */
+int qhk_pipeline_set_background(qhk_pipeline* pipeline, const float* backgrounds);
+/* Page-locked input (count, N, N) float32 and output (nz, m, m) float32 buffers owned by the pipeline. */
+float* qhk_pipeline_input(qhk_pipeline* pipeline);
+const float* qhk_pipeline_output(const qhk_pipeline* pipeline);
+/* input -> output; QHK_LOGIC_ERROR before set_background. Synchronous. */
+int qhk_pipeline_process(qhk_pipeline* pipeline);
+/* Device-resident variant: d_holo (count, N, N) and d_index (nz, m, m) on the device, asynchronous on
+ * `stream`, no host copies (for serving loops and benchmarks). */
+int qhk_pipeline_process_device(qhk_pipeline* pipeline, const float* d_holo, float* d_index, void* stream);
+/* filled fraction and stage timings of the last process(). */
+int qhk_pipeline_result(const qhk_pipeline* pipeline, double* filled, qhk_pipeline_timings* timings);
+/* Filled fraction after process_device (waits for `stream`). */
+int qhk_pipeline_filled(qhk_pipeline* pipeline, void* stream, double* filled);
+int qhk_pipeline_shape(const qhk_pipeline* pipeline, int* nz, int* ny, int* nx);
+size_t qhk_pipeline_device_bytes(const qhk_pipeline* pipeline);
+int qhk_pipeline_destroy(qhk_pipeline* pipeline);
+
+/* ---- Beam propagation: replaces cuda::bpm_forward / bpm_vjp / bpm_reconstruct (src/backends.hpp:117-124,
+ * src/cuda/bpm.cu:236-349), tables as bpm_tables (src/bpm.cpp:10-60). Host in / host out. */
+/* ri: (nz, n, n) refractive index -> out: (count, n, n) complex64 field ratios at z = 0. */
+int qhk_bpm_forward(const float* ri, int nz, int n, const float* illum_fyfx, int count, const qhk_geometry* geometry,
+                    int obliquity, void* out);
+/* x: (nz, n, n) contrast n - n_medium, r: (count, n, n) complex64 -> out = J^T r (nz, n, n). */
+int qhk_bpm_vjp(const float* x, int nz, int n, const void* r, const float* illum_fyfx, int count,
+                const qhk_geometry* geometry, int obliquity, float* out);
+
+/* qoraholo::BpmSolveOptions without the backend field (include/qoraholo/bpm.hpp:29-41). */
+typedef struct qhk_bpm_solve_options {
+  int iterations;
+  int batch;
+  float step;
+  float tv_weight;
+  int tv_inner;
+  int obliquity;
+} qhk_bpm_solve_options;
+
+/* fields (count, n, n) complex64, initial (nz, n, n) index -> out (nz, n, n) index; loss receives
+ * `iterations` doubles (the data term per iteration, BpmResult::loss). */
+int qhk_bpm_reconstruct(const void* fields, int count, int n, const float* illum_fyfx, const qhk_geometry* geometry,
+                        const float* initial, int nz, const qhk_bpm_solve_options* options, float* out, double* loss);
+
+/* Host in / host out 2D FFT of `count` n x n images (used by the fixture generators). */
+int qhk_fft2d_host(void* data, int count, int n, int forward, float scale);
 
 #ifdef __cplusplus
 }

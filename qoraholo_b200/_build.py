@@ -5,7 +5,8 @@
   qoraholo_b200/_core*.so        pybind11 bindings with the reference's Python signatures
 
 nvcc cross-compiles without a GPU. Objects go to qoraholo_b200/_build/; a library is rebuilt
-when any of its sources or headers is newer. Usage: python -m qoraholo_b200._build [--force]
+when any of its sources or headers is newer. Usage: python qoraholo_b200/_build.py [--force]
+(run as a script: importing the package itself needs the built extension).
 """
 
 from __future__ import annotations

@@ -1,0 +1,506 @@
+// Multi-slice beam propagation (BPM) on the device: forward model, its adjoint, and the proximal
+// gradient inversion. Replaces the reference's Bpm class and bpm_reconstruct (src/cuda/bpm.cu:126-349)
+// and follows the CPU form (src/cpu/bpm.cpp:18-243) and the tables of src/bpm.cpp:10-60.
+//
+// A pass of the model processes a chunk of nb illuminations at once, all planes (nb, n, n). Each
+// slice is two 2D FFTs, each split into a row pass and a column pass; the pointwise work of the
+// slice is folded into the column pass epilogues:
+//   forward:  IFFT(S) -> [x (1/n^2), store envelope, times the screen e^{i phase x_k}] ->
+//             FFT -> [S = c (q V + (1 - q) S)]                          (4 launches per slice)
+//   adjoint:  IFFT(b) -> [x 1/n^2] -> gradient kernel (one thread per pixel, sums the nb
+//             illuminations in order, writes conj(screen) b) -> FFT -> [U = conj(c)(g + back),
+//             b = q U, g = (1 - q) U]                                   (5 launches per slice)
+// The gradient has one writer per voxel and a fixed summation order; the data term is summed in
+// double per CTA and reduced in order.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <numbers>
+#include <vector>
+
+#include "bpm.hpp"
+
+namespace qhk {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <class K>
+void allow(K kernel, std::size_t) {
+  ensure_smem(kernel);
+}
+
+// Rows of length n, src -> dst (may alias), COLS rows per CTA.
+template <bool Fwd, int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_rows(const float2* __restrict__ src, float2* __restrict__ dst, std::size_t rows, FftLen L) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  const int n = L.n;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(n) * cp;
+  const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
+  const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
+  const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int row = idx / n;
+    const int pos = idx - row * n;
+    A[pos * cp + row] = row < nr ? src[(r0 + row) * n + pos] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* res = smem_fft<Fwd>(A, B, cp, COLS, L, tid, nth);
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int row = idx / n;
+    const int pos = idx - row * n;
+    if (row < nr) dst[(r0 + row) * n + pos] = res[pos * cp + row];
+  }
+}
+
+enum ColMode : int { kScreen = 0, kPropagate = 1, kScale = 2, kSplit = 3 };
+
+struct ColArgs {
+  float2* data;         // (nb, n, n), transformed in place (kPropagate: read only)
+  float2* s;            // kPropagate: spectrum S, updated; kSplit: g, updated
+  float2* store;        // kScreen: envelope store of this slice (nb, n, n) or null
+  const float* x;       // kScreen: contrast of this slice (n, n)
+  const float2* coef;   // kPropagate / kSplit: propagator table of the chunk (nb, n, n)
+  const float* q;       // obliquity weights (nb, n, n)
+  float phase;          // screen phase per unit contrast
+  float inv;            // 1 / n^2
+  int has_back;         // kSplit: add data (the back-propagated screen term) to g
+};
+
+template <bool Fwd, int Mode, int COLS>
+__global__ void __launch_bounds__(kThreads) k_cols(ColArgs a, FftLen L) {
+  extern __shared__ float2 sm[];
+  const int n = L.n;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(n) * COLS;
+  const int c0 = static_cast<int>(blockIdx.x) * COLS;
+  const int cols = min(COLS, n - c0);
+  const std::size_t base = static_cast<std::size_t>(blockIdx.y) * n * n + c0;
+  const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int pos = idx / COLS;
+    const int col = idx - pos * COLS;
+    A[idx] = col < cols ? a.data[base + static_cast<std::size_t>(pos) * n + col] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* res = smem_fft<Fwd>(A, B, COLS, COLS, L, tid, nth);
+  for (int idx = tid; idx < n * COLS; idx += nth) {
+    const int pos = idx / COLS;
+    const int col = idx - pos * COLS;
+    if (col >= cols) continue;
+    const std::size_t g = base + static_cast<std::size_t>(pos) * n + col;
+    const float2 v = res[idx];
+    if constexpr (Mode == kScreen) {
+      const float2 w = cscale(v, a.inv);
+      if (a.store) a.store[g] = w;
+      float sn, cs;
+      sincosf(a.phase * a.x[static_cast<std::size_t>(pos) * n + c0 + col], &sn, &cs);
+      a.data[g] = cmul(make_float2(cs, sn), w);
+    } else if constexpr (Mode == kPropagate) {
+      const float2 c = a.coef[g];
+      const float q = a.q[g];
+      const float2 s = a.s[g];
+      const float tre = q * v.x + (1.0f - q) * s.x;
+      const float tim = q * v.y + (1.0f - q) * s.y;
+      a.s[g] = make_float2(c.x * tre - c.y * tim, c.x * tim + c.y * tre);
+    } else if constexpr (Mode == kScale) {
+      a.data[g] = cscale(v, a.inv);
+    } else {
+      float2 gi = a.s[g];
+      if (a.has_back) gi = cadd(gi, v);
+      else gi = v;
+      const float2 c = a.coef[g];
+      const float q = a.q[g];
+      const float ure = c.x * gi.x + c.y * gi.y;
+      const float uim = c.x * gi.y - c.y * gi.x;
+      a.data[g] = make_float2(q * ure, q * uim);
+      a.s[g] = make_float2((1.0f - q) * ure, (1.0f - q) * uim);
+    }
+  }
+}
+
+// Spectrum of the unit envelope: n^2 at the zero bin of every plane.
+__global__ void k_unit_spectrum(float2* s, std::size_t plane, std::size_t total) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    s[i] = make_float2(i % plane == 0 ? static_cast<float>(plane) : 0.0f, 0.0f);
+  }
+}
+
+// First slice: the envelope is 1; store it and apply the screen of slice 0.
+__global__ void k_first_screen(float2* w, float2* store, const float* x, float phase, std::size_t plane,
+                               std::size_t total) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    if (store) store[i] = make_float2(1.0f, 0.0f);
+    float sn, cs;
+    sincosf(phase * x[i % plane], &sn, &cs);
+    w[i] = make_float2(cs, sn);
+  }
+}
+
+// r = y - data in place, and per-CTA sums of |r|^2 in double.
+__global__ void __launch_bounds__(kThreads)
+    k_residual(float2* y, const float2* __restrict__ data, std::size_t total, double* partial) {
+  __shared__ double red[kThreads];
+  double acc = 0.0;
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const float2 v = csub(y[i], data[i]);
+    y[i] = v;
+    acc += static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (static_cast<int>(threadIdx.x) < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// Sums `n` partials in order and adds the result to *out.
+__global__ void k_sum_partials(const double* partial, int n, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += partial[i];
+    *out += s;
+  }
+}
+
+// One thread per pixel of slice k: grad += gscale * phase * sum_a Im(conj(t w_a) b_a), and
+// b_a <- conj(t) b_a, t = e^{i phase x}.
+__global__ void k_gradient(float2* b, const float2* __restrict__ store, const float* __restrict__ x, float phase,
+                           int nb, std::size_t plane, float gscale, float* grad) {
+  for (std::size_t p = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; p < plane;
+       p += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    float sn, cs;
+    sincosf(phase * x[p], &sn, &cs);
+    float acc = 0.0f;
+    for (int j = 0; j < nb; ++j) {
+      const std::size_t o = j * plane + p;
+      const float2 bv = b[o];
+      const float2 v = cmul(make_float2(cs, sn), store[o]);
+      acc += v.x * bv.y - v.y * bv.x;
+      b[o] = cmul(make_float2(cs, -sn), bv);
+    }
+    grad[p] += gscale * phase * acc;
+  }
+}
+
+__global__ void k_axpy_clamp(const float* point, const float* grad, float alpha, std::size_t total, float* z,
+                             float* out) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const float v = point[i] - alpha * grad[i];
+    if (z) z[i] = v;
+    if (out) out[i] = fmaxf(v, 0.0f);
+  }
+}
+
+__global__ void k_extrapolate(const float* next, float* x, float momentum, std::size_t total, float* y) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const float nv = next[i];
+    y[i] = nv + momentum * (nv - x[i]);
+    x[i] = nv;
+  }
+}
+
+__global__ void k_contrast(const float* ri, float nm, std::size_t total, float* x, bool clamp) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const float v = __fsub_rn(ri[i], nm);
+    x[i] = clamp ? fmaxf(v, 0.0f) : v;
+  }
+}
+
+__global__ void k_add_medium(const float* x, float nm, std::size_t total, float* ri) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    ri[i] = __fadd_rn(x[i], nm);
+  }
+}
+
+unsigned grid_for(std::size_t total) {
+  return static_cast<unsigned>(std::min<std::size_t>((total + kThreads - 1) / kThreads, 148u * 32u));
+}
+
+int rows_cols(int n) {
+  int c = 16;
+  while (c > 1 && 2 * static_cast<std::size_t>(n) * (c + 1) * sizeof(float2) > 72 * 1024) c /= 2;
+  return c;
+}
+
+}  // namespace
+
+BpmTablesHost bpm_tables(int n, int nz, const float* il, int count, float wavelength, float n_medium, float na,
+                         float pixel, bool obliquity) {
+  constexpr double kPi = std::numbers::pi;
+  const double lambda = wavelength;
+  const double fm = n_medium / lambda;
+  const double fna = na / lambda;
+  const double d = pixel;
+  const double df = 1.0 / (n * d);
+  const double nuz_min = std::sqrt(std::max(fm * fm - fna * fna, 0.01 * fm * fm));
+  const double back = -(nz - 1 - nz / 2) * d;
+  BpmTablesHost t;
+  t.n = n;
+  t.nz = nz;
+  t.count = count;
+  t.phase = static_cast<float>(2.0 * kPi / lambda * d);
+  const std::size_t plane = static_cast<std::size_t>(n) * n;
+  t.step.assign(plane * count, make_float2(0, 0));
+  t.last.assign(plane * count, make_float2(0, 0));
+  t.q.assign(plane * count, 1.0f);
+  double q0 = 0;
+  for (int a = 0; a < count; ++a) {
+    const double fiy = il[2 * a], fix = il[2 * a + 1];
+    const double fiz = std::sqrt(fm * fm - fiy * fiy - fix * fix);
+    for (int ky = 0; ky < n; ++ky) {
+      for (int kx = 0; kx < n; ++kx) {
+        const std::size_t i = a * plane + static_cast<std::size_t>(ky) * n + kx;
+        const double fy = signed_bin(ky, n) * df + fiy;
+        const double fx = signed_bin(kx, n) * df + fix;
+        const double rho2 = fy * fy + fx * fx;
+        double q = 1;
+        if (rho2 < fm * fm) {
+          const double nuz = std::sqrt(fm * fm - rho2);
+          const auto c = std::polar(1.0, 2.0 * kPi * (nuz - fiz) * d);
+          t.step[i] = make_float2(static_cast<float>(c.real()), static_cast<float>(c.imag()));
+          if (rho2 <= fna * fna) {
+            const auto l = std::polar(1.0, 2.0 * kPi * (nuz - fiz) * back);
+            t.last[i] = make_float2(static_cast<float>(l.real()), static_cast<float>(l.imag()));
+          }
+          if (obliquity) q = fm / std::max(nuz, nuz_min);
+        }
+        t.q[i] = static_cast<float>(q);
+      }
+    }
+    q0 += static_cast<double>(t.q[a * plane]) * t.q[a * plane];
+  }
+  t.lipschitz = static_cast<float>(nz * static_cast<double>(t.phase) * t.phase * q0 / count);
+  return t;
+}
+
+BpmPlan::BpmPlan(const BpmTablesHost& t, int chunk, bool store) : t_(t), chunk_(chunk), store_on_(store) {
+  require(t.n >= 4 && t.n % 2 == 0 && t.nz >= 1 && t.count >= 1, "bpm: invalid tables");
+  require(chunk >= 1 && chunk <= t.count && chunk <= 65535, "bpm: invalid chunk");
+  plane_ = static_cast<std::size_t>(t.n) * t.n;
+  const std::size_t all = plane_ * t.count;
+  step_.reset(all);
+  last_.reset(all);
+  q_.reset(all);
+  check(cudaMemcpy(step_.get(), t.step.data(), step_.bytes(), cudaMemcpyHostToDevice), "upload tables");
+  check(cudaMemcpy(last_.get(), t.last.data(), last_.bytes(), cudaMemcpyHostToDevice), "upload tables");
+  check(cudaMemcpy(q_.get(), t.q.data(), q_.bytes(), cudaMemcpyHostToDevice), "upload tables");
+  s_.reset(plane_ * chunk);
+  w_.reset(plane_ * chunk);
+  if (store) stored_.reset(plane_ * chunk * t.nz);
+  partial_.reset(4096);
+}
+
+std::size_t BpmPlan::device_bytes() const {
+  return step_.bytes() + last_.bytes() + q_.bytes() + s_.bytes() + w_.bytes() + stored_.bytes() + partial_.bytes();
+}
+
+void BpmPlan::fft2(const float2* src, float2* dst, bool forward, int nb, int mode, const void* args_v,
+                   cudaStream_t s) {
+  const int n = t_.n;
+  const FftLen& L = fft_len(n);
+  const int c = rows_cols(n);
+  const std::size_t rows = static_cast<std::size_t>(nb) * n;
+  {
+    const std::size_t smem = 2 * static_cast<std::size_t>(n) * (c + 1) * sizeof(float2);
+    const unsigned grid = static_cast<unsigned>((rows + c - 1) / c);
+#define QHK_ROWS(C)                                                      \
+  case C:                                                                \
+    if (forward) {                                                       \
+      allow(k_rows<true, C>, smem);                                      \
+      k_rows<true, C><<<grid, kThreads, smem, s>>>(src, dst, rows, L);   \
+    } else {                                                             \
+      allow(k_rows<false, C>, smem);                                     \
+      k_rows<false, C><<<grid, kThreads, smem, s>>>(src, dst, rows, L);  \
+    }                                                                    \
+    break;
+    switch (c) {
+      QHK_ROWS(16)
+      QHK_ROWS(8)
+      QHK_ROWS(4)
+      QHK_ROWS(2)
+      QHK_ROWS(1)
+    }
+#undef QHK_ROWS
+    check_launch("bpm rows");
+  }
+  ColArgs a = *static_cast<const ColArgs*>(args_v);
+  a.data = dst;
+  const std::size_t smem = 2 * static_cast<std::size_t>(n) * c * sizeof(float2);
+  const dim3 grid((n + c - 1) / c, nb);
+#define QHK_COLS(C)                                                                                   \
+  case C:                                                                                             \
+    switch (mode) {                                                                                   \
+      case kScreen: allow(k_cols<false, kScreen, C>, smem); k_cols<false, kScreen, C><<<grid, kThreads, smem, s>>>(a, L); break; \
+      case kPropagate: allow(k_cols<true, kPropagate, C>, smem); k_cols<true, kPropagate, C><<<grid, kThreads, smem, s>>>(a, L); break; \
+      case kScale: allow(k_cols<false, kScale, C>, smem); k_cols<false, kScale, C><<<grid, kThreads, smem, s>>>(a, L); break; \
+      default: allow(k_cols<true, kSplit, C>, smem); k_cols<true, kSplit, C><<<grid, kThreads, smem, s>>>(a, L); break; \
+    }                                                                                                 \
+    break;
+  switch (c) {
+    QHK_COLS(16)
+    QHK_COLS(8)
+    QHK_COLS(4)
+    QHK_COLS(2)
+    QHK_COLS(1)
+  }
+#undef QHK_COLS
+  check_launch("bpm columns");
+}
+
+void BpmPlan::forward(const float* x, int first, int nb, cudaStream_t s) {
+  const int nz = t_.nz;
+  const std::size_t total = plane_ * nb;
+  const std::size_t off = plane_ * first;
+  const float inv = 1.0f / static_cast<float>(plane_);
+  k_unit_spectrum<<<grid_for(total), kThreads, 0, s>>>(s_.get(), plane_, total);
+  check_launch("bpm start");
+  k_first_screen<<<grid_for(total), kThreads, 0, s>>>(w_.get(), store_on_ ? stored_.get() : nullptr, x, t_.phase,
+                                                      plane_, total);
+  check_launch("bpm start");
+  for (int k = 0; k < nz; ++k) {
+    if (k > 0) {
+      ColArgs a{};
+      a.store = store_on_ ? stored_.get() + k * total : nullptr;
+      a.x = x + k * plane_;
+      a.phase = t_.phase;
+      a.inv = inv;
+      fft2(s_.get(), w_.get(), false, nb, kScreen, &a, s);
+    }
+    ColArgs a{};
+    a.s = s_.get();
+    a.coef = (k == nz - 1 ? last_.get() : step_.get()) + off;
+    a.q = q_.get() + off;
+    fft2(w_.get(), w_.get(), true, nb, kPropagate, &a, s);
+  }
+  ColArgs a{};
+  a.inv = inv;
+  fft2(s_.get(), w_.get(), false, nb, kScale, &a, s);  // envelopes at z = 0 in w
+}
+
+void BpmPlan::adjoint(const float* x, const float2* residual_or_null, int first, int nb, float gscale, float* grad,
+                      cudaStream_t s) {
+  const int nz = t_.nz;
+  const std::size_t total = plane_ * nb;
+  const std::size_t off = plane_ * first;
+  const float inv = 1.0f / static_cast<float>(plane_);
+  // w holds the residual r (or it is copied in); g = FFT(r), split at the last slice.
+  if (residual_or_null) {
+    check(cudaMemcpyAsync(w_.get(), residual_or_null, total * sizeof(float2), cudaMemcpyDeviceToDevice, s),
+          "copy residual");
+  }
+  ColArgs a{};
+  a.s = s_.get();
+  a.coef = last_.get() + off;
+  a.q = q_.get() + off;
+  a.has_back = 0;
+  fft2(w_.get(), w_.get(), true, nb, kSplit, &a, s);
+  for (int k = nz - 1; k >= 0; --k) {
+    ColArgs b{};
+    b.inv = inv;
+    fft2(w_.get(), w_.get(), false, nb, kScale, &b, s);
+    k_gradient<<<grid_for(plane_), kThreads, 0, s>>>(w_.get(), stored_.get() + k * total, x + k * plane_, t_.phase,
+                                                     nb, plane_, gscale, grad + k * plane_);
+    check_launch("bpm gradient");
+    if (k > 0) {
+      ColArgs c{};
+      c.s = s_.get();
+      c.coef = step_.get() + off;
+      c.q = q_.get() + off;
+      c.has_back = 1;
+      fft2(w_.get(), w_.get(), true, nb, kSplit, &c, s);
+    }
+  }
+}
+
+double BpmPlan::residual(const float2* data, int first, int nb, double* d_loss, cudaStream_t s) {
+  const std::size_t total = plane_ * nb;
+  const unsigned blocks = std::min<unsigned>(grid_for(total), 4096);
+  k_residual<<<blocks, kThreads, 0, s>>>(w_.get(), data + plane_ * first, total, partial_.get());
+  check_launch("bpm residual");
+  k_sum_partials<<<1, 32, 0, s>>>(partial_.get(), static_cast<int>(blocks), d_loss);
+  check_launch("bpm residual");
+  return 0.0;
+}
+
+void contrast(const float* ri, float n_medium, std::size_t total, float* x, bool clamp, cudaStream_t s) {
+  k_contrast<<<grid_for(total), kThreads, 0, s>>>(ri, n_medium, total, x, clamp);
+  check_launch("contrast");
+}
+
+void add_medium(const float* x, float n_medium, std::size_t total, float* ri, cudaStream_t s) {
+  k_add_medium<<<grid_for(total), kThreads, 0, s>>>(x, n_medium, total, ri);
+  check_launch("add medium");
+}
+
+void bpm_solve(const BpmTablesHost& t, const float2* d_fields, float* d_x, int iterations, int batch, float step,
+               float tv_weight, int tv_inner, double* d_loss, cudaStream_t s) {
+  const int count = t.count;
+  batch = batch <= 0 || batch >= count ? count : batch;
+  const bool fista = batch == count;
+  const float alpha = step / t.lipschitz;
+  const bool tv = tv_weight > 0;
+  const std::size_t size = static_cast<std::size_t>(t.nz) * t.n * t.n;
+  BpmPlan plan(t, batch, true);
+  DevBuf<float> vols(4 * size);
+  float* y = vols.get();
+  float* next = y + size;
+  float* grad = y + 2 * size;
+  float* z = y + 3 * size;
+  DevBuf<float> dual(tv ? 9 * size : 0);
+  TvBuffers tvb;
+  if (tv) {
+    check(cudaMemsetAsync(dual.get(), 0, 3 * size * sizeof(float), s), "cudaMemset");
+    for (int i = 0; i < 3; ++i)
+      for (int c = 0; c < 3; ++c) tvb.v[i][c] = dual.get() + (3 * i + c) * size;
+  }
+  check(cudaMemcpyAsync(y, d_x, size * sizeof(float), cudaMemcpyDeviceToDevice, s), "copy x");
+  const auto gradient = [&](const float* point, int first, int last, double* loss) {
+    check(cudaMemsetAsync(grad, 0, size * sizeof(float), s), "cudaMemset");
+    plan.forward(point, first, last - first, s);
+    plan.residual(d_fields, first, last - first, loss, s);
+    plan.adjoint(point, nullptr, first, last - first, 1.0f / static_cast<float>(last - first), grad, s);
+  };
+  const auto prox = [&](const float* point, float* out) {
+    if (tv) {
+      k_axpy_clamp<<<grid_for(size), kThreads, 0, s>>>(point, grad, alpha, size, z, nullptr);
+      check_launch("gradient step");
+      tv_prox(z, tvb, t.nz, t.n, t.n, alpha * tv_weight, tv_inner, TvFinal::plain, 0.0f, nullptr, out, 0, 0, s);
+    } else {
+      k_axpy_clamp<<<grid_for(size), kThreads, 0, s>>>(point, grad, alpha, size, nullptr, out);
+      check_launch("gradient step");
+    }
+  };
+  float tk = 1.0f;
+  for (int it = 0; it < iterations; ++it) {
+    if (fista) {
+      gradient(y, 0, count, d_loss + it);
+      prox(y, next);
+      const float tn = fista_t(tk);
+      k_extrapolate<<<grid_for(size), kThreads, 0, s>>>(next, d_x, (tk - 1.0f) / tn, size, y);
+      check_launch("extrapolate");
+      tk = tn;
+    } else {
+      for (int first = 0; first < count; first += batch) {
+        gradient(d_x, first, std::min(first + batch, count), d_loss + it);
+        prox(d_x, d_x);
+      }
+    }
+  }
+  check(cudaStreamSynchronize(s), "bpm_reconstruct");
+}
+
+}  // namespace qhk

@@ -1,12 +1,20 @@
 // extern "C" entry points of libqhk.so (include/qoraholo_b200.h). Every function validates its
 // arguments, converts exceptions into a status code and records the message for qhk_last_error().
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <numbers>
 #include <string>
 
 #include "../../include/qoraholo_b200.h"
+#include <complex>
+#include <vector>
+
+#include "bpm.hpp"
+#include "field.hpp"
 #include "odt.hpp"
+#include "pipeline.hpp"
+#include "unwrap.hpp"
 
 namespace {
 
@@ -70,6 +78,10 @@ qhk::OdtConfig odt_config(int n, int count, const float* il, const qhk_geometry*
 
 struct qhk_odt {
   qhk::OdtPlan plan;
+};
+
+struct qhk_pipeline {
+  qhk::PipelinePlan plan;
 };
 
 extern "C" {
@@ -192,6 +204,27 @@ int qhk_tv_prox(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int
   });
 }
 
+int qhk_tv_prox_device(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int nx, float lambda, int inner,
+                       void* stream) {
+  return guard([&] {
+    qhk::require(d_b && d_x && d_dual, "tv_prox: null argument");
+    qhk::require(nz >= 1 && ny >= 1 && nx >= 1 && lambda > 0 && inner >= 0, "tv_prox: invalid arguments");
+    const std::size_t v = static_cast<std::size_t>(nz) * ny * nx;
+    const cudaStream_t s = as_stream(stream);
+    qhk::TvBuffers t;
+    for (int i = 0; i < 3; ++i)
+      for (int c = 0; c < 3; ++c) t.v[i][c] = d_dual + (3 * i + c) * v;
+    t.p_index = 0;
+    qhk::tv_prox(d_b, t, nz, ny, nx, lambda, inner, qhk::TvFinal::plain, 0.0f, nullptr, d_x, 0, 0, s);
+    if (t.p_index != 0) {
+      qhk::check(cudaMemcpyAsync(d_dual, t.v[t.p_index][0], 3 * v * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                 "copy dual");
+    }
+  });
+}
+
+uint64_t qhk_kernel_launches(void) { return qhk::g_launches.load(std::memory_order_relaxed); }
+
 int qhk_fft2d(void* d_data, int count, int n, int forward, float scale, void* stream) {
   return guard([&] {
     qhk::require(d_data && count >= 1 && n >= 1, "fft2d: invalid arguments");
@@ -222,6 +255,314 @@ int qhk_irfft3(void* d_half, float* d_x, int nz, int ny, int nx, float scale, vo
     qhk::axis_pass(e, ny, h, nz, nh, h, false, qhk::AxisMode::plain, scale, {}, s);
     qhk::axis_pass(e, nz, nh, ny, h, h, false, qhk::AxisMode::plain, 1.0f, {}, s);
     qhk::rows_c2r(e, d_x, static_cast<std::size_t>(nz) * ny, nx, qhk::C2rMode::store, 0, 0, s);
+  });
+}
+
+int qhk_extract_fields(const float* holo, int count, int n, float cy, float cx, float radius, int output_size,
+                       void* out) {
+  return guard([&] {
+    qhk::require(holo && out, "extract_fields: null argument");
+    qhk::require(n >= 4 && n % 2 == 0, "extract_fields: images must be square with an even side");
+    qhk::require(count >= 1, "extract_fields: empty stack");
+    const qhk::CropPlan crop = qhk::make_crop(n, cy, cx, radius, output_size);
+    qhk::FieldPlan plan(crop, count);
+    qhk::Stream stream;
+    const std::size_t nin = static_cast<std::size_t>(count) * n * n;
+    const std::size_t nout = static_cast<std::size_t>(count) * crop.out * crop.out;
+    qhk::DevBuf<float> d_holo(nin);
+    qhk::DevBuf<float2> d_out(nout);
+    qhk::check(cudaMemcpyAsync(d_holo.get(), holo, nin * sizeof(float), cudaMemcpyHostToDevice, stream.get()),
+               "upload holograms");
+    plan.fields(d_holo.get(), d_out.get(), stream.get());
+    qhk::check(cudaMemcpyAsync(out, d_out.get(), nout * sizeof(float2), cudaMemcpyDeviceToHost, stream.get()),
+               "download fields");
+    qhk::check(cudaStreamSynchronize(stream.get()), "extract_fields");
+  });
+}
+
+int qhk_field_ratio(const void* sample, int count, int ny, int nx, const void* background, int bcount, void* out) {
+  return guard([&] {
+    qhk::require(sample && background && out, "field_ratio: null argument");
+    qhk::require(count >= 1 && ny >= 1 && nx >= 1 && (bcount == 1 || bcount == count),
+                 "field_ratio: background shape does not match");
+    qhk::Stream stream;
+    const cudaStream_t s = stream.get();
+    const std::size_t plane = static_cast<std::size_t>(ny) * nx;
+    const std::size_t total = plane * count;
+    qhk::DevBuf<float2> ds(total), db(plane * bcount);
+    qhk::check(cudaMemcpyAsync(ds.get(), sample, ds.bytes(), cudaMemcpyHostToDevice, s), "upload sample");
+    qhk::check(cudaMemcpyAsync(db.get(), background, db.bytes(), cudaMemcpyHostToDevice, s), "upload background");
+    qhk::field_ratio(ds.get(), db.get(), plane, bcount == count && count > 1, total, ds.get(), s);
+    qhk::check(cudaMemcpyAsync(out, ds.get(), ds.bytes(), cudaMemcpyDeviceToHost, s), "download ratio");
+    qhk::check(cudaStreamSynchronize(s), "field_ratio");
+  });
+}
+
+int qhk_find_sideband(const float* holo, int n, float dc_exclusion, int* iy, int* ix, float* y, float* x,
+                      float* magnitude) {
+  return guard([&] {
+    qhk::require(holo && iy && ix && y && x && magnitude, "find_sideband: null argument");
+    qhk::require(n >= 4 && n % 2 == 0, "find_sideband: holograms must be square with an even side");
+    if (dc_exclusion <= 0) dc_exclusion = static_cast<float>(n) / 8.0f;
+    const int h = n / 2 + 1;
+    qhk::Stream stream;
+    const cudaStream_t s = stream.get();
+    qhk::DevBuf<float> d_holo(static_cast<std::size_t>(n) * n);
+    qhk::DevBuf<float2> d_half(static_cast<std::size_t>(n) * h);
+    qhk::DevBuf<float> d_mag(1);
+    qhk::DevBuf<int> d_idx(1);
+    qhk::check(cudaMemcpyAsync(d_holo.get(), holo, d_holo.bytes(), cudaMemcpyHostToDevice, s), "upload hologram");
+    qhk::sideband_peak(d_holo.get(), n, dc_exclusion, d_half.get(), d_mag.get(), d_idx.get(), s);
+    std::vector<float2> half(static_cast<std::size_t>(n) * h);
+    float mag = 0;
+    int idx = -1;
+    qhk::check(cudaMemcpyAsync(half.data(), d_half.get(), d_half.bytes(), cudaMemcpyDeviceToHost, s), "download");
+    qhk::check(cudaMemcpyAsync(&mag, d_mag.get(), sizeof mag, cudaMemcpyDeviceToHost, s), "download");
+    qhk::check(cudaMemcpyAsync(&idx, d_idx.get(), sizeof idx, cudaMemcpyDeviceToHost, s), "download");
+    qhk::check(cudaStreamSynchronize(s), "find_sideband");
+    if (idx < 0 || mag == 0.0f) qhk::fail(qhk::kCudaError, "find_sideband: no peak outside the DC region");
+    const int c = n / 2;
+    // Centred spectrum S[yy][xx] = H(yy - c, xx - c); H(fy, fx < 0) = conj H(-fy, -fx).
+    const auto spec = [&](int yy, int xx) {
+      int fy = yy - c, fx = xx - c;
+      bool conj = false;
+      if (fx < 0) {
+        fy = -fy;
+        fx = -fx;
+        conj = true;
+      }
+      const float2 v = half[static_cast<std::size_t>((fy % n + n) % n) * h + fx];
+      return std::complex<float>(v.x, conj ? -v.y : v.y);
+    };
+    // Jacobsen's three-bin estimator with Candan's bias correction (src/cpu/field.cpp:15-22).
+    const auto refine = [&](std::complex<float> lo, std::complex<float> mid, std::complex<float> hi) {
+      const std::complex<float> den = 2.0f * mid - lo - hi;
+      if (std::abs(den) == 0.0f) return 0.0f;
+      const float cc = std::numbers::pi_v<float> / static_cast<float>(n);
+      const float d = ((lo - hi) / den).real() * std::tan(cc) / cc;
+      return std::clamp(d, -0.5f, 0.5f);
+    };
+    const int py = idx / n, px = idx % n;
+    *iy = py - c;
+    *ix = px - c;
+    *y = static_cast<float>(*iy) + refine(spec(py - 1, px), spec(py, px), spec(py + 1, px));
+    *x = static_cast<float>(*ix) + refine(spec(py, px - 1), spec(py, px), spec(py, px + 1));
+    *magnitude = mag;
+  });
+}
+
+int qhk_unwrap(const float* wrapped, int count, int ny, int nx, float* out) {
+  return guard([&] {
+    qhk::require(wrapped && out, "unwrap: null argument");
+    qhk::UnwrapPlan plan(count, ny, nx);
+    qhk::Stream stream;
+    const std::size_t total = static_cast<std::size_t>(count) * ny * nx;
+    qhk::DevBuf<float> psi(total), phi(total);
+    qhk::check(cudaMemcpyAsync(psi.get(), wrapped, total * sizeof(float), cudaMemcpyHostToDevice, stream.get()),
+               "upload phase");
+    plan.unwrap(psi.get(), phi.get(), stream.get());
+    qhk::check(cudaMemcpyAsync(out, phi.get(), total * sizeof(float), cudaMemcpyDeviceToHost, stream.get()),
+               "download phase");
+    qhk::check(cudaStreamSynchronize(stream.get()), "unwrap");
+  });
+}
+
+int qhk_rytov(const void* ratio, int count, int ny, int nx, void* out) {
+  return guard([&] {
+    qhk::require(ratio && out, "rytov: null argument");
+    qhk::require(ny >= 4 && nx >= 4, "rytov: image sides must be even");
+    qhk::UnwrapPlan plan(count, ny, nx);
+    qhk::Stream stream;
+    const cudaStream_t s = stream.get();
+    const std::size_t total = static_cast<std::size_t>(count) * ny * nx;
+    qhk::DevBuf<float2> r(total);
+    qhk::DevBuf<float> psi(total), logamp(total), phi(total);
+    qhk::check(cudaMemcpyAsync(r.get(), ratio, total * sizeof(float2), cudaMemcpyHostToDevice, s), "upload ratio");
+    qhk::split_ratio(r.get(), total, psi.get(), logamp.get(), s);
+    plan.rytov(psi.get(), logamp.get(), phi.get(), r.get(), s);
+    qhk::check(cudaMemcpyAsync(out, r.get(), total * sizeof(float2), cudaMemcpyDeviceToHost, s), "download rytov");
+    qhk::check(cudaStreamSynchronize(s), "rytov");
+  });
+}
+
+int qhk_pipeline_create(qhk_pipeline** pipeline, const qhk_pipeline_options* o, const float* illum_fyfx,
+                        const qhk_geometry* geometry) {
+  return guard([&] {
+    qhk::require(pipeline && o, "Pipeline: null argument");
+    const int n = o->hologram_size;
+    qhk::require(o->count >= 1, "Pipeline: count must be positive");
+    qhk::require(n >= 4 && n % 2 == 0, "Pipeline: hologram_size must be even");
+    qhk::require(o->upload_chunks >= 1 && o->upload_chunks <= o->count,
+                 "Pipeline: upload_chunks must be between 1 and count");
+    const qhk::CropPlan crop = qhk::make_crop(n, o->center_y, o->center_x, o->radius, o->output_size);
+    const qhk::OdtConfig c = odt_config(crop.out, o->count, illum_fyfx, geometry, &o->odt);
+    *pipeline = new qhk_pipeline{qhk::PipelinePlan(crop, o->count, o->upload_chunks, c, illum_fyfx)};
+  });
+}
+
+int qhk_pipeline_set_background(qhk_pipeline* p, const float* backgrounds) {
+  return guard([&] {
+    qhk::require(p && backgrounds, "Pipeline::set_background: null argument");
+    p->plan.set_background(backgrounds);
+  });
+}
+
+float* qhk_pipeline_input(qhk_pipeline* p) { return p ? p->plan.input() : nullptr; }
+const float* qhk_pipeline_output(const qhk_pipeline* p) { return p ? p->plan.output() : nullptr; }
+
+int qhk_pipeline_process(qhk_pipeline* p) {
+  return guard([&] {
+    qhk::require(p != nullptr, "Pipeline: null pipeline");
+    p->plan.process();
+  });
+}
+
+int qhk_pipeline_process_device(qhk_pipeline* p, const float* d_holo, float* d_index, void* stream) {
+  return guard([&] {
+    qhk::require(p && d_holo && d_index, "Pipeline: null argument");
+    p->plan.process_device(d_holo, d_index, as_stream(stream));
+  });
+}
+
+int qhk_pipeline_result(const qhk_pipeline* p, double* filled, qhk_pipeline_timings* t) {
+  return guard([&] {
+    qhk::require(p != nullptr, "Pipeline: null pipeline");
+    if (filled) *filled = p->plan.filled();
+    if (t) {
+      const qhk::PipelineTimes& v = p->plan.timings();
+      *t = qhk_pipeline_timings{v.upload, v.fields, v.rytov,  v.fft2,     v.clear, v.mapping,
+                                v.normalize, v.solve, v.finish, v.download, v.total};
+    }
+  });
+}
+
+int qhk_pipeline_filled(qhk_pipeline* p, void* stream, double* filled) {
+  return guard([&] {
+    qhk::require(p && filled, "Pipeline: null argument");
+    unsigned long long v = 0;
+    qhk::check(cudaMemcpyAsync(&v, p->plan.odt().filled(), sizeof v, cudaMemcpyDeviceToHost, as_stream(stream)),
+               "download filled");
+    qhk::check(cudaStreamSynchronize(as_stream(stream)), "Pipeline filled");
+    *filled = static_cast<double>(v) / static_cast<double>(p->plan.odt().volume());
+  });
+}
+
+int qhk_pipeline_shape(const qhk_pipeline* p, int* nz, int* ny, int* nx) {
+  return guard([&] {
+    qhk::require(p && nz && ny && nx, "Pipeline: null argument");
+    *nz = p->plan.odt().config().grid.nz;
+    *ny = *nx = p->plan.odt().config().grid.n;
+  });
+}
+
+size_t qhk_pipeline_device_bytes(const qhk_pipeline* p) { return p ? p->plan.device_bytes() : 0; }
+
+int qhk_pipeline_destroy(qhk_pipeline* p) {
+  return guard([&] { delete p; });
+}
+
+int qhk_fft2d_host(void* data, int count, int n, int forward, float scale) {
+  return guard([&] {
+    qhk::require(data && count >= 1 && n >= 1, "fft2d: invalid arguments");
+    qhk::Stream stream;
+    const std::size_t total = static_cast<std::size_t>(count) * n * n;
+    qhk::DevBuf<float2> d(total);
+    qhk::check(cudaMemcpyAsync(d.get(), data, total * sizeof(float2), cudaMemcpyHostToDevice, stream.get()), "upload");
+    qhk::fft2d(d.get(), count, n, forward != 0, scale, stream.get());
+    qhk::check(cudaMemcpyAsync(data, d.get(), total * sizeof(float2), cudaMemcpyDeviceToHost, stream.get()),
+               "download");
+    qhk::check(cudaStreamSynchronize(stream.get()), "fft2d");
+  });
+}
+
+namespace {
+
+qhk::BpmTablesHost checked_tables(int nz, int n, int count, const float* il, const qhk_geometry* g, bool obliquity) {
+  qhk::require(il && g, "bpm: null argument");
+  qhk::require(n >= 4 && n % 2 == 0 && nz >= 1, "bpm: volume must be (nz, n, n) with an even n");
+  qhk::require(count >= 1, "bpm: need one illumination per field");
+  qhk::require(g->wavelength > 0 && g->pixel > 0 && g->n_medium > 0 && g->na > 0, "bpm: geometry values must be positive");
+  const float fm = g->n_medium / g->wavelength;
+  for (int a = 0; a < count; ++a) {
+    qhk::require(il[2 * a] * il[2 * a] + il[2 * a + 1] * il[2 * a + 1] < fm * fm,
+                 "bpm: illumination frequency beyond n_medium / wavelength");
+  }
+  return qhk::bpm_tables(n, nz, il, count, g->wavelength, g->n_medium, g->na, g->pixel, obliquity);
+}
+
+}  // namespace
+
+int qhk_bpm_forward(const float* ri, int nz, int n, const float* illum_fyfx, int count, const qhk_geometry* geometry,
+                    int obliquity, void* out) {
+  return guard([&] {
+    qhk::require(ri && out, "bpm_forward: null argument");
+    const auto t = checked_tables(nz, n, count, illum_fyfx, geometry, obliquity != 0);
+    qhk::Stream stream;
+    const cudaStream_t s = stream.get();
+    const std::size_t vol = static_cast<std::size_t>(nz) * n * n;
+    qhk::DevBuf<float> d_ri(vol), d_x(vol);
+    qhk::check(cudaMemcpyAsync(d_ri.get(), ri, vol * sizeof(float), cudaMemcpyHostToDevice, s), "upload volume");
+    qhk::contrast(d_ri.get(), geometry->n_medium, vol, d_x.get(), false, s);
+    qhk::BpmPlan plan(t, count, false);
+    plan.forward(d_x.get(), 0, count, s);
+    qhk::check(cudaMemcpyAsync(out, plan.fields(), static_cast<std::size_t>(count) * n * n * sizeof(float2),
+                               cudaMemcpyDeviceToHost, s),
+               "download fields");
+    qhk::check(cudaStreamSynchronize(s), "bpm_forward");
+  });
+}
+
+int qhk_bpm_vjp(const float* x, int nz, int n, const void* r, const float* illum_fyfx, int count,
+                const qhk_geometry* geometry, int obliquity, float* out) {
+  return guard([&] {
+    qhk::require(x && r && out, "bpm_vjp: null argument");
+    const auto t = checked_tables(nz, n, count, illum_fyfx, geometry, obliquity != 0);
+    qhk::Stream stream;
+    const cudaStream_t s = stream.get();
+    const std::size_t vol = static_cast<std::size_t>(nz) * n * n;
+    const std::size_t nf = static_cast<std::size_t>(count) * n * n;
+    qhk::DevBuf<float> d_x(vol), d_grad(vol);
+    qhk::DevBuf<float2> d_r(nf);
+    qhk::check(cudaMemcpyAsync(d_x.get(), x, vol * sizeof(float), cudaMemcpyHostToDevice, s), "upload volume");
+    qhk::check(cudaMemcpyAsync(d_r.get(), r, nf * sizeof(float2), cudaMemcpyHostToDevice, s), "upload residual");
+    qhk::check(cudaMemsetAsync(d_grad.get(), 0, vol * sizeof(float), s), "cudaMemset");
+    qhk::BpmPlan plan(t, count, true);
+    plan.forward(d_x.get(), 0, count, s);
+    plan.adjoint(d_x.get(), d_r.get(), 0, count, 1.0f, d_grad.get(), s);
+    qhk::check(cudaMemcpyAsync(out, d_grad.get(), vol * sizeof(float), cudaMemcpyDeviceToHost, s), "download");
+    qhk::check(cudaStreamSynchronize(s), "bpm_vjp");
+  });
+}
+
+int qhk_bpm_reconstruct(const void* fields, int count, int n, const float* illum_fyfx, const qhk_geometry* geometry,
+                        const float* initial, int nz, const qhk_bpm_solve_options* o, float* out, double* loss) {
+  return guard([&] {
+    qhk::require(fields && initial && out && o, "bpm_reconstruct: null argument");
+    qhk::require(o->iterations >= 0 && o->step > 0 && o->tv_weight >= 0 && o->tv_inner >= 1,
+                 "bpm_reconstruct: invalid solver options");
+    qhk::require(o->iterations == 0 || loss != nullptr, "bpm_reconstruct: null loss");
+    const auto t = checked_tables(nz, n, count, illum_fyfx, geometry, o->obliquity != 0);
+    qhk::Stream stream;
+    const cudaStream_t s = stream.get();
+    const std::size_t vol = static_cast<std::size_t>(nz) * n * n;
+    const std::size_t nf = static_cast<std::size_t>(count) * n * n;
+    qhk::DevBuf<float> d_ri(vol), d_x(vol);
+    qhk::DevBuf<float2> d_f(nf);
+    qhk::DevBuf<double> d_loss(std::max(o->iterations, 1));
+    qhk::check(cudaMemcpyAsync(d_ri.get(), initial, vol * sizeof(float), cudaMemcpyHostToDevice, s), "upload");
+    qhk::check(cudaMemcpyAsync(d_f.get(), fields, nf * sizeof(float2), cudaMemcpyHostToDevice, s), "upload");
+    qhk::check(cudaMemsetAsync(d_loss.get(), 0, d_loss.bytes(), s), "cudaMemset");
+    qhk::contrast(d_ri.get(), geometry->n_medium, vol, d_x.get(), true, s);
+    qhk::bpm_solve(t, d_f.get(), d_x.get(), o->iterations, o->batch, o->step, o->tv_weight, o->tv_inner, d_loss.get(),
+                   s);
+    qhk::add_medium(d_x.get(), geometry->n_medium, vol, d_ri.get(), s);
+    qhk::check(cudaMemcpyAsync(out, d_ri.get(), vol * sizeof(float), cudaMemcpyDeviceToHost, s), "download");
+    if (o->iterations > 0) {
+      qhk::check(cudaMemcpyAsync(loss, d_loss.get(), o->iterations * sizeof(double), cudaMemcpyDeviceToHost, s),
+                 "download loss");
+    }
+    qhk::check(cudaStreamSynchronize(s), "bpm_reconstruct");
+    for (int i = 0; i < o->iterations; ++i) loss[i] *= 0.5 / count;
   });
 }
 

@@ -58,21 +58,9 @@ struct TwiddleEntry {
 std::mutex g_tw_mutex;
 std::map<std::pair<int, int>, std::unique_ptr<TwiddleEntry>> g_tw;
 
-// Sets the dynamic shared memory limit of a kernel once per (device, kernel).
-std::mutex g_attr_mutex;
-std::set<std::pair<int, const void*>> g_attr_done;
-
 template <class K>
-void allow_smem(K kernel, std::size_t bytes) {
-  if (bytes <= 48 * 1024) return;
-  int dev = 0;
-  check(cudaGetDevice(&dev), "cudaGetDevice");
-  std::lock_guard<std::mutex> lock(g_attr_mutex);
-  const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
-  if (g_attr_done.count(key)) return;
-  check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
-        "cudaFuncSetAttribute");
-  g_attr_done.insert(key);
+void allow_smem(K kernel, std::size_t) {
+  ensure_smem(kernel);
 }
 
 constexpr int kThreads = 256;

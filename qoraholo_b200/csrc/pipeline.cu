@@ -1,0 +1,125 @@
+// Holograms -> refractive index with everything allocated once: the device side of
+// qoraholo::Pipeline. Replaces the reference's CudaPipeline (src/cuda/pipeline.cu:12-147).
+//
+// process(): the sample holograms go host -> device in `upload_chunks` parts on a copy stream;
+// the field passes of each part start as soon as its copy has landed (event wait), so the copy
+// overlaps field extraction. The last field pass forms the ratio to the resident background
+// fields and its phase / log-amplitude directly; then the unwrap passes, the Rytov assembly,
+// the ODT plan, and one device -> host copy of the volume into page-locked memory. Stage times
+// are event intervals on the compute stream, read after it finishes.
+#include <chrono>
+
+#include "pipeline.hpp"
+
+namespace qhk {
+
+namespace {
+
+int checked_chunk(int count, int upload_chunks) {
+  require(count >= 1, "Pipeline: count must be positive");
+  require(upload_chunks >= 1 && upload_chunks <= count, "Pipeline: upload_chunks must be between 1 and count");
+  return (count + upload_chunks - 1) / upload_chunks;
+}
+
+}  // namespace
+
+PipelinePlan::PipelinePlan(const CropPlan& crop, int count, int upload_chunks, const OdtConfig& odt,
+                           const float* illum_fyfx)
+    : crop_(crop),
+      count_(count),
+      chunk_(checked_chunk(count, upload_chunks)),
+      chunks_((count + chunk_ - 1) / chunk_),
+      field_(crop, count),
+      unwrap_(count, crop.out, crop.out),
+      odt_(odt, illum_fyfx),
+      clock_(kMarks) {
+  require(odt.grid.n == crop.out, "Pipeline: volume side must equal the field side");
+  const std::size_t image = static_cast<std::size_t>(crop.n) * crop.n;
+  const std::size_t field = static_cast<std::size_t>(count) * crop.out * crop.out;
+  input_ = PinnedBuf<float>(count * image);
+  output_ = PinnedBuf<float>(odt_.volume());
+  filled_host_ = PinnedBuf<unsigned long long>(1);
+  holo_.reset(count * image);
+  background_.reset(field);
+  fields_.reset(field);
+  psi_.reset(field);
+  logamp_.reset(field);
+  phi_.reset(field);
+  index_.reset(odt_.volume());
+  for (int k = 0; k < chunks_; ++k) chunk_done_.emplace_back();
+}
+
+std::size_t PipelinePlan::device_bytes() const {
+  return field_.device_bytes() + unwrap_.device_bytes() + odt_.device_bytes() + holo_.bytes() + background_.bytes() +
+         fields_.bytes() + psi_.bytes() + logamp_.bytes() + phi_.bytes() + index_.bytes();
+}
+
+void PipelinePlan::set_background(const float* host_bg) {
+  const cudaStream_t s = compute_.get();
+  const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
+  check(cudaMemcpyAsync(holo_.get(), host_bg, count_ * image * sizeof(float), cudaMemcpyHostToDevice, s),
+        "upload backgrounds");
+  field_.spectra(holo_.get(), 0, count_, s);
+  field_.finish(0, background_.get(), nullptr, nullptr, nullptr, s);
+  check(cudaStreamSynchronize(s), "set_background");
+  has_background_ = true;
+}
+
+void PipelinePlan::compute(const float* d_holo, bool chunked_upload, float* d_index, cudaStream_t s) {
+  const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
+  clock_.mark(kStart, s);
+  if (chunked_upload) {
+    const cudaStream_t c = copy_.get();
+    check(cudaStreamWaitEvent(c, clock_.event(kStart), 0), "cudaStreamWaitEvent");
+    for (int k = 0; k < chunks_; ++k) {
+      const int first = k * chunk_;
+      const int valid = std::min(chunk_, count_ - first);
+      float* dst = holo_.get() + first * image;
+      check(cudaMemcpyAsync(dst, input_.get() + first * image, valid * image * sizeof(float), cudaMemcpyHostToDevice, c),
+            "upload holograms");
+      chunk_done_[k].record(c);
+      check(cudaStreamWaitEvent(s, chunk_done_[k].get(), 0), "cudaStreamWaitEvent");
+      field_.spectra(dst, first, valid, s);
+    }
+  } else {
+    field_.spectra(d_holo, 0, count_, s);
+  }
+  field_.finish(1, nullptr, background_.get(), psi_.get(), logamp_.get(), s);
+  clock_.mark(kFields, s);
+  unwrap_.rytov(psi_.get(), logamp_.get(), phi_.get(), fields_.get(), s);
+  clock_.mark(kRytov, s);
+  odt_.run_marked(fields_.get(), d_index, s, &clock_, kRytov + 1);
+}
+
+void PipelinePlan::process() {
+  if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
+  const auto t0 = std::chrono::steady_clock::now();
+  const cudaStream_t s = compute_.get();
+  compute(nullptr, true, index_.get(), s);
+  check(cudaMemcpyAsync(output_.get(), index_.get(), odt_.volume() * sizeof(float), cudaMemcpyDeviceToHost, s),
+        "download index");
+  check(cudaMemcpyAsync(filled_host_.get(), odt_.filled(), sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+        "download filled");
+  clock_.mark(kDownloaded, s);
+  check(cudaStreamSynchronize(s), "process");
+  filled_ = static_cast<double>(*filled_host_.get()) / static_cast<double>(odt_.volume());
+  const int o = kRytov + 1;
+  timings_.upload = chunk_done_.back().since_event(clock_.event(kStart));
+  timings_.fields = clock_.ms(kStart, kFields);
+  timings_.rytov = clock_.ms(kFields, kRytov);
+  timings_.fft2 = clock_.ms(kRytov, o + OdtPlan::kMarkFft2);
+  timings_.clear = clock_.ms(o + OdtPlan::kMarkFft2, o + OdtPlan::kMarkClear);
+  timings_.mapping = clock_.ms(o + OdtPlan::kMarkClear, o + OdtPlan::kMarkMapping);
+  timings_.normalize = clock_.ms(o + OdtPlan::kMarkMapping, o + OdtPlan::kMarkNormalize);
+  timings_.solve = clock_.ms(o + OdtPlan::kMarkNormalize, o + OdtPlan::kMarkSolve);
+  timings_.finish = clock_.ms(o + OdtPlan::kMarkSolve, o + OdtPlan::kMarkFinish);
+  timings_.download = clock_.ms(o + OdtPlan::kMarkFinish, kDownloaded);
+  timings_.total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void PipelinePlan::process_device(const float* d_holo, float* d_index, cudaStream_t s) {
+  if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
+  compute(d_holo, false, d_index, s);
+}
+
+}  // namespace qhk

@@ -3,8 +3,11 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -39,7 +42,13 @@ inline void check(cudaError_t e, const char* what) {
   throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-inline void check_launch(const char* what) { check(cudaGetLastError(), what); }
+// Kernels launched by this library since load (every launch site calls check_launch once).
+inline std::atomic<std::uint64_t> g_launches{0};
+
+inline void check_launch(const char* what) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  check(cudaGetLastError(), what);
+}
 
 template <class T>
 class DevBuf {
@@ -127,15 +136,37 @@ class Event {
   Event(Event&& o) noexcept : e_(std::exchange(o.e_, nullptr)) {}
   [[nodiscard]] cudaEvent_t get() const { return e_; }
   void record(cudaStream_t s) { check(cudaEventRecord(e_, s), "cudaEventRecord"); }
-  [[nodiscard]] float since(const Event& start) const {
+  [[nodiscard]] float since(const Event& start) const { return since_event(start.get()); }
+  [[nodiscard]] float since_event(cudaEvent_t start) const {
     float ms = 0;
-    check(cudaEventElapsedTime(&ms, start.get(), e_), "cudaEventElapsedTime");
+    check(cudaEventElapsedTime(&ms, start, e_), "cudaEventElapsedTime");
     return ms;
   }
 
  private:
   cudaEvent_t e_{};
 };
+
+// Raises a kernel's dynamic shared memory limit to the device maximum, once per (device, kernel).
+// Launches of any size then succeed as long as dynamic plus static shared memory fit the SM.
+template <class K>
+void ensure_smem(K kernel) {
+  static std::mutex mutex;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(mutex);
+  const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
+  if (done.count(key)) return;
+  cudaFuncAttributes attr{};
+  check(cudaFuncGetAttributes(&attr, kernel), "cudaFuncGetAttributes");
+  int optin = 0;
+  check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "cudaDeviceGetAttribute");
+  check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin - static_cast<int>(attr.sharedSizeBytes)),
+        "cudaFuncSetAttribute");
+  done.insert(key);
+}
 
 inline unsigned blocks_for(std::size_t n, unsigned threads) {
   return static_cast<unsigned>((n + threads - 1) / threads);

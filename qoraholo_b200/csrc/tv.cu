@@ -253,50 +253,41 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Rows per CTA and planes per CTA for an (nz, ny, nx) volume.
+// Rows per CTA and planes per CTA for an (nz, ny, nx) volume: TY rows of full x extent, and as
+// many z chunks as keep every CTA resident in a single wave (a partial second wave would double the
+// time of the step).
 struct FgpShape {
   int ty;
   int zchunk;
   std::size_t smem;
 };
 
-FgpShape fgp_shape(int nz, int ny, int nx, int vec) {
-  const int tx = nx / vec;
-  int ty = 4;
-  const auto smem_of = [&](int t) {
-    return (2 * static_cast<std::size_t>(3) * (t + 2) + 3 * static_cast<std::size_t>(t + 1)) * nx * sizeof(float);
-  };
-  while (ty > 1 && (tx * ty > 1024 || smem_of(ty) > 110 * 1024)) --ty;
-  require(tx * ty <= 1024 && smem_of(ty) <= 220 * 1024, "tv: volume rows too long for the FGP kernel");
-  // About two resident CTAs' worth of work per SM slot, at least 8 planes per CTA.
-  const int ytiles = (ny + ty - 1) / ty;
-  const int per_sm = std::max(1, std::min(static_cast<int>((200 * 1024) / smem_of(ty)), 2048 / (tx * ty)));
-  const int slots = sm_count() * per_sm;
-  int chunks = std::max(1, (slots + ytiles - 1) / ytiles);
-  int zchunk = std::max(8, (nz + chunks - 1) / chunks);
-  zchunk = std::min(zchunk, nz);
-  return {ty, zchunk, smem_of(ty)};
+std::size_t fgp_smem(int nx, int ty) {
+  return (2 * static_cast<std::size_t>(3) * (ty + 2) + 3 * static_cast<std::size_t>(ty + 1)) * nx * sizeof(float);
 }
 
-std::mutex g_fgp_mutex;
-std::set<std::pair<int, const void*>> g_fgp_attr;
-
-template <class K>
-void fgp_allow(K kernel) {
-  int dev = 0;
-  check(cudaGetDevice(&dev), "cudaGetDevice");
-  std::lock_guard<std::mutex> lock(g_fgp_mutex);
-  const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
-  if (g_fgp_attr.count(key)) return;
-  check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
-        "cudaFuncSetAttribute");
-  g_fgp_attr.insert(key);
+template <int VEC>
+FgpShape fgp_shape(int nz, int ny, int nx) {
+  const int tx = nx / VEC;
+  int ty = 4;
+  while (ty > 1 && (tx * ty > 1024 || fgp_smem(nx, ty) > 110 * 1024)) --ty;
+  require(tx * ty <= 1024 && fgp_smem(nx, ty) <= 220 * 1024, "tv: volume rows too long for the FGP kernel");
+  const std::size_t smem = fgp_smem(nx, ty);
+  auto kernel = k_fgp<VEC, false, false>;
+  ensure_smem(kernel);
+  int per_sm = 0;
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tx * ty, smem), "cudaOccupancy");
+  const int slots = sm_count() * std::max(per_sm, 1);
+  const int ytiles = (ny + ty - 1) / ty;
+  const int chunks = std::max(1, std::min(nz, slots / ytiles));
+  const int zchunk = (nz + chunks - 1) / chunks;
+  return {ty, zchunk, smem};
 }
 
 template <int VEC, bool FIRST, bool LAST>
 void launch_fgp(const FgpArgs& a, const FgpShape& sh, cudaStream_t s) {
   auto kernel = k_fgp<VEC, FIRST, LAST>;
-  fgp_allow(kernel);
+  ensure_smem(kernel);
   const dim3 block(a.nx / VEC, sh.ty);
   const dim3 grid((a.ny + sh.ty - 1) / sh.ty, (a.nz + sh.zchunk - 1) / sh.zchunk);
   kernel<<<grid, block, sh.smem, s>>>(a);
@@ -352,7 +343,7 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
   for (int i = 0; i < 3; ++i)
     for (int c = 0; c < 3; ++c) aligned = aligned && reinterpret_cast<std::uintptr_t>(t.v[i][c]) % 16 == 0;
   const int vec = aligned ? 4 : 1;
-  const FgpShape sh = fgp_shape(nz, ny, nx, vec);
+  const FgpShape sh = vec == 4 ? fgp_shape<4>(nz, ny, nx) : fgp_shape<1>(nz, ny, nx);
   const float step = 1.0f / (12.0f * lambda);
   float tk = 1.0f;
   const int ip = t.p_index;

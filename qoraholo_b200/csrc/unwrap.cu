@@ -1,0 +1,433 @@
+// Least-squares phase unwrapping (Ghiglia & Romero 1994) and Rytov assembly on the device.
+// Replaces the reference's Unwrapper (src/cuda/unwrap.cu, src/cuda/stages.cuh:57-80) and follows
+// cpu::unwrap / cpu::rytov (src/cpu/unwrap.cpp:11-82, DCT by Makhoul, src/cpu/fft.cpp:101-133).
+//
+// Three passes over a stack of images, each a batched launch over all images:
+//   1. rows: divergence of the wrapped differences (the Neumann Poisson right-hand side, with
+//      the host's float operations, so bit-identical) and its DCT-II along x;
+//   2. columns: DCT-II along y, division by the eigenvalue of the 5-point Neumann Laplacian,
+//      inverse DCT along y -- the whole spectral solve in one launch;
+//   3. rows: inverse DCT along x, and per-CTA partial sums of exp(i (psi - phi)) in double.
+// A small per-image kernel then reduces the partial sums in a fixed order (no atomics) to the
+// congruence constant and forms the border mean, in the host's summation order, for the 2 pi
+// shift of the Rytov phase.
+#include <cmath>
+#include <numbers>
+#include <vector>
+
+#include "unwrap.hpp"
+
+namespace qhk {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <class K>
+void allow(K kernel, std::size_t) {
+  ensure_smem(kernel);
+}
+
+// Pass 1: COLS rows of image blockIdx.y per CTA.
+template <int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_div_dctx(const float* __restrict__ psi, float* __restrict__ d1, int ny, int nx, FftLen L,
+               const float2* __restrict__ dtw) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  float2* A = sm;
+  float2* B = A + static_cast<std::size_t>(nx) * cp;
+  float* P = reinterpret_cast<float*>(B + static_cast<std::size_t>(nx) * cp);  // rows y0-1 .. y0+COLS
+  const int y0 = static_cast<int>(blockIdx.x) * COLS;
+  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
+  for (int idx = tid; idx < (COLS + 2) * nx; idx += nth) {
+    const int rr = idx / nx;
+    const int x = idx - rr * nx;
+    const int y = y0 - 1 + rr;
+    P[idx] = (y >= 0 && y < ny) ? psi[img + static_cast<std::size_t>(y) * nx + x] : 0.0f;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < COLS * nx; idx += nth) {
+    const int row = idx / nx;
+    const int x = idx - row * nx;
+    const int y = y0 + row;
+    float r = 0.0f;
+    if (y < ny) {
+      const float* c = P + static_cast<std::size_t>(row + 1) * nx;
+      const float p = c[x];
+      if (x + 1 < nx) r = __fadd_rn(r, wrap_phase(__fsub_rn(c[x + 1], p)));
+      if (x > 0) r = __fsub_rn(r, wrap_phase(__fsub_rn(p, c[x - 1])));
+      if (y + 1 < ny) r = __fadd_rn(r, wrap_phase(__fsub_rn(c[x + nx], p)));
+      if (y > 0) r = __fsub_rn(r, wrap_phase(__fsub_rn(p, c[x - nx])));
+    }
+    A[dct_position(x, nx) * cp + row] = make_float2(r, 0.0f);
+  }
+  __syncthreads();
+  const float2* res = smem_fft<true>(A, B, cp, COLS, L, tid, nth);
+  for (int idx = tid; idx < COLS * nx; idx += nth) {
+    const int row = idx / nx;
+    const int k = idx - row * nx;
+    if (y0 + row >= ny) continue;
+    const float2 v = res[k * cp + row];
+    const float2 w = __ldg(dtw + k);
+    d1[img + static_cast<std::size_t>(y0 + row) * nx + k] = w.x * v.x - w.y * v.y;
+  }
+}
+
+// Pass 2: COLS columns of image blockIdx.y per CTA: DCT-II along y, divide, inverse DCT along y.
+template <int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_dcty_solve(const float* __restrict__ d1, float* __restrict__ d2, int ny, int nx, FftLen L,
+                 const float2* __restrict__ dtw, const float* __restrict__ cos_y, const float* __restrict__ cos_x) {
+  extern __shared__ float2 sm[];
+  float2* A = sm;
+  float2* B = A + static_cast<std::size_t>(ny) * COLS;
+  float* Cf = reinterpret_cast<float*>(B + static_cast<std::size_t>(ny) * COLS);
+  const int c0 = static_cast<int>(blockIdx.x) * COLS;
+  const int cols = min(COLS, nx - c0);
+  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
+  for (int idx = tid; idx < ny * COLS; idx += nth) {
+    const int y = idx / COLS;
+    const int col = idx - y * COLS;
+    const float v = col < cols ? d1[img + static_cast<std::size_t>(y) * nx + c0 + col] : 0.0f;
+    A[dct_position(y, ny) * COLS + col] = make_float2(v, 0.0f);
+  }
+  __syncthreads();
+  float2* res = smem_fft<true>(A, B, COLS, COLS, L, tid, nth);
+  float2* other = res == A ? B : A;
+  for (int idx = tid; idx < ny * COLS; idx += nth) {
+    const int k = idx / COLS;
+    const int col = idx - k * COLS;
+    const int kx = c0 + col;
+    const float2 v = res[idx];
+    const float2 w = __ldg(dtw + k);
+    const float c = w.x * v.x - w.y * v.y;
+    float out = 0.0f;
+    if (col < cols && !(k == 0 && kx == 0)) {
+      const float ev = __fsub_rn(__fadd_rn(__ldg(cos_y + k), __ldg(cos_x + kx)), 4.0f);
+      out = __fdiv_rn(c, ev);
+    }
+    Cf[idx] = out;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < ny * COLS; idx += nth) {
+    const int k = idx / COLS;
+    const int col = idx - k * COLS;
+    const float a = Cf[idx];
+    const float mirror = k == 0 ? 0.0f : Cf[(ny - k) * COLS + col];
+    const float2 w = __ldg(dtw + k);  // e^{-i pi k / 2n}; the inverse uses its conjugate
+    other[idx] = cmulc(make_float2(a, -mirror), w);
+  }
+  __syncthreads();
+  const float2* out = smem_fft<false>(other, res, COLS, COLS, L, tid, nth);
+  const float inv = 1.0f / static_cast<float>(ny);
+  for (int idx = tid; idx < ny * COLS; idx += nth) {
+    const int y = idx / COLS;
+    const int col = idx - y * COLS;
+    if (col >= cols) continue;
+    d2[img + static_cast<std::size_t>(y) * nx + c0 + col] = out[dct_position(y, ny) * COLS + col].x * inv;
+  }
+}
+
+// Pass 3: inverse DCT along x of COLS rows (in place), and the congruence partial sums of image
+// blockIdx.y over those rows: partial[(img * gridDim.x + blockIdx.x) * 2 + {0,1}] = sum cos, sin.
+template <int COLS>
+__global__ void __launch_bounds__(kThreads)
+    k_idctx(float* __restrict__ phi, const float* __restrict__ psi, int ny, int nx, FftLen L,
+            const float2* __restrict__ dtw, double* __restrict__ partial) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  float2* A = sm;
+  float2* B = A + static_cast<std::size_t>(nx) * cp;
+  float* F = reinterpret_cast<float*>(B + static_cast<std::size_t>(nx) * cp);
+  __shared__ double red[2][kThreads];
+  const int y0 = static_cast<int>(blockIdx.x) * COLS;
+  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
+  for (int idx = tid; idx < COLS * nx; idx += nth) {
+    const int row = idx / nx;
+    const int k = idx - row * nx;
+    F[idx] = y0 + row < ny ? phi[img + static_cast<std::size_t>(y0 + row) * nx + k] : 0.0f;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < COLS * nx; idx += nth) {
+    const int row = idx / nx;
+    const int k = idx - row * nx;
+    const float a = F[idx];
+    const float mirror = k == 0 ? 0.0f : F[row * nx + nx - k];
+    A[k * cp + row] = cmulc(make_float2(a, -mirror), __ldg(dtw + k));
+  }
+  __syncthreads();
+  const float2* res = smem_fft<false>(A, B, cp, COLS, L, tid, nth);
+  const float inv = 1.0f / static_cast<float>(nx);
+  double sc = 0.0, ss = 0.0;
+  for (int idx = tid; idx < COLS * nx; idx += nth) {
+    const int row = idx / nx;
+    const int x = idx - row * nx;
+    if (y0 + row >= ny) continue;
+    const std::size_t g = img + static_cast<std::size_t>(y0 + row) * nx + x;
+    const float v = res[dct_position(x, nx) * cp + row].x * inv;
+    phi[g] = v;
+    double s, c;
+    sincos(static_cast<double>(__fsub_rn(psi[g], v)), &s, &c);
+    sc += c;
+    ss += s;
+  }
+  red[0][tid] = sc;
+  red[1][tid] = ss;
+  __syncthreads();
+  for (int h = nth / 2; h > 0; h >>= 1) {
+    if (tid < h) {
+      red[0][tid] += red[0][tid + h];
+      red[1][tid] += red[1][tid + h];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const std::size_t o = (static_cast<std::size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * 2;
+    partial[o] = red[0][0];
+    partial[o + 1] = red[1][0];
+  }
+}
+
+// Per image: congruence constant c = arg(sum exp(i (psi - phi))) from the partial sums, then the
+// 2 pi multiple of the border mean of phi + c, summed in the host's order.
+__global__ void __launch_bounds__(kThreads)
+    k_rytov_consts(const float* __restrict__ phi, int ny, int nx, const double* __restrict__ partial, int nblk,
+                   float2* __restrict__ consts) {
+  extern __shared__ float pairs[];
+  __shared__ double red[2][kThreads];
+  __shared__ float cshared;
+  const std::size_t img = static_cast<std::size_t>(blockIdx.x) * ny * nx;
+  const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
+  double sc = 0.0, ss = 0.0;
+  for (int b = tid; b < nblk; b += nth) {
+    const std::size_t o = (static_cast<std::size_t>(blockIdx.x) * nblk + b) * 2;
+    sc += partial[o];
+    ss += partial[o + 1];
+  }
+  red[0][tid] = sc;
+  red[1][tid] = ss;
+  __syncthreads();
+  for (int h = nth / 2; h > 0; h >>= 1) {
+    if (tid < h) {
+      red[0][tid] += red[0][tid + h];
+      red[1][tid] += red[1][tid + h];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) cshared = static_cast<float>(atan2(red[1][0], red[0][0]));
+  __syncthreads();
+  const float c = cshared;
+  // pairs: x = 0..nx-1 -> phase(0, x) + phase(ny-1, x); then y = 1..ny-2 -> phase(y, 0) + phase(y, nx-1)
+  const int npairs = nx + ny - 2;
+  for (int i = tid; i < npairs; i += nth) {
+    float a, b;
+    if (i < nx) {
+      a = __fadd_rn(phi[img + i], c);
+      b = __fadd_rn(phi[img + static_cast<std::size_t>(ny - 1) * nx + i], c);
+    } else {
+      const int y = i - nx + 1;
+      a = __fadd_rn(phi[img + static_cast<std::size_t>(y) * nx], c);
+      b = __fadd_rn(phi[img + static_cast<std::size_t>(y) * nx + nx - 1], c);
+    }
+    pairs[i] = __fadd_rn(a, b);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double sum = 0.0;
+    for (int i = 0; i < npairs; ++i) sum = __dadd_rn(sum, static_cast<double>(pairs[i]));
+    const double mean = sum / (2.0 * nx + 2.0 * (ny - 2));
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    consts[blockIdx.x] = make_float2(c, static_cast<float>(two_pi * round(mean / two_pi)));
+  }
+}
+
+// out = logamp + i ((phi + c) - shift), or phi_out = phi + c when logamp is null.
+__global__ void k_rytov_assemble(const float* __restrict__ phi, const float* __restrict__ logamp,
+                                 const float2* __restrict__ consts, std::size_t plane, std::size_t total,
+                                 float2* __restrict__ out, float* __restrict__ phi_out) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const float2 k = consts[i / plane];
+    const float v = __fadd_rn(phi[i], k.x);
+    if (logamp) {
+      out[i] = make_float2(logamp[i], __fsub_rn(v, k.y));
+    } else {
+      phi_out[i] = v;
+    }
+  }
+}
+
+__global__ void k_split_ratio(const float2* __restrict__ ratio, std::size_t total, float* __restrict__ psi,
+                              float* __restrict__ logamp) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const float2 r = ratio[i];
+    psi[i] = atan2f(r.y, r.x);
+    logamp[i] = logf(hypotf(r.x, r.y));
+  }
+}
+
+// out = sample / background; background holds one image (bplane == 0 offset) or one per image.
+__global__ void k_ratio(const float2* __restrict__ sample, const float2* __restrict__ bg, std::size_t plane,
+                        bool per_image, std::size_t total, float2* __restrict__ out) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    const float2 u = sample[i];
+    const float2 v = bg[per_image ? i : i % plane];
+    const float d = 1.0f / (v.x * v.x + v.y * v.y);
+    out[i] = make_float2((u.x * v.x + u.y * v.y) * d, (u.y * v.x - u.x * v.y) * d);
+  }
+}
+
+int rows_per_cta(int len, std::size_t extra_per_row) {
+  int c = 16;
+  while (c > 1 && 2 * static_cast<std::size_t>(len) * (c + 1) * sizeof(float2) + (c + 2) * extra_per_row > 64 * 1024)
+    c /= 2;
+  return c;
+}
+
+unsigned grid_for(std::size_t total) {
+  return static_cast<unsigned>(std::min<std::size_t>((total + kThreads - 1) / kThreads, 148u * 32u));
+}
+
+}  // namespace
+
+UnwrapPlan::UnwrapPlan(int count, int ny, int nx) : count_(count), ny_(ny), nx_(nx) {
+  require(count >= 1 && count <= 65535 && ny >= 2 && nx >= 2 && ny % 2 == 0 && nx % 2 == 0,
+          "unwrap: image sides must be even");
+  const auto dct_table = [](int n) {
+    std::vector<float2> w(n);
+    for (int k = 0; k < n; ++k) {
+      const double a = -std::numbers::pi * k / (2.0 * n);
+      w[k] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+    }
+    return w;
+  };
+  // 2 cos(pi k / n) in float as the host's neumann_eigenvalue evaluates it.
+  const auto cos_table = [](int n) {
+    std::vector<float> c(n);
+    for (int k = 0; k < n; ++k) c[k] = 2.0f * std::cos(kPiF * static_cast<float>(k) / static_cast<float>(n));
+    return c;
+  };
+  const auto up = [](auto& buf, const auto& host) {
+    buf.reset(host.size());
+    check(cudaMemcpy(buf.get(), host.data(), host.size() * sizeof(host[0]), cudaMemcpyHostToDevice), "upload table");
+  };
+  up(dtw_y_, dct_table(ny));
+  up(dtw_x_, dct_table(nx));
+  up(cos_y_, cos_table(ny));
+  up(cos_x_, cos_table(nx));
+  rows_ = rows_per_cta(nx, static_cast<std::size_t>(nx) * sizeof(float));
+  nblk_ = (ny + rows_ - 1) / rows_;
+  d1_.reset(static_cast<std::size_t>(count) * ny * nx);
+  partial_.reset(static_cast<std::size_t>(count) * nblk_ * 2);
+  consts_.reset(count);
+}
+
+std::size_t UnwrapPlan::device_bytes() const {
+  return d1_.bytes() + partial_.bytes() + consts_.bytes() + dtw_y_.bytes() + dtw_x_.bytes() + cos_y_.bytes() +
+         cos_x_.bytes();
+}
+
+void UnwrapPlan::solve(const float* psi, float* phi, cudaStream_t s) {
+  const int ny = ny_, nx = nx_;
+  const FftLen& Lx = fft_len(nx);
+  const FftLen& Ly = fft_len(ny);
+  const int c = rows_;
+  {
+    const std::size_t smem = 2 * static_cast<std::size_t>(nx) * (c + 1) * sizeof(float2) + (c + 2) * nx * sizeof(float);
+    const dim3 grid(nblk_, count_);
+#define QHK_U1(C)                                                                                \
+  case C:                                                                                        \
+    allow(k_div_dctx<C>, smem);                                                                  \
+    k_div_dctx<C><<<grid, kThreads, smem, s>>>(psi, d1_.get(), ny, nx, Lx, dtw_x_.get());         \
+    break;
+    switch (c) {
+      QHK_U1(16)
+      QHK_U1(8)
+      QHK_U1(4)
+      QHK_U1(2)
+      QHK_U1(1)
+    }
+#undef QHK_U1
+    check_launch("unwrap pass 1");
+  }
+  {
+    int cc = 16;
+    const auto smem_of = [&](int k) {
+      return 2 * static_cast<std::size_t>(ny) * k * sizeof(float2) + static_cast<std::size_t>(ny) * k * sizeof(float);
+    };
+    while (cc > 1 && smem_of(cc) > 80 * 1024) cc /= 2;
+    const std::size_t smem = smem_of(cc);
+    const dim3 grid((nx + cc - 1) / cc, count_);
+#define QHK_U2(C)                                                                                                \
+  case C:                                                                                                        \
+    allow(k_dcty_solve<C>, smem);                                                                                \
+    k_dcty_solve<C><<<grid, kThreads, smem, s>>>(d1_.get(), phi, ny, nx, Ly, dtw_y_.get(), cos_y_.get(),        \
+                                                 cos_x_.get());                                                  \
+    break;
+    switch (cc) {
+      QHK_U2(16)
+      QHK_U2(8)
+      QHK_U2(4)
+      QHK_U2(2)
+      QHK_U2(1)
+    }
+#undef QHK_U2
+    check_launch("unwrap pass 2");
+  }
+  {
+    const std::size_t smem = 2 * static_cast<std::size_t>(nx) * (c + 1) * sizeof(float2) + c * nx * sizeof(float);
+    const dim3 grid(nblk_, count_);
+#define QHK_U3(C)                                                                                    \
+  case C:                                                                                            \
+    allow(k_idctx<C>, smem);                                                                         \
+    k_idctx<C><<<grid, kThreads, smem, s>>>(phi, psi, ny, nx, Lx, dtw_x_.get(), partial_.get());     \
+    break;
+    switch (c) {
+      QHK_U3(16)
+      QHK_U3(8)
+      QHK_U3(4)
+      QHK_U3(2)
+      QHK_U3(1)
+    }
+#undef QHK_U3
+    check_launch("unwrap pass 3");
+  }
+  const std::size_t smem = static_cast<std::size_t>(nx + ny) * sizeof(float);
+  k_rytov_consts<<<count_, kThreads, smem, s>>>(phi, ny, nx, partial_.get(), nblk_, consts_.get());
+  check_launch("rytov constants");
+}
+
+void UnwrapPlan::unwrap(const float* psi, float* phi, cudaStream_t s) {
+  solve(psi, phi, s);
+  const std::size_t total = static_cast<std::size_t>(count_) * ny_ * nx_;
+  k_rytov_assemble<<<grid_for(total), kThreads, 0, s>>>(phi, nullptr, consts_.get(),
+                                                        static_cast<std::size_t>(ny_) * nx_, total, nullptr, phi);
+  check_launch("unwrap constant");
+}
+
+void UnwrapPlan::rytov(const float* psi, const float* logamp, float* phi_scratch, float2* out, cudaStream_t s) {
+  solve(psi, phi_scratch, s);
+  const std::size_t total = static_cast<std::size_t>(count_) * ny_ * nx_;
+  k_rytov_assemble<<<grid_for(total), kThreads, 0, s>>>(phi_scratch, logamp, consts_.get(),
+                                                        static_cast<std::size_t>(ny_) * nx_, total, out, nullptr);
+  check_launch("rytov assemble");
+}
+
+void field_ratio(const float2* sample, const float2* bg, std::size_t plane, bool per_image, std::size_t total,
+                 float2* out, cudaStream_t s) {
+  k_ratio<<<grid_for(total), kThreads, 0, s>>>(sample, bg, plane, per_image, total, out);
+  check_launch("field ratio");
+}
+
+void split_ratio(const float2* ratio, std::size_t total, float* psi, float* logamp, cudaStream_t s) {
+  k_split_ratio<<<grid_for(total), kThreads, 0, s>>>(ratio, total, psi, logamp);
+  check_launch("split ratio");
+}
+
+}  // namespace qhk
