@@ -10,6 +10,7 @@
 //   * complex rows, with the clamp of the complex GP loop between its inverse and forward row
 //     transforms, or the refractive index as the epilogue of the last inverse.
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -397,6 +398,16 @@ void c2c_rows_dispatch(float2* data, std::size_t rows, int nx, bool forward, Row
 
 }  // namespace
 
+std::size_t axis_smem_budget() {
+  // QHK_FFT_AXIS_KIB overrides the shared-memory budget of an axis-pass tile (tuning).
+  static const std::size_t budget = [] {
+    const char* e = std::getenv("QHK_FFT_AXIS_KIB");
+    const long v = e ? std::atol(e) : 0;
+    return static_cast<std::size_t>(v > 0 ? v : 72) * 1024;
+  }();
+  return budget;
+}
+
 const FftLen& fft_len(int n) {
   int dev = 0;
   check(cudaGetDevice(&dev), "cudaGetDevice");
@@ -424,7 +435,10 @@ void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
   require(n_outer >= 1 && n_outer <= 65535, "fft: too many lines in the outer dimension");
   require(static_cast<std::size_t>(n) * 2 * sizeof(float2) <= 200 * 1024, "fft: transform length too large");
-  const auto fits = [&](int cols) { return 2 * static_cast<std::size_t>(n) * cols * sizeof(float2) <= 72 * 1024; };
+  // Tile width: the widest tile whose double buffer fits `axis_smem_budget()` bytes.
+  const auto fits = [&](int cols) {
+    return 2 * static_cast<std::size_t>(n) * cols * sizeof(float2) <= axis_smem_budget();
+  };
   if (fits(16)) {
     axis_dispatch<16>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
   } else if (fits(8)) {

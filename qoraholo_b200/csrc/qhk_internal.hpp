@@ -32,6 +32,8 @@ struct AxisAux {
   const float2* a = nullptr;        // half-spectrum data, or measured spectrum
   const std::uint8_t* hits = nullptr;  // hits (0..2) or mask (0/1)
 };
+// Shared-memory budget of one axis-pass tile (bytes); QHK_FFT_AXIS_KIB overrides it.
+std::size_t axis_smem_budget();
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s);
 

@@ -3,11 +3,11 @@
 // its CPU form src/cpu/tv.cpp:7-44, with the per-voxel math of src/common.hpp:107-153).
 //
 // One FGP step is one kernel. A CTA owns TY full rows (all x) of a y-slab and marches along z
-// through `zchunk` planes. Shared memory holds the input dual r for two planes (rows y0-1 ..
-// y0+TY, three components) and the primal point z = max(b - lambda L(r), 0) for two planes (rows
-// y0 .. y0+TY): z of plane k+1 is computed once from the ring and reused as plane k of the next
-// step, so z is never written to HBM, and each r value is read from HBM once (the one-row halos
-// come from L2). Per step the HBM traffic is b, r_in (3), p (3) read and p (3), r_out (3) written
+// through `zchunk` planes. Shared memory holds a three-plane ring of the input dual r (rows y0-1 ..
+// y0+TY, three components), filled by cp.async one plane ahead, and the primal point
+// z = max(b - lambda L(r), 0) for two planes (rows y0 .. y0+TY): z of plane k+1 is computed once
+// from the ring and reused as plane k of the next step, so z is never written to HBM, and each r
+// value is read from HBM once (the one-row halos come from L2). Per step the HBM traffic is b, r_in (3), p (3) read and p (3), r_out (3) written
 // -- 13 volumes; the first step reads p as r (10 volumes) and the last writes no r (10 volumes).
 //
 // All arithmetic uses the round-to-nearest intrinsics in the reference's operation order, so the
@@ -53,9 +53,27 @@ struct Vec<1> {
   __device__ static void store(float* p, const float* v) { *p = v[0]; }
 };
 
+// Asynchronous 16-byte (VEC = 4) or 4-byte (VEC = 1) global -> shared copies (cp.async), grouped
+// per plane so that plane z+2 streams in while plane z+1's primal point and plane z's dual step are
+// computed.
+template <int VEC>
+__device__ __forceinline__ void copy_async(float* dst, const float* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (VEC == 4) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+  }
+}
+__device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void copy_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
 template <int VEC, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(1024) k_fgp(FgpArgs A) {
-  extern __shared__ float sm[];
+__global__ void __launch_bounds__(512) k_fgp(FgpArgs A) {
+  extern __shared__ __align__(16) float sm[];
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   const int TY = static_cast<int>(blockDim.y);
   const int tx = static_cast<int>(threadIdx.x);
@@ -65,46 +83,47 @@ __global__ void __launch_bounds__(1024) k_fgp(FgpArgs A) {
   const int z0 = static_cast<int>(blockIdx.y) * A.zchunk;
   if (z0 >= nz) return;
   const int z1 = min(z0 + A.zchunk, nz);
+  const int zlast = min(z1, nz - 1);  // last plane whose dual r is needed (for the primal of z1)
   const int ring_rows = TY + 2;
   const std::size_t plane_sz = static_cast<std::size_t>(3) * ring_rows * nx;
-  float* R0 = sm;
-  float* R1 = sm + plane_sz;
-  float* Z0 = sm + 2 * plane_sz;
-  float* Z1 = Z0 + static_cast<std::size_t>(TY + 1) * nx;
-  float* Bs = Z1 + static_cast<std::size_t>(TY + 1) * nx;
+  const std::size_t zb_sz = static_cast<std::size_t>(TY + 1) * nx;
+  // Ring of r planes: plane z lives in slot (z - z0 + 1) % 3 (plane z0 - 1 in slot 0).
+  float* R = sm;
+  float* Z = sm + 3 * plane_sz;  // primal of plane z in slot (z - z0) & 1
+  float* Bs = Z + 2 * zb_sz;     // b of plane z in slot (z - z0) & 1
   const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
+  const auto rslot = [&](int z) { return R + static_cast<std::size_t>((z - z0 + 1) % 3) * plane_sz; };
+  const auto zslot = [&](int z) { return Z + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
+  const auto bslot = [&](int z) { return Bs + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
 
-  // r of plane z (rows y0-1 .. y0+TY), zeros outside the volume.
-  const auto load_r = [&](float* R, int z) {
-    for (int rc = ty; rc < 3 * ring_rows; rc += TY) {
+  // Rows outside the volume are never read by the arithmetic below (the boundary terms drop
+  // them), so they are not copied.
+  const auto issue_r = [&](int z, int comps) {
+    float* dst = rslot(z);
+    for (int rc = ty; rc < comps * ring_rows; rc += TY) {
       const int c = rc / ring_rows;
       const int rr = rc - c * ring_rows;
       const int y = y0 - 1 + rr;
-      float v[VEC];
-      if (z >= 0 && z < nz && y >= 0 && y < ny) {
-        Vec<VEC>::load(A.rin[c] + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0, v);
-      } else {
-#pragma unroll
-        for (int i = 0; i < VEC; ++i) v[i] = 0.0f;
-      }
-      Vec<VEC>::store(R + (static_cast<std::size_t>(c) * ring_rows + rr) * nx + x0, v);
+      if (y < 0 || y >= ny) continue;
+      copy_async<VEC>(dst + (static_cast<std::size_t>(c) * ring_rows + rr) * nx + x0,
+                      A.rin[c] + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
     }
   };
-  const auto load_b = [&](int z) {
+  const auto issue_b = [&](int z) {
+    float* dst = bslot(z);
     for (int rr = ty; rr < TY + 1; rr += TY) {
       const int y = y0 + rr;
-      float v[VEC];
-      if (y < ny) {
-        Vec<VEC>::load(A.b + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0, v);
-      } else {
-#pragma unroll
-        for (int i = 0; i < VEC; ++i) v[i] = 0.0f;
-      }
-      Vec<VEC>::store(Bs + static_cast<std::size_t>(rr) * nx + x0, v);
+      if (y >= ny) continue;
+      copy_async<VEC>(dst + static_cast<std::size_t>(rr) * nx + x0,
+                      A.b + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
     }
   };
-  // z on plane z (rows y0 .. y0+TY) from r of that plane (Rc) and of the plane below (Rb).
-  const auto primal = [&](float* Z, int z, const float* Rc, const float* Rb) {
+  // z on plane z (rows y0 .. y0+TY) from r of that plane and of the plane below.
+  const auto primal = [&](int z) {
+    const float* Rc = rslot(z);
+    const float* Rb = rslot(z - 1);
+    const float* B = bslot(z);
+    float* Zd = zslot(z);
     for (int rr = ty; rr < TY + 1; rr += TY) {
       const int y = y0 + rr;
       const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
@@ -125,27 +144,39 @@ __global__ void __launch_bounds__(1024) k_fgp(FgpArgs A) {
           if (y > 0) s = __fsub_rn(s, rym[x]);
           if (x < nx - 1) s = __fadd_rn(s, rx[x]);
           if (x > 0) s = __fsub_rn(s, rx[x - 1]);
-          zv = tv_primal(Bs[static_cast<std::size_t>(rr) * nx + x], A.lambda, s);
+          zv = tv_primal(B[static_cast<std::size_t>(rr) * nx + x], A.lambda, s);
         }
         out[i] = zv;
       }
-      Vec<VEC>::store(Z + static_cast<std::size_t>(rr) * nx + x0, out);
+      Vec<VEC>::store(Zd + static_cast<std::size_t>(rr) * nx + x0, out);
     }
   };
 
-  load_r(R0, z0);
-  load_r(R1, z0 - 1);
-  load_b(z0);
+  // Prologue: planes z0 - 1 (z component only), z0 (and b) in one group, z0 + 1 in the next.
+  if (z0 > 0) issue_r(z0 - 1, 1);
+  issue_r(z0, 3);
+  issue_b(z0);
+  copy_commit();
+  const bool second = z0 + 1 <= zlast;
+  if (second) {
+    issue_r(z0 + 1, 3);
+    issue_b(z0 + 1);
+    copy_commit();
+    copy_wait<1>();
+  } else {
+    copy_wait<0>();
+  }
   __syncthreads();
-  primal(Z0, z0, R0, R1);
+  primal(z0);
   __syncthreads();
 
   const int y = y0 + ty;
   for (int z = z0; z < z1; ++z) {
-    const bool next = z + 1 < nz;
-    if (next) {
-      load_r(R1, z + 1);
-      load_b(z + 1);
+    const bool prefetch = z + 2 <= zlast;
+    if (prefetch) {
+      issue_r(z + 2, 3);
+      issue_b(z + 2);
+      copy_commit();
     }
     const std::size_t at = static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0;
     float pv[3][VEC];
@@ -153,22 +184,28 @@ __global__ void __launch_bounds__(1024) k_fgp(FgpArgs A) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) Vec<VEC>::load(A.pin[c] + at, pv[c]);
     }
+    if (prefetch) {
+      copy_wait<1>();
+    } else {
+      copy_wait<0>();
+    }
     __syncthreads();
-    if (next) primal(Z1, z + 1, R1, R0);
+    if (z + 1 < nz) primal(z + 1);
     __syncthreads();
     if (y < ny) {
+      const float* Rc = rslot(z);
       float rv[3][VEC];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        Vec<VEC>::load(R0 + (static_cast<std::size_t>(c) * ring_rows + ty + 1) * nx + x0, rv[c]);
+        Vec<VEC>::load(Rc + (static_cast<std::size_t>(c) * ring_rows + ty + 1) * nx + x0, rv[c]);
         if (FIRST) {
 #pragma unroll
           for (int i = 0; i < VEC; ++i) pv[c][i] = rv[c][i];
         }
       }
-      const float* zc = Z0 + static_cast<std::size_t>(ty) * nx;
-      const float* zy = Z0 + static_cast<std::size_t>(ty + 1) * nx;
-      const float* zz = Z1 + static_cast<std::size_t>(ty) * nx;
+      const float* zc = zslot(z) + static_cast<std::size_t>(ty) * nx;
+      const float* zy = zslot(z) + static_cast<std::size_t>(ty + 1) * nx;
+      const float* zz = zslot(z + 1) + static_cast<std::size_t>(ty) * nx;
 #pragma unroll
       for (int i = 0; i < VEC; ++i) {
         const int x = x0 + i;
@@ -193,12 +230,6 @@ __global__ void __launch_bounds__(1024) k_fgp(FgpArgs A) {
       }
     }
     __syncthreads();
-    float* t = R0;
-    R0 = R1;
-    R1 = t;
-    t = Z0;
-    Z0 = Z1;
-    Z1 = t;
   }
 }
 
@@ -263,15 +294,15 @@ struct FgpShape {
 };
 
 std::size_t fgp_smem(int nx, int ty) {
-  return (2 * static_cast<std::size_t>(3) * (ty + 2) + 3 * static_cast<std::size_t>(ty + 1)) * nx * sizeof(float);
+  return (3 * static_cast<std::size_t>(3) * (ty + 2) + 4 * static_cast<std::size_t>(ty + 1)) * nx * sizeof(float);
 }
 
 template <int VEC>
 FgpShape fgp_shape(int nz, int ny, int nx) {
   const int tx = nx / VEC;
   int ty = 4;
-  while (ty > 1 && (tx * ty > 1024 || fgp_smem(nx, ty) > 110 * 1024)) --ty;
-  require(tx * ty <= 1024 && fgp_smem(nx, ty) <= 220 * 1024, "tv: volume rows too long for the FGP kernel");
+  while (ty > 1 && (tx * ty > 512 || fgp_smem(nx, ty) > 110 * 1024)) --ty;
+  require(tx * ty <= 512 && fgp_smem(nx, ty) <= 220 * 1024, "tv: volume rows too long for the FGP kernel");
   const std::size_t smem = fgp_smem(nx, ty);
   auto kernel = k_fgp<VEC, false, false>;
   ensure_smem(kernel);
