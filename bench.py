@@ -339,14 +339,21 @@ def run_reference_arm(args):
 
 def kernel_case(name, reps):
     """Small standalone launches of one kernel family for profiling (no JSON line): `fgp` runs the
-    TV proximal step at 256^3 (10 FGP steps + final primal per rep); `pipeline` runs the full
-    device pipeline on 9 x 128^2 holograms -> 64^3."""
+    TV proximal step at 256^3 (10 FGP steps + final primal per rep); `fft` a 256^3 rfft3 + irfft3
+    per rep; `pipeline` the full device pipeline on 9 x 128^2 holograms -> 64^3."""
     import torch
 
     from qoraholo_b200 import capi
 
     stream = torch.cuda.current_stream().cuda_stream
-    if name == "fgp":
+    if name == "fft":
+        n = FIELD_N
+        x = torch.rand((n, n, n), device="cuda")
+        half = torch.empty((n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+        for _ in range(reps):
+            capi.rfft3(x.data_ptr(), half.data_ptr(), n, n, n, stream)
+            capi.irfft3(half.data_ptr(), x.data_ptr(), n, n, n, 1.0 / n ** 3, stream)
+    elif name == "fgp":
         n = FIELD_N
         b = torch.rand((n, n, n), device="cuda")
         x = torch.empty_like(b)
@@ -378,7 +385,7 @@ def kernel_case(name, reps):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", choices=["fgp", "pipeline"], default=None,
+    ap.add_argument("--kernel-case", choices=["fgp", "fft", "pipeline"], default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)

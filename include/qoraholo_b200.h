@@ -141,6 +141,21 @@ int qhk_find_sideband(const float* holo, int n, float dc_exclusion, int* iy, int
 int qhk_unwrap(const float* wrapped, int count, int ny, int nx, float* out);
 int qhk_rytov(const void* ratio, int count, int ny, int nx, void* out);
 
+/* Unwrap with no allocation -- no counterpart in the reference. The same least-squares unwrap as
+ * qhk_unwrap, device in / device out: d_wrapped and d_unwrapped are (count, ny, nx) float32 buffers on
+ * the device, owned by the caller; the function calls no cudaMalloc, cudaFree or other allocating
+ * routine. It exists for callers that cannot allocate device memory during a run: a serving process
+ * whose device memory is already reserved by its own allocator or HBM budget (where a library
+ * allocation would fail or evict cached state), and real-time loops that must not pay for, or
+ * synchronise on, allocation and release. All scratch lives in one static device array of about
+ * 17.8 MB that every GPU loading the library holds until exit. Limits: even sides, ny and nx <= 1024,
+ * count <= 4096, count * ny * nx <= 4194304 pixels; larger requests return QHK_INVALID_ARGUMENT.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) for that
+ * device; make that first call before any stream capture. Every call writes all the scratch it reads
+ * (nothing must start at zero), asynchronously on `stream`; calls that overlap on the GPU share the
+ * array and race, so serialise them (one stream, or events). */
+int qhk_unwrap_noalloc(const float* d_wrapped, float* d_unwrapped, int count, int ny, int nx, void* stream);
+
 /* ---- Pipeline: replaces cuda::make_pipeline and Pipeline::Impl (src/backends.hpp:75-89,
  * src/cuda/pipeline.cu:12-161). Validation of the Pipeline constructor (src/pipeline.cpp:72-91). */
 typedef struct qhk_pipeline_options {

@@ -72,6 +72,7 @@ _PROTOS = {
     "qhk_irfft3": (_I, [_VP, _VP, _I, _I, _I, _F, _VP]),
     "qhk_tv_prox_device": (_I, [_VP, _VP, _VP, _I, _I, _I, _F, _I, _VP]),
     "qhk_kernel_launches": (C.c_uint64, []),
+    "qhk_unwrap_noalloc": (_I, [_VP, _VP, _I, _I, _I, _VP]),
     "qhk_bpm_vjp": (_I, [_VP, _I, _I, _VP, _VP, _I, C.POINTER(Geometry), _I, _VP]),
     "qhk_pipeline_create": (_I, [C.POINTER(_VP), _VP, _VP, C.POINTER(Geometry)]),
     "qhk_pipeline_set_background": (_I, [_VP, _VP]),
@@ -193,6 +194,11 @@ def tv_prox(d_b, d_x, d_dual, nz, ny, nx, lam, inner, stream=0):
 def tv_prox_device(d_b, d_x, d_dual9, nz, ny, nx, lam, inner, stream=0):
     """No-allocation proximal step: d_dual9 holds the dual (3 volumes) and 6 volumes of scratch."""
     check(lib().qhk_tv_prox_device(_VP(d_b), _VP(d_x), _VP(d_dual9), nz, ny, nx, float(lam), int(inner), _VP(stream)))
+
+
+def unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, stream=0):
+    """qhk_unwrap_noalloc: device in / device out, no allocation (scratch in a static device array)."""
+    check(lib().qhk_unwrap_noalloc(_VP(d_wrapped), _VP(d_unwrapped), count, ny, nx, _VP(stream)))
 
 
 def kernel_launches() -> int:

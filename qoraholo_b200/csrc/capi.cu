@@ -367,6 +367,10 @@ int qhk_unwrap(const float* wrapped, int count, int ny, int nx, float* out) {
   });
 }
 
+int qhk_unwrap_noalloc(const float* d_wrapped, float* d_unwrapped, int count, int ny, int nx, void* stream) {
+  return guard([&] { qhk::unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, as_stream(stream)); });
+}
+
 int qhk_rytov(const void* ratio, int count, int ny, int nx, void* out) {
   return guard([&] {
     qhk::require(ratio && out, "rytov: null argument");

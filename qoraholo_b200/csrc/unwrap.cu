@@ -12,6 +12,7 @@
 // congruence constant and forms the border mean, in the host's summation order, for the 2 pi
 // shift of the Rytov phase.
 #include <cmath>
+#include <mutex>
 #include <numbers>
 #include <vector>
 
@@ -428,6 +429,165 @@ void field_ratio(const float2* sample, const float2* bg, std::size_t plane, bool
 void split_ratio(const float2* ratio, std::size_t total, float* psi, float* logamp, cudaStream_t s) {
   k_split_ratio<<<grid_for(total), kThreads, 0, s>>>(ratio, total, psi, logamp);
   check_launch("split ratio");
+}
+
+}  // namespace qhk
+
+// ---- Unwrap with no allocation -----------------------------------------------------------------
+// The least-squares unwrap above, for callers that cannot allocate device memory: all scratch (the
+// DCT intermediate, the congruence partial sums, the per-image constants and every twiddle /
+// eigenvalue table, including the FFT twiddles that the planned path keeps in a cudaMalloc'd cache)
+// lives in one file-scope device array, sized for at most kNoAllocPixels pixels per call.
+
+namespace qhk {
+
+namespace {
+
+constexpr std::size_t kNoAllocPixels = std::size_t(1) << 22;  // count * ny * nx, 16 MiB of float
+constexpr int kNoAllocMaxSide = 1024;                           // ny, nx
+constexpr int kNoAllocMaxImages = 4096;                         // count
+constexpr std::size_t kNoAllocPartials = std::size_t(1) << 16;  // (image, row block) pairs
+// Layout in floats; every region starts on a 256-byte boundary.
+constexpr std::size_t kOffD1 = 0;
+constexpr std::size_t kOffPartial = kOffD1 + kNoAllocPixels;                   // 2 doubles per pair
+constexpr std::size_t kOffConsts = kOffPartial + 4 * kNoAllocPartials;         // float2 per image
+constexpr std::size_t kOffTables = kOffConsts + 2 * kNoAllocMaxImages;
+constexpr std::size_t kTableFloats = 4 * 2 * kNoAllocMaxSide + 2 * kNoAllocMaxSide;  // 4 float2 + 2 float tables
+constexpr std::size_t kNoAllocFloats = kOffTables + kTableFloats;
+
+}  // namespace
+
+// File-scope scratch of unwrap_noalloc, about 17.8 MB on every device that loads the library.
+static __device__ __align__(256) float g_unwrap_scratch[kNoAllocFloats];
+
+namespace {
+
+// Per-device address of g_unwrap_scratch (host code must not pass the symbol itself to a kernel).
+std::mutex g_scratch_mutex;
+float* g_scratch_ptr[64] = {};
+
+float* scratch_base() {
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  require(dev >= 0 && dev < 64, "unwrap_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    check(cudaGetSymbolAddress(&p, g_unwrap_scratch), "cudaGetSymbolAddress");
+    g_scratch_ptr[dev] = static_cast<float*>(p);
+  }
+  return g_scratch_ptr[dev];
+}
+
+// DCT twiddles e^{-i pi k / 2n}, 2 cos(pi k / n) and FFT twiddles e^{-2 pi i k / n} for one side.
+__global__ void k_side_tables(int n, float2* dtw, float* cos2, float2* fftw) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    double s, c;
+    sincos(-3.141592653589793238462643 * k / (2.0 * n), &s, &c);
+    dtw[k] = make_float2(static_cast<float>(c), static_cast<float>(s));
+    cos2[k] = 2.0f * cosf(kPiF * static_cast<float>(k) / static_cast<float>(n));
+    sincos(6.283185307179586476925287 * k / n, &s, &c);
+    fftw[k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+  }
+}
+
+}  // namespace
+
+void unwrap_noalloc(const float* psi, float* phi, int count, int ny, int nx, cudaStream_t s) {
+  require(psi && phi, "unwrap_noalloc: null argument");
+  require(count >= 1 && ny >= 2 && nx >= 2 && ny % 2 == 0 && nx % 2 == 0, "unwrap: image sides must be even");
+  require(ny <= kNoAllocMaxSide && nx <= kNoAllocMaxSide && count <= kNoAllocMaxImages &&
+              static_cast<std::size_t>(count) * ny * nx <= kNoAllocPixels,
+          "unwrap_noalloc: at most 4096 images of at most 1024 x 1024 and 4194304 pixels per call");
+  const int rows = rows_per_cta(nx, static_cast<std::size_t>(nx) * sizeof(float));
+  const int nblk = (ny + rows - 1) / rows;
+  require(static_cast<std::size_t>(count) * nblk <= kNoAllocPartials,
+          "unwrap_noalloc: too many images for the partial-sum scratch");
+  float* base = scratch_base();
+  float* d1 = base + kOffD1;
+  auto* partial = reinterpret_cast<double*>(base + kOffPartial);
+  auto* consts = reinterpret_cast<float2*>(base + kOffConsts);
+  float* t = base + kOffTables;
+  auto* dtw_y = reinterpret_cast<float2*>(t);
+  auto* dtw_x = reinterpret_cast<float2*>(t + 2 * kNoAllocMaxSide);
+  auto* fft_y = reinterpret_cast<float2*>(t + 4 * kNoAllocMaxSide);
+  auto* fft_x = reinterpret_cast<float2*>(t + 6 * kNoAllocMaxSide);
+  float* cos_y = t + 8 * kNoAllocMaxSide;
+  float* cos_x = t + 9 * kNoAllocMaxSide;
+  k_side_tables<<<4, 256, 0, s>>>(ny, dtw_y, cos_y, fft_y);
+  check_launch("unwrap_noalloc tables");
+  k_side_tables<<<4, 256, 0, s>>>(nx, dtw_x, cos_x, fft_x);
+  check_launch("unwrap_noalloc tables");
+  FftLen Ly = make_fft_len(ny);
+  FftLen Lx = make_fft_len(nx);
+  Ly.tw = fft_y;
+  Lx.tw = fft_x;
+  {
+    const std::size_t smem = 2 * static_cast<std::size_t>(nx) * (rows + 1) * sizeof(float2) + (rows + 2) * nx * sizeof(float);
+    const dim3 grid(nblk, count);
+#define QHK_S1(C)                                                                   \
+  case C:                                                                           \
+    allow(k_div_dctx<C>, smem);                                                     \
+    k_div_dctx<C><<<grid, kThreads, smem, s>>>(psi, d1, ny, nx, Lx, dtw_x);         \
+    break;
+    switch (rows) {
+      QHK_S1(16)
+      QHK_S1(8)
+      QHK_S1(4)
+      QHK_S1(2)
+      QHK_S1(1)
+    }
+#undef QHK_S1
+    check_launch("unwrap_noalloc pass 1");
+  }
+  {
+    int cc = 16;
+    const auto smem_of = [&](int k) {
+      return 2 * static_cast<std::size_t>(ny) * k * sizeof(float2) + static_cast<std::size_t>(ny) * k * sizeof(float);
+    };
+    while (cc > 1 && smem_of(cc) > 80 * 1024) cc /= 2;
+    const std::size_t smem = smem_of(cc);
+    const dim3 grid((nx + cc - 1) / cc, count);
+#define QHK_S2(C)                                                                                        \
+  case C:                                                                                                \
+    allow(k_dcty_solve<C>, smem);                                                                        \
+    k_dcty_solve<C><<<grid, kThreads, smem, s>>>(d1, phi, ny, nx, Ly, dtw_y, cos_y, cos_x);            \
+    break;
+    switch (cc) {
+      QHK_S2(16)
+      QHK_S2(8)
+      QHK_S2(4)
+      QHK_S2(2)
+      QHK_S2(1)
+    }
+#undef QHK_S2
+    check_launch("unwrap_noalloc pass 2");
+  }
+  {
+    const std::size_t smem = 2 * static_cast<std::size_t>(nx) * (rows + 1) * sizeof(float2) + rows * nx * sizeof(float);
+    const dim3 grid(nblk, count);
+#define QHK_S3(C)                                                                              \
+  case C:                                                                                      \
+    allow(k_idctx<C>, smem);                                                                   \
+    k_idctx<C><<<grid, kThreads, smem, s>>>(phi, psi, ny, nx, Lx, dtw_x, partial);             \
+    break;
+    switch (rows) {
+      QHK_S3(16)
+      QHK_S3(8)
+      QHK_S3(4)
+      QHK_S3(2)
+      QHK_S3(1)
+    }
+#undef QHK_S3
+    check_launch("unwrap_noalloc pass 3");
+  }
+  k_rytov_consts<<<count, kThreads, static_cast<std::size_t>(nx + ny) * sizeof(float), s>>>(phi, ny, nx, partial,
+                                                                                           nblk, consts);
+  check_launch("unwrap_noalloc constants");
+  const std::size_t total = static_cast<std::size_t>(count) * ny * nx;
+  k_rytov_assemble<<<grid_for(total), kThreads, 0, s>>>(phi, nullptr, consts, static_cast<std::size_t>(ny) * nx, total,
+                                                        nullptr, phi);
+  check_launch("unwrap_noalloc constant");
 }
 
 }  // namespace qhk

@@ -30,6 +30,12 @@ class UnwrapPlan {
   DevBuf<float2> consts_;  // (congruence constant, 2 pi shift) per image
 };
 
+// Least-squares unwrap of count images (ny, nx) from psi into phi (both on the device) with no
+// allocation: scratch and tables live in a file-scope device array (unwrap.cu); at most 4096 images
+// of at most 1024 x 1024 and 4194304 pixels per call. Asynchronous on `s`; calls that overlap on the
+// GPU share the scratch and race.
+void unwrap_noalloc(const float* psi, float* phi, int count, int ny, int nx, cudaStream_t s);
+
 // out = sample / background (background: one image, or one per image when per_image).
 void field_ratio(const float2* sample, const float2* bg, std::size_t plane, bool per_image, std::size_t total,
                  float2* out, cudaStream_t s);
