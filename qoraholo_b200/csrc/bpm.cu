@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kThreads)
     A[pos * cp + row] = row < nr ? src[(r0 + row) * n + pos] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  const float2* res = smem_fft<Fwd>(A, B, cp, COLS, L, tid, nth);
+  const float2* res = smem_fft_cols<Fwd, COLS>(A, B, cp, L, tid, nth);
   for (int idx = tid; idx < n * COLS; idx += nth) {
     const int row = idx / n;
     const int pos = idx - row * n;
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kThreads) k_cols(ColArgs a, FftLen L) {
     A[idx] = col < cols ? a.data[base + static_cast<std::size_t>(pos) * n + col] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  const float2* res = smem_fft<Fwd>(A, B, COLS, COLS, L, tid, nth);
+  const float2* res = smem_fft_cols<Fwd, COLS>(A, B, COLS, L, tid, nth);
   for (int idx = tid; idx < n * COLS; idx += nth) {
     const int pos = idx / COLS;
     const int col = idx - pos * COLS;

@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kThreads)
 
   float2* res;
   if constexpr (Mode == kHalf || Mode == kMask) {
-    res = smem_fft<true>(A, B, COLS, COLS, L, tid, nth);
+    res = smem_fft_cols<true, COLS>(A, B, COLS, L, tid, nth);
     float2* other = res == A ? B : A;
     for (int idx = tid; idx < n * COLS; idx += nth) {
       const int pos = idx / COLS;
@@ -117,9 +117,9 @@ __global__ void __launch_bounds__(kThreads)
       res[idx] = v;
     }
     __syncthreads();
-    res = smem_fft<false>(res, other, COLS, COLS, L, tid, nth);
+    res = smem_fft_cols<false, COLS>(res, other, COLS, L, tid, nth);
   } else {
-    res = smem_fft<Fwd>(A, B, COLS, COLS, L, tid, nth);
+    res = smem_fft_cols<Fwd, COLS>(A, B, COLS, L, tid, nth);
   }
 
   for (int idx = tid; idx < n * COLS; idx += nth) {
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kThreads)
     A[m * cp + row] = v;
   }
   __syncthreads();
-  const float2* res = smem_fft<true>(A, B, cp, COLS, Lm, tid, nth);
+  const float2* res = smem_fft_cols<true, COLS>(A, B, cp, Lm, tid, nth);
 
   for (int idx = tid; idx < h * COLS; idx += nth) {
     const int row = idx / h;
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kThreads)
     B[k * cp + row] = make_float2(sv.x - t.y, sv.y + t.x);     // sv + i t
   }
   __syncthreads();
-  const float2* res = smem_fft<false>(B, A, cp, COLS, Lm, tid, nth);
+  const float2* res = smem_fft_cols<false, COLS>(B, A, cp, Lm, tid, nth);
 
   for (int idx = tid; idx < M * COLS; idx += nth) {
     const int row = idx / M;
@@ -292,9 +292,9 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   float2* res;
   if constexpr (Mode == static_cast<int>(RowMode::plain)) {
-    res = smem_fft<Fwd>(A, B, cp, COLS, L, tid, nth);
+    res = smem_fft_cols<Fwd, COLS>(A, B, cp, L, tid, nth);
   } else {
-    res = smem_fft<false>(A, B, cp, COLS, L, tid, nth);
+    res = smem_fft_cols<false, COLS>(A, B, cp, L, tid, nth);
     if constexpr (Mode == static_cast<int>(RowMode::inv_clamp_fwd)) {
       float2* other = res == A ? B : A;
       for (int idx = tid; idx < n * COLS; idx += nth) {
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kThreads)
         res[pos * cp + row] = make_float2(fmaxf(v.x * scale, 0.0f), 0.0f);
       }
       __syncthreads();
-      res = smem_fft<true>(res, other, cp, COLS, L, tid, nth);
+      res = smem_fft_cols<true, COLS>(res, other, cp, L, tid, nth);
     }
   }
   for (int idx = tid; idx < n * COLS; idx += nth) {

@@ -207,4 +207,97 @@ __device__ float2* smem_fft(float2* a, float2* b, int cp, int cols, const FftLen
   return a;
 }
 
+// ---- Compile-time lengths -----------------------------------------------------------------------
+// The same passes with the length, the radix sequence and every pass's stride known at compile
+// time, so all index arithmetic is by constants. Used for the common lengths; others take the
+// runtime engine above.
+
+struct RadixSeq {
+  int r[kMaxPasses] = {};
+  int count = 0;
+};
+
+constexpr RadixSeq radix_seq(int n) {
+  RadixSeq s{};
+  int m = n;
+  while (m % 8 == 0) {
+    s.r[s.count++] = 8;
+    m /= 8;
+  }
+  if (m % 4 == 0) {
+    s.r[s.count++] = 4;
+    m /= 4;
+  }
+  if (m % 2 == 0) {
+    s.r[s.count++] = 2;
+    m /= 2;
+  }
+  while (m % 3 == 0) {
+    s.r[s.count++] = 3;
+    m /= 3;
+  }
+  while (m % 5 == 0) {
+    s.r[s.count++] = 5;
+    m /= 5;
+  }
+  return s;
+}
+
+namespace fftdev {
+
+template <int N, int R, int NS, bool Fwd, int COLS>
+__device__ __forceinline__ void pass_fixed(const float2* src, float2* dst, int cp, const float2* tw, int tid,
+                                           int nth) {
+  constexpr int m = N / R;
+  constexpr int tws = N / (NS * R);
+  constexpr int total = m * COLS;
+  for (int t = tid; t < total; t += nth) {
+    const int col = t % COLS;
+    const int j = t / COLS;
+    const int k = j % NS;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = src[(j + q * m) * cp + col];
+    if (NS > 1 && k) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle<Fwd>(tw, k * q * tws));
+    }
+    dft<R, Fwd>(v);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst[(base + q * NS) * cp + col] = v[q];
+  }
+}
+
+template <int N, int S, int NS, bool Fwd, int COLS>
+__device__ __forceinline__ float2* passes_fixed(float2* a, float2* b, int cp, const float2* tw, int tid, int nth) {
+  constexpr RadixSeq seq = radix_seq(N);
+  if constexpr (S == seq.count) {
+    return a;
+  } else {
+    constexpr int R = seq.r[S];
+    pass_fixed<N, R, NS, Fwd, COLS>(a, b, cp, tw, tid, nth);
+    __syncthreads();
+    return passes_fixed<N, S + 1, NS * R, Fwd, COLS>(b, a, cp, tw, tid, nth);
+  }
+}
+
+}  // namespace fftdev
+
+// Lines of length L.n in `a` (pitch cp, COLS lines), result buffer returned; specialised for the
+// common lengths.
+template <bool Fwd, int COLS>
+__device__ float2* smem_fft_cols(float2* a, float2* b, int cp, const FftLen& L, int tid, int nth) {
+  switch (L.n) {
+    case 64: return fftdev::passes_fixed<64, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+    case 128: return fftdev::passes_fixed<128, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+    case 192: return fftdev::passes_fixed<192, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+    case 256: return fftdev::passes_fixed<256, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+    case 384: return fftdev::passes_fixed<384, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+    case 512: return fftdev::passes_fixed<512, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+    case 1024: return fftdev::passes_fixed<1024, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+    default: return smem_fft<Fwd>(a, b, cp, COLS, L, tid, nth);
+  }
+}
+
 }  // namespace qhk

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kThreads)
     A[m * cp + row] = row < nr ? *reinterpret_cast<const float2*>(holo + (r0 + row) * N + 2 * m) : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  const float2* res = smem_fft<true>(A, B, cp, COLS, Lm, tid, nth);
+  const float2* res = smem_fft_cols<true, COLS>(A, B, cp, Lm, tid, nth);
   for (int idx = tid; idx < W * COLS; idx += nth) {
     const int row = idx / W;
     const int j = idx - row * W;
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(kThreads)
     A[idx] = col < cols ? src[static_cast<std::size_t>(pos) * W + col] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2* res = smem_fft<true>(A, B, COLS, COLS, Ln, tid, nth);
+  float2* res = smem_fft_cols<true, COLS>(A, B, COLS, Ln, tid, nth);
   float2* C = res == A ? B : A;
   for (int idx = tid; idx < m * COLS; idx += nth) {
     const int jy = idx / COLS;
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kThreads)
     C[idx] = v;
   }
   __syncthreads();
-  const float2* out = smem_fft<false>(C, res, COLS, COLS, Lmo, tid, nth);
+  const float2* out = smem_fft_cols<false, COLS>(C, res, COLS, Lmo, tid, nth);
   float2* dst = t2 + img * m * W + c0;
   for (int idx = tid; idx < m * COLS; idx += nth) {
     const int pos = idx / COLS;
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(kThreads)
     if (row < nr) A[(x0 + j) * cp + row] = t2[(r0 + row) * W + j];
   }
   __syncthreads();
-  const float2* res = smem_fft<false>(A, B, cp, COLS, Lmo, tid, nth);
+  const float2* res = smem_fft_cols<false, COLS>(A, B, cp, Lmo, tid, nth);
   for (int idx = tid; idx < m * COLS; idx += nth) {
     const int row = idx / m;
     const int x = idx - row * m;

@@ -72,7 +72,7 @@ __device__ __forceinline__ void copy_wait() {
 }
 
 template <int VEC, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(512) k_fgp(FgpArgs A) {
+__global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
   extern __shared__ __align__(16) float sm[];
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   const int TY = static_cast<int>(blockDim.y);
@@ -118,19 +118,44 @@ __global__ void __launch_bounds__(512) k_fgp(FgpArgs A) {
                       A.b + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
     }
   };
-  // z on plane z (rows y0 .. y0+TY) from r of that plane and of the plane below.
+  // z on plane z (rows y0 .. y0+TY) from r of that plane and of the plane below. Every thread runs
+  // the same number of row iterations so that all lanes reach the shuffles; with VEC = 4 a thread
+  // reads its four x values as one float4 and gets x - 1 from the lane on its left.
+  const int linear = static_cast<int>(threadIdx.y * blockDim.x + threadIdx.x);
+  const int lane = linear & 31;
+  // Lanes that exist in this thread's warp (the block's last warp may be partial).
+  const int warp_threads = min(32, static_cast<int>(blockDim.x * blockDim.y) - (linear & ~31));
+  const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
   const auto primal = [&](int z) {
     const float* Rc = rslot(z);
     const float* Rb = rslot(z - 1);
     const float* B = bslot(z);
     float* Zd = zslot(z);
-    for (int rr = ty; rr < TY + 1; rr += TY) {
-      const int y = y0 + rr;
-      const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
-      const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
-      const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
-      const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr) * nx;
-      const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+    for (int it = 0; it < 2; ++it) {
+      const int rr = ty + it * TY;
+      const bool active = rr < TY + 1;
+      const int rrc = active ? rr : 0;
+      const int y = y0 + rrc;
+      const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+      const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+      const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+      const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc) * nx;
+      const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+      float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
+      Vec<VEC>::load(rz + x0, vz);
+      Vec<VEC>::load(rzb + x0, vzb);
+      Vec<VEC>::load(ry + x0, vy);
+      Vec<VEC>::load(rym + x0, vym);
+      Vec<VEC>::load(rx + x0, vx);
+      Vec<VEC>::load(B + static_cast<std::size_t>(rrc) * nx + x0, vb);
+      float left;
+      if constexpr (VEC == 4) {
+        const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
+        left = (x0 > 0 && lane == 0) ? rx[x0 - 1] : from_lane;
+      } else {
+        left = x0 > 0 ? rx[x0 - 1] : 0.0f;
+      }
+      if (!active) continue;
       float out[VEC];
 #pragma unroll
       for (int i = 0; i < VEC; ++i) {
@@ -138,13 +163,13 @@ __global__ void __launch_bounds__(512) k_fgp(FgpArgs A) {
         float zv = 0.0f;
         if (y < ny) {
           float s = 0.0f;
-          if (z < nz - 1) s = __fadd_rn(s, rz[x]);
-          if (z > 0) s = __fsub_rn(s, rzb[x]);
-          if (y < ny - 1) s = __fadd_rn(s, ry[x]);
-          if (y > 0) s = __fsub_rn(s, rym[x]);
-          if (x < nx - 1) s = __fadd_rn(s, rx[x]);
-          if (x > 0) s = __fsub_rn(s, rx[x - 1]);
-          zv = tv_primal(B[static_cast<std::size_t>(rr) * nx + x], A.lambda, s);
+          if (z < nz - 1) s = __fadd_rn(s, vz[i]);
+          if (z > 0) s = __fsub_rn(s, vzb[i]);
+          if (y < ny - 1) s = __fadd_rn(s, vy[i]);
+          if (y > 0) s = __fsub_rn(s, vym[i]);
+          if (x < nx - 1) s = __fadd_rn(s, vx[i]);
+          if (x > 0) s = __fsub_rn(s, i == 0 ? left : vx[i > 0 ? i - 1 : 0]);
+          zv = tv_primal(vb[i], A.lambda, s);
         }
         out[i] = zv;
       }
@@ -192,7 +217,7 @@ __global__ void __launch_bounds__(512) k_fgp(FgpArgs A) {
     __syncthreads();
     if (z + 1 < nz) primal(z + 1);
     __syncthreads();
-    if (y < ny) {
+    {
       const float* Rc = rslot(z);
       float rv[3][VEC];
 #pragma unroll
@@ -203,30 +228,41 @@ __global__ void __launch_bounds__(512) k_fgp(FgpArgs A) {
           for (int i = 0; i < VEC; ++i) pv[c][i] = rv[c][i];
         }
       }
-      const float* zc = zslot(z) + static_cast<std::size_t>(ty) * nx;
-      const float* zy = zslot(z) + static_cast<std::size_t>(ty + 1) * nx;
-      const float* zz = zslot(z + 1) + static_cast<std::size_t>(ty) * nx;
-#pragma unroll
-      for (int i = 0; i < VEC; ++i) {
-        const int x = x0 + i;
-        const float c = zc[x];
-        float g[3];
-        g[0] = z < nz - 1 ? __fsub_rn(c, zz[x]) : 0.0f;
-        g[1] = y < ny - 1 ? __fsub_rn(c, zy[x]) : 0.0f;
-        g[2] = x < nx - 1 ? __fsub_rn(c, zc[x + 1]) : 0.0f;
-        float p[3] = {pv[0][i], pv[1][i], pv[2][i]};
-        float r[3] = {rv[0][i], rv[1][i], rv[2][i]};
-        tv_dual_step(g, A.step, A.momentum, p, r);
-#pragma unroll
-        for (int c2 = 0; c2 < 3; ++c2) {
-          pv[c2][i] = p[c2];
-          rv[c2][i] = r[c2];
-        }
+      const float* zcp = zslot(z) + static_cast<std::size_t>(ty) * nx;
+      float zc[VEC], zy[VEC], zz[VEC];
+      Vec<VEC>::load(zcp + x0, zc);
+      Vec<VEC>::load(zslot(z) + static_cast<std::size_t>(ty + 1) * nx + x0, zy);
+      Vec<VEC>::load(zslot(z + 1) + static_cast<std::size_t>(ty) * nx + x0, zz);
+      float right;
+      if constexpr (VEC == 4) {
+        const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
+        right = (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? zcp[x0 + VEC] : from_lane;
+      } else {
+        right = x0 + 1 < nx ? zcp[x0 + 1] : 0.0f;
       }
+      if (y < ny) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        Vec<VEC>::store(A.pout[c] + at, pv[c]);
-        if (!LAST) Vec<VEC>::store(A.rout[c] + at, rv[c]);
+        for (int i = 0; i < VEC; ++i) {
+          const int x = x0 + i;
+          const float c = zc[i];
+          float g[3];
+          g[0] = z < nz - 1 ? __fsub_rn(c, zz[i]) : 0.0f;
+          g[1] = y < ny - 1 ? __fsub_rn(c, zy[i]) : 0.0f;
+          g[2] = x < nx - 1 ? __fsub_rn(c, i == VEC - 1 ? right : zc[i < VEC - 1 ? i + 1 : 0]) : 0.0f;
+          float p[3] = {pv[0][i], pv[1][i], pv[2][i]};
+          float r[3] = {rv[0][i], rv[1][i], rv[2][i]};
+          tv_dual_step(g, A.step, A.momentum, p, r);
+#pragma unroll
+          for (int c2 = 0; c2 < 3; ++c2) {
+            pv[c2][i] = p[c2];
+            rv[c2][i] = r[c2];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          Vec<VEC>::store(A.pout[c] + at, pv[c]);
+          if (!LAST) Vec<VEC>::store(A.rout[c] + at, rv[c]);
+        }
       }
     }
     __syncthreads();
@@ -301,8 +337,9 @@ template <int VEC>
 FgpShape fgp_shape(int nz, int ny, int nx) {
   const int tx = nx / VEC;
   int ty = 4;
-  while (ty > 1 && (tx * ty > 512 || fgp_smem(nx, ty) > 110 * 1024)) --ty;
-  require(tx * ty <= 512 && fgp_smem(nx, ty) <= 220 * 1024, "tv: volume rows too long for the FGP kernel");
+  while (ty > 1 && (tx * ty > 256 || fgp_smem(nx, ty) > 110 * 1024)) --ty;
+  require(tx * ty <= 256 && fgp_smem(nx, ty) <= 220 * 1024,
+          "tv: volume rows too long for the FGP kernel (at most 1024 float4-aligned or 256 other x values)");
   const std::size_t smem = fgp_smem(nx, ty);
   auto kernel = k_fgp<VEC, false, false>;
   ensure_smem(kernel);

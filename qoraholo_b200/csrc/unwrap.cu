@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(kThreads)
     A[dct_position(x, nx) * cp + row] = make_float2(r, 0.0f);
   }
   __syncthreads();
-  const float2* res = smem_fft<true>(A, B, cp, COLS, L, tid, nth);
+  const float2* res = smem_fft_cols<true, COLS>(A, B, cp, L, tid, nth);
   for (int idx = tid; idx < COLS * nx; idx += nth) {
     const int row = idx / nx;
     const int k = idx - row * nx;
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kThreads)
     A[dct_position(y, ny) * COLS + col] = make_float2(v, 0.0f);
   }
   __syncthreads();
-  float2* res = smem_fft<true>(A, B, COLS, COLS, L, tid, nth);
+  float2* res = smem_fft_cols<true, COLS>(A, B, COLS, L, tid, nth);
   float2* other = res == A ? B : A;
   for (int idx = tid; idx < ny * COLS; idx += nth) {
     const int k = idx / COLS;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kThreads)
     other[idx] = cmulc(make_float2(a, -mirror), w);
   }
   __syncthreads();
-  const float2* out = smem_fft<false>(other, res, COLS, COLS, L, tid, nth);
+  const float2* out = smem_fft_cols<false, COLS>(other, res, COLS, L, tid, nth);
   const float inv = 1.0f / static_cast<float>(ny);
   for (int idx = tid; idx < ny * COLS; idx += nth) {
     const int y = idx / COLS;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kThreads)
     A[k * cp + row] = cmulc(make_float2(a, -mirror), __ldg(dtw + k));
   }
   __syncthreads();
-  const float2* res = smem_fft<false>(A, B, cp, COLS, L, tid, nth);
+  const float2* res = smem_fft_cols<false, COLS>(A, B, cp, L, tid, nth);
   const float inv = 1.0f / static_cast<float>(nx);
   double sc = 0.0, ss = 0.0;
   for (int idx = tid; idx < COLS * nx; idx += nth) {
