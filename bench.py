@@ -67,20 +67,21 @@ def _inside(shape, z, y, x):
     return ((z - c[0]) / a[0]) ** 2 + ((y - c[1]) / a[1]) ** 2 + ((x - c[2]) / a[2]) ** 2 <= 1.0
 
 
-def _parent_index(i):
+def _parent_index(shapes, i):
     n = N_MEDIUM
-    c = CELL[i][1]
-    for s in CELL[:i]:
+    c = shapes[i][1]
+    for s in shapes[:i]:
         if _inside(s, *c):
             n = s[3]
     return n
 
 
-def cell_fields(illum, n, pixel, device):
-    """Rytov field ratios (count, n, n) of CELL at z = 0 for each illumination: the analytic first
-    Born spectrum of the nested ellipsoids placed on the Ewald caps (an ellipsoid is an affinely
-    scaled ball), taken as a Rytov phase -- the construction of the reference's forward_fields for
-    spheres, extended to ellipsoids. Computed in float64 with torch on the GPU."""
+def phantom_fields(shapes, illum, n, pixel, device):
+    """Rytov field ratios (count, n, n) at z = 0 of nested ellipsoids `shapes` (painter's order)
+    for each illumination: the analytic first Born spectrum of each shape placed on the Ewald caps
+    (an ellipsoid is an affinely scaled ball), taken as a Rytov phase -- the construction of the
+    reference's forward_fields for spheres (src/phantom.cpp:102-191), extended to ellipsoids.
+    Computed in float64 with torch on the GPU (fixture generation, not the measured path)."""
     import torch
 
     k0 = 2 * math.pi / WAVELENGTH
@@ -93,9 +94,9 @@ def cell_fields(illum, n, pixel, device):
     par = torch.where(((torch.arange(n, device=device)[:, None] + torch.arange(n, device=device)[None, :]) % 2) == 1,
                       -1.0, 1.0).to(torch.float64)
     steps = []
-    for i, (_, c, a, nn) in enumerate(CELL):
+    for i, (_, c, a, nn) in enumerate(shapes):
         vol = 4.0 / 3.0 * math.pi * a[0] * a[1] * a[2]
-        steps.append(k0 * k0 * (nn * nn - _parent_index(i) ** 2) * vol)
+        steps.append(k0 * k0 * (nn * nn - _parent_index(shapes, i) ** 2) * vol)
     out = torch.empty((len(illum), n, n), dtype=torch.complex64, device=device)
     for j, (fiy, fix) in enumerate(np.asarray(illum, np.float64)):
         fiz = math.sqrt(fm2 - fiy * fiy - fix * fix)
@@ -105,7 +106,7 @@ def cell_fields(illum, n, pixel, device):
         nuz = torch.sqrt(torch.where(ok, fm2 - rho2, torch.ones_like(rho2)))
         qz = nuz - fiz
         o = torch.zeros((n, n), dtype=torch.complex128, device=device)
-        for (_, c, a, _), st in zip(CELL, steps):
+        for (_, c, a, _), st in zip(shapes, steps):
             arg = 2 * math.pi * torch.sqrt((a[0] * qz) ** 2 + (a[1] * my) ** 2 + (a[2] * mx) ** 2)
             ball = torch.where(arg < 1e-3, 1.0 - arg * arg / 10.0,
                                3.0 * (torch.sin(arg) - arg * torch.cos(arg)) / arg.clamp_min(1e-3) ** 3)
@@ -115,6 +116,11 @@ def cell_fields(illum, n, pixel, device):
         u = torch.where(ok, u, torch.zeros_like(u))
         out[j] = torch.exp(torch.fft.ifft2(u)).to(torch.complex64)
     return out.cpu().numpy()
+
+
+def cell_fields(illum, n, pixel, device):
+    """Rytov field ratios of CELL (see phantom_fields)."""
+    return phantom_fields(CELL, illum, n, pixel, device)
 
 
 def make_inputs(qh, device):
@@ -337,6 +343,156 @@ def run_reference_arm(args):
     return 0
 
 
+# Serving mix (three geometries with resident state, Poisson arrivals):
+# (name, share, count, N, hologram pixel, field side, carrier px, crop radius, solver options)
+SERVE_MIX = [
+    ("49x256^2 -> 128^3 GP-20", 0.4, 49, 256, 0.1, 128, 70, 59.0, dict(iterations=20, solver="gp")),
+    ("49x512^2 -> 256^3 FISTA-TV 20x10", 0.4, 49, 512, 0.055, 256, 141, 65.0,
+     dict(iterations=20, solver="tv", tv_weight=TV_WEIGHT, tv_inner=TV_INNER)),
+    ("97x1024^2 -> 384^3 GP-20", 0.2, 97, 1024, 0.04125, 384, 212, 98.0, dict(iterations=20, solver="gp")),
+]
+SERVE_BUDGET = 40 << 30
+SERVE_INFLIGHT = 4
+
+
+def serve_sample(rng, kind):
+    """A seeded phantom with a random position and index step dn ~ U[0.01, 0.04]: a bead of radius
+    2.5 um for the small geometry, the nested cell (body, nucleus, vesicles) otherwise."""
+    dn = rng.uniform(0.01, 0.04)
+    dy, dx = rng.uniform(-2.0, 2.0, 2)
+    if kind == 0:
+        return [("ellipsoid", (0.0, dy, dx), (2.5, 2.5, 2.5), N_MEDIUM + dn)]
+    out = []
+    for i, (k, c, a, n) in enumerate(CELL):
+        step = (n - CELL[0][3]) if i else 0.0
+        out.append((k, (c[0], c[1] + dy, c[2] + dx), a, N_MEDIUM + dn + step))
+    return out
+
+
+def serving_setup(qh, stacks_per_geometry=2, seed=2024):
+    """Per mix entry: illuminations, geometry, background holograms and distinct request stacks."""
+    rng = np.random.default_rng(seed)
+    geos = []
+    for idx, (name, share, count, n, hpix, out, carrier, radius, opts) in enumerate(SERVE_MIX):
+        fpix = hpix * n / out
+        geom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=fpix)
+        hgeom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=hpix)
+        illum = qh.circular_scan(count, 0.9, geom)
+        c = carrier / (n * hpix)
+        stacks = []
+        for k in range(stacks_per_geometry):
+            ratio = phantom_fields(serve_sample(rng, idx), illum, n, hpix, "cuda")
+            stacks.append(qh.synthesize_holograms(ratio, illum, hgeom, carrier=(c, c), noise=NOISE,
+                                                  seed=100 * idx + k + 1))
+        bg = qh.synthesize_holograms(np.ones((count, n, n), np.complex64), illum, hgeom, carrier=(c, c), noise=NOISE,
+                                     seed=100 * idx + 99)
+        geos.append(dict(name=name, share=share, count=count, n=n, out=out, carrier=carrier, radius=radius,
+                         opts=opts, geom=geom, illum=illum, stacks=stacks, bg=bg))
+    return geos
+
+
+def serving_stream(geos, requests, rate, seed=7):
+    """(arrival seconds, geometry index, stack index) for `requests` Poisson arrivals at `rate`/s
+    with the mix's shares."""
+    rng = np.random.default_rng(seed)
+    shares = np.array([g["share"] for g in geos])
+    kinds = rng.choice(len(geos), size=requests, p=shares / shares.sum())
+    gaps = rng.exponential(1.0 / rate, size=requests)
+    t = np.cumsum(gaps) - gaps[0]
+    return [(float(t[i]), int(kinds[i]), int(rng.integers(len(geos[kinds[i]]["stacks"])))) for i in range(requests)]
+
+
+def plain_request(qh, g, bg_fields, holo):
+    """The per-call API, one call per stage, host arrays in and out (the reference's per-call
+    chain: extract_fields, field_ratio, rytov, reconstruct)."""
+    crop = dict(center=(g["carrier"], g["carrier"]), radius=g["radius"], output_size=g["out"])
+    f = qh.extract_fields(holo, **crop)
+    u = qh.rytov(qh.field_ratio(f, bg_fields))
+    return qh.reconstruct(u, g["illum"], g["geom"], **g["opts"])
+
+
+def serving_leg(qh, capi, requests, rate):
+    """Served stream vs the plain per-call path on the same arrivals. Latency = completion - arrival
+    (host clock); throughput = requests / (last completion - first arrival)."""
+    geos = serving_setup(qh)
+    stream = serving_stream(geos, requests, rate)
+    # Plain path: serial per-call API; background fields computed once per geometry (a per-call
+    # user would cache them too).
+    bgf = [qh.extract_fields(g["bg"], center=(g["carrier"], g["carrier"]), radius=g["radius"], output_size=g["out"])
+           for g in geos]
+    for i, g in enumerate(geos):
+        plain_request(qh, g, bgf[i], g["stacks"][0])
+    plain_out = {}
+    plain_lat = []
+    t0 = time.perf_counter()
+    for j, (arr, gi, si) in enumerate(stream):
+        now = time.perf_counter() - t0
+        if now < arr:
+            time.sleep(arr - now)
+        ri = plain_request(qh, geos[gi], bgf[gi], geos[gi]["stacks"][si])
+        plain_lat.append(1000.0 * (time.perf_counter() - t0 - arr))
+        plain_out.setdefault((gi, si), ri)
+    plain_span = time.perf_counter() - t0
+
+    served_lat = []
+    gpu_ms = []
+    worst = 0.0
+    with capi.Server(hbm_budget=SERVE_BUDGET, max_inflight=SERVE_INFLIGHT) as sv:
+        ids = []
+        for g in geos:
+            ids.append(sv.add_geometry(g["count"], g["n"], (g["carrier"], g["carrier"]), g["illum"], g["geom"],
+                                       g["bg"], radius=g["radius"], output_size=g["out"], **g["opts"]))
+        for _ in range(2):  # every workspace runs once eagerly, then is captured as a graph
+            warm = [sv.submit(ids[gi], geos[gi]["stacks"][0]) for gi in range(len(geos)) for _ in range(SERVE_INFLIGHT)]
+            for t in warm:
+                sv.wait(t)
+        tickets = [None] * len(stream)
+        t0 = time.perf_counter()
+
+        def submitter():
+            for j, (arr, gi, si) in enumerate(stream):
+                now = time.perf_counter() - t0
+                if now < arr:
+                    time.sleep(arr - now)
+                start = time.perf_counter() - t0
+                tickets[j] = (sv.submit(ids[gi], geos[gi]["stacks"][si]), start)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        done_at = 0.0
+        for j, (arr, gi, si) in enumerate(stream):
+            while tickets[j] is None:
+                time.sleep(0.0002)
+            ri, _, times = sv.wait(tickets[j][0])
+            done_at = max(done_at, tickets[j][1] + times["total"] / 1000.0)
+            served_lat.append(1000.0 * (tickets[j][1] - arr) + times["total"])
+            gpu_ms.append(times["gpu"])
+            ref = plain_out[(gi, si)]
+            worst = max(worst, float(np.linalg.norm(ri.astype(np.float64) - ref) /
+                                     np.linalg.norm(ref.astype(np.float64) - N_MEDIUM)))
+        th.join()
+        stats = sv.stats()
+    served_span = done_at
+    sl, pl = sorted(served_lat), sorted(plain_lat)
+    served_v = requests / served_span
+    plain_v = requests / plain_span
+    counts = {g["name"]: sum(1 for _, gi, _ in stream if gi == i) for i, g in enumerate(geos)}
+    return {
+        "value": round(served_v, 3), "unit": UNIT, "p50_ms": round(statistics.median(sl), 2),
+        "p99_ms": round(percentile(sl, 0.99), 2),
+        "plain": {"value": round(plain_v, 3), "unit": UNIT, "p50_ms": round(statistics.median(pl), 2),
+                  "p99_ms": round(percentile(pl, 0.99), 2),
+                  "path": "per-call API (extract_fields, field_ratio, rytov, reconstruct) serially, numpy in/out"},
+        "speedup": round(served_v / plain_v, 3),
+        "path": "qoraholo_b200.capi.Server (submit/wait from Python, numpy in/out), host clock",
+        "requests": requests, "arrival_rate_per_s": rate, "mix": counts,
+        "hbm_budget_bytes": SERVE_BUDGET, "max_inflight": SERVE_INFLIGHT,
+        "max_rel_err_served_vs_plain": worst, "gpu_ms_mean": round(float(np.mean(gpu_ms)), 3),
+        "server": {k: stats[k] for k in ("workspaces_created", "workspaces_evicted", "graph_launches",
+                                          "passed_over", "peak_used", "peak_inflight")},
+    }
+
+
 def kernel_case(name, reps):
     """Small standalone launches of one kernel family for profiling (no JSON line): `fgp` runs the
     TV proximal step at 256^3 (10 FGP steps + final primal per rep); `fft` a 256^3 rfft3 + irfft3
@@ -385,14 +541,23 @@ def kernel_case(name, reps):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", choices=["fgp", "fft", "pipeline"], default=None,
+    ap.add_argument("--kernel-case", choices=["fgp", "fft", "pipeline", "serve"], default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--serve-requests", type=int, default=120, help="requests in the served / plain stream")
+    ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of that stream, per s")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving comparison")
     args = ap.parse_args()
+    if args.kernel_case == "serve":
+        import qoraholo_b200 as qh
+        from qoraholo_b200 import capi
+
+        print(json.dumps(serving_leg(qh, capi, args.serve_requests, args.serve_rate)))
+        return 0
     if args.kernel_case:
         return kernel_case(args.kernel_case, args.reps)
     if args.impl == "reference":
@@ -464,6 +629,13 @@ def main():
 
     roof = fgp_roofline(torch, capi, stream)
 
+    served = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        try:
+            served = serving_leg(qh, capi, args.serve_requests, args.serve_rate)
+        except Exception as e:  # noqa: BLE001
+            served = {"value": None, "error": f"{type(e).__name__}: {e}"}
+
     cpu = None
     parity = None
     if rank == 0 and world == 1:
@@ -495,7 +667,7 @@ def main():
                        "tv_weight": TV_WEIGHT, "parallelism": f"replicas{world}",
                        "l2": "flushed (256 MiB write) before every timed step; inputs resident in HBM"},
             "latency_ms": {"p50": round(statistics.median(lat), 3), "p99": round(p99, 3), "path": "plain device pipeline"},
-            "served": None,
+            "served": served,
             "roofline": roof,
             "cpu_baseline": cpu,
             "rel_err_vs_reference_cpu": parity,

@@ -195,6 +195,64 @@ int qhk_pipeline_shape(const qhk_pipeline* pipeline, int* nz, int* ny, int* nx);
 size_t qhk_pipeline_device_bytes(const qhk_pipeline* pipeline);
 int qhk_pipeline_destroy(qhk_pipeline* pipeline);
 
+/* ---- Serving loop (no counterpart in the reference; its nearest form is one Pipeline per geometry,
+ * src/cuda/pipeline.cu:12-147, used by one caller at a time). One scheduler thread per server admits
+ * reconstruction requests of registered geometries as execution slots and device memory free up
+ * (continuous batching against `hbm_budget_bytes`), keeps each geometry's background fields resident,
+ * reuses per-geometry workspaces, runs requests of different workspaces concurrently on their own
+ * streams and replays each workspace's pipeline as a CUDA graph from its second request on
+ * (`use_graphs`). A request's result is bitwise the same alone and in any mix. Thread-safe: submit
+ * and wait may be called from any threads. */
+typedef struct qhk_server qhk_server;
+
+/* Host timings of one request, milliseconds. */
+typedef struct qhk_request_times {
+  double queue_ms;    /* submit -> admitted */
+  double service_ms;  /* admitted -> completion seen by the host */
+  double total_ms;    /* submit -> completion seen by the host */
+  double gpu_ms;      /* device time of the request (its copies and kernels) */
+} qhk_request_times;
+
+typedef struct qhk_server_counters {
+  uint64_t submitted, completed, failed;
+  uint64_t workspaces_created, workspaces_evicted, graph_launches, passed_over;
+  size_t budget, used, peak_used;
+  int geometries, inflight, peak_inflight;
+} qhk_server_counters;
+
+int qhk_server_create(qhk_server** server, size_t hbm_budget_bytes, int max_inflight, int use_graphs);
+/* Registers a geometry, validated as qhk_pipeline_create (`upload_chunks` is ignored), with its
+ * background holograms (count, N, N) on the host. Synchronous. QHK_INVALID_ARGUMENT when its
+ * background fields plus one workspace cannot fit the budget. */
+int qhk_server_add_geometry(qhk_server* server, const qhk_pipeline_options* options, const float* illum_fyfx,
+                            const qhk_geometry* geometry, const float* backgrounds, int* geometry_id);
+/* QHK_LOGIC_ERROR while requests of the geometry are queued or running. */
+int qhk_server_remove_geometry(qhk_server* server, int geometry_id);
+int qhk_server_volume_shape(qhk_server* server, int geometry_id, int* nz, int* n);
+/* Queues holograms (count, N, N) float32 -> index (nz, n, n) float32 into `index_out`. Host buffers,
+ * pageable (staged by the calling thread) or page-locked (copied directly); `index_out` must stay
+ * valid until qhk_server_wait returns. */
+int qhk_server_submit(qhk_server* server, int geometry_id, const float* holograms, float* index_out,
+                      uint64_t* ticket);
+/* *done = 1 once the request has completed. */
+int qhk_server_done(qhk_server* server, uint64_t ticket, int* done);
+/* Blocks until the request is done; `filled` and `times` may be NULL. Returns the request's error. */
+int qhk_server_wait(qhk_server* server, uint64_t ticket, double* filled, qhk_request_times* times);
+int qhk_server_stats(qhk_server* server, qhk_server_counters* stats);
+/* Drains running requests (queued ones fail with QHK_LOGIC_ERROR) and frees everything. */
+int qhk_server_destroy(qhk_server* server);
+
+/* The server's admission policy run on the host alone, for tests and capacity planning (no device
+ * work). Geometries g = 0..n_geometries-1 hold resident[g] bytes and workspace[g] bytes per workspace
+ * (one workspace each is created at registration). ops: g >= 0 submits a request of geometry g; -1
+ * completes the oldest running request. After every op as many requests as possible are admitted;
+ * each admission appends the request's submission index to admitted[], its action to action[] (0
+ * reuse, 1 allocate, 2 allocate after evicting idle workspaces) and the budget in use after it to
+ * used[] (arrays of n_ops entries). *n_admitted receives the count. */
+int qhk_admission_simulate(size_t budget, int max_inflight, int max_pass, int n_geometries, const size_t* resident,
+                           const size_t* workspace, const int* ops, int n_ops, int* admitted, int* action,
+                           size_t* used, int* n_admitted);
+
 /* ---- Beam propagation: replaces cuda::bpm_forward / bpm_vjp / bpm_reconstruct (src/backends.hpp:117-124,
  * src/cuda/bpm.cu:236-349), tables as bpm_tables (src/bpm.cpp:10-60). Host in / host out. */
 /* ri: (nz, n, n) refractive index -> out: (count, n, n) complex64 field ratios at z = 0. */

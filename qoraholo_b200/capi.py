@@ -51,6 +51,19 @@ class PipelineTimings(C.Structure):
     _fields_ = [(name, C.c_double) for name in TIMING_NAMES]
 
 
+class RequestTimes(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("service_ms", C.c_double), ("total_ms", C.c_double),
+                ("gpu_ms", C.c_double)]
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("workspaces_created", C.c_uint64), ("workspaces_evicted", C.c_uint64),
+                ("graph_launches", C.c_uint64), ("passed_over", C.c_uint64), ("budget", C.c_size_t),
+                ("used", C.c_size_t), ("peak_used", C.c_size_t), ("geometries", C.c_int), ("inflight", C.c_int),
+                ("peak_inflight", C.c_int)]
+
+
 _VP = C.c_void_p
 _I = C.c_int
 _F = C.c_float
@@ -85,6 +98,16 @@ _PROTOS = {
     "qhk_pipeline_shape": (_I, [_VP, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "qhk_pipeline_device_bytes": (C.c_size_t, [_VP]),
     "qhk_pipeline_destroy": (_I, [_VP]),
+    "qhk_server_create": (_I, [C.POINTER(_VP), C.c_size_t, _I, _I]),
+    "qhk_server_add_geometry": (_I, [_VP, _VP, _VP, C.POINTER(Geometry), _VP, C.POINTER(_I)]),
+    "qhk_server_remove_geometry": (_I, [_VP, _I]),
+    "qhk_server_volume_shape": (_I, [_VP, _I, C.POINTER(_I), C.POINTER(_I)]),
+    "qhk_server_submit": (_I, [_VP, _I, _VP, _VP, C.POINTER(C.c_uint64)]),
+    "qhk_server_done": (_I, [_VP, C.c_uint64, C.POINTER(_I)]),
+    "qhk_server_wait": (_I, [_VP, C.c_uint64, C.POINTER(C.c_double), C.POINTER(RequestTimes)]),
+    "qhk_server_stats": (_I, [_VP, C.POINTER(ServerCounters)]),
+    "qhk_server_destroy": (_I, [_VP]),
+    "qhk_admission_simulate": (_I, [C.c_size_t, _I, _I, _I, _VP, _VP, _VP, _I, _VP, _VP, _VP, C.POINTER(_I)]),
 }
 
 
@@ -287,3 +310,117 @@ class Pipeline:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """qhk_server_*: the serving loop. Register geometries (resident background fields and plans),
+    then submit hologram stacks from any thread and wait for their index volumes. Requests are
+    admitted as execution slots and device memory (``hbm_budget`` bytes) free up, and run
+    concurrently on the GPU; each result is the same as that request run alone."""
+
+    def __init__(self, hbm_budget=40 << 30, max_inflight=4, use_graphs=True):
+        self._h = _VP()
+        check(lib().qhk_server_create(C.byref(self._h), int(hbm_budget), int(max_inflight), int(bool(use_graphs))))
+        self._shapes = {}
+        self._inputs = {}
+        self._live = {}
+
+    def add_geometry(self, count, hologram_size, center, illuminations, geom, backgrounds, radius=0.0,
+                     output_size=0, **odt):
+        """Registers a geometry (validated like Pipeline) with its background holograms
+        (count, N, N); returns its id."""
+        il = np.ascontiguousarray(np.reshape(illuminations, (-1, 2)), np.float32)
+        o = PipelineOptions(int(count), int(hologram_size), float(center[0]), float(center[1]), float(radius),
+                            int(output_size), 1, odt_options(**odt))
+        bg = np.ascontiguousarray(backgrounds, np.float32)
+        if bg.shape != (int(count), int(hologram_size), int(hologram_size)):
+            raise ValueError("Server: backgrounds must be (count, N, N)")
+        gid = _I()
+        check(lib().qhk_server_add_geometry(self._h, C.byref(o), host_ptr(il), C.byref(geometry(geom)), host_ptr(bg),
+                                            C.byref(gid)))
+        nz, n = _I(), _I()
+        check(lib().qhk_server_volume_shape(self._h, gid.value, C.byref(nz), C.byref(n)))
+        self._shapes[gid.value] = ((int(count), int(hologram_size), int(hologram_size)), (nz.value, n.value, n.value))
+        return gid.value
+
+    def remove_geometry(self, gid):
+        check(lib().qhk_server_remove_geometry(self._h, int(gid)))
+        self._shapes.pop(int(gid), None)
+
+    def volume_shape(self, gid):
+        return self._shapes[int(gid)][1]
+
+    def submit(self, gid, holograms, out=None):
+        """Queues one stack (count, N, N) float32; returns a ticket. `out` (optional) is a float32
+        array of the volume's shape to write into; both arrays are kept alive until wait()."""
+        in_shape, vol_shape = self._shapes[int(gid)]
+        h = np.ascontiguousarray(holograms, np.float32)
+        if h.shape != in_shape:
+            raise ValueError(f"Server: holograms must be {in_shape}")
+        if out is None:
+            out = np.empty(vol_shape, np.float32)
+        elif out.shape != vol_shape or out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"Server: out must be a C-contiguous float32 array of shape {vol_shape}")
+        t = C.c_uint64()
+        check(lib().qhk_server_submit(self._h, int(gid), host_ptr(h), host_ptr(out), C.byref(t)))
+        self._live[t.value] = (h, out)
+        return t.value
+
+    def done(self, ticket):
+        d = _I()
+        check(lib().qhk_server_done(self._h, int(ticket), C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket):
+        """Blocks until the request is done: (index volume, filled fraction, timings dict in ms)."""
+        filled = C.c_double()
+        t = RequestTimes()
+        try:
+            check(lib().qhk_server_wait(self._h, int(ticket), C.byref(filled), C.byref(t)))
+        finally:
+            arrays = self._live.pop(int(ticket), None)
+        times = {"queue": t.queue_ms, "service": t.service_ms, "total": t.total_ms, "gpu": t.gpu_ms}
+        return arrays[1], filled.value, times
+
+    def stats(self):
+        c = ServerCounters()
+        check(lib().qhk_server_stats(self._h, C.byref(c)))
+        return {name: getattr(c, name) for name, _ in ServerCounters._fields_}
+
+    def close(self):
+        if self._h:
+            check(lib().qhk_server_destroy(self._h))
+            self._h = _VP()
+        self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def admission_simulate(budget, max_inflight, max_pass, resident, workspace, ops):
+    """The serving loop's admission policy on the host alone (no device work): returns a list of
+    (submission index, action, bytes in use) per admission, action 0 reuse, 1 allocate, 2 allocate
+    after evicting idle workspaces. ops: geometry id to submit, or -1 to complete the oldest
+    running request."""
+    res = np.ascontiguousarray(resident, np.uint64)
+    ws = np.ascontiguousarray(workspace, np.uint64)
+    o = np.ascontiguousarray(ops, np.int32)
+    n = max(len(o), 1)
+    admitted = np.zeros(n, np.int32)
+    action = np.zeros(n, np.int32)
+    used = np.zeros(n, np.uint64)
+    count = _I()
+    check(lib().qhk_admission_simulate(int(budget), int(max_inflight), int(max_pass), len(res), host_ptr(res),
+                                       host_ptr(ws), host_ptr(o), len(o), host_ptr(admitted), host_ptr(action),
+                                       host_ptr(used), C.byref(count)))
+    k = count.value
+    return [(int(admitted[i]), int(action[i]), int(used[i])) for i in range(k)]

@@ -8,12 +8,14 @@
 
 #include "../../include/qoraholo_b200.h"
 #include <complex>
+#include <deque>
 #include <vector>
 
 #include "bpm.hpp"
 #include "field.hpp"
 #include "odt.hpp"
 #include "pipeline.hpp"
+#include "server.hpp"
 #include "unwrap.hpp"
 
 namespace {
@@ -567,6 +569,127 @@ int qhk_bpm_reconstruct(const void* fields, int count, int n, const float* illum
     }
     qhk::check(cudaStreamSynchronize(s), "bpm_reconstruct");
     for (int i = 0; i < o->iterations; ++i) loss[i] *= 0.5 / count;
+  });
+}
+
+
+struct qhk_server {
+  qhk::Server server;
+};
+
+int qhk_server_create(qhk_server** server, size_t hbm_budget_bytes, int max_inflight, int use_graphs) {
+  return guard([&] {
+    qhk::require(server != nullptr, "Server: null argument");
+    *server = new qhk_server{qhk::Server(hbm_budget_bytes, max_inflight, use_graphs != 0)};
+  });
+}
+
+int qhk_server_add_geometry(qhk_server* sv, const qhk_pipeline_options* o, const float* illum_fyfx,
+                            const qhk_geometry* geometry, const float* backgrounds, int* geometry_id) {
+  return guard([&] {
+    qhk::require(sv && o && backgrounds && geometry_id, "Server: null argument");
+    const int n = o->hologram_size;
+    qhk::require(o->count >= 1, "Server: count must be positive");
+    qhk::require(n >= 4 && n % 2 == 0, "Server: hologram_size must be even");
+    const qhk::CropPlan crop = qhk::make_crop(n, o->center_y, o->center_x, o->radius, o->output_size);
+    const qhk::OdtConfig c = odt_config(crop.out, o->count, illum_fyfx, geometry, &o->odt);
+    *geometry_id = sv->server.add_geometry(crop, o->count, c, illum_fyfx, backgrounds);
+  });
+}
+
+int qhk_server_remove_geometry(qhk_server* sv, int geometry_id) {
+  return guard([&] {
+    qhk::require(sv != nullptr, "Server: null server");
+    sv->server.remove_geometry(geometry_id);
+  });
+}
+
+int qhk_server_volume_shape(qhk_server* sv, int geometry_id, int* nz, int* n) {
+  return guard([&] {
+    qhk::require(sv && nz && n, "Server: null argument");
+    sv->server.volume_shape(geometry_id, nz, n);
+  });
+}
+
+int qhk_server_submit(qhk_server* sv, int geometry_id, const float* holograms, float* index_out, uint64_t* ticket) {
+  return guard([&] {
+    qhk::require(sv && ticket, "Server: null argument");
+    *ticket = sv->server.submit(geometry_id, holograms, index_out);
+  });
+}
+
+int qhk_server_done(qhk_server* sv, uint64_t ticket, int* done) {
+  return guard([&] {
+    qhk::require(sv && done, "Server: null argument");
+    *done = sv->server.done(ticket) ? 1 : 0;
+  });
+}
+
+int qhk_server_wait(qhk_server* sv, uint64_t ticket, double* filled, qhk_request_times* times) {
+  return guard([&] {
+    qhk::require(sv != nullptr, "Server: null server");
+    qhk::RequestTimes t;
+    sv->server.wait(ticket, filled, &t);
+    if (times) *times = qhk_request_times{t.queue, t.service, t.total, t.gpu};
+  });
+}
+
+int qhk_server_stats(qhk_server* sv, qhk_server_counters* out) {
+  return guard([&] {
+    qhk::require(sv && out, "Server: null argument");
+    const qhk::ServerStats s = sv->server.stats();
+    *out = qhk_server_counters{s.submitted, s.completed, s.failed, s.workspaces_created, s.workspaces_evicted,
+                            s.graph_launches, s.passed_over, s.budget, s.used, s.peak_used, s.geometries,
+                            s.inflight, s.peak_inflight};
+  });
+}
+
+int qhk_server_destroy(qhk_server* sv) {
+  return guard([&] { delete sv; });
+}
+
+int qhk_admission_simulate(size_t budget, int max_inflight, int max_pass, int n_geometries, const size_t* resident,
+                           const size_t* workspace, const int* ops, int n_ops, int* admitted, int* action,
+                           size_t* used, int* n_admitted) {
+  return guard([&] {
+    qhk::require(n_geometries >= 1 && resident && workspace && n_admitted && (n_ops == 0 || ops),
+                 "admission: null argument");
+    qhk::require(n_ops == 0 || (admitted && action && used), "admission: null output");
+    qhk::Admission a(budget, max_inflight, max_pass);
+    int next_ws = 0;
+    for (int g = 0; g < n_geometries; ++g) {
+      qhk::require(a.add_geometry(resident[g], workspace[g]) == g, "admission: geometry does not fit the budget");
+      (void)a.make_room(workspace[g]);
+      a.add_idle(g, next_ws++);
+    }
+    std::deque<std::pair<int, int>> pending;  // (submission index, geometry)
+    std::deque<int> running;                  // workspaces, oldest first
+    int submitted = 0, count = 0;
+    for (int k = 0; k < n_ops; ++k) {
+      if (ops[k] >= 0) {
+        qhk::require(ops[k] < n_geometries, "admission: unknown geometry in ops");
+        pending.emplace_back(submitted++, ops[k]);
+      } else if (!running.empty()) {
+        a.release(running.front());
+        running.pop_front();
+      }
+      for (;;) {
+        std::vector<int> order;
+        for (const auto& p : pending) order.push_back(p.second);
+        const auto d = a.choose(order);
+        if (!d) break;
+        const int wid = d->action == qhk::Admission::Action::reuse ? d->workspace : next_ws++;
+        a.commit(*d, wid);
+        qhk::require(count < n_ops, "admission: more admissions than ops");
+        admitted[count] = pending[d->position].first;
+        action[count] = d->action == qhk::Admission::Action::reuse ? 0 : (d->evict.empty() ? 1 : 2);
+        used[count] = a.used();
+        ++count;
+        pending.erase(pending.begin() + static_cast<std::ptrdiff_t>(d->position));
+        running.push_back(wid);
+      }
+    }
+    *n_admitted = count;
   });
 }
 

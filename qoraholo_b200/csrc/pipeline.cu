@@ -24,7 +24,7 @@ int checked_chunk(int count, int upload_chunks) {
 }  // namespace
 
 PipelinePlan::PipelinePlan(const CropPlan& crop, int count, int upload_chunks, const OdtConfig& odt,
-                           const float* illum_fyfx)
+                           const float* illum_fyfx, bool own_io)
     : crop_(crop),
       count_(count),
       chunk_(checked_chunk(count, upload_chunks)),
@@ -36,11 +36,13 @@ PipelinePlan::PipelinePlan(const CropPlan& crop, int count, int upload_chunks, c
   require(odt.grid.n == crop.out, "Pipeline: volume side must equal the field side");
   const std::size_t image = static_cast<std::size_t>(crop.n) * crop.n;
   const std::size_t field = static_cast<std::size_t>(count) * crop.out * crop.out;
-  input_ = PinnedBuf<float>(count * image);
-  output_ = PinnedBuf<float>(odt_.volume());
-  filled_host_ = PinnedBuf<unsigned long long>(1);
+  if (own_io) {
+    input_ = PinnedBuf<float>(count * image);
+    output_ = PinnedBuf<float>(odt_.volume());
+    filled_host_ = PinnedBuf<unsigned long long>(1);
+    background_.reset(field);
+  }
   holo_.reset(count * image);
-  background_.reset(field);
   fields_.reset(field);
   psi_.reset(field);
   logamp_.reset(field);
@@ -55,6 +57,7 @@ std::size_t PipelinePlan::device_bytes() const {
 }
 
 void PipelinePlan::set_background(const float* host_bg) {
+  require(background_.get() != nullptr, "Pipeline: serving workspaces take their background fields per call");
   const cudaStream_t s = compute_.get();
   const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
   check(cudaMemcpyAsync(holo_.get(), host_bg, count_ * image * sizeof(float), cudaMemcpyHostToDevice, s),
@@ -65,9 +68,19 @@ void PipelinePlan::set_background(const float* host_bg) {
   has_background_ = true;
 }
 
-void PipelinePlan::compute(const float* d_holo, bool chunked_upload, float* d_index, cudaStream_t s) {
+void PipelinePlan::enqueue_background(const float* d_bg_holo, float2* bg_out, cudaStream_t s) {
+  field_.spectra(d_bg_holo, 0, count_, s);
+  field_.finish(0, bg_out, nullptr, nullptr, nullptr, s);
+}
+
+void PipelinePlan::enqueue(const float* d_holo, const float2* bg, float* d_index, cudaStream_t s) {
+  compute(d_holo, false, bg, d_index, s, false);
+}
+
+void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float2* bg, float* d_index, cudaStream_t s,
+                           bool marks) {
   const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
-  clock_.mark(kStart, s);
+  if (marks) clock_.mark(kStart, s);
   if (chunked_upload) {
     const cudaStream_t c = copy_.get();
     check(cudaStreamWaitEvent(c, clock_.event(kStart), 0), "cudaStreamWaitEvent");
@@ -84,18 +97,22 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, float* d_in
   } else {
     field_.spectra(d_holo, 0, count_, s);
   }
-  field_.finish(1, nullptr, background_.get(), psi_.get(), logamp_.get(), s);
-  clock_.mark(kFields, s);
+  field_.finish(1, nullptr, bg, psi_.get(), logamp_.get(), s);
+  if (marks) clock_.mark(kFields, s);
   unwrap_.rytov(psi_.get(), logamp_.get(), phi_.get(), fields_.get(), s);
-  clock_.mark(kRytov, s);
-  odt_.run_marked(fields_.get(), d_index, s, &clock_, kRytov + 1);
+  if (marks) clock_.mark(kRytov, s);
+  if (marks) {
+    odt_.run_marked(fields_.get(), d_index, s, &clock_, kRytov + 1);
+  } else {
+    odt_.run(fields_.get(), d_index, s);
+  }
 }
 
 void PipelinePlan::process() {
   if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
   const auto t0 = std::chrono::steady_clock::now();
   const cudaStream_t s = compute_.get();
-  compute(nullptr, true, index_.get(), s);
+  compute(nullptr, true, background_.get(), index_.get(), s, true);
   check(cudaMemcpyAsync(output_.get(), index_.get(), odt_.volume() * sizeof(float), cudaMemcpyDeviceToHost, s),
         "download index");
   check(cudaMemcpyAsync(filled_host_.get(), odt_.filled(), sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
@@ -119,7 +136,7 @@ void PipelinePlan::process() {
 
 void PipelinePlan::process_device(const float* d_holo, float* d_index, cudaStream_t s) {
   if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
-  compute(d_holo, false, d_index, s);
+  compute(d_holo, false, background_.get(), d_index, s, true);
 }
 
 }  // namespace qhk

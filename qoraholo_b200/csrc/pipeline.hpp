@@ -15,7 +15,11 @@ struct PipelineTimes {
 
 class PipelinePlan {
  public:
-  PipelinePlan(const CropPlan& crop, int count, int upload_chunks, const OdtConfig& odt, const float* illum_fyfx);
+  // `own_io`: allocate the page-locked input / output buffers and the resident background fields
+  // (the Pipeline form). Without them the plan is a serving workspace: device buffers only, with the
+  // background fields passed to enqueue().
+  PipelinePlan(const CropPlan& crop, int count, int upload_chunks, const OdtConfig& odt, const float* illum_fyfx,
+               bool own_io = true);
 
   // Background holograms (count, N, N) on the host; their fields stay on the device.
   void set_background(const float* host_bg);
@@ -27,6 +31,21 @@ class PipelinePlan {
   // Holograms already on the device -> index on the device, asynchronous on `s` (no host copies).
   void process_device(const float* d_holo, float* d_index, cudaStream_t s);
 
+  // Serving-workspace forms, asynchronous on `s`, no stage marks (so they can be graph-captured):
+  // background holograms (device) -> demodulated background fields `bg_out` (count, m, m); and
+  // holograms (device) -> index (device) against background fields `bg`. The filled-voxel count of
+  // the last enqueue is odt().filled().
+  void enqueue_background(const float* d_bg_holo, float2* bg_out, cudaStream_t s);
+  void enqueue(const float* d_holo, const float2* bg, float* d_index, cudaStream_t s);
+  // The plan's own stream, and the device buffers the serving loop copies into / out of.
+  [[nodiscard]] cudaStream_t stream() const { return compute_.get(); }
+  [[nodiscard]] float* holo_buffer() const { return holo_.get(); }
+  [[nodiscard]] float* index_buffer() const { return index_.get(); }
+  [[nodiscard]] std::size_t hologram_floats() const {
+    return static_cast<std::size_t>(count_) * crop_.n * crop_.n;
+  }
+  [[nodiscard]] std::size_t field_elems() const { return static_cast<std::size_t>(count_) * crop_.out * crop_.out; }
+
   [[nodiscard]] double filled() const { return filled_; }
   [[nodiscard]] const PipelineTimes& timings() const { return timings_; }
   [[nodiscard]] std::size_t device_bytes() const;
@@ -37,7 +56,8 @@ class PipelinePlan {
 
  private:
   enum { kStart, kFields, kRytov, kDownloaded = kRytov + 1 + OdtPlan::kMarks, kMarks };
-  void compute(const float* d_holo, bool chunked_upload, float* d_index, cudaStream_t s);
+  void compute(const float* d_holo, bool chunked_upload, const float2* bg, float* d_index, cudaStream_t s,
+               bool marks);
 
   CropPlan crop_;
   int count_;
