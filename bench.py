@@ -411,7 +411,7 @@ def plain_request(qh, g, bg_fields, holo):
     return qh.reconstruct(u, g["illum"], g["geom"], **g["opts"])
 
 
-def serving_leg(qh, capi, requests, rate):
+def serving_leg(qh, capi, requests, rate, inflight=SERVE_INFLIGHT, plain=True):
     """Served stream vs the plain per-call path on the same arrivals. Latency = completion - arrival
     (host clock); throughput = requests / (last completion - first arrival)."""
     geos = serving_setup(qh)
@@ -425,7 +425,7 @@ def serving_leg(qh, capi, requests, rate):
     plain_out = {}
     plain_lat = []
     t0 = time.perf_counter()
-    for j, (arr, gi, si) in enumerate(stream):
+    for j, (arr, gi, si) in enumerate(stream if plain else []):
         now = time.perf_counter() - t0
         if now < arr:
             time.sleep(arr - now)
@@ -437,15 +437,18 @@ def serving_leg(qh, capi, requests, rate):
     served_lat = []
     gpu_ms = []
     worst = 0.0
-    with capi.Server(hbm_budget=SERVE_BUDGET, max_inflight=SERVE_INFLIGHT) as sv:
+    with capi.Server(hbm_budget=SERVE_BUDGET, max_inflight=inflight) as sv:
         ids = []
         for g in geos:
             ids.append(sv.add_geometry(g["count"], g["n"], (g["carrier"], g["carrier"]), g["illum"], g["geom"],
                                        g["bg"], radius=g["radius"], output_size=g["out"], **g["opts"]))
         for _ in range(2):  # every workspace runs once eagerly, then is captured as a graph
-            warm = [sv.submit(ids[gi], geos[gi]["stacks"][0]) for gi in range(len(geos)) for _ in range(SERVE_INFLIGHT)]
+            warm = [sv.submit(ids[gi], geos[gi]["stacks"][0]) for gi in range(len(geos)) for _ in range(inflight)]
             for t in warm:
                 sv.wait(t)
+        alone_ms = []
+        for gi in range(len(geos)):  # each geometry alone on an idle device: its service time
+            alone_ms.append(sv.wait(sv.submit(ids[gi], geos[gi]["stacks"][0]))[2]["gpu"])
         tickets = [None] * len(stream)
         t0 = time.perf_counter()
 
@@ -467,15 +470,16 @@ def serving_leg(qh, capi, requests, rate):
             done_at = max(done_at, tickets[j][1] + times["total"] / 1000.0)
             served_lat.append(1000.0 * (tickets[j][1] - arr) + times["total"])
             gpu_ms.append(times["gpu"])
-            ref = plain_out[(gi, si)]
-            worst = max(worst, float(np.linalg.norm(ri.astype(np.float64) - ref) /
-                                     np.linalg.norm(ref.astype(np.float64) - N_MEDIUM)))
+            ref = plain_out.get((gi, si))
+            if ref is not None:
+                worst = max(worst, float(np.linalg.norm(ri.astype(np.float64) - ref) /
+                                         np.linalg.norm(ref.astype(np.float64) - N_MEDIUM)))
         th.join()
         stats = sv.stats()
     served_span = done_at
-    sl, pl = sorted(served_lat), sorted(plain_lat)
+    sl, pl = sorted(served_lat), sorted(plain_lat) or [float("nan")]
     served_v = requests / served_span
-    plain_v = requests / plain_span
+    plain_v = requests / plain_span if plain else float("nan")
     counts = {g["name"]: sum(1 for _, gi, _ in stream if gi == i) for i, g in enumerate(geos)}
     return {
         "value": round(served_v, 3), "unit": UNIT, "p50_ms": round(statistics.median(sl), 2),
@@ -486,8 +490,10 @@ def serving_leg(qh, capi, requests, rate):
         "speedup": round(served_v / plain_v, 3),
         "path": "qoraholo_b200.capi.Server (submit/wait from Python, numpy in/out), host clock",
         "requests": requests, "arrival_rate_per_s": rate, "mix": counts,
-        "hbm_budget_bytes": SERVE_BUDGET, "max_inflight": SERVE_INFLIGHT,
+        "hbm_budget_bytes": SERVE_BUDGET, "max_inflight": inflight,
         "max_rel_err_served_vs_plain": worst, "gpu_ms_mean": round(float(np.mean(gpu_ms)), 3),
+        "alone_gpu_ms": {g["name"]: round(alone_ms[i], 3) for i, g in enumerate(geos)},
+        "serial_gpu_bound": round(1000.0 / sum(g["share"] * alone_ms[i] for i, g in enumerate(geos)), 3),
         "server": {k: stats[k] for k in ("workspaces_created", "workspaces_evicted", "graph_launches",
                                           "passed_over", "peak_used", "peak_inflight")},
     }
@@ -548,15 +554,18 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--serve-requests", type=int, default=120, help="requests in the served / plain stream")
+    ap.add_argument("--serve-requests", type=int, default=80, help="requests in the served / plain stream")
+    ap.add_argument("--serve-no-plain", action="store_true", help="with --kernel-case serve: served stream only")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of that stream, per s")
+    ap.add_argument("--serve-inflight", type=int, default=SERVE_INFLIGHT, help="concurrent requests of the server")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving comparison")
     args = ap.parse_args()
     if args.kernel_case == "serve":
         import qoraholo_b200 as qh
         from qoraholo_b200 import capi
 
-        print(json.dumps(serving_leg(qh, capi, args.serve_requests, args.serve_rate)))
+        print(json.dumps(serving_leg(qh, capi, args.serve_requests, args.serve_rate, args.serve_inflight,
+                                     plain=not args.serve_no_plain)))
         return 0
     if args.kernel_case:
         return kernel_case(args.kernel_case, args.reps)
@@ -632,7 +641,7 @@ def main():
     served = None
     if rank == 0 and world == 1 and not args.no_serve:
         try:
-            served = serving_leg(qh, capi, args.serve_requests, args.serve_rate)
+            served = serving_leg(qh, capi, args.serve_requests, args.serve_rate, args.serve_inflight)
         except Exception as e:  # noqa: BLE001
             served = {"value": None, "error": f"{type(e).__name__}: {e}"}
 

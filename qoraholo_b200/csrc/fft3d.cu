@@ -65,6 +65,7 @@ void allow_smem(K kernel, std::size_t) {
 }
 
 constexpr int kThreads = 256;
+constexpr int kBatch = 8;  // loads in flight per thread in the strided passes
 
 // ---- axis passes ------------------------------------------------------------------------------
 
@@ -85,15 +86,28 @@ __global__ void __launch_bounds__(kThreads)
   constexpr int kHalf = static_cast<int>(AxisMode::restore_half);
   constexpr int kMask = static_cast<int>(AxisMode::restore_mask);
 
-  for (int idx = tid; idx < n * COLS; idx += nth) {
-    const int pos = idx / COLS;
-    const int col = idx - pos * COLS;
-    float2 v = make_float2(0.0f, 0.0f);
-    if (col < cols) {
-      const std::size_t g = base + pos * sp + col;
-      v = Mode == kFrom ? cscale(aux_a[g], scale) : data[g];
+  // Loads are issued kBatch at a time per thread before any is used, so that a CTA keeps
+  // kBatch * blockDim loads in flight (the columns are strided lines; a load-use loop is
+  // latency bound).
+  const int total = n * COLS;
+  for (int i0 = tid; i0 < total; i0 += nth * kBatch) {
+    float2 v[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int idx = i0 + b * nth;
+      const int pos = idx / COLS;
+      const int col = idx - pos * COLS;
+      v[b] = make_float2(0.0f, 0.0f);
+      if (idx < total && col < cols) {
+        const std::size_t g = base + pos * sp + col;
+        v[b] = Mode == kFrom ? cscale(aux_a[g], scale) : data[g];
+      }
     }
-    A[idx] = v;
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int idx = i0 + b * nth;
+      if (idx < total) A[idx] = v[b];
+    }
   }
   __syncthreads();
 
@@ -101,20 +115,38 @@ __global__ void __launch_bounds__(kThreads)
   if constexpr (Mode == kHalf || Mode == kMask) {
     res = smem_fft_cols<true, COLS>(A, B, COLS, L, tid, nth);
     float2* other = res == A ? B : A;
-    for (int idx = tid; idx < n * COLS; idx += nth) {
-      const int pos = idx / COLS;
-      const int col = idx - pos * COLS;
-      if (col >= cols) continue;
-      const std::size_t g = base + pos * sp + col;
-      float2 v = res[idx];
-      if constexpr (Mode == kHalf) {
-        const float2 a = aux_a[g];
-        const float b = 1.0f - 0.5f * static_cast<float>(aux_h[g]);
-        v = make_float2((a.x + b * v.x) * scale, (a.y + b * v.y) * scale);
-      } else {
-        if (aux_h[g]) v = aux_a[g];
+    for (int i0 = tid; i0 < total; i0 += nth * kBatch) {
+      float2 av[kBatch];
+      std::uint8_t hv[kBatch];
+#pragma unroll
+      for (int b = 0; b < kBatch; ++b) {
+        const int idx = i0 + b * nth;
+        const int pos = idx / COLS;
+        const int col = idx - pos * COLS;
+        av[b] = make_float2(0.0f, 0.0f);
+        hv[b] = 0;
+        if (idx < total && col < cols) {
+          const std::size_t g = base + pos * sp + col;
+          av[b] = aux_a[g];
+          hv[b] = aux_h[g];
+        }
       }
-      res[idx] = v;
+#pragma unroll
+      for (int b = 0; b < kBatch; ++b) {
+        const int idx = i0 + b * nth;
+        const int pos = idx / COLS;
+        const int col = idx - pos * COLS;
+        if (idx >= total || col >= cols) continue;
+        float2 v = res[idx];
+        if constexpr (Mode == kHalf) {
+          const float2 a = av[b];
+          const float w = 1.0f - 0.5f * static_cast<float>(hv[b]);
+          v = make_float2((a.x + w * v.x) * scale, (a.y + w * v.y) * scale);
+        } else {
+          if (hv[b]) v = av[b];
+        }
+        res[idx] = v;
+      }
     }
     __syncthreads();
     res = smem_fft_cols<false, COLS>(res, other, COLS, L, tid, nth);

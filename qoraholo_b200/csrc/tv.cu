@@ -2,13 +2,15 @@
 // the FISTA-TV reconstruction (it follows the reference's tv_prox, src/cuda/tv.cu:256-293, and
 // its CPU form src/cpu/tv.cpp:7-44, with the per-voxel math of src/common.hpp:107-153).
 //
-// One FGP step is one kernel. A CTA owns TY full rows (all x) of a y-slab and marches along z
-// through `zchunk` planes. Shared memory holds a three-plane ring of the input dual r (rows y0-1 ..
-// y0+TY, three components), filled by cp.async one plane ahead, and the primal point
-// z = max(b - lambda L(r), 0) for two planes (rows y0 .. y0+TY): z of plane k+1 is computed once
-// from the ring and reused as plane k of the next step, so z is never written to HBM, and each r
-// value is read from HBM once (the one-row halos come from L2). Per step the HBM traffic is b, r_in (3), p (3) read and p (3), r_out (3) written
-// -- 13 volumes; the first step reads p as r (10 volumes) and the last writes no r (10 volumes).
+// One FGP step is one kernel of exactly one wave of CTAs. The (y-tile, z) plane units -- TY full
+// rows (all x) of one plane -- are split evenly over the CTAs in y-tile-major order, and a CTA
+// marches along z through its units (one march per y-tile it touches). Shared memory holds a
+// three-plane ring of the input dual r (rows y0-1 .. y0+TY, three components), filled by cp.async
+// one plane ahead, and the primal point z = max(b - lambda L(r), 0) for two planes (rows y0 ..
+// y0+TY): z of plane k+1 is computed once from the ring and reused as plane k of the next step, so
+// z is never written to HBM, and each r value is read from HBM once (the one-row halos come from
+// L2). Per step the HBM traffic is b, r_in (3), p (3) read and p (3), r_out (3) written -- 13
+// volumes; the first step reads p as r (10 volumes) and the last writes no r (10 volumes).
 //
 // All arithmetic uses the round-to-nearest intrinsics in the reference's operation order, so the
 // device iterates are bit-identical to the CPU's.
@@ -30,7 +32,7 @@ struct FgpArgs {
   float* pout[3];
   float* rout[3];
   int nz, ny, nx;
-  int zchunk;
+  int ytiles;  // ceil(ny / TY)
   float lambda, step, momentum;
 };
 
@@ -79,11 +81,6 @@ __global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
   const int tx = static_cast<int>(threadIdx.x);
   const int ty = static_cast<int>(threadIdx.y);
   const int x0 = tx * VEC;
-  const int y0 = static_cast<int>(blockIdx.x) * TY;
-  const int z0 = static_cast<int>(blockIdx.y) * A.zchunk;
-  if (z0 >= nz) return;
-  const int z1 = min(z0 + A.zchunk, nz);
-  const int zlast = min(z1, nz - 1);  // last plane whose dual r is needed (for the primal of z1)
   const int ring_rows = TY + 2;
   const std::size_t plane_sz = static_cast<std::size_t>(3) * ring_rows * nx;
   const std::size_t zb_sz = static_cast<std::size_t>(TY + 1) * nx;
@@ -92,180 +89,191 @@ __global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
   float* Z = sm + 3 * plane_sz;  // primal of plane z in slot (z - z0) & 1
   float* Bs = Z + 2 * zb_sz;     // b of plane z in slot (z - z0) & 1
   const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
-  const auto rslot = [&](int z) { return R + static_cast<std::size_t>((z - z0 + 1) % 3) * plane_sz; };
-  const auto zslot = [&](int z) { return Z + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
-  const auto bslot = [&](int z) { return Bs + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
+  // This CTA's share of the (y-tile, z) plane units, y-tile major: an even split over a grid that
+  // is exactly one wave, walked as one z-march per y-tile it touches.
+  const long long units = static_cast<long long>(A.ytiles) * nz;
+  const long long u_end = units * (blockIdx.x + 1) / gridDim.x;
+  for (long long u = units * blockIdx.x / gridDim.x; u < u_end;) {
+    const int y0 = static_cast<int>(u / nz) * TY;
+    const int z0 = static_cast<int>(u % nz);
+    const int z1 = static_cast<int>(min(static_cast<long long>(nz), z0 + (u_end - u)));
+    u += z1 - z0;
+    const int zlast = min(z1, nz - 1);  // last plane whose dual r is needed (for the primal of z1)
+    const auto rslot = [&](int z) { return R + static_cast<std::size_t>((z - z0 + 1) % 3) * plane_sz; };
+    const auto zslot = [&](int z) { return Z + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
+    const auto bslot = [&](int z) { return Bs + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
 
-  // Rows outside the volume are never read by the arithmetic below (the boundary terms drop
-  // them), so they are not copied.
-  const auto issue_r = [&](int z, int comps) {
-    float* dst = rslot(z);
-    for (int rc = ty; rc < comps * ring_rows; rc += TY) {
-      const int c = rc / ring_rows;
-      const int rr = rc - c * ring_rows;
-      const int y = y0 - 1 + rr;
-      if (y < 0 || y >= ny) continue;
-      copy_async<VEC>(dst + (static_cast<std::size_t>(c) * ring_rows + rr) * nx + x0,
-                      A.rin[c] + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
-    }
-  };
-  const auto issue_b = [&](int z) {
-    float* dst = bslot(z);
-    for (int rr = ty; rr < TY + 1; rr += TY) {
-      const int y = y0 + rr;
-      if (y >= ny) continue;
-      copy_async<VEC>(dst + static_cast<std::size_t>(rr) * nx + x0,
-                      A.b + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
-    }
-  };
-  // z on plane z (rows y0 .. y0+TY) from r of that plane and of the plane below. Every thread runs
-  // the same number of row iterations so that all lanes reach the shuffles; with VEC = 4 a thread
-  // reads its four x values as one float4 and gets x - 1 from the lane on its left.
-  const int linear = static_cast<int>(threadIdx.y * blockDim.x + threadIdx.x);
-  const int lane = linear & 31;
-  // Lanes that exist in this thread's warp (the block's last warp may be partial).
-  const int warp_threads = min(32, static_cast<int>(blockDim.x * blockDim.y) - (linear & ~31));
-  const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
-  const auto primal = [&](int z) {
-    const float* Rc = rslot(z);
-    const float* Rb = rslot(z - 1);
-    const float* B = bslot(z);
-    float* Zd = zslot(z);
-    for (int it = 0; it < 2; ++it) {
-      const int rr = ty + it * TY;
-      const bool active = rr < TY + 1;
-      const int rrc = active ? rr : 0;
-      const int y = y0 + rrc;
-      const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
-      const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
-      const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
-      const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc) * nx;
-      const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
-      float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
-      Vec<VEC>::load(rz + x0, vz);
-      Vec<VEC>::load(rzb + x0, vzb);
-      Vec<VEC>::load(ry + x0, vy);
-      Vec<VEC>::load(rym + x0, vym);
-      Vec<VEC>::load(rx + x0, vx);
-      Vec<VEC>::load(B + static_cast<std::size_t>(rrc) * nx + x0, vb);
-      float left;
-      if constexpr (VEC == 4) {
-        const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
-        left = (x0 > 0 && lane == 0) ? rx[x0 - 1] : from_lane;
-      } else {
-        left = x0 > 0 ? rx[x0 - 1] : 0.0f;
+    // Rows outside the volume are never read by the arithmetic below (the boundary terms drop
+    // them), so they are not copied.
+    const auto issue_r = [&](int z, int comps) {
+      float* dst = rslot(z);
+      for (int rc = ty; rc < comps * ring_rows; rc += TY) {
+        const int c = rc / ring_rows;
+        const int rr = rc - c * ring_rows;
+        const int y = y0 - 1 + rr;
+        if (y < 0 || y >= ny) continue;
+        copy_async<VEC>(dst + (static_cast<std::size_t>(c) * ring_rows + rr) * nx + x0,
+                        A.rin[c] + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
       }
-      if (!active) continue;
-      float out[VEC];
-#pragma unroll
-      for (int i = 0; i < VEC; ++i) {
-        const int x = x0 + i;
-        float zv = 0.0f;
-        if (y < ny) {
-          float s = 0.0f;
-          if (z < nz - 1) s = __fadd_rn(s, vz[i]);
-          if (z > 0) s = __fsub_rn(s, vzb[i]);
-          if (y < ny - 1) s = __fadd_rn(s, vy[i]);
-          if (y > 0) s = __fsub_rn(s, vym[i]);
-          if (x < nx - 1) s = __fadd_rn(s, vx[i]);
-          if (x > 0) s = __fsub_rn(s, i == 0 ? left : vx[i > 0 ? i - 1 : 0]);
-          zv = tv_primal(vb[i], A.lambda, s);
+    };
+    const auto issue_b = [&](int z) {
+      float* dst = bslot(z);
+      for (int rr = ty; rr < TY + 1; rr += TY) {
+        const int y = y0 + rr;
+        if (y >= ny) continue;
+        copy_async<VEC>(dst + static_cast<std::size_t>(rr) * nx + x0,
+                        A.b + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
+      }
+    };
+    // z on plane z (rows y0 .. y0+TY) from r of that plane and of the plane below. Every thread runs
+    // the same number of row iterations so that all lanes reach the shuffles; with VEC = 4 a thread
+    // reads its four x values as one float4 and gets x - 1 from the lane on its left.
+    const int linear = static_cast<int>(threadIdx.y * blockDim.x + threadIdx.x);
+    const int lane = linear & 31;
+    // Lanes that exist in this thread's warp (the block's last warp may be partial).
+    const int warp_threads = min(32, static_cast<int>(blockDim.x * blockDim.y) - (linear & ~31));
+    const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
+    const auto primal = [&](int z) {
+      const float* Rc = rslot(z);
+      const float* Rb = rslot(z - 1);
+      const float* B = bslot(z);
+      float* Zd = zslot(z);
+      for (int it = 0; it < 2; ++it) {
+        const int rr = ty + it * TY;
+        const bool active = rr < TY + 1;
+        const int rrc = active ? rr : 0;
+        const int y = y0 + rrc;
+        const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc) * nx;
+        const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
+        Vec<VEC>::load(rz + x0, vz);
+        Vec<VEC>::load(rzb + x0, vzb);
+        Vec<VEC>::load(ry + x0, vy);
+        Vec<VEC>::load(rym + x0, vym);
+        Vec<VEC>::load(rx + x0, vx);
+        Vec<VEC>::load(B + static_cast<std::size_t>(rrc) * nx + x0, vb);
+        float left;
+        if constexpr (VEC == 4) {
+          const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
+          left = (x0 > 0 && lane == 0) ? rx[x0 - 1] : from_lane;
+        } else {
+          left = x0 > 0 ? rx[x0 - 1] : 0.0f;
         }
-        out[i] = zv;
-      }
-      Vec<VEC>::store(Zd + static_cast<std::size_t>(rr) * nx + x0, out);
-    }
-  };
-
-  // Prologue: planes z0 - 1 (z component only), z0 (and b) in one group, z0 + 1 in the next.
-  if (z0 > 0) issue_r(z0 - 1, 1);
-  issue_r(z0, 3);
-  issue_b(z0);
-  copy_commit();
-  const bool second = z0 + 1 <= zlast;
-  if (second) {
-    issue_r(z0 + 1, 3);
-    issue_b(z0 + 1);
-    copy_commit();
-    copy_wait<1>();
-  } else {
-    copy_wait<0>();
-  }
-  __syncthreads();
-  primal(z0);
-  __syncthreads();
-
-  const int y = y0 + ty;
-  for (int z = z0; z < z1; ++z) {
-    const bool prefetch = z + 2 <= zlast;
-    if (prefetch) {
-      issue_r(z + 2, 3);
-      issue_b(z + 2);
-      copy_commit();
-    }
-    const std::size_t at = static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0;
-    float pv[3][VEC];
-    if (!FIRST && y < ny) {
+        if (!active) continue;
+        float out[VEC];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Vec<VEC>::load(A.pin[c] + at, pv[c]);
-    }
-    if (prefetch) {
+        for (int i = 0; i < VEC; ++i) {
+          const int x = x0 + i;
+          float zv = 0.0f;
+          if (y < ny) {
+            float s = 0.0f;
+            if (z < nz - 1) s = __fadd_rn(s, vz[i]);
+            if (z > 0) s = __fsub_rn(s, vzb[i]);
+            if (y < ny - 1) s = __fadd_rn(s, vy[i]);
+            if (y > 0) s = __fsub_rn(s, vym[i]);
+            if (x < nx - 1) s = __fadd_rn(s, vx[i]);
+            if (x > 0) s = __fsub_rn(s, i == 0 ? left : vx[i > 0 ? i - 1 : 0]);
+            zv = tv_primal(vb[i], A.lambda, s);
+          }
+          out[i] = zv;
+        }
+        Vec<VEC>::store(Zd + static_cast<std::size_t>(rr) * nx + x0, out);
+      }
+    };
+
+    // Prologue: planes z0 - 1 (z component only), z0 (and b) in one group, z0 + 1 in the next.
+    if (z0 > 0) issue_r(z0 - 1, 1);
+    issue_r(z0, 3);
+    issue_b(z0);
+    copy_commit();
+    const bool second = z0 + 1 <= zlast;
+    if (second) {
+      issue_r(z0 + 1, 3);
+      issue_b(z0 + 1);
+      copy_commit();
       copy_wait<1>();
     } else {
       copy_wait<0>();
     }
     __syncthreads();
-    if (z + 1 < nz) primal(z + 1);
+    primal(z0);
     __syncthreads();
-    {
-      const float* Rc = rslot(z);
-      float rv[3][VEC];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        Vec<VEC>::load(Rc + (static_cast<std::size_t>(c) * ring_rows + ty + 1) * nx + x0, rv[c]);
-        if (FIRST) {
-#pragma unroll
-          for (int i = 0; i < VEC; ++i) pv[c][i] = rv[c][i];
-        }
+
+    const int y = y0 + ty;
+    for (int z = z0; z < z1; ++z) {
+      const bool prefetch = z + 2 <= zlast;
+      if (prefetch) {
+        issue_r(z + 2, 3);
+        issue_b(z + 2);
+        copy_commit();
       }
-      const float* zcp = zslot(z) + static_cast<std::size_t>(ty) * nx;
-      float zc[VEC], zy[VEC], zz[VEC];
-      Vec<VEC>::load(zcp + x0, zc);
-      Vec<VEC>::load(zslot(z) + static_cast<std::size_t>(ty + 1) * nx + x0, zy);
-      Vec<VEC>::load(zslot(z + 1) + static_cast<std::size_t>(ty) * nx + x0, zz);
-      float right;
-      if constexpr (VEC == 4) {
-        const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
-        right = (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? zcp[x0 + VEC] : from_lane;
+      const std::size_t at = static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0;
+      float pv[3][VEC];
+      if (!FIRST && y < ny) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Vec<VEC>::load(A.pin[c] + at, pv[c]);
+      }
+      if (prefetch) {
+        copy_wait<1>();
       } else {
-        right = x0 + 1 < nx ? zcp[x0 + 1] : 0.0f;
+        copy_wait<0>();
       }
-      if (y < ny) {
-#pragma unroll
-        for (int i = 0; i < VEC; ++i) {
-          const int x = x0 + i;
-          const float c = zc[i];
-          float g[3];
-          g[0] = z < nz - 1 ? __fsub_rn(c, zz[i]) : 0.0f;
-          g[1] = y < ny - 1 ? __fsub_rn(c, zy[i]) : 0.0f;
-          g[2] = x < nx - 1 ? __fsub_rn(c, i == VEC - 1 ? right : zc[i < VEC - 1 ? i + 1 : 0]) : 0.0f;
-          float p[3] = {pv[0][i], pv[1][i], pv[2][i]};
-          float r[3] = {rv[0][i], rv[1][i], rv[2][i]};
-          tv_dual_step(g, A.step, A.momentum, p, r);
-#pragma unroll
-          for (int c2 = 0; c2 < 3; ++c2) {
-            pv[c2][i] = p[c2];
-            rv[c2][i] = r[c2];
-          }
-        }
+      __syncthreads();
+      if (z + 1 < nz) primal(z + 1);
+      __syncthreads();
+      {
+        const float* Rc = rslot(z);
+        float rv[3][VEC];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          Vec<VEC>::store(A.pout[c] + at, pv[c]);
-          if (!LAST) Vec<VEC>::store(A.rout[c] + at, rv[c]);
+          Vec<VEC>::load(Rc + (static_cast<std::size_t>(c) * ring_rows + ty + 1) * nx + x0, rv[c]);
+          if (FIRST) {
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) pv[c][i] = rv[c][i];
+          }
+        }
+        const float* zcp = zslot(z) + static_cast<std::size_t>(ty) * nx;
+        float zc[VEC], zy[VEC], zz[VEC];
+        Vec<VEC>::load(zcp + x0, zc);
+        Vec<VEC>::load(zslot(z) + static_cast<std::size_t>(ty + 1) * nx + x0, zy);
+        Vec<VEC>::load(zslot(z + 1) + static_cast<std::size_t>(ty) * nx + x0, zz);
+        float right;
+        if constexpr (VEC == 4) {
+          const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
+          right = (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? zcp[x0 + VEC] : from_lane;
+        } else {
+          right = x0 + 1 < nx ? zcp[x0 + 1] : 0.0f;
+        }
+        if (y < ny) {
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) {
+            const int x = x0 + i;
+            const float c = zc[i];
+            float g[3];
+            g[0] = z < nz - 1 ? __fsub_rn(c, zz[i]) : 0.0f;
+            g[1] = y < ny - 1 ? __fsub_rn(c, zy[i]) : 0.0f;
+            g[2] = x < nx - 1 ? __fsub_rn(c, i == VEC - 1 ? right : zc[i < VEC - 1 ? i + 1 : 0]) : 0.0f;
+            float p[3] = {pv[0][i], pv[1][i], pv[2][i]};
+            float r[3] = {rv[0][i], rv[1][i], rv[2][i]};
+            tv_dual_step(g, A.step, A.momentum, p, r);
+#pragma unroll
+            for (int c2 = 0; c2 < 3; ++c2) {
+              pv[c2][i] = p[c2];
+              rv[c2][i] = r[c2];
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            Vec<VEC>::store(A.pout[c] + at, pv[c]);
+            if (!LAST) Vec<VEC>::store(A.rout[c] + at, rv[c]);
+          }
         }
       }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
@@ -320,12 +328,12 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Rows per CTA and planes per CTA for an (nz, ny, nx) volume: TY rows of full x extent, and as
-// many z chunks as keep every CTA resident in a single wave (a partial second wave would double the
-// time of the step).
+// Rows per CTA for an (nz, ny, nx) volume (TY rows of full x extent) and the grid: every CTA
+// resident at once (a partial second wave would double the time of the step), with an even share of
+// the plane units each.
 struct FgpShape {
   int ty;
-  int zchunk;
+  int grid;
   std::size_t smem;
 };
 
@@ -345,11 +353,9 @@ FgpShape fgp_shape(int nz, int ny, int nx) {
   ensure_smem(kernel);
   int per_sm = 0;
   check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tx * ty, smem), "cudaOccupancy");
-  const int slots = sm_count() * std::max(per_sm, 1);
-  const int ytiles = (ny + ty - 1) / ty;
-  const int chunks = std::max(1, std::min(nz, slots / ytiles));
-  const int zchunk = (nz + chunks - 1) / chunks;
-  return {ty, zchunk, smem};
+  const long long slots = static_cast<long long>(sm_count()) * std::max(per_sm, 1);
+  const long long units = static_cast<long long>((ny + ty - 1) / ty) * nz;
+  return {ty, static_cast<int>(std::min(slots, units)), smem};
 }
 
 template <int VEC, bool FIRST, bool LAST>
@@ -357,8 +363,7 @@ void launch_fgp(const FgpArgs& a, const FgpShape& sh, cudaStream_t s) {
   auto kernel = k_fgp<VEC, FIRST, LAST>;
   ensure_smem(kernel);
   const dim3 block(a.nx / VEC, sh.ty);
-  const dim3 grid((a.ny + sh.ty - 1) / sh.ty, (a.nz + sh.zchunk - 1) / sh.zchunk);
-  kernel<<<grid, block, sh.smem, s>>>(a);
+  kernel<<<sh.grid, block, sh.smem, s>>>(a);
   check_launch("fgp step");
 }
 
@@ -423,7 +428,7 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
     FgpArgs a{};
     a.b = b;
     a.nz = nz, a.ny = ny, a.nx = nx;
-    a.zchunk = sh.zchunk;
+    a.ytiles = (ny + sh.ty - 1) / sh.ty;
     a.lambda = lambda, a.step = step, a.momentum = m;
     const int rout = k == 0 ? (ip + 2) % 3 : 3 - ia - cur_r;
     for (int c = 0; c < 3; ++c) {
