@@ -499,6 +499,83 @@ def serving_leg(qh, capi, requests, rate, inflight=SERVE_INFLIGHT, plain=True):
     }
 
 
+BPM_N, BPM_NZ, BPM_VIEWS, BPM_PIXEL, BPM_ITERS, BPM_EVERY = 256, 128, 49, 0.2, 50, 16
+
+
+def bpm_leg(qh, torch, iterations=BPM_ITERS, reference=True):
+    """Gradient inversion with the BPM model behind torch.autograd: 256^2 x 128 slices (dz = pixel =
+    0.2 um), 49 views at NA 0.9, 20 overlapping spheres (radii 1-3 um, dn <= 0.05) rendered on the
+    grid, data = the model's fields of that volume; `iterations` steps of gradient descent on
+    1/2 |y - data|^2 / views with step 1 / Lipschitz, checkpoint every 16 slices. Times one
+    iteration (forward + backward) with CUDA events; the reference CPU gradient (bpm_forward +
+    bpm_vjp of oracle/_ref) is timed once at the starting point and compared."""
+    from qoraholo_b200.autograd import BpmModel
+
+    rng = np.random.default_rng(17)
+    geom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=BPM_PIXEL)
+    illum = qh.circular_scan(BPM_VIEWS, 0.9, geom)
+    spheres = [qh.Sphere(z=float(rng.uniform(-5, 5)), y=float(rng.uniform(-8, 8)), x=float(rng.uniform(-8, 8)),
+                         radius=float(rng.uniform(1, 3)), n=float(N_MEDIUM + rng.uniform(0.005, 0.05)))
+               for _ in range(20)]
+    truth = qh.render_phantom(spheres, geom, BPM_NZ, BPM_N)
+    model = BpmModel(BPM_NZ, BPM_N, illum, geom, checkpoint_every=BPM_EVERY)
+    with torch.no_grad():
+        data = model(torch.from_numpy(np.ascontiguousarray(truth, np.float32)).cuda())
+    x = torch.full((BPM_NZ, BPM_N, BPM_N), N_MEDIUM, device="cuda", requires_grad=True)
+    phase = 2 * math.pi / WAVELENGTH * BPM_PIXEL
+    opt = torch.optim.SGD([x], lr=1.0 / (BPM_NZ * phase * phase))
+
+    def step():
+        opt.zero_grad(set_to_none=False)
+        loss = 0.5 * (model(x) - data).abs().pow(2).sum() / BPM_VIEWS
+        loss.backward()
+        opt.step()
+        return loss
+
+    first = float(step())  # warm-up (allocations, twiddles)
+    grad0 = None
+    if reference:
+        x0 = torch.full_like(x, N_MEDIUM).requires_grad_(True)
+        (0.5 * (model(x0) - data).abs().pow(2).sum()).backward()
+        grad0 = x0.grad.cpu().numpy()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(iterations - 1):
+        last = step()
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / max(iterations - 1, 1)
+    flops = BPM_VIEWS * BPM_NZ * 6 * 5.0 * BPM_N * BPM_N * math.log2(BPM_N * BPM_N)
+    out = {"workload": f"BPM gradient inversion {BPM_N}^2 x {BPM_NZ}, {BPM_VIEWS} views, 20 spheres, "
+                       f"{iterations} iterations, checkpoint every {BPM_EVERY} slices",
+           "ms_per_iteration": round(ms, 3), "iterations_per_s": round(1000.0 / ms, 3),
+           "fft_gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+           "fft_flop_model": "6 2D FFTs (2 forward, 2 recompute, 2 adjoint) per slice per view x 5 N log2 N",
+           "plan_device_bytes": model.plan.device_bytes, "loss_first": first, "loss_last": float(last)}
+    if reference:
+        try:
+            from oracle import refimpl
+
+            if refimpl.available():
+                x0n = np.full((BPM_NZ, BPM_N, BPM_N), N_MEDIUM, np.float32)
+                t0 = time.perf_counter()
+                y = refimpl.bpm_forward(x0n, illum, geom_bpm_tuple())
+                want = refimpl.bpm_vjp(x0n - N_MEDIUM, (y - data.cpu().numpy()).astype(np.complex64), illum,
+                                       geom_bpm_tuple())
+                ref_ms = 1000.0 * (time.perf_counter() - t0)
+                out["reference_cpu_ms_per_gradient"] = round(ref_ms, 1)
+                out["reference_cpu_cores"] = refimpl.threads()
+                out["rel_err_gradient_vs_reference_cpu"] = float(np.linalg.norm(grad0 - want) / np.linalg.norm(want))
+        except Exception as ex:  # noqa: BLE001
+            out["reference_cpu_error"] = f"{type(ex).__name__}: {ex}"
+    model.plan.close()
+    return out
+
+
+def geom_bpm_tuple():
+    return (WAVELENGTH, N_MEDIUM, NA, BPM_PIXEL)
+
+
 def kernel_case(name, reps):
     """Small standalone launches of one kernel family for profiling (no JSON line): `fgp` runs the
     TV proximal step at 256^3 (10 FGP steps + final primal per rep); `fft` a 256^3 rfft3 + irfft3
@@ -547,7 +624,7 @@ def kernel_case(name, reps):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", choices=["fgp", "fft", "pipeline", "serve"], default=None,
+    ap.add_argument("--kernel-case", choices=["fgp", "fft", "pipeline", "serve", "bpm"], default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)
@@ -559,6 +636,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of that stream, per s")
     ap.add_argument("--serve-inflight", type=int, default=SERVE_INFLIGHT, help="concurrent requests of the server")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving comparison")
+    ap.add_argument("--no-bpm", action="store_true", help="skip the BPM gradient-inversion leg")
     args = ap.parse_args()
     if args.kernel_case == "serve":
         import qoraholo_b200 as qh
@@ -566,6 +644,13 @@ def main():
 
         print(json.dumps(serving_leg(qh, capi, args.serve_requests, args.serve_rate, args.serve_inflight,
                                      plain=not args.serve_no_plain)))
+        return 0
+    if args.kernel_case == "bpm":
+        import torch
+
+        import qoraholo_b200 as qh
+
+        print(json.dumps(bpm_leg(qh, torch)))
         return 0
     if args.kernel_case:
         return kernel_case(args.kernel_case, args.reps)
@@ -638,6 +723,13 @@ def main():
 
     roof = fgp_roofline(torch, capi, stream)
 
+    bpm = None
+    if rank == 0 and world == 1 and not args.no_bpm:
+        try:
+            bpm = bpm_leg(qh, torch)
+        except Exception as e:  # noqa: BLE001
+            bpm = {"error": f"{type(e).__name__}: {e}"}
+
     served = None
     if rank == 0 and world == 1 and not args.no_serve:
         try:
@@ -677,6 +769,7 @@ def main():
                        "l2": "flushed (256 MiB write) before every timed step; inputs resident in HBM"},
             "latency_ms": {"p50": round(statistics.median(lat), 3), "p99": round(p99, 3), "path": "plain device pipeline"},
             "served": served,
+            "bpm_gradient": bpm,
             "roofline": roof,
             "cpu_baseline": cpu,
             "rel_err_vs_reference_cpu": parity,

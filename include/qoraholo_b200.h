@@ -263,6 +263,25 @@ int qhk_bpm_vjp(const float* x, int nz, int n, const void* r, const float* illum
                 const qhk_geometry* geometry, int obliquity, float* out);
 
 /* qoraholo::BpmSolveOptions without the backend field (include/qoraholo/bpm.hpp:29-41). */
+/* Device-level BPM plan for gradient-based inversion (autograd): the forward model on device
+ * buffers, and its vector-Jacobian product with slice checkpointing. Replaces the Bpm class of the
+ * reference's CUDA backend (src/cuda/bpm.cu:126-199; forward and adjoint sweeps, envelopes stored
+ * for every slice) with a plan that keeps, per illumination, only the spectrum entering every
+ * `checkpoint_every`-th slice (0: every envelope, as the reference) and recomputes each segment of
+ * slices before sweeping it backwards. `chunk` illuminations run per device pass (0: all). */
+typedef struct qhk_bpm_plan qhk_bpm_plan;
+int qhk_bpm_plan_create(qhk_bpm_plan** plan, int nz, int n, const float* illum_fyfx, int count,
+                        const qhk_geometry* geometry, int obliquity, int chunk, int checkpoint_every);
+/* d_ri (nz, n, n) float32 -> d_fields (count, n, n) complex64, the field ratios at z = 0; keeps the
+ * checkpoints of this volume for a following qhk_bpm_plan_vjp. Asynchronous on `stream`. */
+int qhk_bpm_plan_forward(qhk_bpm_plan* plan, const float* d_ri, void* d_fields, void* stream);
+/* d_grad_ri (nz, n, n) = Re(J^H g) for g = d_grad_fields (count, n, n) complex64, J the Jacobian of
+ * the forward model at d_ri, which must be the volume of the last qhk_bpm_plan_forward. For
+ * g = forward(ri) - data this is the gradient of 1/2 |forward(ri) - data|^2 (src/cuda/bpm.cu:250-272). */
+int qhk_bpm_plan_vjp(qhk_bpm_plan* plan, const float* d_ri, const void* d_grad_fields, float* d_grad_ri, void* stream);
+size_t qhk_bpm_plan_device_bytes(const qhk_bpm_plan* plan);
+int qhk_bpm_plan_destroy(qhk_bpm_plan* plan);
+
 typedef struct qhk_bpm_solve_options {
   int iterations;
   int batch;

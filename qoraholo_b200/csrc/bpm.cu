@@ -287,7 +287,8 @@ BpmTablesHost bpm_tables(int n, int nz, const float* il, int count, float wavele
   return t;
 }
 
-BpmPlan::BpmPlan(const BpmTablesHost& t, int chunk, bool store) : t_(t), chunk_(chunk), store_on_(store) {
+BpmPlan::BpmPlan(const BpmTablesHost& t, int chunk, bool store, int checkpoint_every)
+    : t_(t), chunk_(chunk), store_on_(store && checkpoint_every <= 0), every_(std::max(checkpoint_every, 0)) {
   require(t.n >= 4 && t.n % 2 == 0 && t.nz >= 1 && t.count >= 1, "bpm: invalid tables");
   require(chunk >= 1 && chunk <= t.count && chunk <= 65535, "bpm: invalid chunk");
   plane_ = static_cast<std::size_t>(t.n) * t.n;
@@ -300,12 +301,20 @@ BpmPlan::BpmPlan(const BpmTablesHost& t, int chunk, bool store) : t_(t), chunk_(
   check(cudaMemcpy(q_.get(), t.q.data(), q_.bytes(), cudaMemcpyHostToDevice), "upload tables");
   s_.reset(plane_ * chunk);
   w_.reset(plane_ * chunk);
-  if (store) stored_.reset(plane_ * chunk * t.nz);
+  if (store_on_) stored_.reset(plane_ * chunk * t.nz);
+  if (every_ > 0) {
+    const int segments = (t.nz + every_ - 1) / every_;
+    ckpt_.reset(plane_ * t.count * segments);
+    env_.reset(plane_ * chunk * std::min(every_, t.nz));
+    rs_.reset(plane_ * chunk);
+    rw_.reset(plane_ * chunk);
+  }
   partial_.reset(4096);
 }
 
 std::size_t BpmPlan::device_bytes() const {
-  return step_.bytes() + last_.bytes() + q_.bytes() + s_.bytes() + w_.bytes() + stored_.bytes() + partial_.bytes();
+  return step_.bytes() + last_.bytes() + q_.bytes() + s_.bytes() + w_.bytes() + stored_.bytes() + partial_.bytes() +
+         ckpt_.bytes() + env_.bytes() + rs_.bytes() + rw_.bytes();
 }
 
 void BpmPlan::fft2(const float2* src, float2* dst, bool forward, int nb, int mode, const void* args_v,
@@ -372,6 +381,11 @@ void BpmPlan::forward(const float* x, int first, int nb, cudaStream_t s) {
                                                       plane_, total);
   check_launch("bpm start");
   for (int k = 0; k < nz; ++k) {
+    if (every_ > 0 && k % every_ == 0) {
+      // Spectrum entering slice k of illuminations first .. first + nb - 1.
+      float2* ck = ckpt_.get() + (static_cast<std::size_t>(k / every_) * t_.count + first) * plane_;
+      check(cudaMemcpyAsync(ck, s_.get(), total * sizeof(float2), cudaMemcpyDeviceToDevice, s), "bpm checkpoint");
+    }
     if (k > 0) {
       ColArgs a{};
       a.store = store_on_ ? stored_.get() + k * total : nullptr;
@@ -408,12 +422,21 @@ void BpmPlan::adjoint(const float* x, const float2* residual_or_null, int first,
   a.q = q_.get() + off;
   a.has_back = 0;
   fft2(w_.get(), w_.get(), true, nb, kSplit, &a, s);
+  require(store_on_ || every_ > 0, "bpm: the plan keeps no envelopes for an adjoint");
   for (int k = nz - 1; k >= 0; --k) {
+    const float2* env = nullptr;
+    if (every_ > 0) {
+      const int k0 = (k / every_) * every_;
+      if (k == nz - 1 || k % every_ == every_ - 1) recompute(x, first, nb, k0, std::min(k0 + every_, nz), s);
+      env = env_.get() + (k - k0) * total;
+    } else {
+      env = stored_.get() + k * total;
+    }
     ColArgs b{};
     b.inv = inv;
     fft2(w_.get(), w_.get(), false, nb, kScale, &b, s);
-    k_gradient<<<grid_for(plane_), kThreads, 0, s>>>(w_.get(), stored_.get() + k * total, x + k * plane_, t_.phase,
-                                                     nb, plane_, gscale, grad + k * plane_);
+    k_gradient<<<grid_for(plane_), kThreads, 0, s>>>(w_.get(), env, x + k * plane_, t_.phase, nb, plane_, gscale,
+                                                     grad + k * plane_);
     check_launch("bpm gradient");
     if (k > 0) {
       ColArgs c{};
@@ -422,6 +445,35 @@ void BpmPlan::adjoint(const float* x, const float2* residual_or_null, int first,
       c.q = q_.get() + off;
       c.has_back = 1;
       fft2(w_.get(), w_.get(), true, nb, kSplit, &c, s);
+    }
+  }
+}
+
+void BpmPlan::recompute(const float* x, int first, int nb, int k0, int k1, cudaStream_t s) {
+  const std::size_t total = plane_ * nb;
+  const std::size_t off = plane_ * first;
+  const float inv = 1.0f / static_cast<float>(plane_);
+  const float2* ck = ckpt_.get() + (static_cast<std::size_t>(k0 / every_) * t_.count + first) * plane_;
+  check(cudaMemcpyAsync(rs_.get(), ck, total * sizeof(float2), cudaMemcpyDeviceToDevice, s), "bpm restore");
+  for (int k = k0; k < k1; ++k) {
+    float2* env = env_.get() + (k - k0) * total;
+    if (k == 0) {
+      k_first_screen<<<grid_for(total), kThreads, 0, s>>>(rw_.get(), env, x, t_.phase, plane_, total);
+      check_launch("bpm recompute");
+    } else {
+      ColArgs a{};
+      a.store = env;
+      a.x = x + k * plane_;
+      a.phase = t_.phase;
+      a.inv = inv;
+      fft2(rs_.get(), rw_.get(), false, nb, kScreen, &a, s);
+    }
+    if (k + 1 < k1) {  // the spectrum entering slice k + 1 (slices k1 .. have their own checkpoint)
+      ColArgs a{};
+      a.s = rs_.get();
+      a.coef = step_.get() + off;
+      a.q = q_.get() + off;
+      fft2(rw_.get(), rw_.get(), true, nb, kPropagate, &a, s);
     }
   }
 }

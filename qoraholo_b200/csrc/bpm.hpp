@@ -25,8 +25,10 @@ BpmTablesHost bpm_tables(int n, int nz, const float* illum_fyfx, int count, floa
 class BpmPlan {
  public:
   // chunk: illuminations per device pass; store: keep the envelope in front of every screen for
-  // the adjoint.
-  BpmPlan(const BpmTablesHost& t, int chunk, bool store);
+  // the adjoint. checkpoint_every = K > 0 instead keeps only the spectrum entering every K-th
+  // slice, for every illumination (ceil(nz / K) planes per illumination); the adjoint then
+  // recomputes each segment's K envelopes from its checkpoint before sweeping it backwards.
+  BpmPlan(const BpmTablesHost& t, int chunk, bool store, int checkpoint_every = 0);
 
   // Envelopes at z = 0 of illuminations first .. first + nb - 1 for contrast x (device), left in
   // fields() (normalised).
@@ -39,9 +41,12 @@ class BpmPlan {
 
   [[nodiscard]] float2* fields() const { return w_.get(); }
   [[nodiscard]] std::size_t device_bytes() const;
+  [[nodiscard]] int checkpoint_every() const { return every_; }
 
  private:
   void fft2(const float2* src, float2* dst, bool forward, int nb, int mode, const void* args, cudaStream_t s);
+  // Envelopes of slices k0 .. k1-1 of the chunk into env_, from the checkpoint of slice k0.
+  void recompute(const float* x, int first, int nb, int k0, int k1, cudaStream_t s);
 
   const BpmTablesHost& t_;
   int chunk_;
@@ -51,6 +56,8 @@ class BpmPlan {
   DevBuf<float> q_;
   DevBuf<float2> s_, w_, stored_;
   DevBuf<double> partial_;
+  int every_ = 0;
+  DevBuf<float2> ckpt_, env_, rs_, rw_;  // checkpoint mode
 };
 
 // x = ri - n_medium (optionally clamped at 0), and back.

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numbers>
 #include <string>
 
@@ -538,6 +539,72 @@ int qhk_bpm_vjp(const float* x, int nz, int n, const void* r, const float* illum
     qhk::check(cudaMemcpyAsync(out, d_grad.get(), vol * sizeof(float), cudaMemcpyDeviceToHost, s), "download");
     qhk::check(cudaStreamSynchronize(s), "bpm_vjp");
   });
+}
+
+struct qhk_bpm_plan {
+  qhk::BpmTablesHost tables;
+  float n_medium = 0;
+  int chunk = 0;
+  qhk::DevBuf<float> x;
+  std::unique_ptr<qhk::BpmPlan> plan;
+};
+
+int qhk_bpm_plan_create(qhk_bpm_plan** plan, int nz, int n, const float* illum_fyfx, int count,
+                        const qhk_geometry* geometry, int obliquity, int chunk, int checkpoint_every) {
+  return guard([&] {
+    qhk::require(plan != nullptr, "bpm: null argument");
+    qhk::require(chunk >= 0 && checkpoint_every >= 0, "bpm: chunk and checkpoint_every must be non-negative");
+    auto p = std::make_unique<qhk_bpm_plan>();
+    p->tables = checked_tables(nz, n, count, illum_fyfx, geometry, obliquity != 0);
+    p->n_medium = geometry->n_medium;
+    p->chunk = chunk > 0 ? std::min(chunk, count) : count;
+    p->x.reset(static_cast<std::size_t>(nz) * n * n);
+    p->plan = std::make_unique<qhk::BpmPlan>(p->tables, p->chunk, checkpoint_every == 0, checkpoint_every);
+    *plan = p.release();
+  });
+}
+
+int qhk_bpm_plan_forward(qhk_bpm_plan* p, const float* d_ri, void* d_fields, void* stream) {
+  return guard([&] {
+    qhk::require(p && d_ri && d_fields, "bpm: null argument");
+    qhk::require(p->plan->checkpoint_every() > 0 || p->chunk == p->tables.count,
+                 "bpm: without checkpoints the plan must take all illuminations in one chunk");
+    const cudaStream_t s = as_stream(stream);
+    const auto& t = p->tables;
+    const std::size_t plane = static_cast<std::size_t>(t.n) * t.n;
+    qhk::contrast(d_ri, p->n_medium, plane * t.nz, p->x.get(), false, s);
+    for (int first = 0; first < t.count; first += p->chunk) {
+      const int nb = std::min(p->chunk, t.count - first);
+      p->plan->forward(p->x.get(), first, nb, s);
+      qhk::check(cudaMemcpyAsync(static_cast<float2*>(d_fields) + first * plane, p->plan->fields(),
+                                 nb * plane * sizeof(float2), cudaMemcpyDeviceToDevice, s),
+                 "bpm fields");
+    }
+  });
+}
+
+int qhk_bpm_plan_vjp(qhk_bpm_plan* p, const float* d_ri, const void* d_grad_fields, float* d_grad_ri, void* stream) {
+  return guard([&] {
+    qhk::require(p && d_ri && d_grad_fields && d_grad_ri, "bpm: null argument");
+    const cudaStream_t s = as_stream(stream);
+    const auto& t = p->tables;
+    const std::size_t plane = static_cast<std::size_t>(t.n) * t.n;
+    const std::size_t vol = plane * t.nz;
+    qhk::contrast(d_ri, p->n_medium, vol, p->x.get(), false, s);
+    qhk::check(cudaMemsetAsync(d_grad_ri, 0, vol * sizeof(float), s), "cudaMemset");
+    const auto* g = static_cast<const float2*>(d_grad_fields);
+    for (int first = 0; first < t.count; first += p->chunk) {
+      const int nb = std::min(p->chunk, t.count - first);
+      if (p->plan->checkpoint_every() == 0) p->plan->forward(p->x.get(), first, nb, s);  // envelopes of this chunk
+      p->plan->adjoint(p->x.get(), g + first * plane, first, nb, 1.0f, d_grad_ri, s);
+    }
+  });
+}
+
+size_t qhk_bpm_plan_device_bytes(const qhk_bpm_plan* p) { return p ? p->plan->device_bytes() + p->x.bytes() : 0; }
+
+int qhk_bpm_plan_destroy(qhk_bpm_plan* p) {
+  return guard([&] { delete p; });
 }
 
 int qhk_bpm_reconstruct(const void* fields, int count, int n, const float* illum_fyfx, const qhk_geometry* geometry,
