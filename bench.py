@@ -579,7 +579,8 @@ def geom_bpm_tuple():
 def kernel_case(name, reps):
     """Small standalone launches of one kernel family for profiling (no JSON line): `fgp` runs the
     TV proximal step at 256^3 (10 FGP steps + final primal per rep); `fft` a 256^3 rfft3 + irfft3
-    per rep; `pipeline` the full device pipeline on 9 x 128^2 holograms -> 64^3."""
+    per rep; `kspace` a 256^3 GP-4 solve from 49 random 256^2 fields per rep (the k-space step's
+    row and axis passes); `pipeline` the full device pipeline on 9 x 128^2 holograms -> 64^3."""
     import torch
 
     from qoraholo_b200 import capi
@@ -592,6 +593,17 @@ def kernel_case(name, reps):
         for _ in range(reps):
             capi.rfft3(x.data_ptr(), half.data_ptr(), n, n, n, stream)
             capi.irfft3(half.data_ptr(), x.data_ptr(), n, n, n, 1.0 / n ** 3, stream)
+    elif name == "kspace":
+        import qoraholo_b200 as qh
+
+        n = FIELD_N
+        geom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=FIELD_PIXEL)
+        illum = qh.circular_scan(COUNT, 0.9, geom)
+        plan = capi.OdtPlan(n, COUNT, illum, geom_tuple(), iterations=4, solver="gp")
+        fields = torch.randn((COUNT, n, n), dtype=torch.complex64, device="cuda")
+        index = torch.empty(plan.shape, dtype=torch.float32, device="cuda")
+        for _ in range(reps):
+            plan.run(fields.data_ptr(), index.data_ptr(), stream)
     elif name == "fgp":
         n = FIELD_N
         b = torch.rand((n, n, n), device="cuda")
@@ -624,7 +636,7 @@ def kernel_case(name, reps):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", choices=["fgp", "fft", "pipeline", "serve", "bpm"], default=None,
+    ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "serve", "bpm"], default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)

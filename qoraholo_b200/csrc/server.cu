@@ -187,11 +187,13 @@ Server::Workspace::~Workspace() {
   if (graph) cudaGraphExecDestroy(graph);
 }
 
-Server::Server(std::size_t hbm_budget, int max_inflight, bool use_graphs)
+Server::Server(std::size_t hbm_budget, int max_inflight, bool use_graphs, int stagers)
     : use_graphs_(use_graphs), admission_(hbm_budget, max_inflight) {
+  require(stagers >= 1, "Server: need at least one stager thread");
   check(cudaGetDevice(&device_), "cudaGetDevice");
   stats_.budget = hbm_budget;
   thread_ = std::thread([this] { loop(); });
+  for (int i = 0; i < stagers; ++i) stagers_.emplace_back([this] { stager(); });
 }
 
 Server::~Server() {
@@ -200,7 +202,13 @@ Server::~Server() {
     stop_ = true;
   }
   wake_.notify_all();
-  if (thread_.joinable()) thread_.join();
+  if (thread_.joinable()) thread_.join();  // returns once nothing is in flight
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    stop_stagers_ = true;
+  }
+  jobs_cv_.notify_all();
+  for (auto& t : stagers_) t.join();
   cudaSetDevice(device_);
   workspaces_.clear();
   geoms_.clear();
@@ -233,7 +241,6 @@ int Server::add_geometry(const CropPlan& crop, int count, const OdtConfig& odt, 
   g->holo_floats = static_cast<std::size_t>(count) * crop.n * crop.n;
   g->volume = static_cast<std::size_t>(odt.grid.nz) * odt.grid.n * odt.grid.n;
   auto w = make_workspace(*g);
-  w->geometry = -1;
   g->background.reset(w->plan->field_elems());
   const cudaStream_t s = w->plan->stream();
   check(cudaMemcpyAsync(w->plan->holo_buffer(), host_bg, g->holo_floats * sizeof(float), cudaMemcpyHostToDevice, s),
@@ -304,46 +311,17 @@ std::uint64_t Server::submit(int geometry, const float* host_holo, float* host_o
   auto r = std::make_unique<Request>();
   r->submitted = Clock::now();
   r->geometry = geometry;
+  r->caller_in = host_holo;
   r->caller_out = host_out;
-  Geometry* g = nullptr;
+  r->in_pinned = is_pinned(host_holo);
+  r->out_pinned = is_pinned(host_out);
+  std::uint64_t ticket = 0;
   {
     std::lock_guard<std::mutex> lk(mu_);
     require(!stop_, "Server: closed");
     require(geometry >= 0 && geometry < static_cast<int>(geoms_.size()) && geoms_[geometry],
             "Server: unknown geometry");
-    g = geoms_[geometry].get();
-    ++g->pending;  // keeps the geometry (and its staging pools) alive until this request is done
-    if (!is_pinned(host_holo) && !g->free_in.empty()) {
-      r->in_stage = std::move(g->free_in.back());
-      g->free_in.pop_back();
-    }
-    if (!is_pinned(host_out) && !g->free_out.empty()) {
-      r->out_stage = std::move(g->free_out.back());
-      g->free_out.pop_back();
-    }
-  }
-  try {
-    if (is_pinned(host_holo)) {
-      r->in = host_holo;
-    } else {
-      if (!r->in_stage) r->in_stage = std::make_unique<PinnedBuf<float>>(g->holo_floats);
-      parallel_copy(r->in_stage->get(), host_holo, g->holo_floats * sizeof(float));
-      r->in = r->in_stage->get();
-    }
-    if (is_pinned(host_out)) {
-      r->out = host_out;
-    } else {
-      if (!r->out_stage) r->out_stage = std::make_unique<PinnedBuf<float>>(g->volume);
-      r->out = r->out_stage->get();
-    }
-  } catch (...) {
-    std::lock_guard<std::mutex> lk(mu_);
-    --g->pending;
-    throw;
-  }
-  std::uint64_t ticket = 0;
-  {
-    std::lock_guard<std::mutex> lk(mu_);
+    ++geoms_[geometry]->pending;  // keeps the geometry alive until this request is waited for
     ticket = next_ticket_++;
     r->ticket = ticket;
     requests_[ticket] = std::move(r);
@@ -364,7 +342,6 @@ bool Server::done(std::uint64_t ticket) {
 
 void Server::wait(std::uint64_t ticket, double* filled, RequestTimes* times) {
   std::unique_ptr<Request> r;
-  Geometry* g = nullptr;
   {
     std::unique_lock<std::mutex> lk(mu_);
     const auto it = requests_.find(ticket);
@@ -373,16 +350,7 @@ void Server::wait(std::uint64_t ticket, double* filled, RequestTimes* times) {
     done_.wait(lk, [p] { return p->done; });
     r = std::move(it->second);
     requests_.erase(it);
-    g = geoms_[r->geometry].get();
-  }
-  if (r->error.empty() && r->out_stage) {
-    parallel_copy(r->caller_out, r->out_stage->get(), g->volume * sizeof(float));
-  }
-  {
-    std::lock_guard<std::mutex> lk(mu_);
-    if (r->in_stage) g->free_in.push_back(std::move(r->in_stage));
-    if (r->out_stage) g->free_out.push_back(std::move(r->out_stage));
-    --g->pending;
+    --geoms_[r->geometry]->pending;
   }
   if (!r->error.empty()) throw Error(r->error_status, r->error);
   if (filled) *filled = r->filled;
@@ -414,10 +382,12 @@ void CUDART_CB Server::on_complete(void* data) {
   sv->wake_.notify_one();
 }
 
-void Server::launch(Request& r, Workspace& w, const Geometry& g) {
+void Server::launch(const Request& r, Workspace& w, const Geometry& g) {
   const cudaStream_t s = w.plan->stream();
+  const float* in = r.in_pinned ? r.caller_in : w.in.get();
+  float* out = r.out_pinned ? r.caller_out : w.out.get();
   w.start.record(s);
-  check(cudaMemcpyAsync(w.plan->holo_buffer(), r.in, g.holo_floats * sizeof(float), cudaMemcpyHostToDevice, s),
+  check(cudaMemcpyAsync(w.plan->holo_buffer(), in, g.holo_floats * sizeof(float), cudaMemcpyHostToDevice, s),
         "Server: upload holograms");
   const float2* bg = g.background.get();
   if (!w.warmed || !use_graphs_) {
@@ -459,7 +429,7 @@ void Server::launch(Request& r, Workspace& w, const Geometry& g) {
     std::lock_guard<std::mutex> lk(mu_);
     ++stats_.graph_launches;
   }
-  check(cudaMemcpyAsync(r.out, w.plan->index_buffer(), g.volume * sizeof(float), cudaMemcpyDeviceToHost, s),
+  check(cudaMemcpyAsync(out, w.plan->index_buffer(), g.volume * sizeof(float), cudaMemcpyDeviceToHost, s),
         "Server: download index");
   check(cudaMemcpyAsync(w.filled.get(), w.plan->odt().filled(), sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                         s),
@@ -473,28 +443,134 @@ void Server::launch(Request& r, Workspace& w, const Geometry& g) {
   }
 }
 
-void Server::finish(Request& r) {
-  Workspace& w = *workspaces_.at(r.workspace);
-  const Geometry& g = *geoms_[r.geometry];
-  r.finished = Clock::now();
-  try {
-    r.gpu_ms = w.stop.since(w.start);
-  } catch (const Error&) {
-    r.gpu_ms = 0;
-  }
-  r.filled = static_cast<double>(*w.filled.get()) / static_cast<double>(g.volume);
+void Server::fail_request(Request& r, const std::string& error, Status status) {
+  // Called with the lock held. The workspace (if any) is dropped: its state is unknown.
+  r.error = error;
+  r.error_status = status;
   r.done = true;
-  admission_.release(r.workspace);
+  ++stats_.failed;
+  if (r.workspace >= 0) admission_.drop(r.workspace);
+  kick_ = true;
+  wake_.notify_one();
+  done_.notify_all();
+}
+
+// Stager: stage the input into the workspace (pageable callers), allocate the workspace if it is
+// new, and enqueue the request's device work.
+void Server::start_request(std::uint64_t ticket) {
+  Request* r = nullptr;
+  Workspace* w = nullptr;
+  const Geometry* g = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    r = requests_.at(ticket).get();
+    g = geoms_[r->geometry].get();
+    if (!r->fresh_workspace) w = workspaces_.at(r->workspace).get();
+  }
+  try {
+    std::unique_ptr<Workspace> fresh;
+    if (!w) {
+      fresh = make_workspace(*g);
+      fresh->geometry = r->geometry;
+      w = fresh.get();
+    }
+    if (!r->in_pinned) {
+      if (!w->in.get()) w->in = PinnedBuf<float>(g->holo_floats);
+      parallel_copy(w->in.get(), r->caller_in, g->holo_floats * sizeof(float));
+    }
+    if (!r->out_pinned && !w->out.get()) w->out = PinnedBuf<float>(g->volume);
+    if (fresh) {
+      std::lock_guard<std::mutex> lk(mu_);
+      workspaces_[r->workspace] = std::move(fresh);
+      ++stats_.workspaces_created;
+    }
+    launch(*r, *w, *g);
+  } catch (const std::exception& e) {
+    std::unique_ptr<Workspace> failed;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (const auto it = workspaces_.find(r->workspace); it != workspaces_.end()) {
+        failed = std::move(it->second);
+        workspaces_.erase(it);
+      }
+      const auto* qe = dynamic_cast<const Error*>(&e);
+      fail_request(*r, e.what(), qe ? qe->status : kInternal);
+    }
+    // Freeing device memory waits for the device, including other requests' completion callbacks,
+    // which take the lock: it is released first.
+    failed.reset();
+  }
+}
+
+// Stager: copy a finished request's volume out of the workspace's staging buffer, then release the
+// workspace.
+void Server::drain_request(std::uint64_t ticket) {
+  Request* r = nullptr;
+  const Workspace* w = nullptr;
+  std::size_t bytes = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    r = requests_.at(ticket).get();
+    w = workspaces_.at(r->workspace).get();
+    bytes = geoms_[r->geometry]->volume * sizeof(float);
+  }
+  parallel_copy(r->caller_out, w->out.get(), bytes);
+  std::lock_guard<std::mutex> lk(mu_);
+  r->finished = Clock::now();
+  r->done = true;
+  admission_.release(r->workspace);
   ++stats_.completed;
+  kick_ = true;
+  wake_.notify_one();
+  done_.notify_all();
+}
+
+void Server::stager() {
+  cudaSetDevice(device_);
+  std::unique_lock<std::mutex> lk(mu_);
+  for (;;) {
+    jobs_cv_.wait(lk, [this] { return stop_stagers_ || !jobs_.empty(); });
+    if (jobs_.empty()) return;  // stopping, nothing left
+    const Job job = jobs_.front();
+    jobs_.pop_front();
+    lk.unlock();
+    if (job.kind == Job::start) {
+      start_request(job.ticket);
+    } else {
+      drain_request(job.ticket);
+    }
+    lk.lock();
+  }
 }
 
 void Server::loop() {
   cudaSetDevice(device_);
   std::unique_lock<std::mutex> lk(mu_);
   for (;;) {
-    for (const std::uint64_t t : completed_) finish(*requests_.at(t));
-    if (!completed_.empty()) done_.notify_all();
+    // Completions: device work done. Pageable outputs go to a stager; the rest are done here.
+    bool any_done = false;
+    for (const std::uint64_t t : completed_) {
+      Request& r = *requests_.at(t);
+      Workspace& w = *workspaces_.at(r.workspace);
+      try {
+        r.gpu_ms = w.stop.since(w.start);
+      } catch (const Error&) {
+        r.gpu_ms = 0;
+      }
+      r.filled = static_cast<double>(*w.filled.get()) / static_cast<double>(geoms_[r.geometry]->volume);
+      if (r.out_pinned) {
+        r.finished = Clock::now();
+        r.done = true;
+        admission_.release(r.workspace);
+        ++stats_.completed;
+        any_done = true;
+      } else {
+        jobs_.push_back(Job{Job::drain, t});
+        jobs_cv_.notify_one();
+      }
+    }
     completed_.clear();
+    if (any_done) done_.notify_all();
 
     if (stop_) {
       for (const std::uint64_t t : pending_) {
@@ -509,7 +585,7 @@ void Server::loop() {
       if (admission_.inflight() == 0) break;
     }
 
-    // Admit as many pending requests as slots and memory allow.
+    // Admit as many pending requests as slots and memory allow; stagers take them from here.
     while (!stop_ && !pending_.empty()) {
       std::vector<int> order;
       const std::size_t look = std::min<std::size_t>(pending_.size(), 64);
@@ -522,7 +598,8 @@ void Server::loop() {
         workspaces_.erase(e);
         ++stats_.workspaces_evicted;
       }
-      const int wid = d->action == Admission::Action::reuse ? d->workspace : next_workspace_++;
+      const bool reuse = d->action == Admission::Action::reuse;
+      const int wid = reuse ? d->workspace : next_workspace_++;
       admission_.commit(*d, wid);
       if (d->position > 0) ++stats_.passed_over;
       const std::uint64_t t = pending_[d->position];
@@ -530,52 +607,15 @@ void Server::loop() {
       Request& r = *requests_.at(t);
       r.admitted = Clock::now();
       r.workspace = wid;
-      const Geometry& g = *geoms_[r.geometry];
+      r.fresh_workspace = !reuse;
       stats_.used = admission_.used();
       stats_.peak_used = std::max(stats_.peak_used, stats_.used);
       stats_.peak_inflight = std::max(stats_.peak_inflight, admission_.inflight());
-      Workspace* w = d->action == Admission::Action::reuse ? workspaces_.at(wid).get() : nullptr;
-      lk.unlock();
-      std::string error;
-      Status status = kOk;
-      try {
-        dead.clear();  // frees device memory (synchronises the device)
-        std::unique_ptr<Workspace> fresh;
-        if (!w) {
-          fresh = make_workspace(g);
-          fresh->geometry = r.geometry;
-          w = fresh.get();
-        }
-        if (fresh) {
-          std::lock_guard<std::mutex> relk(mu_);
-          workspaces_[wid] = std::move(fresh);
-          ++stats_.workspaces_created;
-        }
-        launch(r, *w, g);
-      } catch (const Error& e) {
-        error = e.what();
-        status = e.status;
-      } catch (const std::exception& e) {
-        error = e.what();
-        status = kInternal;
-      }
-      lk.lock();
-      if (!error.empty()) {
-        r.error = error;
-        r.error_status = status;
-        r.done = true;
-        ++stats_.failed;
-        admission_.drop(wid);
-        std::unique_ptr<Workspace> failed;
-        if (const auto it = workspaces_.find(wid); it != workspaces_.end()) {
-          failed = std::move(it->second);
-          workspaces_.erase(it);
-        }
-        done_.notify_all();
-        // Freeing device memory waits for the device, including other requests' completion
-        // callbacks, which take the lock: release it first.
+      jobs_.push_back(Job{Job::start, t});
+      jobs_cv_.notify_one();
+      if (!dead.empty()) {
         lk.unlock();
-        failed.reset();
+        dead.clear();  // frees device memory (waits for the device): never under the lock
         lk.lock();
       }
     }

@@ -114,7 +114,7 @@ struct ServerStats {
 
 class Server {
  public:
-  Server(std::size_t hbm_budget, int max_inflight, bool use_graphs = true);
+  Server(std::size_t hbm_budget, int max_inflight, bool use_graphs = true, int stagers = 2);
   ~Server();
   Server(const Server&) = delete;
   Server& operator=(const Server&) = delete;
@@ -127,8 +127,9 @@ class Server {
   // pending or running.
   void remove_geometry(int geometry);
   // Queues one request: holograms (count, N, N) on the host -> index (nz, n, n) into `host_out`.
-  // Both may be pageable (staged through page-locked buffers by the calling thread) or page-locked
-  // (copied directly); `host_out` must stay valid until wait() returns. Returns a ticket.
+  // Both may be pageable (staged through the workspace's page-locked buffers by the server's stager
+  // threads) or page-locked (copied directly). Both must stay valid until wait() returns. Returns a
+  // ticket.
   std::uint64_t submit(int geometry, const float* host_holo, float* host_out);
   // Blocks until the request is done; its filled fraction and timings. Throws the request's error.
   void wait(std::uint64_t ticket, double* filled, RequestTimes* times);
@@ -146,8 +147,7 @@ class Server {
     std::vector<float> illum;
     DevBuf<float2> background;
     std::size_t holo_floats = 0, volume = 0;
-    int pending = 0;  // requests queued or running
-    std::vector<std::unique_ptr<PinnedBuf<float>>> free_in, free_out;  // staging pools
+    int pending = 0;  // requests not yet waited for
   };
   struct Workspace {
     int geometry = -1;
@@ -157,17 +157,18 @@ class Server {
     bool warmed = false;
     Event start, stop;
     PinnedBuf<unsigned long long> filled{1};
+    PinnedBuf<float> in, out;  // staging for pageable callers, allocated on first use
     ~Workspace();
   };
   struct Request {
     std::uint64_t ticket = 0;
     int geometry = -1;
-    const float* in = nullptr;  // page-locked: caller's or staging
-    float* out = nullptr;       // page-locked: caller's or staging
+    const float* caller_in = nullptr;
     float* caller_out = nullptr;
-    std::unique_ptr<PinnedBuf<float>> in_stage, out_stage;
+    bool in_pinned = false, out_pinned = false;
     Clock::time_point submitted, admitted, finished;
     int workspace = -1;
+    bool fresh_workspace = false;  // admitted with a workspace still to be allocated
     bool done = false;
     double filled = 0;
     float gpu_ms = 0;
@@ -178,21 +179,32 @@ class Server {
     Server* server;
     std::uint64_t ticket;
   };
+  // Work for the stager threads: stage a request's input and enqueue its device work, or copy its
+  // result out of the workspace's staging buffer.
+  struct Job {
+    enum Kind { start, drain } kind;
+    std::uint64_t ticket;
+  };
 
   static void CUDART_CB on_complete(void* data);
   void loop();
-  void launch(Request& r, Workspace& w, const Geometry& g);
-  void finish(Request& r);
+  void stager();
+  void start_request(std::uint64_t ticket);
+  void drain_request(std::uint64_t ticket);
+  void launch(const Request& r, Workspace& w, const Geometry& g);
+  void fail_request(Request& r, const std::string& error, Status status);
   static std::unique_ptr<Workspace> make_workspace(const Geometry& g);
   static bool is_pinned(const void* p);
 
   std::mutex mu_;
-  std::condition_variable wake_;   // scheduler: submissions, completions, stop
+  std::condition_variable wake_;   // scheduler: submissions, completions, released workspaces, stop
   std::condition_variable done_;   // waiters
+  std::condition_variable jobs_cv_;  // stagers
   int device_ = 0;
   bool use_graphs_;
   bool stop_ = false;
-  bool kick_ = false;  // pending_ changed since the scheduler last looked
+  bool stop_stagers_ = false;
+  bool kick_ = false;  // something the scheduler acts on changed since it last looked
   Admission admission_;
   std::vector<std::unique_ptr<Geometry>> geoms_;
   std::map<int, std::unique_ptr<Workspace>> workspaces_;
@@ -200,9 +212,11 @@ class Server {
   std::deque<std::uint64_t> pending_;
   std::map<std::uint64_t, std::unique_ptr<Request>> requests_;
   std::vector<std::uint64_t> completed_;
+  std::deque<Job> jobs_;
   std::uint64_t next_ticket_ = 1;
   ServerStats stats_;
   std::thread thread_;
+  std::vector<std::thread> stagers_;
 };
 
 }  // namespace qhk
