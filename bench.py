@@ -782,6 +782,7 @@ def main():
             "latency_ms": {"p50": round(statistics.median(lat), 3), "p99": round(p99, 3), "path": "plain device pipeline"},
             "served": served,
             "bpm_gradient": bpm,
+            "autotune": capi.autotune_report().strip().splitlines(),
             "roofline": roof,
             "cpu_baseline": cpu,
             "rel_err_vs_reference_cpu": parity,

@@ -156,6 +156,16 @@ int qhk_rytov(const void* ratio, int count, int ny, int nx, void* out);
  * array and race, so serialise them (one stream, or events). */
 int qhk_unwrap_noalloc(const float* d_wrapped, float* d_unwrapped, int count, int ny, int nx, void* stream);
 
+/* ---- Launch-shape autotuner (no counterpart in the reference, which uses cuFFT plans and fixed
+ * launch shapes). Plans time the candidate tile shapes of their FFT axis passes (columns per CTA)
+ * and of the FGP step (rows per CTA) on their own buffers when they are built, and keep the fastest
+ * per (device, shape) for the process; results are bitwise the same for every shape. On by default
+ * (environment QHK_AUTOTUNE=0 turns it off). */
+int qhk_autotune_enable(int enabled);
+/* The tuned choices, one line each, into `buf` (NUL-terminated, truncated to `size`); returns the
+ * full length. */
+size_t qhk_autotune_report(char* buf, size_t size);
+
 /* ---- Pipeline: replaces cuda::make_pipeline and Pipeline::Impl (src/backends.hpp:75-89,
  * src/cuda/pipeline.cu:12-161). Validation of the Pipeline constructor (src/pipeline.cpp:72-91). */
 typedef struct qhk_pipeline_options {

@@ -98,6 +98,8 @@ _PROTOS = {
     "qhk_pipeline_shape": (_I, [_VP, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "qhk_pipeline_device_bytes": (C.c_size_t, [_VP]),
     "qhk_pipeline_destroy": (_I, [_VP]),
+    "qhk_autotune_enable": (_I, [_I]),
+    "qhk_autotune_report": (C.c_size_t, [_VP, C.c_size_t]),
     "qhk_server_create": (_I, [C.POINTER(_VP), C.c_size_t, _I, _I]),
     "qhk_server_add_geometry": (_I, [_VP, _VP, _VP, C.POINTER(Geometry), _VP, C.POINTER(_I)]),
     "qhk_server_remove_geometry": (_I, [_VP, _I]),
@@ -222,6 +224,19 @@ def tv_prox_device(d_b, d_x, d_dual9, nz, ny, nx, lam, inner, stream=0):
 def unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, stream=0):
     """qhk_unwrap_noalloc: device in / device out, no allocation (scratch in a static device array)."""
     check(lib().qhk_unwrap_noalloc(_VP(d_wrapped), _VP(d_unwrapped), count, ny, nx, _VP(stream)))
+
+
+def autotune_enable(enabled: bool = True):
+    """Plans built from now on time their launch shapes (on by default)."""
+    check(lib().qhk_autotune_enable(int(bool(enabled))))
+
+
+def autotune_report() -> str:
+    """The tuned launch shapes so far, one line per (family, shape)."""
+    n = lib().qhk_autotune_report(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib().qhk_autotune_report(C.cast(buf, _VP), n + 1)
+    return buf.value.decode()
 
 
 def kernel_launches() -> int:

@@ -12,6 +12,7 @@
 #include <deque>
 #include <vector>
 
+#include "autotune.hpp"
 #include "bpm.hpp"
 #include "field.hpp"
 #include "odt.hpp"
@@ -639,6 +640,20 @@ int qhk_bpm_reconstruct(const void* fields, int count, int n, const float* illum
   });
 }
 
+
+int qhk_autotune_enable(int enabled) {
+  return guard([&] { qhk::set_autotune_enabled(enabled != 0); });
+}
+
+size_t qhk_autotune_report(char* buf, size_t size) {
+  const std::string r = qhk::autotune_report();
+  if (buf && size > 0) {
+    const std::size_t n = std::min(size - 1, r.size());
+    std::memcpy(buf, r.data(), n);
+    buf[n] = '\0';
+  }
+  return r.size();
+}
 
 struct qhk_server {
   qhk::Server server;

@@ -16,6 +16,7 @@
 #include <mutex>
 #include <set>
 
+#include "autotune.hpp"
 #include "qhk_internal.hpp"
 
 namespace qhk {
@@ -205,15 +206,26 @@ void axis_dispatch(float2* data, int n_outer, std::size_t so, int n, std::size_t
   }
 }
 
+// Row transforms with the length known at compile time (MC > 0) or at run time (MC = 0): with
+// MC the index arithmetic of the staging loops is by constants, not runtime divisions.
+template <bool Fwd, int COLS, int MC>
+__device__ __forceinline__ float2* row_fft(float2* a, float2* b, int cp, const FftLen& L, int tid, int nth) {
+  if constexpr (MC > 0) {
+    return fftdev::passes_fixed<MC, 0, 1, Fwd, COLS>(a, b, cp, L.tw, tid, nth);
+  } else {
+    return smem_fft_cols<Fwd, COLS>(a, b, cp, L, tid, nth);
+  }
+}
+
 // ---- real rows <-> half spectra -----------------------------------------------------------------
 
-template <bool Clamp, int COLS>
+template <bool Clamp, int COLS, int MC>
 __global__ void __launch_bounds__(kThreads)
     k_rows_r2c(const float* __restrict__ x, float2* __restrict__ e, std::size_t rows, int nx, FftLen Lm,
                const float2* __restrict__ twn) {
   extern __shared__ float2 sm[];
   constexpr int cp = COLS + 1;
-  const int M = Lm.n;
+  const int M = MC > 0 ? MC : Lm.n;
   const int h = M + 1;
   float2* A = sm;
   float2* B = sm + static_cast<std::size_t>(h) * cp;
@@ -233,7 +245,7 @@ __global__ void __launch_bounds__(kThreads)
     A[m * cp + row] = v;
   }
   __syncthreads();
-  const float2* res = smem_fft_cols<true, COLS>(A, B, cp, Lm, tid, nth);
+  const float2* res = row_fft<true, COLS, MC>(A, B, cp, Lm, tid, nth);
 
   for (int idx = tid; idx < h * COLS; idx += nth) {
     const int row = idx / h;
@@ -249,13 +261,13 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <int Mode, int COLS>
+template <int Mode, int COLS, int MC>
 __global__ void __launch_bounds__(kThreads)
     k_rows_c2r(const float2* __restrict__ e, float* __restrict__ x, std::size_t rows, int nx, FftLen Lm,
                const float2* __restrict__ twn, float nm2, float inv_k02) {
   extern __shared__ float2 sm[];
   constexpr int cp = COLS + 1;
-  const int M = Lm.n;
+  const int M = MC > 0 ? MC : Lm.n;
   const int h = M + 1;
   float2* A = sm;
   float2* B = sm + static_cast<std::size_t>(h) * cp;
@@ -286,7 +298,7 @@ __global__ void __launch_bounds__(kThreads)
     B[k * cp + row] = make_float2(sv.x - t.y, sv.y + t.x);     // sv + i t
   }
   __syncthreads();
-  const float2* res = smem_fft_cols<false, COLS>(B, A, cp, Lm, tid, nth);
+  const float2* res = row_fft<false, COLS, MC>(B, A, cp, Lm, tid, nth);
 
   for (int idx = tid; idx < M * COLS; idx += nth) {
     const int row = idx / M;
@@ -302,13 +314,13 @@ __global__ void __launch_bounds__(kThreads)
 
 // ---- complex rows -----------------------------------------------------------------------------------
 
-template <bool Fwd, int Mode, int COLS>
+template <bool Fwd, int Mode, int COLS, int NC>
 __global__ void __launch_bounds__(kThreads)
     k_rows_c2c(float2* __restrict__ data, std::size_t rows, FftLen L, float scale, float* __restrict__ index,
                float nm2, float inv_k02) {
   extern __shared__ float2 sm[];
   constexpr int cp = COLS + 1;
-  const int n = L.n;
+  const int n = NC > 0 ? NC : L.n;
   float2* A = sm;
   float2* B = sm + static_cast<std::size_t>(n) * cp;
   const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
@@ -324,9 +336,9 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   float2* res;
   if constexpr (Mode == static_cast<int>(RowMode::plain)) {
-    res = smem_fft_cols<Fwd, COLS>(A, B, cp, L, tid, nth);
+    res = row_fft<Fwd, COLS, NC>(A, B, cp, L, tid, nth);
   } else {
-    res = smem_fft_cols<false, COLS>(A, B, cp, L, tid, nth);
+    res = row_fft<false, COLS, NC>(A, B, cp, L, tid, nth);
     if constexpr (Mode == static_cast<int>(RowMode::inv_clamp_fwd)) {
       float2* other = res == A ? B : A;
       for (int idx = tid; idx < n * COLS; idx += nth) {
@@ -336,7 +348,7 @@ __global__ void __launch_bounds__(kThreads)
         res[pos * cp + row] = make_float2(fmaxf(v.x * scale, 0.0f), 0.0f);
       }
       __syncthreads();
-      res = smem_fft_cols<true, COLS>(res, other, cp, L, tid, nth);
+      res = row_fft<true, COLS, NC>(res, other, cp, L, tid, nth);
     }
   }
   for (int idx = tid; idx < n * COLS; idx += nth) {
@@ -355,13 +367,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // Rows per CTA: as many as fit a 64 KiB double buffer, at most 16.
-int rows_per_cta(int n) {
+constexpr int rows_per_cta(int n) {
   int c = 16;
   while (c > 1 && 2 * static_cast<std::size_t>(n + 1) * (c + 1) * sizeof(float2) > 64 * 1024) c /= 2;
   return c;
 }
 
-template <int COLS>
+template <int COLS, int MC>
 void launch_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, cudaStream_t s) {
   const int M = nx / 2;
   const FftLen& Lm = fft_len(M);
@@ -369,16 +381,16 @@ void launch_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp,
   const std::size_t smem = 2 * static_cast<std::size_t>(M + 1) * (COLS + 1) * sizeof(float2);
   const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
   if (clamp) {
-    allow_smem(k_rows_r2c<true, COLS>, smem);
-    k_rows_r2c<true, COLS><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
+    allow_smem(k_rows_r2c<true, COLS, MC>, smem);
+    k_rows_r2c<true, COLS, MC><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
   } else {
-    allow_smem(k_rows_r2c<false, COLS>, smem);
-    k_rows_r2c<false, COLS><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
+    allow_smem(k_rows_r2c<false, COLS, MC>, smem);
+    k_rows_r2c<false, COLS, MC><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
   }
   check_launch("rows r2c");
 }
 
-template <int COLS>
+template <int COLS, int MC>
 void launch_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
                 cudaStream_t s) {
   const int M = nx / 2;
@@ -387,43 +399,43 @@ void launch_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mod
   const std::size_t smem = 2 * static_cast<std::size_t>(M + 1) * (COLS + 1) * sizeof(float2);
   const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
   if (mode == C2rMode::index) {
-    allow_smem(k_rows_c2r<1, COLS>, smem);
-    k_rows_c2r<1, COLS><<<grid, kThreads, smem, s>>>(e, x, rows, nx, Lm, Ln.tw, nm2, inv_k02);
+    allow_smem(k_rows_c2r<1, COLS, MC>, smem);
+    k_rows_c2r<1, COLS, MC><<<grid, kThreads, smem, s>>>(e, x, rows, nx, Lm, Ln.tw, nm2, inv_k02);
   } else {
-    allow_smem(k_rows_c2r<0, COLS>, smem);
-    k_rows_c2r<0, COLS><<<grid, kThreads, smem, s>>>(e, x, rows, nx, Lm, Ln.tw, nm2, inv_k02);
+    allow_smem(k_rows_c2r<0, COLS, MC>, smem);
+    k_rows_c2r<0, COLS, MC><<<grid, kThreads, smem, s>>>(e, x, rows, nx, Lm, Ln.tw, nm2, inv_k02);
   }
   check_launch("rows c2r");
 }
 
-template <bool Fwd, int Mode, int COLS>
+template <bool Fwd, int Mode, int COLS, int NC>
 void launch_c2c_rows(float2* data, std::size_t rows, int nx, float scale, float* index, float nm2,
                      float inv_k02, cudaStream_t s) {
   const FftLen& L = fft_len(nx);
   const std::size_t smem = 2 * static_cast<std::size_t>(nx) * (COLS + 1) * sizeof(float2);
-  auto kernel = k_rows_c2c<Fwd, Mode, COLS>;
+  auto kernel = k_rows_c2c<Fwd, Mode, COLS, NC>;
   allow_smem(kernel, smem);
   const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
   kernel<<<grid, kThreads, smem, s>>>(data, rows, L, scale, index, nm2, inv_k02);
   check_launch("rows c2c");
 }
 
-template <int COLS>
+template <int COLS, int NC>
 void c2c_rows_dispatch(float2* data, std::size_t rows, int nx, bool forward, RowMode mode, float scale,
                        float* index, float nm2, float inv_k02, cudaStream_t s) {
   switch (mode) {
     case RowMode::plain:
       if (forward) {
-        launch_c2c_rows<true, 0, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+        launch_c2c_rows<true, 0, COLS, NC>(data, rows, nx, scale, index, nm2, inv_k02, s);
       } else {
-        launch_c2c_rows<false, 0, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+        launch_c2c_rows<false, 0, COLS, NC>(data, rows, nx, scale, index, nm2, inv_k02, s);
       }
       break;
     case RowMode::inv_clamp_fwd:
-      launch_c2c_rows<false, 1, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+      launch_c2c_rows<false, 1, COLS, NC>(data, rows, nx, scale, index, nm2, inv_k02, s);
       break;
     case RowMode::inv_index:
-      launch_c2c_rows<false, 2, COLS>(data, rows, nx, scale, index, nm2, inv_k02, s);
+      launch_c2c_rows<false, 2, COLS, NC>(data, rows, nx, scale, index, nm2, inv_k02, s);
       break;
   }
 }
@@ -463,58 +475,123 @@ const FftLen& fft_len(int n) {
   return slot->len;
 }
 
+namespace {
+
+void axis_cols(int cols, float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
+               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
+  switch (cols) {
+    case 16: axis_dispatch<16>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
+    case 8: axis_dispatch<8>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
+    case 4: axis_dispatch<4>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
+    default: axis_dispatch<1>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
+  }
+}
+
+// Tile widths whose double buffer fits a CTA, widest first, and the default: the widest whose
+// buffer fits `axis_smem_budget()`.
+std::vector<int> axis_candidates(int n) {
+  std::vector<int> out;
+  for (const int c : {16, 8, 4}) {
+    if (2 * static_cast<std::size_t>(n) * c * sizeof(float2) <= 200 * 1024) out.push_back(c);
+  }
+  return out;
+}
+
+int axis_default(int n) {
+  for (const int c : {16, 8, 4}) {
+    if (2 * static_cast<std::size_t>(n) * c * sizeof(float2) <= axis_smem_budget()) return c;
+  }
+  return 1;
+}
+
+TuneKey axis_key(int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward, AxisMode mode) {
+  return tune_key(TuneFamily::axis, {n, ni, n_outer, static_cast<long long>(so), static_cast<long long>(sp),
+                                     2 * static_cast<long long>(mode) + (forward ? 1 : 0)});
+}
+
+}  // namespace
+
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
   require(n_outer >= 1 && n_outer <= 65535, "fft: too many lines in the outer dimension");
   require(static_cast<std::size_t>(n) * 2 * sizeof(float2) <= 200 * 1024, "fft: transform length too large");
-  // Tile width: the widest tile whose double buffer fits `axis_smem_budget()` bytes.
-  const auto fits = [&](int cols) {
-    return 2 * static_cast<std::size_t>(n) * cols * sizeof(float2) <= axis_smem_budget();
-  };
-  if (fits(16)) {
-    axis_dispatch<16>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
-  } else if (fits(8)) {
-    axis_dispatch<8>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
-  } else if (fits(4)) {
-    axis_dispatch<4>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
-  } else {
-    axis_dispatch<1>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
-  }
+  const int cols = tuned_choice(axis_key(n_outer, so, n, sp, ni, forward, mode), axis_default(n));
+  axis_cols(cols, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
 }
+
+void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
+                    AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
+  require(n_outer >= 1 && n_outer <= 65535, "fft: too many lines in the outer dimension");
+  autotune(axis_key(n_outer, so, n, sp, ni, forward, mode), axis_candidates(n), axis_default(n),
+           [&](int c) { axis_cols(c, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); }, s);
+}
+
+// Lengths with compile-time row kernels (the common volume and image sides); others run the
+// runtime-length kernels.
+#define QHK_FIXED_LENGTHS(X) X(32) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
 
 void rows_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, cudaStream_t s) {
   require(nx >= 2 && nx % 2 == 0, "rfft: row length must be even");
+  switch (nx / 2) {
+#define QHK_R2C(M)                                                \
+  case M:                                                         \
+    launch_r2c<rows_per_cta(M), M>(x, e, rows, nx, clamp, s);     \
+    return;
+    QHK_FIXED_LENGTHS(QHK_R2C)
+#undef QHK_R2C
+    default: break;
+  }
   switch (rows_per_cta(nx / 2)) {
-    case 16: launch_r2c<16>(x, e, rows, nx, clamp, s); break;
-    case 8: launch_r2c<8>(x, e, rows, nx, clamp, s); break;
-    case 4: launch_r2c<4>(x, e, rows, nx, clamp, s); break;
-    case 2: launch_r2c<2>(x, e, rows, nx, clamp, s); break;
-    default: launch_r2c<1>(x, e, rows, nx, clamp, s); break;
+    case 16: launch_r2c<16, 0>(x, e, rows, nx, clamp, s); break;
+    case 8: launch_r2c<8, 0>(x, e, rows, nx, clamp, s); break;
+    case 4: launch_r2c<4, 0>(x, e, rows, nx, clamp, s); break;
+    case 2: launch_r2c<2, 0>(x, e, rows, nx, clamp, s); break;
+    default: launch_r2c<1, 0>(x, e, rows, nx, clamp, s); break;
   }
 }
 
 void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
               cudaStream_t s) {
   require(nx >= 2 && nx % 2 == 0, "irfft: row length must be even");
+  switch (nx / 2) {
+#define QHK_C2R(M)                                                          \
+  case M:                                                                   \
+    launch_c2r<rows_per_cta(M), M>(e, x, rows, nx, mode, nm2, inv_k02, s);  \
+    return;
+    QHK_FIXED_LENGTHS(QHK_C2R)
+#undef QHK_C2R
+    default: break;
+  }
   switch (rows_per_cta(nx / 2)) {
-    case 16: launch_c2r<16>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
-    case 8: launch_c2r<8>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
-    case 4: launch_c2r<4>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
-    case 2: launch_c2r<2>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
-    default: launch_c2r<1>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    case 16: launch_c2r<16, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    case 8: launch_c2r<8, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    case 4: launch_c2r<4, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    case 2: launch_c2r<2, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+    default: launch_c2r<1, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
   }
 }
 
 void rows_c2c(float2* data, std::size_t rows, int nx, bool forward, RowMode mode, float scale, float* index,
               float nm2, float inv_k02, cudaStream_t s) {
+  switch (nx) {
+#define QHK_C2C(N)                                                                                        \
+  case N:                                                                                                 \
+    c2c_rows_dispatch<rows_per_cta(N), N>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s);  \
+    return;
+    QHK_FIXED_LENGTHS(QHK_C2C)
+#undef QHK_C2C
+    default: break;
+  }
   switch (rows_per_cta(nx)) {
-    case 16: c2c_rows_dispatch<16>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
-    case 8: c2c_rows_dispatch<8>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
-    case 4: c2c_rows_dispatch<4>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
-    case 2: c2c_rows_dispatch<2>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
-    default: c2c_rows_dispatch<1>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    case 16: c2c_rows_dispatch<16, 0>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    case 8: c2c_rows_dispatch<8, 0>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    case 4: c2c_rows_dispatch<4, 0>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    case 2: c2c_rows_dispatch<2, 0>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
+    default: c2c_rows_dispatch<1, 0>(data, rows, nx, forward, mode, scale, index, nm2, inv_k02, s); break;
   }
 }
+
+#undef QHK_FIXED_LENGTHS
 
 void fft2d(float2* data, int count, int n, bool forward, float scale, cudaStream_t s) {
   rows_c2c(data, static_cast<std::size_t>(count) * n, n, forward, RowMode::plain, 1.0f, nullptr, 0, 0, s);

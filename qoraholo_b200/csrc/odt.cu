@@ -17,6 +17,7 @@
 #include <numbers>
 #include <vector>
 
+#include "autotune.hpp"
 #include "odt.hpp"
 
 namespace qhk {
@@ -228,6 +229,48 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
     mask_.reset(vol_);
     if (cfg_.iterations > 0) measured_.reset(vol_);
   }
+  tune();
+}
+
+// Autotunes the launch shapes of this plan's passes on its own buffers (scratch at this point):
+// the axis passes' tile widths and the FGP tile height (autotune.hpp). Results do not depend on
+// the shapes chosen.
+void OdtPlan::tune() {
+  if (!autotune_enabled()) return;
+  const Grid& g = cfg_.grid;
+  const int n = g.n, nz = g.nz, h = n / 2 + 1;
+  const std::size_t nh = static_cast<std::size_t>(n) * h;
+  const std::size_t nn = static_cast<std::size_t>(n) * n;
+  Stream stream;
+  const cudaStream_t s = stream.get();
+  float2* scratch = real_ ? e_.get() : pot_.get();
+  const std::size_t room = real_ ? half_ : vol_;
+  if (static_cast<std::size_t>(cfg_.count) * nn <= room) {  // the 2D FFT of the fields
+    tune_axis_pass(scratch, cfg_.count, nn, n, static_cast<std::size_t>(n), n, true, AxisMode::plain, 1.0f,
+                   AxisAux{}, s);
+  }
+  if (real_) {
+    const AxisAux aux{a_.get(), hits_.get()};
+    check(cudaMemsetAsync(a_.get(), 0, a_.bytes(), s), "cudaMemset");
+    check(cudaMemsetAsync(hits_.get(), 0, hits_.bytes(), s), "cudaMemset");
+    for (const bool fwd : {true, false}) {
+      tune_axis_pass(scratch, nz, nh, n, h, h, fwd, AxisMode::plain, 1.0f, AxisAux{}, s);
+    }
+    tune_axis_pass(scratch, n, h, nz, nh, h, false, AxisMode::from_data, 1.0f, aux, s);
+    tune_axis_pass(scratch, n, h, nz, nh, h, true, AxisMode::restore_half, 1.0f, aux, s);
+    if (cfg_.tv) tune_tv(x_.get(), tv_, nz, n, n, cfg_.lambda, s);
+  } else {
+    for (const bool fwd : {true, false}) {
+      tune_axis_pass(scratch, nz, nn, n, static_cast<std::size_t>(n), n, fwd, AxisMode::plain, 1.0f, AxisAux{}, s);
+      tune_axis_pass(scratch, n, static_cast<std::size_t>(n), nz, nn, n, fwd, AxisMode::plain, 1.0f, AxisAux{}, s);
+    }
+    if (cfg_.iterations > 0) {
+      check(cudaMemsetAsync(mask_.get(), 0, mask_.bytes(), s), "cudaMemset");
+      tune_axis_pass(scratch, n, static_cast<std::size_t>(n), nz, nn, n, true, AxisMode::restore_mask, 1.0f,
+                     AxisAux{measured_.get(), mask_.get()}, s);
+    }
+  }
+  check(cudaStreamSynchronize(s), "autotune");
 }
 
 std::size_t OdtPlan::device_bytes() const {

@@ -70,6 +70,7 @@ class OdtPlan {
 
  private:
   void mark(StageClock* clock, int m, cudaStream_t s) const;
+  void tune();
   void solve_real(float* index, float inv, cudaStream_t s);
   void solve_complex(float* index, float inv, cudaStream_t s);
 

@@ -36,6 +36,10 @@ struct AxisAux {
 std::size_t axis_smem_budget();
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s);
+// Times the tile widths of this axis pass on `data` (scratch: it is overwritten) and keeps the
+// fastest for later axis_pass calls of the same shape. Never inside a stream capture.
+void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
+                    AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s);
 
 // Rows of real length nx <-> half spectra of nx / 2 + 1 bins (rows dense, row pitches nx and
 // nx / 2 + 1). R2C optionally clamps its input at 0 (Gerchberg-Papoulis). C2R writes the real
@@ -80,5 +84,9 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
 
 // t_{k+1} of FISTA and FGP, 0.5 (1 + sqrt(1 + 4 t^2)) in float (host).
 float fista_t(float t);
+
+// Times the FGP tile heights on this volume's shape and keeps the fastest for later tv_prox calls.
+// b and all three dual triplets of t are scratch (overwritten). Never inside a stream capture.
+void tune_tv(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s);
 
 }  // namespace qhk

@@ -18,7 +18,9 @@
 #include <cmath>
 #include <mutex>
 #include <set>
+#include <vector>
 
+#include "autotune.hpp"
 #include "qhk_internal.hpp"
 
 namespace qhk {
@@ -341,21 +343,49 @@ std::size_t fgp_smem(int nx, int ty) {
   return (3 * static_cast<std::size_t>(3) * (ty + 2) + 4 * static_cast<std::size_t>(ty + 1)) * nx * sizeof(float);
 }
 
+// Rows per CTA that a CTA of this volume can take: tx * ty <= 256 threads and the shared memory
+// within the SM's limit; the default is the tallest of at most 4 rows within 110 KiB.
 template <int VEC>
-FgpShape fgp_shape(int nz, int ny, int nx) {
+std::vector<int> fgp_rows_candidates(int nx) {
+  std::vector<int> out;
+  const int tx = nx / VEC;
+  for (const int ty : {8, 4, 2, 1}) {
+    if (tx * ty <= 256 && fgp_smem(nx, ty) <= 200 * 1024) out.push_back(ty);
+  }
+  return out;
+}
+
+template <int VEC>
+int fgp_rows_default(int nx) {
   const int tx = nx / VEC;
   int ty = 4;
   while (ty > 1 && (tx * ty > 256 || fgp_smem(nx, ty) > 110 * 1024)) --ty;
-  require(tx * ty <= 256 && fgp_smem(nx, ty) <= 220 * 1024,
+  require(tx * ty <= 256 && fgp_smem(nx, ty) <= 200 * 1024,
           "tv: volume rows too long for the FGP kernel (at most 1024 float4-aligned or 256 other x values)");
+  return ty;
+}
+
+template <int VEC>
+TuneKey fgp_key(int nz, int ny, int nx) {
+  return tune_key(TuneFamily::fgp, {nz, ny, nx, VEC, 0, 0});
+}
+
+template <int VEC>
+FgpShape fgp_shape_rows(int nz, int ny, int nx, int ty) {
   const std::size_t smem = fgp_smem(nx, ty);
   auto kernel = k_fgp<VEC, false, false>;
   ensure_smem(kernel);
   int per_sm = 0;
-  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tx * ty, smem), "cudaOccupancy");
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (nx / VEC) * ty, smem), "cudaOccupancy");
   const long long slots = static_cast<long long>(sm_count()) * std::max(per_sm, 1);
   const long long units = static_cast<long long>((ny + ty - 1) / ty) * nz;
   return {ty, static_cast<int>(std::min(slots, units)), smem};
+}
+
+template <int VEC>
+FgpShape fgp_shape(int nz, int ny, int nx) {
+  const int ty = tuned_choice(fgp_key<VEC>(nz, ny, nx), fgp_rows_default<VEC>(nx));
+  return fgp_shape_rows<VEC>(nz, ny, nx, ty);
 }
 
 template <int VEC, bool FIRST, bool LAST>
@@ -451,6 +481,66 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
     launch_final<4>(final_mode, b, p, nz, ny, nx, lambda, momentum, xprev, out, nm2, inv_k02, s);
   } else {
     launch_final<1>(final_mode, b, p, nz, ny, nx, lambda, momentum, xprev, out, nm2, inv_k02, s);
+  }
+}
+
+namespace {
+
+// Deterministic pseudo-random values in [lo, hi) (tuning inputs only).
+__global__ void k_fill_hash(float* p, std::size_t n, float lo, float hi, unsigned seed) {
+  for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    unsigned h = static_cast<unsigned>(i) * 0x9E3779B1u + seed;
+    h ^= h >> 15;
+    h *= 0x85EBCA77u;
+    h ^= h >> 13;
+    p[i] = lo + (hi - lo) * static_cast<float>(h >> 8) * (1.0f / 16777216.0f);
+  }
+}
+
+template <int VEC>
+void tune_fgp_rows(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s) {
+  FgpArgs a{};
+  a.b = b;
+  a.nz = nz, a.ny = ny, a.nx = nx;
+  a.lambda = lambda, a.step = 1.0f / (12.0f * lambda), a.momentum = 0.5f;
+  for (int c = 0; c < 3; ++c) {
+    a.rin[c] = t.v[0][c];
+    a.pin[c] = t.v[1][c];
+    a.pout[c] = t.v[1][c];
+    a.rout[c] = t.v[2][c];
+  }
+  autotune(fgp_key<VEC>(nz, ny, nx), fgp_rows_candidates<VEC>(nx), fgp_rows_default<VEC>(nx),
+           [&](int ty) {
+             a.ytiles = (ny + ty - 1) / ty;
+             launch_fgp<VEC, false, false>(a, fgp_shape_rows<VEC>(nz, ny, nx, ty), s);
+           },
+           s);
+}
+
+}  // namespace
+
+void tune_tv(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s) {
+  require(nz >= 1 && ny >= 1 && nx >= 1, "tv: empty volume");
+  if (!autotune_enabled()) return;
+  const std::size_t vol = static_cast<std::size_t>(nz) * ny * nx;
+  const unsigned grid = static_cast<unsigned>(std::min<std::size_t>((vol + 255) / 256, 148u * 16u));
+  // Representative inputs: b in [0, 2), r in [-1, 1) (about half the dual points get projected),
+  // p = 0. All of them are scratch of the caller.
+  k_fill_hash<<<grid, 256, 0, s>>>(b, vol, 0.0f, 2.0f, 1u);
+  check_launch("tv tune fill");
+  for (int c = 0; c < 3; ++c) {
+    k_fill_hash<<<grid, 256, 0, s>>>(t.v[0][c], vol, -1.0f, 1.0f, 2u + c);
+    check_launch("tv tune fill");
+    check(cudaMemsetAsync(t.v[1][c], 0, vol * sizeof(float), s), "cudaMemset");
+  }
+  bool aligned = nx % 4 == 0 && reinterpret_cast<std::uintptr_t>(b) % 16 == 0;
+  for (int i = 0; i < 3; ++i)
+    for (int c = 0; c < 3; ++c) aligned = aligned && reinterpret_cast<std::uintptr_t>(t.v[i][c]) % 16 == 0;
+  if (aligned) {
+    tune_fgp_rows<4>(b, t, nz, ny, nx, lambda, s);
+  } else {
+    tune_fgp_rows<1>(b, t, nz, ny, nx, lambda, s);
   }
 }
 
