@@ -576,6 +576,157 @@ def geom_bpm_tuple():
     return (WAVELENGTH, N_MEDIUM, NA, BPM_PIXEL)
 
 
+C4_UNWRAP, C4_SIDES, C4_ODT = 512, (128, 192, 256, 384, 512), 64
+
+
+def phase_maps(torch, shapes, seed=31):
+    """Wrapped phase maps of smooth random surfaces: 3-6 Gaussians plus a tilt, peak-to-peak
+    ~U[10, 60] rad, plus N(0, 0.1 rad) noise (computed with torch on the GPU; fixture data)."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    rng = np.random.default_rng(seed)
+    out = []
+    for ny, nx in shapes:
+        y = torch.arange(ny, device="cuda", dtype=torch.float32)[:, None] / ny
+        x = torch.arange(nx, device="cuda", dtype=torch.float32)[None, :] / nx
+        surf = float(rng.uniform(-1, 1)) * y + float(rng.uniform(-1, 1)) * x
+        for _ in range(int(rng.integers(3, 7))):
+            cy, cx, sy, sx = rng.uniform(0, 1), rng.uniform(0, 1), rng.uniform(0.05, 0.3), rng.uniform(0.05, 0.3)
+            surf = surf + float(rng.uniform(-1, 1)) * torch.exp(-((y - cy) / sy) ** 2 - ((x - cx) / sx) ** 2)
+        surf = (surf - surf.min()) / (surf.max() - surf.min()).clamp_min(1e-9) * float(rng.uniform(10, 60))
+        surf = surf + 0.1 * torch.randn((ny, nx), device="cuda", generator=g)
+        out.append(torch.remainder(surf + math.pi, 2 * math.pi) - math.pi)
+    return out
+
+
+def c4_leg(qh, capi, torch, reps=5):
+    """C4 batching: (1) 512 least-squares unwrap instances of sizes drawn from {128..512}^2 in single
+    persistent launches (one per pass, graph-replayed) vs a per-image launch loop and the reference
+    CPU; (2) 64 reconstructions 49 x 128^2 -> 64^2 -> 64^3 GP-10 in one batched, graph-replayed
+    pipeline vs one pipeline run per request and the reference CPU."""
+    out = {}
+    stream = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(5)
+    sides = [int(v) for v in rng.choice(C4_SIDES, C4_UNWRAP)]
+    shapes = [(s_, s_) for s_ in sides]
+    maps = phase_maps(torch, shapes)
+    plan = capi.UnwrapBatch(shapes)
+    d_in = torch.cat([m.reshape(-1) for m in maps])
+    d_out = torch.empty_like(d_in)
+    pixels = plan.total
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(n):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / n
+
+    launches0 = capi.kernel_launches()
+    plan.run(d_in.data_ptr(), d_out.data_ptr(), stream, graph=True)  # direct first call
+    launches_batch = capi.kernel_launches() - launches0
+    t_graph = timed(lambda: plan.run(d_in.data_ptr(), d_out.data_ptr(), stream, graph=True), reps)
+    t_direct = timed(lambda: plan.run(d_in.data_ptr(), d_out.data_ptr(), stream, graph=False), reps)
+    batch_result = d_out.clone()
+    loop_out = torch.empty_like(d_in)
+
+    def per_image():
+        for off, (ny, nx) in zip(plan.offsets, shapes):
+            capi.unwrap_noalloc(d_in.data_ptr() + 4 * off, loop_out.data_ptr() + 4 * off, 1, ny, nx, stream)
+
+    t_loop = timed(per_image, 2)
+    diff = float((batch_result - loop_out).abs().max())
+    peak, which = measured_peaks()
+    alg = 8.0 * pixels
+    out["unwrap"] = {
+        "workload": f"{C4_UNWRAP} unwrap instances, sides drawn from {list(C4_SIDES)} (seeded), "
+                    f"{pixels} pixels, {alg / 1e6:.0f} MB algorithmic (read + write one float per pixel)",
+        "batched_graph_ms": round(t_graph, 3), "batched_direct_ms": round(t_direct, 3),
+        "per_image_loop_ms": round(t_loop, 3), "instances_per_s": round(C4_UNWRAP / (t_graph * 1e-3), 1),
+        "launches_per_batch": int(launches_batch), "launches_per_image_loop": 5 * C4_UNWRAP,
+        "achieved_gbs": round(alg / (t_graph * 1e-3) / 1e9, 1), "peak_gbs": peak, "peak_source": which,
+        "max_abs_diff_vs_per_image_loop": diff,
+        "per_image_loop": "qhk_unwrap_noalloc per image (five launches each), device buffers"}
+    try:
+        from oracle import refimpl
+
+        if refimpl.available():
+            sample = list(range(0, C4_UNWRAP, C4_UNWRAP // 16))
+            host = [maps[i].cpu().numpy() for i in sample]
+            t0 = time.perf_counter()
+            for h in host:
+                refimpl.unwrap(h[None])
+            ref_s = time.perf_counter() - t0
+            frac = sum(shapes[i][0] * shapes[i][1] for i in sample) / pixels
+            out["unwrap"]["reference_cpu_ms"] = round(1000.0 * ref_s / frac, 1)
+            out["unwrap"]["reference_cpu_sample"] = (f"{len(sample)} of the {C4_UNWRAP} instances, "
+                                                     f"scaled by pixel count, {refimpl.threads()} threads")
+    except Exception as e:  # noqa: BLE001
+        out["unwrap"]["reference_cpu_error"] = str(e)
+    del d_in, d_out, batch_result, loop_out, maps
+
+    # (2) small reconstructions
+    n_holo, m, count, carrier = 128, 64, 49, 35
+    geom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=0.2)
+    hgeom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=0.1)
+    illum = qh.circular_scan(count, 0.9, geom)
+    c = carrier / (n_holo * 0.1)
+    stacks = []
+    for k in range(C4_ODT):
+        sample_ = [("ellipsoid", (0.0, float(rng.uniform(-2, 2)), float(rng.uniform(-2, 2))), (2.5, 2.5, 2.5),
+                    N_MEDIUM + float(rng.uniform(0.01, 0.04)))]
+        ratio = phantom_fields(sample_, illum, n_holo, 0.1, "cuda")
+        stacks.append(qh.synthesize_holograms(ratio, illum, hgeom, carrier=(c, c), noise=NOISE, seed=k + 1))
+    bg = qh.synthesize_holograms(np.ones((count, n_holo, n_holo), np.complex64), illum, hgeom, carrier=(c, c),
+                                 noise=NOISE, seed=999)
+    gt = (WAVELENGTH, N_MEDIUM, NA, 0.2)
+    kw = dict(radius=30.0, output_size=m, iterations=10, solver="gp")
+    batched = capi.Pipeline(count, n_holo, (carrier, carrier), illum, gt, batch=C4_ODT, **kw)
+    batched.set_background(bg)
+    single = capi.Pipeline(count, n_holo, (carrier, carrier), illum, gt, **kw)
+    single.set_background(bg)
+    d_holo = torch.from_numpy(np.concatenate(stacks)).cuda()
+    d_index = torch.empty(batched.shape, dtype=torch.float32, device="cuda")
+    d_one = torch.empty(single.shape, dtype=torch.float32, device="cuda")
+    batched.process_device_graph(d_holo.data_ptr(), d_index.data_ptr(), stream)
+    launches0 = capi.kernel_launches()
+    batched.process_device_graph(d_holo.data_ptr(), d_index.data_ptr(), stream)
+    launches_b = capi.kernel_launches() - launches0
+    t_b = timed(lambda: batched.process_device_graph(d_holo.data_ptr(), d_index.data_ptr(), stream), reps)
+    stack = count * n_holo * n_holo
+
+    def per_request():
+        for k in range(C4_ODT):
+            single.process_device(d_holo.data_ptr() + 4 * k * stack, d_one.data_ptr(), stream)
+
+    t_s = timed(per_request, 2)
+    same = True
+    for k in (0, C4_ODT // 2, C4_ODT - 1):
+        single.process_device(d_holo.data_ptr() + 4 * k * stack, d_one.data_ptr(), stream)
+        same = same and bool(torch.equal(d_one, d_index[k]))
+    out["small_odt"] = {
+        "workload": f"{C4_ODT} x ({count}x{n_holo}^2 holograms -> {m}^2 fields -> {m}^3 GP-10), bead phantoms",
+        "batched_graph_ms": round(t_b, 3), "per_request_loop_ms": round(t_s, 3),
+        "recons_per_s": round(C4_ODT / (t_b * 1e-3), 1), "launches_per_batch": int(launches_b),
+        "batch_equals_single": same}
+    try:
+        from oracle import refimpl
+
+        if refimpl.available():
+            _, _, ms = refimpl.pipeline(stacks[0], bg, (carrier, carrier), 30.0, m, illum, gt, iterations=10,
+                                        solver="gp")
+            out["small_odt"]["reference_cpu_ms_per_recon"] = round(ms["run"], 1)
+            out["small_odt"]["reference_cpu_cores"] = refimpl.threads()
+    except Exception as e:  # noqa: BLE001
+        out["small_odt"]["reference_cpu_error"] = str(e)
+    batched.close()
+    single.close()
+    return out
+
+
 def kernel_case(name, reps):
     """Small standalone launches of one kernel family for profiling (no JSON line): `fgp` runs the
     TV proximal step at 256^3 (10 FGP steps + final primal per rep); `fft` a 256^3 rfft3 + irfft3
@@ -636,7 +787,7 @@ def kernel_case(name, reps):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "serve", "bpm"], default=None,
+    ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "serve", "bpm", "c4"], default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)
@@ -656,6 +807,14 @@ def main():
 
         print(json.dumps(serving_leg(qh, capi, args.serve_requests, args.serve_rate, args.serve_inflight,
                                      plain=not args.serve_no_plain)))
+        return 0
+    if args.kernel_case == "c4":
+        import torch
+
+        import qoraholo_b200 as qh
+        from qoraholo_b200 import capi
+
+        print(json.dumps(c4_leg(qh, capi, torch)))
         return 0
     if args.kernel_case == "bpm":
         import torch

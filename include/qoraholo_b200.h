@@ -166,6 +166,22 @@ int qhk_autotune_enable(int enabled);
  * full length. */
 size_t qhk_autotune_report(char* buf, size_t size);
 
+/* ---- Uneven unwrap batches (no counterpart in the reference, whose Unwrapper runs one image size per
+ * call and loops over images for the y transform, src/cuda/unwrap.cu:156-234). `count` images of
+ * their own even sizes ny[i] x nx[i], packed one after another on the device (image i starts at
+ * qhk_unwrap_batch_offset(plan, i) floats); each of the five passes is one persistent launch over the
+ * whole batch whose CTAs drain an (image, tile) queue. Every image's result is bitwise what
+ * qhk_unwrap gives for it alone. `use_graph` != 0 replays the five launches as one CUDA graph (the
+ * first call runs them directly). */
+typedef struct qhk_unwrap_batch qhk_unwrap_batch;
+int qhk_unwrap_batch_create(qhk_unwrap_batch** plan, const int* ny, const int* nx, int count);
+size_t qhk_unwrap_batch_offset(const qhk_unwrap_batch* plan, int image);
+size_t qhk_unwrap_batch_total(const qhk_unwrap_batch* plan);
+int qhk_unwrap_batch_run(qhk_unwrap_batch* plan, const float* d_wrapped, float* d_unwrapped, int use_graph,
+                         void* stream);
+size_t qhk_unwrap_batch_device_bytes(const qhk_unwrap_batch* plan);
+int qhk_unwrap_batch_destroy(qhk_unwrap_batch* plan);
+
 /* ---- Pipeline: replaces cuda::make_pipeline and Pipeline::Impl (src/backends.hpp:75-89,
  * src/cuda/pipeline.cu:12-161). Validation of the Pipeline constructor (src/pipeline.cpp:72-91). */
 typedef struct qhk_pipeline_options {
@@ -202,6 +218,15 @@ int qhk_pipeline_result(const qhk_pipeline* pipeline, double* filled, qhk_pipeli
 /* Filled fraction after process_device (waits for `stream`). */
 int qhk_pipeline_filled(qhk_pipeline* pipeline, void* stream, double* filled);
 int qhk_pipeline_shape(const qhk_pipeline* pipeline, int* nz, int* ny, int* nx);
+/* Batched pipeline (no counterpart in the reference): `batch` requests of this geometry per run, each
+ * pass one launch for all of them. Input (batch * count, N, N), output (batch, nz, m, m); the
+ * background holograms stay one stack (count, N, N). Supports the GP solver and plain Rytov ODT. */
+int qhk_pipeline_create_batched(qhk_pipeline** pipeline, const qhk_pipeline_options* options, const float* illum_fyfx,
+                                const qhk_geometry* geometry, int batch);
+/* process_device replayed as one CUDA graph (the first call for a pair of buffers runs directly). */
+int qhk_pipeline_process_device_graph(qhk_pipeline* pipeline, const float* d_holo, float* d_index, void* stream);
+/* Filled fraction of each of the batch's volumes after process_device (waits for `stream`). */
+int qhk_pipeline_filled_batch(qhk_pipeline* pipeline, void* stream, double* filled);
 size_t qhk_pipeline_device_bytes(const qhk_pipeline* pipeline);
 int qhk_pipeline_destroy(qhk_pipeline* pipeline);
 

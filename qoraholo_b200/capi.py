@@ -98,6 +98,15 @@ _PROTOS = {
     "qhk_pipeline_shape": (_I, [_VP, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "qhk_pipeline_device_bytes": (C.c_size_t, [_VP]),
     "qhk_pipeline_destroy": (_I, [_VP]),
+    "qhk_pipeline_create_batched": (_I, [C.POINTER(_VP), _VP, _VP, C.POINTER(Geometry), _I]),
+    "qhk_pipeline_process_device_graph": (_I, [_VP, _VP, _VP, _VP]),
+    "qhk_pipeline_filled_batch": (_I, [_VP, _VP, _VP]),
+    "qhk_unwrap_batch_create": (_I, [C.POINTER(_VP), _VP, _VP, _I]),
+    "qhk_unwrap_batch_offset": (C.c_size_t, [_VP, _I]),
+    "qhk_unwrap_batch_total": (C.c_size_t, [_VP]),
+    "qhk_unwrap_batch_run": (_I, [_VP, _VP, _VP, _I, _VP]),
+    "qhk_unwrap_batch_device_bytes": (C.c_size_t, [_VP]),
+    "qhk_unwrap_batch_destroy": (_I, [_VP]),
     "qhk_autotune_enable": (_I, [_I]),
     "qhk_autotune_report": (C.c_size_t, [_VP, C.c_size_t]),
     "qhk_server_create": (_I, [C.POINTER(_VP), C.c_size_t, _I, _I]),
@@ -266,21 +275,70 @@ def bpm_vjp(x, r, illuminations, geom, obliquity=True):
     return out
 
 
+class UnwrapBatch:
+    """qhk_unwrap_batch_*: least-squares unwrap of images of uneven sizes packed in one device buffer,
+    one persistent launch per pass for the whole batch. `shapes`: (ny, nx) per image; `offsets[i]`
+    is the first float of image i; `total` the packed length."""
+
+    def __init__(self, shapes):
+        sh = np.ascontiguousarray(np.reshape(shapes, (-1, 2)), np.int32)
+        ny = np.ascontiguousarray(sh[:, 0])
+        nx = np.ascontiguousarray(sh[:, 1])
+        self._h = _VP()
+        check(lib().qhk_unwrap_batch_create(C.byref(self._h), host_ptr(ny), host_ptr(nx), len(sh)))
+        self.shapes = [tuple(map(int, r)) for r in sh]
+        self.offsets = [int(lib().qhk_unwrap_batch_offset(self._h, i)) for i in range(len(sh))]
+        self.total = int(lib().qhk_unwrap_batch_total(self._h))
+
+    def run(self, d_wrapped, d_unwrapped, stream=0, graph=False):
+        check(lib().qhk_unwrap_batch_run(self._h, _VP(d_wrapped), _VP(d_unwrapped), int(bool(graph)), _VP(stream)))
+
+    @property
+    def device_bytes(self):
+        return int(lib().qhk_unwrap_batch_device_bytes(self._h))
+
+    def pack(self, images):
+        """Host images (a list of (ny, nx) float32 arrays) -> one packed float32 array."""
+        return np.concatenate([np.ascontiguousarray(a, np.float32).ravel() for a in images])
+
+    def unpack(self, packed):
+        return [packed[o:o + ny * nx].reshape(ny, nx) for o, (ny, nx) in zip(self.offsets, self.shapes)]
+
+    def close(self):
+        if self._h:
+            check(lib().qhk_unwrap_batch_destroy(self._h))
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Pipeline:
     """qhk_pipeline_*: holograms -> index with resident device state. `process()` works from the
-    page-locked input buffer (``input`` view); `process_device` from device pointers."""
+    page-locked input buffer (``input`` view); `process_device` from device pointers. With
+    ``batch`` > 1, `batch` requests of this geometry run together (one launch per pass): input
+    (batch * count, N, N), output (batch, nz, n, n)."""
 
     def __init__(self, count, hologram_size, center, illuminations, geom, radius=0.0, output_size=0, upload_chunks=1,
-                 **odt):
+                 batch=1, **odt):
         self._il = np.ascontiguousarray(np.reshape(illuminations, (-1, 2)), np.float32)
         o = PipelineOptions(int(count), int(hologram_size), float(center[0]), float(center[1]), float(radius),
                             int(output_size), int(upload_chunks), odt_options(**odt))
         self._h = _VP()
-        check(lib().qhk_pipeline_create(C.byref(self._h), C.byref(o), host_ptr(self._il), C.byref(geometry(geom))))
+        self.batch = int(batch)
+        if self.batch == 1:
+            check(lib().qhk_pipeline_create(C.byref(self._h), C.byref(o), host_ptr(self._il),
+                                            C.byref(geometry(geom))))
+        else:
+            check(lib().qhk_pipeline_create_batched(C.byref(self._h), C.byref(o), host_ptr(self._il),
+                                                    C.byref(geometry(geom)), self.batch))
         nz, ny, nx = _I(), _I(), _I()
         check(lib().qhk_pipeline_shape(self._h, C.byref(nz), C.byref(ny), C.byref(nx)))
-        self.shape = (nz.value, ny.value, nx.value)
-        self.input_shape = (int(count), int(hologram_size), int(hologram_size))
+        self.shape = (nz.value, ny.value, nx.value) if self.batch == 1 else (self.batch, nz.value, ny.value, nx.value)
+        self.input_shape = (int(count) * self.batch, int(hologram_size), int(hologram_size))
         n_in = int(np.prod(self.input_shape))
         n_out = int(np.prod(self.shape))
         self.input = np.ctypeslib.as_array(C.cast(lib().qhk_pipeline_input(self._h), C.POINTER(C.c_float)),
@@ -297,6 +355,15 @@ class Pipeline:
 
     def process_device(self, d_holo, d_index, stream=0):
         check(lib().qhk_pipeline_process_device(self._h, _VP(d_holo), _VP(d_index), _VP(stream)))
+
+    def process_device_graph(self, d_holo, d_index, stream=0):
+        """process_device replayed as one CUDA graph (the first call for these buffers runs directly)."""
+        check(lib().qhk_pipeline_process_device_graph(self._h, _VP(d_holo), _VP(d_index), _VP(stream)))
+
+    def filled_batch(self, stream=0):
+        out = np.zeros(self.batch, np.float64)
+        check(lib().qhk_pipeline_filled_batch(self._h, _VP(stream), host_ptr(out)))
+        return out
 
     def result(self):
         filled = C.c_double()

@@ -408,6 +408,44 @@ int qhk_pipeline_create(qhk_pipeline** pipeline, const qhk_pipeline_options* o, 
   });
 }
 
+int qhk_pipeline_create_batched(qhk_pipeline** pipeline, const qhk_pipeline_options* o, const float* illum_fyfx,
+                                const qhk_geometry* geometry, int batch) {
+  return guard([&] {
+    qhk::require(pipeline && o, "Pipeline: null argument");
+    qhk::require(batch >= 1, "Pipeline: batch must be positive");
+    const int n = o->hologram_size;
+    qhk::require(o->count >= 1, "Pipeline: count must be positive");
+    qhk::require(n >= 4 && n % 2 == 0, "Pipeline: hologram_size must be even");
+    const qhk::CropPlan crop = qhk::make_crop(n, o->center_y, o->center_x, o->radius, o->output_size);
+    qhk::OdtConfig c = odt_config(crop.out, o->count, illum_fyfx, geometry, &o->odt);
+    qhk::require(batch == 1 || !c.tv, "Pipeline: batches need the GP solver or plain Rytov ODT");
+    c.batch = batch;
+    qhk::require(o->upload_chunks >= 1 && o->upload_chunks <= o->count * batch,
+                 "Pipeline: upload_chunks must be between 1 and count * batch");
+    *pipeline = new qhk_pipeline{qhk::PipelinePlan(crop, o->count, o->upload_chunks, c, illum_fyfx)};
+  });
+}
+
+int qhk_pipeline_process_device_graph(qhk_pipeline* p, const float* d_holo, float* d_index, void* stream) {
+  return guard([&] {
+    qhk::require(p && d_holo && d_index, "Pipeline: null argument");
+    p->plan.process_device_graph(d_holo, d_index, as_stream(stream));
+  });
+}
+
+int qhk_pipeline_filled_batch(qhk_pipeline* p, void* stream, double* filled) {
+  return guard([&] {
+    qhk::require(p && filled, "Pipeline: null argument");
+    const int b = p->plan.batch();
+    std::vector<unsigned long long> v(b);
+    qhk::check(cudaMemcpyAsync(v.data(), p->plan.odt().filled(), b * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, as_stream(stream)),
+               "download filled");
+    qhk::check(cudaStreamSynchronize(as_stream(stream)), "qhk_pipeline_filled_batch");
+    for (int i = 0; i < b; ++i) filled[i] = static_cast<double>(v[i]) / static_cast<double>(p->plan.odt().volume());
+  });
+}
+
 int qhk_pipeline_set_background(qhk_pipeline* p, const float* backgrounds) {
   return guard([&] {
     qhk::require(p && backgrounds, "Pipeline::set_background: null argument");
@@ -653,6 +691,41 @@ size_t qhk_autotune_report(char* buf, size_t size) {
     buf[n] = '\0';
   }
   return r.size();
+}
+
+struct qhk_unwrap_batch {
+  qhk::UnwrapBatchPlan plan;
+};
+
+int qhk_unwrap_batch_create(qhk_unwrap_batch** plan, const int* ny, const int* nx, int count) {
+  return guard([&] {
+    qhk::require(plan != nullptr, "unwrap batch: null argument");
+    *plan = new qhk_unwrap_batch{qhk::UnwrapBatchPlan(ny, nx, count)};
+  });
+}
+
+size_t qhk_unwrap_batch_offset(const qhk_unwrap_batch* p, int image) {
+  return p && image >= 0 && image < p->plan.count() ? p->plan.offset(image) : 0;
+}
+
+size_t qhk_unwrap_batch_total(const qhk_unwrap_batch* p) { return p ? p->plan.total() : 0; }
+
+int qhk_unwrap_batch_run(qhk_unwrap_batch* p, const float* d_wrapped, float* d_unwrapped, int use_graph,
+                         void* stream) {
+  return guard([&] {
+    qhk::require(p && d_wrapped && d_unwrapped, "unwrap batch: null argument");
+    if (use_graph) {
+      p->plan.unwrap_graph(d_wrapped, d_unwrapped, as_stream(stream));
+    } else {
+      p->plan.unwrap(d_wrapped, d_unwrapped, as_stream(stream));
+    }
+  });
+}
+
+size_t qhk_unwrap_batch_device_bytes(const qhk_unwrap_batch* p) { return p ? p->plan.device_bytes() : 0; }
+
+int qhk_unwrap_batch_destroy(qhk_unwrap_batch* p) {
+  return guard([&] { delete p; });
 }
 
 struct qhk_server {

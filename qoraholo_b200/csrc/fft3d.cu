@@ -73,14 +73,15 @@ constexpr int kBatch = 8;  // loads in flight per thread in the strided passes
 template <bool Fwd, int Mode, int COLS>
 __global__ void __launch_bounds__(kThreads)
     k_axis(float2* __restrict__ data, std::size_t so, std::size_t sp, int ni, FftLen L, float scale,
-           const float2* __restrict__ aux_a, const std::uint8_t* __restrict__ aux_h) {
+           const float2* __restrict__ aux_a, const std::uint8_t* __restrict__ aux_h, std::size_t sb) {
   extern __shared__ float2 sm[];
   const int n = L.n;
   float2* A = sm;
   float2* B = sm + static_cast<std::size_t>(n) * COLS;
   const int c0 = static_cast<int>(blockIdx.x) * COLS;
   const int cols = min(COLS, ni - c0);
-  const std::size_t base = static_cast<std::size_t>(blockIdx.y) * so + c0;
+  // Volume blockIdx.z of a batch starts sb elements after the previous one (data and aux alike).
+  const std::size_t base = static_cast<std::size_t>(blockIdx.z) * sb + static_cast<std::size_t>(blockIdx.y) * so + c0;
   const int tid = static_cast<int>(threadIdx.x);
   const int nth = static_cast<int>(blockDim.x);
   constexpr int kFrom = static_cast<int>(AxisMode::from_data);
@@ -167,41 +168,41 @@ __global__ void __launch_bounds__(kThreads)
 
 template <bool Fwd, int Mode, int COLS>
 void launch_axis(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, float scale,
-                 const AxisAux& aux, cudaStream_t s) {
+                 const AxisAux& aux, int batch, std::size_t sb, cudaStream_t s) {
   const FftLen& L = fft_len(n);
   const std::size_t smem = 2 * static_cast<std::size_t>(n) * COLS * sizeof(float2);
   auto kernel = k_axis<Fwd, Mode, COLS>;
   allow_smem(kernel, smem);
-  const dim3 grid((ni + COLS - 1) / COLS, n_outer);
-  kernel<<<grid, kThreads, smem, s>>>(data, so, sp, ni, L, scale, aux.a, aux.hits);
+  const dim3 grid((ni + COLS - 1) / COLS, n_outer, batch);
+  kernel<<<grid, kThreads, smem, s>>>(data, so, sp, ni, L, scale, aux.a, aux.hits, sb);
   check_launch("fft axis pass");
 }
 
 template <int Mode, int COLS>
 void axis_dispatch_dir(bool forward, float2* data, int n_outer, std::size_t so, int n, std::size_t sp,
-                       int ni, float scale, const AxisAux& aux, cudaStream_t s) {
+                       int ni, float scale, const AxisAux& aux, int batch, std::size_t sb, cudaStream_t s) {
   if (forward) {
-    launch_axis<true, Mode, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+    launch_axis<true, Mode, COLS>(data, n_outer, so, n, sp, ni, scale, aux, batch, sb, s);
   } else {
-    launch_axis<false, Mode, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+    launch_axis<false, Mode, COLS>(data, n_outer, so, n, sp, ni, scale, aux, batch, sb, s);
   }
 }
 
 template <int COLS>
 void axis_dispatch(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-                   AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
+                   AxisMode mode, float scale, const AxisAux& aux, int batch, std::size_t sb, cudaStream_t s) {
   switch (mode) {
     case AxisMode::plain:
-      axis_dispatch_dir<0, COLS>(forward, data, n_outer, so, n, sp, ni, scale, aux, s);
+      axis_dispatch_dir<0, COLS>(forward, data, n_outer, so, n, sp, ni, scale, aux, batch, sb, s);
       break;
     case AxisMode::restore_half:
-      launch_axis<true, 1, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+      launch_axis<true, 1, COLS>(data, n_outer, so, n, sp, ni, scale, aux, batch, sb, s);
       break;
     case AxisMode::restore_mask:
-      launch_axis<true, 2, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+      launch_axis<true, 2, COLS>(data, n_outer, so, n, sp, ni, scale, aux, batch, sb, s);
       break;
     case AxisMode::from_data:
-      launch_axis<false, 3, COLS>(data, n_outer, so, n, sp, ni, scale, aux, s);
+      launch_axis<false, 3, COLS>(data, n_outer, so, n, sp, ni, scale, aux, batch, sb, s);
       break;
   }
 }
@@ -478,12 +479,12 @@ const FftLen& fft_len(int n) {
 namespace {
 
 void axis_cols(int cols, float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
+               AxisMode mode, float scale, const AxisAux& aux, int batch, std::size_t sb, cudaStream_t s) {
   switch (cols) {
-    case 16: axis_dispatch<16>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
-    case 8: axis_dispatch<8>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
-    case 4: axis_dispatch<4>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
-    default: axis_dispatch<1>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); break;
+    case 16: axis_dispatch<16>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); break;
+    case 8: axis_dispatch<8>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); break;
+    case 4: axis_dispatch<4>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); break;
+    default: axis_dispatch<1>(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); break;
   }
 }
 
@@ -504,26 +505,29 @@ int axis_default(int n) {
   return 1;
 }
 
-TuneKey axis_key(int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward, AxisMode mode) {
+TuneKey axis_key(int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward, AxisMode mode,
+                 int batch) {
   return tune_key(TuneFamily::axis, {n, ni, n_outer, static_cast<long long>(so), static_cast<long long>(sp),
-                                     2 * static_cast<long long>(mode) + (forward ? 1 : 0)});
+                                     2 * static_cast<long long>(mode) + (forward ? 1 : 0) + 16LL * batch});
 }
 
 }  // namespace
 
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
-  require(n_outer >= 1 && n_outer <= 65535, "fft: too many lines in the outer dimension");
+               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
+  require(n_outer >= 1 && n_outer <= 65535 && batch >= 1 && batch <= 65535,
+          "fft: too many lines in the outer dimension");
   require(static_cast<std::size_t>(n) * 2 * sizeof(float2) <= 200 * 1024, "fft: transform length too large");
-  const int cols = tuned_choice(axis_key(n_outer, so, n, sp, ni, forward, mode), axis_default(n));
-  axis_cols(cols, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s);
+  const int cols = tuned_choice(axis_key(n_outer, so, n, sp, ni, forward, mode, batch), axis_default(n));
+  axis_cols(cols, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s);
 }
 
 void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-                    AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s) {
-  require(n_outer >= 1 && n_outer <= 65535, "fft: too many lines in the outer dimension");
-  autotune(axis_key(n_outer, so, n, sp, ni, forward, mode), axis_candidates(n), axis_default(n),
-           [&](int c) { axis_cols(c, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s); }, s);
+                    AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
+  require(n_outer >= 1 && n_outer <= 65535 && batch >= 1 && batch <= 65535,
+          "fft: too many lines in the outer dimension");
+  autotune(axis_key(n_outer, so, n, sp, ni, forward, mode, batch), axis_candidates(n), axis_default(n),
+           [&](int c) { axis_cols(c, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); }, s);
 }
 
 // Lengths with compile-time row kernels (the common volume and image sides); others run the

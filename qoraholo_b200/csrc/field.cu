@@ -113,12 +113,13 @@ __global__ void __launch_bounds__(kThreads)
 // Pass 3. Output rows (count * m rows of m), COLS rows per CTA: place the W columns at
 // m/2 + dxlo + j, inverse m-point FFT along x, then the epilogue of `Mode`.
 //   0: field = v * (-1)^(x+y) / N^2
-//   1: ratio to `bg` (a demodulated field) -> psi = arg, logamp = log |.|
+//   1: ratio to `bg` (a demodulated field; stacks of several requests reuse the bg_rows rows of one
+//      geometry's backgrounds) -> psi = arg, logamp = log |.|
 template <int Mode, int COLS>
 __global__ void __launch_bounds__(kThreads)
     k_field_rows(const float2* __restrict__ t2, std::size_t rows, int m, int W, int x0, FftLen Lmo, float inv_nn,
                  float2* __restrict__ field, const float2* __restrict__ bg, float* __restrict__ psi,
-                 float* __restrict__ logamp) {
+                 float* __restrict__ logamp, std::size_t bg_rows) {
   extern __shared__ float2 sm[];
   constexpr int cp = COLS + 1;
   float2* A = sm;
@@ -126,6 +127,8 @@ __global__ void __launch_bounds__(kThreads)
   const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
   const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
   const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
+  __shared__ std::size_t bg_row[COLS];  // first background element of each row
+  if (Mode == 1 && tid < COLS) bg_row[tid] = ((r0 + tid) % bg_rows) * m;
   for (int idx = tid; idx < m * COLS; idx += nth) A[idx + idx / COLS] = make_float2(0.f, 0.f);  // pitch cp
   __syncthreads();
   for (int idx = tid; idx < W * COLS; idx += nth) {
@@ -145,7 +148,7 @@ __global__ void __launch_bounds__(kThreads)
     if constexpr (Mode == 0) {
       field[g] = v;
     } else {
-      const float2 b = bg[g];
+      const float2 b = bg[bg_row[row] + x];  // the background stack repeats every bg_rows rows
       const float d = 1.0f / (b.x * b.x + b.y * b.y);
       const float re = (v.x * b.x + v.y * b.y) * d;
       const float im = (v.y * b.x - v.x * b.y) * d;
@@ -251,10 +254,13 @@ void FieldPlan::spectra(const float* holo, int first, int valid, cudaStream_t s)
   }
 }
 
-void FieldPlan::finish(int mode, float2* field, const float2* bg, float* psi, float* logamp, cudaStream_t s) {
+void FieldPlan::finish(int mode, float2* field, const float2* bg, float* psi, float* logamp, cudaStream_t s,
+                       int bg_count, int images) {
   const int N = plan_.n, m = plan_.out;
+  const std::size_t bg_rows = static_cast<std::size_t>(bg_count > 0 ? bg_count : count_) * m;
   const FftLen& Lo = fft_len(m);
-  const std::size_t rows = static_cast<std::size_t>(count_) * m;
+  require(images >= 0 && images <= count_, "fields: image count beyond the plan");
+  const std::size_t rows = static_cast<std::size_t>(images > 0 ? images : count_) * m;
   const int c = rows_per_cta(m);
   const std::size_t smem = 2 * static_cast<std::size_t>(m) * (c + 1) * sizeof(float2);
   const unsigned grid = static_cast<unsigned>((rows + c - 1) / c);
@@ -265,11 +271,11 @@ void FieldPlan::finish(int mode, float2* field, const float2* bg, float* psi, fl
     if (mode == 0) {                                                                                      \
       allow(k_field_rows<0, C>, smem);                                                                    \
       k_field_rows<0, C><<<grid, kThreads, smem, s>>>(t2_.get(), rows, m, W_, x0, Lo, inv_nn, field, bg, psi, \
-                                                       logamp);                                             \
+                                                       logamp, bg_rows);                                    \
     } else {                                                                                              \
       allow(k_field_rows<1, C>, smem);                                                                    \
       k_field_rows<1, C><<<grid, kThreads, smem, s>>>(t2_.get(), rows, m, W_, x0, Lo, inv_nn, field, bg, psi, \
-                                                       logamp);                                             \
+                                                       logamp, bg_rows);                                    \
     }                                                                                                     \
     break;
   switch (c) {

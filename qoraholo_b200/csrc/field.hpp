@@ -25,7 +25,10 @@ class FieldPlan {
   void spectra(const float* holo, int first, int valid, cudaStream_t s);
   // Pass 3 for all holograms: mode 0 writes demodulated fields (count, m, m); mode 1 writes the
   // phase and log-amplitude of the ratio to the background fields `bg`.
-  void finish(int mode, float2* field, const float2* bg, float* psi, float* logamp, cudaStream_t s);
+  // bg_count > 0: `bg` holds that many images and image i uses background i % bg_count (a stack of
+  // several requests of one geometry). images > 0: only the first `images` images.
+  void finish(int mode, float2* field, const float2* bg, float* psi, float* logamp, cudaStream_t s,
+              int bg_count = 0, int images = 0);
   // All three passes, demodulated fields.
   void fields(const float* holo, float2* out, cudaStream_t s);
 

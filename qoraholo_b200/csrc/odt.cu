@@ -57,6 +57,13 @@ __global__ void __launch_bounds__(256)
     k_map_half(const float2* __restrict__ spectra, const float4* __restrict__ illum, int count, Grid g,
                float2* __restrict__ a, std::uint8_t* __restrict__ hits, unsigned long long* __restrict__ filled) {
   const int n = g.n, nz = g.nz, h = n / 2 + 1;
+  {  // volume blockIdx.y of a batch: its own spectra, k-space arrays and filled count
+    const std::size_t v = blockIdx.y;
+    spectra += v * count * static_cast<std::size_t>(n) * n;
+    a += v * nz * static_cast<std::size_t>(n) * h;
+    hits += v * nz * static_cast<std::size_t>(n) * h;
+    filled += v;
+  }
   const int chunks = (nz + kMapK - 1) / kMapK;
   const std::size_t total = static_cast<std::size_t>(chunks) * n * h;
   const std::size_t t = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x;
@@ -120,6 +127,15 @@ __global__ void __launch_bounds__(256)
                float2* __restrict__ pot, float2* __restrict__ measured, std::uint8_t* __restrict__ mask,
                unsigned long long* __restrict__ filled) {
   const int n = g.n, nz = g.nz;
+  {  // volume blockIdx.y of a batch
+    const std::size_t v = blockIdx.y;
+    const std::size_t vol = nz * static_cast<std::size_t>(n) * n;
+    spectra += v * count * static_cast<std::size_t>(n) * n;
+    pot += v * vol;
+    if (measured) measured += v * vol;
+    mask += v * vol;
+    filled += v;
+  }
   const int chunks = (nz + kMapK - 1) / kMapK;
   const std::size_t total = static_cast<std::size_t>(chunks) * n * n;
   const std::size_t t = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x;
@@ -164,18 +180,21 @@ __global__ void __launch_bounds__(256)
 }  // namespace
 
 void map_half(const float2* spectra, const float4* illum, int count, const Grid& g, float2* a, std::uint8_t* hits,
-              unsigned long long* filled, cudaStream_t s) {
+              unsigned long long* filled, cudaStream_t s, int batch) {
+  require(batch >= 1 && batch <= 65535, "ewald mapping: invalid batch");
   const int chunks = (g.nz + kMapK - 1) / kMapK;
   const std::size_t threads = static_cast<std::size_t>(chunks) * g.n * (g.n / 2 + 1);
-  k_map_half<<<blocks_for(threads, 256), 256, 0, s>>>(spectra, illum, count, g, a, hits, filled);
+  k_map_half<<<dim3(blocks_for(threads, 256), batch), 256, 0, s>>>(spectra, illum, count, g, a, hits, filled);
   check_launch("ewald mapping");
 }
 
 void map_full(const float2* spectra, const float4* illum, int count, const Grid& g, float2* pot, float2* measured,
-              std::uint8_t* mask, unsigned long long* filled, cudaStream_t s) {
+              std::uint8_t* mask, unsigned long long* filled, cudaStream_t s, int batch) {
+  require(batch >= 1 && batch <= 65535, "ewald mapping: invalid batch");
   const int chunks = (g.nz + kMapK - 1) / kMapK;
   const std::size_t threads = static_cast<std::size_t>(chunks) * g.n * g.n;
-  k_map_full<<<blocks_for(threads, 256), 256, 0, s>>>(spectra, illum, count, g, pot, measured, mask, filled);
+  k_map_full<<<dim3(blocks_for(threads, 256), batch), 256, 0, s>>>(spectra, illum, count, g, pot, measured, mask,
+                                                                   filled);
   check_launch("ewald mapping");
 }
 
@@ -206,18 +225,22 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
   const int n = g.n, nz = g.nz, h = n / 2 + 1;
   require(n >= 4 && n % 2 == 0 && nz >= 2 && nz % 2 == 0, "odt: invalid grid");
   require(cfg_.count >= 1, "odt: need at least one field");
+  require(cfg_.batch >= 1 && cfg_.batch <= 65535 && (cfg_.batch == 1 || !cfg_.tv) &&
+              static_cast<long long>(cfg_.batch) * nz <= 65535,
+          "odt: batches of reconstructions need the GP solver and batch * nz <= 65535");
   real_ = cfg_.iterations > 0 && (cfg_.tv || cfg_.r2c);
   half_ = static_cast<std::size_t>(nz) * n * h;
   vol_ = static_cast<std::size_t>(nz) * n * n;
+  const std::size_t b = cfg_.batch;
   const std::vector<float4> il = illumination_table(g, illum_fyfx, cfg_.count);
   illum_.reset(cfg_.count);
   check(cudaMemcpy(illum_.get(), il.data(), il.size() * sizeof(float4), cudaMemcpyHostToDevice), "upload illuminations");
-  filled_.reset(1);
+  filled_.reset(b);
   if (real_) {
-    a_.reset(half_);
-    hits_.reset(half_);
-    e_.reset(half_);
-    x_.reset(vol_);
+    a_.reset(b * half_);
+    hits_.reset(b * half_);
+    e_.reset(b * half_);
+    x_.reset(b * vol_);
     if (cfg_.tv) {
       xprev_.reset(vol_);
       dual_.reset(9 * vol_);
@@ -225,9 +248,9 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
         for (int c = 0; c < 3; ++c) tv_.v[i][c] = dual_.get() + (3 * i + c) * vol_;
     }
   } else {
-    pot_.reset(vol_);
-    mask_.reset(vol_);
-    if (cfg_.iterations > 0) measured_.reset(vol_);
+    pot_.reset(b * vol_);
+    mask_.reset(b * vol_);
+    if (cfg_.iterations > 0) measured_.reset(b * vol_);
   }
   tune();
 }
@@ -243,10 +266,11 @@ void OdtPlan::tune() {
   const std::size_t nn = static_cast<std::size_t>(n) * n;
   Stream stream;
   const cudaStream_t s = stream.get();
+  const int b = cfg_.batch;
   float2* scratch = real_ ? e_.get() : pot_.get();
-  const std::size_t room = real_ ? half_ : vol_;
-  if (static_cast<std::size_t>(cfg_.count) * nn <= room) {  // the 2D FFT of the fields
-    tune_axis_pass(scratch, cfg_.count, nn, n, static_cast<std::size_t>(n), n, true, AxisMode::plain, 1.0f,
+  const std::size_t room = static_cast<std::size_t>(b) * (real_ ? half_ : vol_);
+  if (static_cast<std::size_t>(cfg_.count) * b * nn <= room) {  // the 2D FFT of the fields
+    tune_axis_pass(scratch, cfg_.count * b, nn, n, static_cast<std::size_t>(n), n, true, AxisMode::plain, 1.0f,
                    AxisAux{}, s);
   }
   if (real_) {
@@ -254,20 +278,22 @@ void OdtPlan::tune() {
     check(cudaMemsetAsync(a_.get(), 0, a_.bytes(), s), "cudaMemset");
     check(cudaMemsetAsync(hits_.get(), 0, hits_.bytes(), s), "cudaMemset");
     for (const bool fwd : {true, false}) {
-      tune_axis_pass(scratch, nz, nh, n, h, h, fwd, AxisMode::plain, 1.0f, AxisAux{}, s);
+      tune_axis_pass(scratch, b * nz, nh, n, h, h, fwd, AxisMode::plain, 1.0f, AxisAux{}, s);
     }
-    tune_axis_pass(scratch, n, h, nz, nh, h, false, AxisMode::from_data, 1.0f, aux, s);
-    tune_axis_pass(scratch, n, h, nz, nh, h, true, AxisMode::restore_half, 1.0f, aux, s);
+    tune_axis_pass(scratch, n, h, nz, nh, h, false, AxisMode::from_data, 1.0f, aux, s, b, half_);
+    tune_axis_pass(scratch, n, h, nz, nh, h, true, AxisMode::restore_half, 1.0f, aux, s, b, half_);
     if (cfg_.tv) tune_tv(x_.get(), tv_, nz, n, n, cfg_.lambda, s);
   } else {
     for (const bool fwd : {true, false}) {
-      tune_axis_pass(scratch, nz, nn, n, static_cast<std::size_t>(n), n, fwd, AxisMode::plain, 1.0f, AxisAux{}, s);
-      tune_axis_pass(scratch, n, static_cast<std::size_t>(n), nz, nn, n, fwd, AxisMode::plain, 1.0f, AxisAux{}, s);
+      tune_axis_pass(scratch, b * nz, nn, n, static_cast<std::size_t>(n), n, fwd, AxisMode::plain, 1.0f, AxisAux{},
+                     s);
+      tune_axis_pass(scratch, n, static_cast<std::size_t>(n), nz, nn, n, fwd, AxisMode::plain, 1.0f, AxisAux{}, s,
+                     b, vol_);
     }
     if (cfg_.iterations > 0) {
       check(cudaMemsetAsync(mask_.get(), 0, mask_.bytes(), s), "cudaMemset");
       tune_axis_pass(scratch, n, static_cast<std::size_t>(n), nz, nn, n, true, AxisMode::restore_mask, 1.0f,
-                     AxisAux{measured_.get(), mask_.get()}, s);
+                     AxisAux{measured_.get(), mask_.get()}, s, b, vol_);
     }
   }
   check(cudaStreamSynchronize(s), "autotune");
@@ -289,14 +315,15 @@ void OdtPlan::run(float2* fields, float* index, cudaStream_t s, StageClock* cloc
   const std::size_t nn = static_cast<std::size_t>(n) * n;
   const float inv = 1.0f / (static_cast<float>(nz) * static_cast<float>(n) * static_cast<float>(n));
 
-  fft2d(fields, cfg_.count, n, true, 1.0f, s);
+  fft2d(fields, cfg_.count * cfg_.batch, n, true, 1.0f, s);
   mark(clock, kMarkFft2, s);
-  check(cudaMemsetAsync(filled_.get(), 0, sizeof(unsigned long long), s), "cudaMemset");
+  check(cudaMemsetAsync(filled_.get(), 0, filled_.bytes(), s), "cudaMemset");
   mark(clock, kMarkClear, s);
   if (real_) {
-    map_half(fields, illum_.get(), cfg_.count, g, a_.get(), hits_.get(), filled_.get(), s);
+    map_half(fields, illum_.get(), cfg_.count, g, a_.get(), hits_.get(), filled_.get(), s, cfg_.batch);
   } else {
-    map_full(fields, illum_.get(), cfg_.count, g, pot_.get(), measured_.get(), mask_.get(), filled_.get(), s);
+    map_full(fields, illum_.get(), cfg_.count, g, pot_.get(), measured_.get(), mask_.get(), filled_.get(), s,
+             cfg_.batch);
   }
   mark(clock, kMarkMapping, s);
   mark(clock, kMarkNormalize, s);
@@ -316,18 +343,19 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
   const Grid& g = cfg_.grid;
   const int n = g.n, nz = g.nz, h = n / 2 + 1;
   const std::size_t nh = static_cast<std::size_t>(n) * h;
-  const std::size_t rows = static_cast<std::size_t>(nz) * n;
+  const int b = cfg_.batch;  // volumes, one after another: y passes and rows span the batch
+  const std::size_t rows = static_cast<std::size_t>(b) * nz * n;
   float2* e = e_.get();
   const AxisAux aux{a_.get(), hits_.get()};
   // E = a * inv, inverse along z, then y, then C2R along x.
-  axis_pass(e, n, h, nz, nh, h, false, AxisMode::from_data, inv, aux, s);
-  axis_pass(e, nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+  axis_pass(e, n, h, nz, nh, h, false, AxisMode::from_data, inv, aux, s, b, half_);
+  axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
   rows_c2r(e, x_.get(), rows, n, C2rMode::store, cfg_.nm2, cfg_.inv_k02, s);
   const auto kspace_step = [&](const float* in, bool clamp, float* out, C2rMode mode) {
     rows_r2c(in, e, rows, n, clamp, s);
-    axis_pass(e, nz, nh, n, h, h, true, AxisMode::plain, 1.0f, AxisAux{}, s);
-    axis_pass(e, n, h, nz, nh, h, true, AxisMode::restore_half, inv, aux, s);
-    axis_pass(e, nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+    axis_pass(e, b * nz, nh, n, h, h, true, AxisMode::plain, 1.0f, AxisAux{}, s);
+    axis_pass(e, n, h, nz, nh, h, true, AxisMode::restore_half, inv, aux, s, b, half_);
+    axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
     rows_c2r(e, out, rows, n, mode, cfg_.nm2, cfg_.inv_k02, s);
   };
   if (!cfg_.tv) {
@@ -359,16 +387,17 @@ void OdtPlan::solve_complex(float* index, float inv, cudaStream_t s) {
   const Grid& g = cfg_.grid;
   const int n = g.n, nz = g.nz;
   const std::size_t nn = static_cast<std::size_t>(n) * n;
-  const std::size_t rows = static_cast<std::size_t>(nz) * n;
+  const int b = cfg_.batch;
+  const std::size_t rows = static_cast<std::size_t>(b) * nz * n;
   float2* p = pot_.get();
   const AxisAux aux{measured_.get(), mask_.get()};
-  axis_pass(p, n, n, nz, nn, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
-  axis_pass(p, nz, nn, n, n, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+  axis_pass(p, n, n, nz, nn, n, false, AxisMode::plain, 1.0f, AxisAux{}, s, b, vol_);
+  axis_pass(p, b * nz, nn, n, n, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
   for (int it = 0; it < cfg_.iterations; ++it) {
     rows_c2c(p, rows, n, false, RowMode::inv_clamp_fwd, inv, nullptr, 0, 0, s);
-    axis_pass(p, nz, nn, n, n, n, true, AxisMode::plain, 1.0f, AxisAux{}, s);
-    axis_pass(p, n, n, nz, nn, n, true, AxisMode::restore_mask, 1.0f, aux, s);
-    axis_pass(p, nz, nn, n, n, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+    axis_pass(p, b * nz, nn, n, n, n, true, AxisMode::plain, 1.0f, AxisAux{}, s);
+    axis_pass(p, n, n, nz, nn, n, true, AxisMode::restore_mask, 1.0f, aux, s, b, vol_);
+    axis_pass(p, b * nz, nn, n, n, n, false, AxisMode::plain, 1.0f, AxisAux{}, s);
   }
   rows_c2c(p, rows, n, false, RowMode::inv_index, inv, index, cfg_.nm2, cfg_.inv_k02, s);
 }

@@ -28,10 +28,11 @@ std::vector<float4> illumination_table(const Grid& g, const float* illum_fyfx, i
 // Ewald mapping of `count` spectra (count, n, n): half-spectrum data and hit counts (nz, n, n/2+1)
 // for the real solvers, or the full normalised potential and mask (nz, n, n) for the complex one
 // (`measured`, optional, gets a copy). `filled` is incremented by the number of voxels with data.
+// `batch` volumes at once: volume b maps spectra b * count .. into its own arrays and filled[b].
 void map_half(const float2* spectra, const float4* illum, int count, const Grid& g, float2* a, std::uint8_t* hits,
-              unsigned long long* filled, cudaStream_t s);
+              unsigned long long* filled, cudaStream_t s, int batch = 1);
 void map_full(const float2* spectra, const float4* illum, int count, const Grid& g, float2* pot, float2* measured,
-              std::uint8_t* mask, unsigned long long* filled, cudaStream_t s);
+              std::uint8_t* mask, unsigned long long* filled, cudaStream_t s, int batch = 1);
 
 struct OdtConfig {
   Grid grid{};
@@ -43,6 +44,7 @@ struct OdtConfig {
   int tv_inner = 10;
   float nm2 = 0;       // n_medium^2
   float inv_k02 = 0;   // 1 / k0^2
+  int batch = 1;       // independent reconstructions of this geometry per run (not with TV)
 };
 
 class OdtPlan {
@@ -53,8 +55,8 @@ class OdtPlan {
   // illum_fyfx: count (fy, fx) pairs on the host.
   OdtPlan(const OdtConfig& cfg, const float* illum_fyfx);
 
-  // fields: (count, n, n) Rytov fields on the device, overwritten by their spectra. index: (nz, n,
-  // n) output on the device. Clock marks are `first + Mark`.
+  // fields: (batch * count, n, n) Rytov fields on the device, overwritten by their spectra. index:
+  // (batch, nz, n, n) output on the device. Clock marks are `first + Mark`.
   void run(float2* fields, float* index, cudaStream_t s, StageClock* clock = nullptr);
   void run_marked(float2* fields, float* index, cudaStream_t s, StageClock* clock, int first) {
     first_mark_ = first;
@@ -62,9 +64,9 @@ class OdtPlan {
     first_mark_ = 0;
   }
 
-  // Voxels that received data in the last run, on the device.
+  // Voxels that received data in the last run, on the device (one count per volume of the batch).
   [[nodiscard]] const unsigned long long* filled() const { return filled_.get(); }
-  [[nodiscard]] std::size_t volume() const { return vol_; }
+  [[nodiscard]] std::size_t volume() const { return vol_; }  // of one reconstruction
   [[nodiscard]] std::size_t device_bytes() const;
   [[nodiscard]] const OdtConfig& config() const { return cfg_; }
 

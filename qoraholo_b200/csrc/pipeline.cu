@@ -27,27 +27,29 @@ PipelinePlan::PipelinePlan(const CropPlan& crop, int count, int upload_chunks, c
                            const float* illum_fyfx, bool own_io)
     : crop_(crop),
       count_(count),
-      chunk_(checked_chunk(count, upload_chunks)),
-      chunks_((count + chunk_ - 1) / chunk_),
-      field_(crop, count),
-      unwrap_(count, crop.out, crop.out),
+      batch_(odt.batch),
+      chunk_(checked_chunk(count * odt.batch, upload_chunks)),
+      chunks_((count * odt.batch + chunk_ - 1) / chunk_),
+      field_(crop, count * odt.batch),
+      unwrap_(count * odt.batch, crop.out, crop.out),
       odt_(odt, illum_fyfx),
       clock_(kMarks) {
   require(odt.grid.n == crop.out, "Pipeline: volume side must equal the field side");
   const std::size_t image = static_cast<std::size_t>(crop.n) * crop.n;
   const std::size_t field = static_cast<std::size_t>(count) * crop.out * crop.out;
+  const std::size_t b = batch_;
   if (own_io) {
-    input_ = PinnedBuf<float>(count * image);
-    output_ = PinnedBuf<float>(odt_.volume());
-    filled_host_ = PinnedBuf<unsigned long long>(1);
+    input_ = PinnedBuf<float>(b * count * image);
+    output_ = PinnedBuf<float>(b * odt_.volume());
+    filled_host_ = PinnedBuf<unsigned long long>(b);
     background_.reset(field);
   }
-  holo_.reset(count * image);
-  fields_.reset(field);
-  psi_.reset(field);
-  logamp_.reset(field);
-  phi_.reset(field);
-  index_.reset(odt_.volume());
+  holo_.reset(b * count * image);
+  fields_.reset(b * field);
+  psi_.reset(b * field);
+  logamp_.reset(b * field);
+  phi_.reset(b * field);
+  index_.reset(b * odt_.volume());
   for (int k = 0; k < chunks_; ++k) chunk_done_.emplace_back();
 }
 
@@ -63,14 +65,14 @@ void PipelinePlan::set_background(const float* host_bg) {
   check(cudaMemcpyAsync(holo_.get(), host_bg, count_ * image * sizeof(float), cudaMemcpyHostToDevice, s),
         "upload backgrounds");
   field_.spectra(holo_.get(), 0, count_, s);
-  field_.finish(0, background_.get(), nullptr, nullptr, nullptr, s);
+  field_.finish(0, background_.get(), nullptr, nullptr, nullptr, s, 0, count_);
   check(cudaStreamSynchronize(s), "set_background");
   has_background_ = true;
 }
 
 void PipelinePlan::enqueue_background(const float* d_bg_holo, float2* bg_out, cudaStream_t s) {
   field_.spectra(d_bg_holo, 0, count_, s);
-  field_.finish(0, bg_out, nullptr, nullptr, nullptr, s);
+  field_.finish(0, bg_out, nullptr, nullptr, nullptr, s, 0, count_);
 }
 
 void PipelinePlan::enqueue(const float* d_holo, const float2* bg, float* d_index, cudaStream_t s) {
@@ -81,12 +83,13 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
                            bool marks) {
   const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
   if (marks) clock_.mark(kStart, s);
+  const int images = count_ * batch_;
   if (chunked_upload) {
     const cudaStream_t c = copy_.get();
     check(cudaStreamWaitEvent(c, clock_.event(kStart), 0), "cudaStreamWaitEvent");
     for (int k = 0; k < chunks_; ++k) {
       const int first = k * chunk_;
-      const int valid = std::min(chunk_, count_ - first);
+      const int valid = std::min(chunk_, images - first);
       float* dst = holo_.get() + first * image;
       check(cudaMemcpyAsync(dst, input_.get() + first * image, valid * image * sizeof(float), cudaMemcpyHostToDevice, c),
             "upload holograms");
@@ -95,9 +98,9 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
       field_.spectra(dst, first, valid, s);
     }
   } else {
-    field_.spectra(d_holo, 0, count_, s);
+    field_.spectra(d_holo, 0, images, s);
   }
-  field_.finish(1, nullptr, bg, psi_.get(), logamp_.get(), s);
+  field_.finish(1, nullptr, bg, psi_.get(), logamp_.get(), s, count_);
   if (marks) clock_.mark(kFields, s);
   unwrap_.rytov(psi_.get(), logamp_.get(), phi_.get(), fields_.get(), s);
   if (marks) clock_.mark(kRytov, s);
@@ -113,9 +116,11 @@ void PipelinePlan::process() {
   const auto t0 = std::chrono::steady_clock::now();
   const cudaStream_t s = compute_.get();
   compute(nullptr, true, background_.get(), index_.get(), s, true);
-  check(cudaMemcpyAsync(output_.get(), index_.get(), odt_.volume() * sizeof(float), cudaMemcpyDeviceToHost, s),
+  check(cudaMemcpyAsync(output_.get(), index_.get(), batch_ * odt_.volume() * sizeof(float), cudaMemcpyDeviceToHost,
+                        s),
         "download index");
-  check(cudaMemcpyAsync(filled_host_.get(), odt_.filled(), sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+  check(cudaMemcpyAsync(filled_host_.get(), odt_.filled(), batch_ * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, s),
         "download filled");
   clock_.mark(kDownloaded, s);
   check(cudaStreamSynchronize(s), "process");
@@ -137,6 +142,16 @@ void PipelinePlan::process() {
 void PipelinePlan::process_device(const float* d_holo, float* d_index, cudaStream_t s) {
   if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
   compute(d_holo, false, background_.get(), d_index, s, true);
+}
+
+void PipelinePlan::process_device_graph(const float* d_holo, float* d_index, cudaStream_t s) {
+  if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
+  if (!graph_warm_) {
+    enqueue(d_holo, background_.get(), d_index, s);
+    graph_warm_ = true;
+    return;
+  }
+  graph_.run({d_holo, d_index}, s, [&](cudaStream_t c) { enqueue(d_holo, background_.get(), d_index, c); });
 }
 
 }  // namespace qhk

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "field.hpp"
+#include "graph.hpp"
 #include "odt.hpp"
 #include "unwrap.hpp"
 
@@ -23,13 +24,16 @@ class PipelinePlan {
 
   // Background holograms (count, N, N) on the host; their fields stay on the device.
   void set_background(const float* host_bg);
-  // Page-locked input (count, N, N) and output (nz, n, n) buffers.
+  // Page-locked input (batch * count, N, N) and output (batch, nz, n, n) buffers.
   [[nodiscard]] float* input() const { return input_.get(); }
   [[nodiscard]] const float* output() const { return output_.get(); }
   // input() -> output(), synchronous, with stage timings.
   void process();
   // Holograms already on the device -> index on the device, asynchronous on `s` (no host copies).
   void process_device(const float* d_holo, float* d_index, cudaStream_t s);
+  // The same replayed as one CUDA graph (captured on the second call for these buffers; the first
+  // call runs directly so that lazy setup happens outside the capture). No stage timings.
+  void process_device_graph(const float* d_holo, float* d_index, cudaStream_t s);
 
   // Serving-workspace forms, asynchronous on `s`, no stage marks (so they can be graph-captured):
   // background holograms (device) -> demodulated background fields `bg_out` (count, m, m); and
@@ -41,6 +45,7 @@ class PipelinePlan {
   [[nodiscard]] cudaStream_t stream() const { return compute_.get(); }
   [[nodiscard]] float* holo_buffer() const { return holo_.get(); }
   [[nodiscard]] float* index_buffer() const { return index_.get(); }
+  // Of one request (one stack of `count` holograms / fields).
   [[nodiscard]] std::size_t hologram_floats() const {
     return static_cast<std::size_t>(count_) * crop_.n * crop_.n;
   }
@@ -53,6 +58,9 @@ class PipelinePlan {
   [[nodiscard]] const OdtPlan& odt() const { return odt_; }
   [[nodiscard]] const CropPlan& crop() const { return crop_; }
   [[nodiscard]] int count() const { return count_; }
+  // Requests of this geometry per run (OdtConfig::batch): inputs, fields and volumes are that many
+  // stacks one after another; the background fields are one stack.
+  [[nodiscard]] int batch() const { return batch_; }
 
  private:
   enum { kStart, kFields, kRytov, kDownloaded = kRytov + 1 + OdtPlan::kMarks, kMarks };
@@ -61,6 +69,7 @@ class PipelinePlan {
 
   CropPlan crop_;
   int count_;
+  int batch_;
   int chunk_;
   int chunks_;
   Stream compute_;
@@ -80,6 +89,8 @@ class PipelinePlan {
   DevBuf<float> index_;
   std::vector<Event> chunk_done_;
   StageClock clock_;
+  CapturedWork graph_;
+  bool graph_warm_ = false;
   PipelineTimes timings_;
   double filled_ = 0;
   bool has_background_ = false;

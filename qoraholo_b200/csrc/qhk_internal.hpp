@@ -34,12 +34,14 @@ struct AxisAux {
 };
 // Shared-memory budget of one axis-pass tile (bytes); QHK_FFT_AXIS_KIB overrides it.
 std::size_t axis_smem_budget();
+// `batch` arrays of that layout, each sb elements after the previous (data and aux alike).
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s);
+               AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch = 1, std::size_t sb = 0);
 // Times the tile widths of this axis pass on `data` (scratch: it is overwritten) and keeps the
 // fastest for later axis_pass calls of the same shape. Never inside a stream capture.
 void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-                    AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s);
+                    AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch = 1,
+                    std::size_t sb = 0);
 
 // Rows of real length nx <-> half spectra of nx / 2 + 1 bins (rows dense, row pitches nx and
 // nx / 2 + 1). R2C optionally clamps its input at 0 (Gerchberg-Papoulis). C2R writes the real

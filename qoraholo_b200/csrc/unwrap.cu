@@ -11,7 +11,9 @@
 // A small per-image kernel then reduces the partial sums in a fixed order (no atomics) to the
 // congruence constant and forms the border mean, in the host's summation order, for the 2 pi
 // shift of the Rytov phase.
+#include <algorithm>
 #include <cmath>
+#include <map>
 #include <mutex>
 #include <numbers>
 #include <vector>
@@ -29,18 +31,19 @@ void allow(K kernel, std::size_t) {
   ensure_smem(kernel);
 }
 
-// Pass 1: COLS rows of image blockIdx.y per CTA.
+// Each pass is written as the work of one tile (a CTA's share) of one image, so that the stacked
+// launches below (grid = tiles x images of one size) and the uneven-batch launches (persistent
+// CTAs draining an (image, tile) queue) run the same code. `psi`, `d1`, `phi` point at the image.
+
+// Pass 1: COLS rows y0 .. y0 + COLS - 1 of one image.
 template <int COLS>
-__global__ void __launch_bounds__(kThreads)
-    k_div_dctx(const float* __restrict__ psi, float* __restrict__ d1, int ny, int nx, FftLen L,
-               const float2* __restrict__ dtw) {
-  extern __shared__ float2 sm[];
+__device__ __forceinline__ void div_dctx_tile(const float* __restrict__ psi, float* __restrict__ d1, int ny, int nx,
+                                              const FftLen& L, const float2* __restrict__ dtw, int y0, float2* sm) {
   constexpr int cp = COLS + 1;
   float2* A = sm;
   float2* B = A + static_cast<std::size_t>(nx) * cp;
   float* P = reinterpret_cast<float*>(B + static_cast<std::size_t>(nx) * cp);  // rows y0-1 .. y0+COLS
-  const int y0 = static_cast<int>(blockIdx.x) * COLS;
-  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  constexpr std::size_t img = 0;
   const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
   for (int idx = tid; idx < (COLS + 2) * nx; idx += nth) {
     const int rr = idx / nx;
@@ -76,18 +79,27 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Pass 2: COLS columns of image blockIdx.y per CTA: DCT-II along y, divide, inverse DCT along y.
 template <int COLS>
 __global__ void __launch_bounds__(kThreads)
-    k_dcty_solve(const float* __restrict__ d1, float* __restrict__ d2, int ny, int nx, FftLen L,
-                 const float2* __restrict__ dtw, const float* __restrict__ cos_y, const float* __restrict__ cos_x) {
+    k_div_dctx(const float* __restrict__ psi, float* __restrict__ d1, int ny, int nx, FftLen L,
+               const float2* __restrict__ dtw) {
   extern __shared__ float2 sm[];
+  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  div_dctx_tile<COLS>(psi + img, d1 + img, ny, nx, L, dtw, static_cast<int>(blockIdx.x) * COLS, sm);
+}
+
+// Pass 2: COLS columns c0 .. c0 + COLS - 1 of one image: DCT-II along y, divide, inverse DCT
+// along y.
+template <int COLS>
+__device__ __forceinline__ void dcty_solve_tile(const float* __restrict__ d1, float* __restrict__ d2, int ny, int nx,
+                                                const FftLen& L, const float2* __restrict__ dtw,
+                                                const float* __restrict__ cos_y, const float* __restrict__ cos_x,
+                                                int c0, float2* sm) {
   float2* A = sm;
   float2* B = A + static_cast<std::size_t>(ny) * COLS;
   float* Cf = reinterpret_cast<float*>(B + static_cast<std::size_t>(ny) * COLS);
-  const int c0 = static_cast<int>(blockIdx.x) * COLS;
   const int cols = min(COLS, nx - c0);
-  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  constexpr std::size_t img = 0;
   const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
   for (int idx = tid; idx < ny * COLS; idx += nth) {
     const int y = idx / COLS;
@@ -132,20 +144,27 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Pass 3: inverse DCT along x of COLS rows (in place), and the congruence partial sums of image
-// blockIdx.y over those rows: partial[(img * gridDim.x + blockIdx.x) * 2 + {0,1}] = sum cos, sin.
 template <int COLS>
 __global__ void __launch_bounds__(kThreads)
-    k_idctx(float* __restrict__ phi, const float* __restrict__ psi, int ny, int nx, FftLen L,
-            const float2* __restrict__ dtw, double* __restrict__ partial) {
+    k_dcty_solve(const float* __restrict__ d1, float* __restrict__ d2, int ny, int nx, FftLen L,
+                 const float2* __restrict__ dtw, const float* __restrict__ cos_y, const float* __restrict__ cos_x) {
   extern __shared__ float2 sm[];
+  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  dcty_solve_tile<COLS>(d1 + img, d2 + img, ny, nx, L, dtw, cos_y, cos_x, static_cast<int>(blockIdx.x) * COLS, sm);
+}
+
+// Pass 3: inverse DCT along x of COLS rows y0 .. y0 + COLS - 1 (in place), and the congruence
+// partial sums over those rows: pair[0] = sum cos(psi - phi), pair[1] = sum sin(psi - phi).
+// `red` is the CTA's shared reduction buffer of 2 x kThreads doubles.
+template <int COLS>
+__device__ __forceinline__ void idctx_tile(float* __restrict__ phi, const float* __restrict__ psi, int ny, int nx,
+                                           const FftLen& L, const float2* __restrict__ dtw, int y0,
+                                           double* __restrict__ pair, float2* sm, double (*red)[kThreads]) {
   constexpr int cp = COLS + 1;
   float2* A = sm;
   float2* B = A + static_cast<std::size_t>(nx) * cp;
   float* F = reinterpret_cast<float*>(B + static_cast<std::size_t>(nx) * cp);
-  __shared__ double red[2][kThreads];
-  const int y0 = static_cast<int>(blockIdx.x) * COLS;
-  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  constexpr std::size_t img = 0;
   const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
   for (int idx = tid; idx < COLS * nx; idx += nth) {
     const int row = idx / nx;
@@ -187,27 +206,36 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
   }
   if (tid == 0) {
-    const std::size_t o = (static_cast<std::size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * 2;
-    partial[o] = red[0][0];
-    partial[o + 1] = red[1][0];
+    pair[0] = red[0][0];
+    pair[1] = red[1][0];
   }
 }
 
-// Per image: congruence constant c = arg(sum exp(i (psi - phi))) from the partial sums, then the
-// 2 pi multiple of the border mean of phi + c, summed in the host's order.
+// Stacked form: partial[(image * gridDim.x + blockIdx.x) * 2 + {0, 1}].
+template <int COLS>
 __global__ void __launch_bounds__(kThreads)
-    k_rytov_consts(const float* __restrict__ phi, int ny, int nx, const double* __restrict__ partial, int nblk,
-                   float2* __restrict__ consts) {
-  extern __shared__ float pairs[];
+    k_idctx(float* __restrict__ phi, const float* __restrict__ psi, int ny, int nx, FftLen L,
+            const float2* __restrict__ dtw, double* __restrict__ partial) {
+  extern __shared__ float2 sm[];
+  __shared__ double red[2][kThreads];
+  const std::size_t img = static_cast<std::size_t>(blockIdx.y) * ny * nx;
+  idctx_tile<COLS>(phi + img, psi + img, ny, nx, L, dtw, static_cast<int>(blockIdx.x) * COLS,
+                   partial + (static_cast<std::size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * 2, sm, red);
+}
+
+// Per image: congruence constant c = arg(sum exp(i (psi - phi))) from the image's nblk partial
+// pairs, then the 2 pi multiple of the border mean of phi + c, summed in the host's order.
+__device__ __forceinline__ void rytov_consts_image(const float* __restrict__ phi, int ny, int nx,
+                                                   const double* __restrict__ partial, int nblk,
+                                                   float2* __restrict__ out, float* pairs) {
   __shared__ double red[2][kThreads];
   __shared__ float cshared;
-  const std::size_t img = static_cast<std::size_t>(blockIdx.x) * ny * nx;
+  constexpr std::size_t img = 0;
   const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
   double sc = 0.0, ss = 0.0;
   for (int b = tid; b < nblk; b += nth) {
-    const std::size_t o = (static_cast<std::size_t>(blockIdx.x) * nblk + b) * 2;
-    sc += partial[o];
-    ss += partial[o + 1];
+    sc += partial[2 * b];
+    ss += partial[2 * b + 1];
   }
   red[0][tid] = sc;
   red[1][tid] = ss;
@@ -242,8 +270,17 @@ __global__ void __launch_bounds__(kThreads)
     for (int i = 0; i < npairs; ++i) sum = __dadd_rn(sum, static_cast<double>(pairs[i]));
     const double mean = sum / (2.0 * nx + 2.0 * (ny - 2));
     const double two_pi = 2.0 * 3.14159265358979323846;
-    consts[blockIdx.x] = make_float2(c, static_cast<float>(two_pi * round(mean / two_pi)));
+    *out = make_float2(c, static_cast<float>(two_pi * round(mean / two_pi)));
   }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_rytov_consts(const float* __restrict__ phi, int ny, int nx, const double* __restrict__ partial, int nblk,
+                   float2* __restrict__ consts) {
+  extern __shared__ float pairs[];
+  const std::size_t img = static_cast<std::size_t>(blockIdx.x) * ny * nx;
+  rytov_consts_image(phi + img, ny, nx, partial + static_cast<std::size_t>(blockIdx.x) * nblk * 2, nblk,
+                     consts + blockIdx.x, pairs);
 }
 
 // out = logamp + i ((phi + c) - shift), or phi_out = phi + c when logamp is null.
@@ -418,6 +455,274 @@ void UnwrapPlan::rytov(const float* psi, const float* logamp, float* phi_scratch
   k_rytov_assemble<<<grid_for(total), kThreads, 0, s>>>(phi_scratch, logamp, consts_.get(),
                                                         static_cast<std::size_t>(ny_) * nx_, total, out, nullptr);
   check_launch("rytov assemble");
+}
+
+// ---- Uneven batches --------------------------------------------------------------------------
+
+namespace {
+
+// One image of an uneven batch, as the batch kernels see it.
+struct BatchImage {
+  std::size_t offset;  // first pixel in the packed buffers
+  int ny, nx;
+  int rows;            // rows per tile of passes 1 and 3 (as UnwrapPlan for this size)
+  int cols;            // columns per tile of pass 2
+  int nblk;            // row tiles
+  int partial;         // first congruence partial pair of this image
+  FftLen Lx, Ly;
+  const float2* dtw_x;
+  const float2* dtw_y;
+  const float* cos_x;
+  const float* cos_y;
+};
+
+constexpr int kAssembleChunk = 16384;  // pixels per item of the last pass
+
+// Next queue item for the whole CTA (thread 0 takes it, everyone reads it).
+__device__ __forceinline__ int next_item(int* counter) {
+  __shared__ int item;
+  if (threadIdx.x == 0) item = atomicAdd(counter, 1);
+  __syncthreads();
+  const int it = item;
+  __syncthreads();
+  return it;
+}
+
+#define QHK_ROWS_SWITCH(R, CALL) \
+  switch (R) {                   \
+    case 16: CALL(16); break;    \
+    case 8: CALL(8); break;      \
+    case 4: CALL(4); break;      \
+    case 2: CALL(2); break;      \
+    default: CALL(1); break;     \
+  }
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_pass1(const float* __restrict__ psi, float* __restrict__ d1, const BatchImage* __restrict__ imgs,
+                  const int2* __restrict__ items, int n, int* counter) {
+  extern __shared__ float2 sm[];
+  for (int it = next_item(counter); it < n; it = next_item(counter)) {
+    const int2 w = items[it];
+    const BatchImage& im = imgs[w.x];
+#define QHK_P1(C) div_dctx_tile<C>(psi + im.offset, d1 + im.offset, im.ny, im.nx, im.Lx, im.dtw_x, w.y * (C), sm)
+    QHK_ROWS_SWITCH(im.rows, QHK_P1)
+#undef QHK_P1
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_pass2(const float* __restrict__ d1, float* __restrict__ phi, const BatchImage* __restrict__ imgs,
+                  const int2* __restrict__ items, int n, int* counter) {
+  extern __shared__ float2 sm[];
+  for (int it = next_item(counter); it < n; it = next_item(counter)) {
+    const int2 w = items[it];
+    const BatchImage& im = imgs[w.x];
+#define QHK_P2(C)                                                                                                  \
+  dcty_solve_tile<C>(d1 + im.offset, phi + im.offset, im.ny, im.nx, im.Ly, im.dtw_y, im.cos_y, im.cos_x, w.y * (C), \
+                     sm)
+    QHK_ROWS_SWITCH(im.cols, QHK_P2)
+#undef QHK_P2
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_pass3(float* __restrict__ phi, const float* __restrict__ psi, double* __restrict__ partial,
+                  const BatchImage* __restrict__ imgs, const int2* __restrict__ items, int n, int* counter) {
+  extern __shared__ float2 sm[];
+  __shared__ double red[2][kThreads];
+  for (int it = next_item(counter); it < n; it = next_item(counter)) {
+    const int2 w = items[it];
+    const BatchImage& im = imgs[w.x];
+    double* pair = partial + 2 * (static_cast<std::size_t>(im.partial) + w.y);
+#define QHK_P3(C) \
+  idctx_tile<C>(phi + im.offset, psi + im.offset, im.ny, im.nx, im.Lx, im.dtw_x, w.y * (C), pair, sm, red)
+    QHK_ROWS_SWITCH(im.rows, QHK_P3)
+#undef QHK_P3
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_pass4(const float* __restrict__ phi, const double* __restrict__ partial, float2* __restrict__ consts,
+                  const BatchImage* __restrict__ imgs, const int2* __restrict__ items, int n, int* counter) {
+  extern __shared__ float pairs[];
+  for (int it = next_item(counter); it < n; it = next_item(counter)) {
+    const int2 w = items[it];
+    const BatchImage& im = imgs[w.x];
+    rytov_consts_image(phi + im.offset, im.ny, im.nx, partial + 2 * static_cast<std::size_t>(im.partial), im.nblk,
+                       consts + w.x, pairs);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_pass5(float* __restrict__ phi, const float2* __restrict__ consts, const BatchImage* __restrict__ imgs,
+                  const int2* __restrict__ items, int n, int* counter) {
+  for (int it = next_item(counter); it < n; it = next_item(counter)) {
+    const int2 w = items[it];
+    const BatchImage& im = imgs[w.x];
+    const float c = consts[w.x].x;
+    const std::size_t pixels = static_cast<std::size_t>(im.ny) * im.nx;
+    const std::size_t a = static_cast<std::size_t>(w.y) * kAssembleChunk;
+    const std::size_t b = min(pixels, a + kAssembleChunk);
+    for (std::size_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+      phi[im.offset + i] = __fadd_rn(phi[im.offset + i], c);
+    }
+  }
+}
+
+#undef QHK_ROWS_SWITCH
+
+int solve_cols(int ny) {
+  int cc = 16;
+  const auto smem_of = [&](int k) {
+    return 2 * static_cast<std::size_t>(ny) * k * sizeof(float2) + static_cast<std::size_t>(ny) * k * sizeof(float);
+  };
+  while (cc > 1 && smem_of(cc) > 80 * 1024) cc /= 2;
+  return cc;
+}
+
+template <class K>
+unsigned persistent_grid(K kernel, std::size_t smem, int items) {
+  ensure_smem(kernel);
+  int per_sm = 0;
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem), "cudaOccupancy");
+  const long long slots = static_cast<long long>(sm_count()) * std::max(per_sm, 1);
+  return static_cast<unsigned>(std::max<long long>(1, std::min<long long>(slots, items)));
+}
+
+}  // namespace
+
+UnwrapBatchPlan::UnwrapBatchPlan(const int* ny, const int* nx, int count) {
+  require(ny && nx && count >= 1, "unwrap batch: need at least one image");
+  std::vector<BatchImage> im(count);
+  std::map<int, int> side;  // side length -> table index
+  const auto table = [&](int n) {
+    const auto it = side.find(n);
+    if (it != side.end()) return it->second;
+    std::vector<float2> w(n);
+    std::vector<float> c(n);
+    for (int k = 0; k < n; ++k) {
+      const double a = -std::numbers::pi * k / (2.0 * n);
+      w[k] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+      c[k] = 2.0f * std::cos(kPiF * static_cast<float>(k) / static_cast<float>(n));
+    }
+    dtw_.emplace_back(n);
+    cos_.emplace_back(n);
+    check(cudaMemcpy(dtw_.back().get(), w.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "upload table");
+    check(cudaMemcpy(cos_.back().get(), c.data(), n * sizeof(float), cudaMemcpyHostToDevice), "upload table");
+    side[n] = static_cast<int>(dtw_.size()) - 1;
+    return side[n];
+  };
+  int partial = 0;
+  std::size_t smem[5] = {0, 0, 0, 0, 0};
+  for (int i = 0; i < count; ++i) {
+    require(ny[i] >= 2 && nx[i] >= 2 && ny[i] % 2 == 0 && nx[i] % 2 == 0, "unwrap: image sides must be even");
+    BatchImage& b = im[i];
+    b.offset = total_;
+    offsets_.push_back(total_);
+    total_ += static_cast<std::size_t>(ny[i]) * nx[i];
+    b.ny = ny[i];
+    b.nx = nx[i];
+    b.rows = rows_per_cta(b.nx, static_cast<std::size_t>(b.nx) * sizeof(float));
+    b.cols = solve_cols(b.ny);
+    b.nblk = (b.ny + b.rows - 1) / b.rows;
+    b.partial = partial;
+    partial += b.nblk;
+    b.Lx = fft_len(b.nx);
+    b.Ly = fft_len(b.ny);
+    const int tx = table(b.nx), ty = table(b.ny);
+    b.dtw_x = dtw_[tx].get();
+    b.cos_x = cos_[tx].get();
+    b.dtw_y = dtw_[ty].get();
+    b.cos_y = cos_[ty].get();
+    const std::size_t row_buf = 2 * static_cast<std::size_t>(b.nx) * (b.rows + 1) * sizeof(float2);
+    smem[0] = std::max(smem[0], row_buf + (b.rows + 2) * static_cast<std::size_t>(b.nx) * sizeof(float));
+    smem[1] = std::max(smem[1], 2 * static_cast<std::size_t>(b.ny) * b.cols * sizeof(float2) +
+                                    static_cast<std::size_t>(b.ny) * b.cols * sizeof(float));
+    smem[2] = std::max(smem[2], row_buf + b.rows * static_cast<std::size_t>(b.nx) * sizeof(float));
+    smem[3] = std::max(smem[3], static_cast<std::size_t>(b.nx + b.ny) * sizeof(float));
+  }
+  // Items, largest images first so that the queue ends with small tiles.
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return static_cast<std::size_t>(im[a].ny) * im[a].nx > static_cast<std::size_t>(im[b].ny) * im[b].nx;
+  });
+  std::vector<int2> items[5];
+  for (const int i : order) {
+    const BatchImage& b = im[i];
+    for (int t = 0; t < b.nblk; ++t) items[0].push_back(make_int2(i, t));
+    for (int t = 0; t < (b.nx + b.cols - 1) / b.cols; ++t) items[1].push_back(make_int2(i, t));
+    items[3].push_back(make_int2(i, 0));
+    const std::size_t pixels = static_cast<std::size_t>(b.ny) * b.nx;
+    for (std::size_t t = 0; t * kAssembleChunk < pixels; ++t) items[4].push_back(make_int2(i, static_cast<int>(t)));
+  }
+  items[2] = items[0];
+  std::vector<int2> all;
+  std::size_t at[5];
+  for (int p = 0; p < 5; ++p) {
+    at[p] = all.size();
+    all.insert(all.end(), items[p].begin(), items[p].end());
+  }
+  items_.reset(all.size());
+  check(cudaMemcpy(items_.get(), all.data(), all.size() * sizeof(int2), cudaMemcpyHostToDevice), "upload items");
+  images_.reset(count * sizeof(BatchImage));
+  check(cudaMemcpy(images_.get(), im.data(), count * sizeof(BatchImage), cudaMemcpyHostToDevice), "upload images");
+  counters_.reset(5);
+  d1_.reset(total_);
+  partial_.reset(2 * static_cast<std::size_t>(partial));
+  consts_.reset(count);
+  for (int p = 0; p < 5; ++p) {
+    pass_[p].items = items_.get() + at[p];
+    pass_[p].n = static_cast<int>(items[p].size());
+    pass_[p].smem = smem[p];
+  }
+  pass_[0].grid = persistent_grid(k_batch_pass1, smem[0], pass_[0].n);
+  pass_[1].grid = persistent_grid(k_batch_pass2, smem[1], pass_[1].n);
+  pass_[2].grid = persistent_grid(k_batch_pass3, smem[2], pass_[2].n);
+  pass_[3].grid = persistent_grid(k_batch_pass4, smem[3], pass_[3].n);
+  pass_[4].grid = persistent_grid(k_batch_pass5, 0, pass_[4].n);
+}
+
+UnwrapBatchPlan::~UnwrapBatchPlan() = default;
+
+std::size_t UnwrapBatchPlan::device_bytes() const {
+  std::size_t t = images_.bytes() + items_.bytes() + counters_.bytes() + d1_.bytes() + partial_.bytes() +
+                  consts_.bytes();
+  for (const auto& d : dtw_) t += d.bytes();
+  for (const auto& c : cos_) t += c.bytes();
+  return t;
+}
+
+void UnwrapBatchPlan::unwrap(const float* psi, float* phi, cudaStream_t s) {
+  const auto* imgs = reinterpret_cast<const BatchImage*>(images_.get());
+  int* q = counters_.get();
+  const auto items = [&](int p) { return static_cast<const int2*>(pass_[p].items); };
+  check(cudaMemsetAsync(q, 0, 5 * sizeof(int), s), "cudaMemset");
+  k_batch_pass1<<<pass_[0].grid, kThreads, pass_[0].smem, s>>>(psi, d1_.get(), imgs, items(0), pass_[0].n, q);
+  check_launch("unwrap batch pass 1");
+  k_batch_pass2<<<pass_[1].grid, kThreads, pass_[1].smem, s>>>(d1_.get(), phi, imgs, items(1), pass_[1].n, q + 1);
+  check_launch("unwrap batch pass 2");
+  k_batch_pass3<<<pass_[2].grid, kThreads, pass_[2].smem, s>>>(phi, psi, partial_.get(), imgs, items(2),
+                                                               pass_[2].n, q + 2);
+  check_launch("unwrap batch pass 3");
+  k_batch_pass4<<<pass_[3].grid, kThreads, pass_[3].smem, s>>>(phi, partial_.get(), consts_.get(), imgs, items(3),
+                                                               pass_[3].n, q + 3);
+  check_launch("unwrap batch constants");
+  k_batch_pass5<<<pass_[4].grid, kThreads, 0, s>>>(phi, consts_.get(), imgs, items(4), pass_[4].n, q + 4);
+  check_launch("unwrap batch constant");
+}
+
+void UnwrapBatchPlan::unwrap_graph(const float* psi, float* phi, cudaStream_t s) {
+  if (!warmed_) {  // lazy per-device setup happens here, outside any capture
+    unwrap(psi, phi, s);
+    warmed_ = true;
+    return;
+  }
+  graph_.run({psi, phi}, s, [&](cudaStream_t c) { unwrap(psi, phi, c); });
 }
 
 void field_ratio(const float2* sample, const float2* bg, std::size_t plane, bool per_image, std::size_t total,

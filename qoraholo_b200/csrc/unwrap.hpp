@@ -1,6 +1,9 @@
 // Unwrap / Rytov plan of the CUDA backend (unwrap.cu).
 #pragma once
 
+#include <vector>
+
+#include "graph.hpp"
 #include "qhk_internal.hpp"
 
 namespace qhk {
@@ -28,6 +31,51 @@ class UnwrapPlan {
   DevBuf<float> d1_;
   DevBuf<double> partial_;
   DevBuf<float2> consts_;  // (congruence constant, 2 pi shift) per image
+};
+
+// Least-squares unwrap of an uneven batch: `count` images, image i of its own (even) size ny[i] x
+// nx[i], packed one after another in the input and output buffers (image i starts at offset(i) =
+// the pixel count of images 0 .. i-1). Each of the five passes is ONE launch for the whole batch:
+// persistent CTAs (as many as are resident at once) take (image, tile) items off a device queue,
+// largest images first, and run the tile code of the stacked plan above for that image's size, so
+// every image's result is bitwise the one UnwrapPlan gives for it. unwrap_graph replays the five
+// launches as one captured CUDA graph.
+class UnwrapBatchPlan {
+ public:
+  UnwrapBatchPlan(const int* ny, const int* nx, int count);
+  ~UnwrapBatchPlan();
+  UnwrapBatchPlan(const UnwrapBatchPlan&) = delete;
+  UnwrapBatchPlan& operator=(const UnwrapBatchPlan&) = delete;
+
+  void unwrap(const float* psi, float* phi, cudaStream_t s);
+  void unwrap_graph(const float* psi, float* phi, cudaStream_t s);
+
+  [[nodiscard]] int count() const { return static_cast<int>(offsets_.size()); }
+  [[nodiscard]] std::size_t offset(int i) const { return offsets_.at(i); }
+  [[nodiscard]] std::size_t total() const { return total_; }
+  [[nodiscard]] std::size_t device_bytes() const;
+  [[nodiscard]] std::uint64_t graph_replays() const { return graph_.replays(); }
+
+ private:
+  struct Pass {
+    void* items = nullptr;  // int2 (image, tile) on the device
+    int n = 0;
+    std::size_t smem = 0;
+    unsigned grid = 0;
+  };
+  std::vector<std::size_t> offsets_;
+  std::size_t total_ = 0;
+  std::vector<DevBuf<float2>> dtw_;  // per distinct side length
+  std::vector<DevBuf<float>> cos_;
+  DevBuf<unsigned char> images_;     // per-image descriptors
+  DevBuf<int2> items_;               // all passes' items, concatenated
+  DevBuf<int> counters_;             // one queue head per pass
+  DevBuf<float> d1_;
+  DevBuf<double> partial_;
+  DevBuf<float2> consts_;
+  Pass pass_[5];
+  CapturedWork graph_;
+  bool warmed_ = false;
 };
 
 // Least-squares unwrap of count images (ny, nx) from psi into phi (both on the device) with no
