@@ -162,6 +162,10 @@ int qhk_unwrap_noalloc(const float* d_wrapped, float* d_unwrapped, int count, in
  * per (device, shape) for the process; results are bitwise the same for every shape. On by default
  * (environment QHK_AUTOTUNE=0 turns it off). */
 int qhk_autotune_enable(int enabled);
+/* FGP step form of tv_prox (bitwise the same results): 0 the tuned one, 1 the extrapolated point
+ * stored between steps (13 volumes of traffic per step), 2 recomputed from the two previous duals
+ * (10 volumes). */
+int qhk_tv_form(int form);
 /* The tuned choices, one line each, into `buf` (NUL-terminated, truncated to `size`); returns the
  * full length. */
 size_t qhk_autotune_report(char* buf, size_t size);

@@ -108,6 +108,7 @@ _PROTOS = {
     "qhk_unwrap_batch_device_bytes": (C.c_size_t, [_VP]),
     "qhk_unwrap_batch_destroy": (_I, [_VP]),
     "qhk_autotune_enable": (_I, [_I]),
+    "qhk_tv_form": (_I, [_I]),
     "qhk_autotune_report": (C.c_size_t, [_VP, C.c_size_t]),
     "qhk_server_create": (_I, [C.POINTER(_VP), C.c_size_t, _I, _I]),
     "qhk_server_add_geometry": (_I, [_VP, _VP, _VP, C.POINTER(Geometry), _VP, C.POINTER(_I)]),
@@ -238,6 +239,11 @@ def unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, stream=0):
 def autotune_enable(enabled: bool = True):
     """Plans built from now on time their launch shapes (on by default)."""
     check(lib().qhk_autotune_enable(int(bool(enabled))))
+
+
+def tv_form(form: int):
+    """FGP step form: 0 tuned (default), 1 stored extrapolated point, 2 recomputed (same results)."""
+    check(lib().qhk_tv_form(int(form)))
 
 
 def autotune_report() -> str:

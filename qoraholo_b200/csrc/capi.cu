@@ -679,6 +679,10 @@ int qhk_bpm_reconstruct(const void* fields, int count, int n, const float* illum
 }
 
 
+int qhk_tv_form(int form) {
+  return guard([&] { qhk::set_tv_form(form); });
+}
+
 int qhk_autotune_enable(int enabled) {
   return guard([&] { qhk::set_autotune_enabled(enabled != 0); });
 }

@@ -87,6 +87,10 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
 // t_{k+1} of FISTA and FGP, 0.5 (1 + sqrt(1 + 4 t^2)) in float (host).
 float fista_t(float t);
 
+// FGP step form: 0 the autotuned one (untuned default: r stored), 1 the extrapolated point r
+// stored between steps, 2 r recomputed from the two previous duals. Results are bitwise the same.
+void set_tv_form(int form);
+
 // Times the FGP tile heights on this volume's shape and keeps the fastest for later tv_prox calls.
 // b and all three dual triplets of t are scratch (overwritten). Never inside a stream capture.
 void tune_tv(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s);

@@ -87,6 +87,20 @@ __device__ __forceinline__ void tv_dual_step(const float g[3], float step, float
   }
 }
 
+// The projection part of tv_dual_step alone: p = proj(r + step g), the same operations.
+__device__ __forceinline__ void tv_dual_project(const float g[3], float step, const float r[3], float p[3]) {
+  float q[3];
+  float norm2 = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    q[a] = __fadd_rn(r[a], __fmul_rn(step, g[a]));
+    norm2 = __fadd_rn(norm2, __fmul_rn(q[a], q[a]));
+  }
+  const float scale = norm2 > 1.0f ? __fdiv_rn(1.0f, __fsqrt_rn(norm2)) : 1.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) p[a] = __fmul_rn(q[a], scale);
+}
+
 // Primal point max(b - lambda adj, 0).
 __device__ __forceinline__ float tv_primal(float b, float lambda, float adj) {
   const float x = __fsub_rn(b, __fmul_rn(lambda, adj));

@@ -15,6 +15,7 @@
 // All arithmetic uses the round-to-nearest intrinsics in the reference's operation order, so the
 // device iterates are bit-identical to the CPU's.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <set>
@@ -279,6 +280,231 @@ __global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
   }
 }
 
+// The same FGP step without a stored extrapolated point: r_k = p_k + m (p_k - p_{k-1}) (the
+// formula of the step above, the same float operations on the same stored values, so bitwise the
+// same r) is recomputed where it is needed from the two previous duals. A step then reads b, p_k
+// (3) and p_{k-1} (3) and writes p_{k+1} (3) -- 10 volumes instead of 13 (the first step, r_0 =
+// p_0, reads b and p_0 and writes p_1: 7). The ring holds r: plane z+2's p_k lands in its ring
+// slot and its p_{k-1} in a staging plane by cp.async, and each thread turns its own copied
+// elements into r once they land. It is an autotuner candidate: on B200 at 256^3 it loses (274 vs
+// 156 us per step), because the one-row halos of two duals are re-read from DRAM (709 MB read
+// against 470 MB algorithmic) and the staging plane halves the resident CTAs.
+struct FgpPArgs {
+  const float* b;
+  const float* pk[3];    // p_k; on the first step p_0 = r_0
+  const float* pkm1[3];  // p_{k-1} (not read on the first step)
+  float* pout[3];        // p_{k+1}
+  int nz, ny, nx;
+  int ytiles;
+  float lambda, step;
+  float momentum;  // m_{k-1}: r_k = p_k + m_{k-1} (p_k - p_{k-1})
+};
+
+template <int VEC, bool FIRST>
+__global__ void __launch_bounds__(256, 2) k_fgp_p(FgpPArgs A) {
+  extern __shared__ __align__(16) float sm[];
+  const int nx = A.nx, ny = A.ny, nz = A.nz;
+  const int TY = static_cast<int>(blockDim.y);
+  const int tx = static_cast<int>(threadIdx.x);
+  const int ty = static_cast<int>(threadIdx.y);
+  const int x0 = tx * VEC;
+  const int ring_rows = TY + 2;
+  const std::size_t plane_sz = static_cast<std::size_t>(3) * ring_rows * nx;
+  const std::size_t zb_sz = static_cast<std::size_t>(TY + 1) * nx;
+  float* R = sm;                                // 3 slots: r of planes z, z+1; p_k of plane z+2
+  float* S = R + 3 * plane_sz;                  // p_{k-1} of the plane in flight
+  float* Z = S + (FIRST ? 0 : plane_sz);        // primal of plane z in slot (z - z0) & 1
+  float* Bs = Z + 2 * zb_sz;                    // b of plane z in slot (z - z0) & 1
+  const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
+  const int linear = static_cast<int>(threadIdx.y * blockDim.x + threadIdx.x);
+  const int lane = linear & 31;
+  const int warp_threads = min(32, static_cast<int>(blockDim.x * blockDim.y) - (linear & ~31));
+  const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
+  const float m = A.momentum;
+
+  const long long units = static_cast<long long>(A.ytiles) * nz;
+  const long long u_end = units * (blockIdx.x + 1) / gridDim.x;
+  for (long long u = units * blockIdx.x / gridDim.x; u < u_end;) {
+    const int y0 = static_cast<int>(u / nz) * TY;
+    const int z0 = static_cast<int>(u % nz);
+    const int z1 = static_cast<int>(min(static_cast<long long>(nz), z0 + (u_end - u)));
+    u += z1 - z0;
+    const int zlast = min(z1, nz - 1);  // last plane whose r is needed (for the primal of z1)
+    const auto rslot = [&](int z) { return R + static_cast<std::size_t>((z - z0 + 1) % 3) * plane_sz; };
+    const auto zslot = [&](int z) { return Z + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
+    const auto bslot = [&](int z) { return Bs + static_cast<std::size_t>((z - z0) & 1) * zb_sz; };
+
+    // Each thread copies, and later converts, the same elements: row-components rc = ty, ty + TY,
+    // ... of the ring, x0 .. x0 + VEC - 1. Rows outside the volume are neither copied nor read.
+    const auto issue_p = [&](int z, int comps) {
+      float* dst = rslot(z);
+      for (int rc = ty; rc < comps * ring_rows; rc += TY) {
+        const int c = rc / ring_rows;
+        const int rr = rc - c * ring_rows;
+        const int y = y0 - 1 + rr;
+        if (y < 0 || y >= ny) continue;
+        const std::size_t off = static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0;
+        const std::size_t at = (static_cast<std::size_t>(c) * ring_rows + rr) * nx + x0;
+        copy_async<VEC>(dst + at, A.pk[c] + off);
+        if (!FIRST) copy_async<VEC>(S + at, A.pkm1[c] + off);
+      }
+    };
+    const auto convert = [&](int z, int comps) {
+      if (FIRST) return;
+      float* dst = rslot(z);
+      for (int rc = ty; rc < comps * ring_rows; rc += TY) {
+        const int c = rc / ring_rows;
+        const int rr = rc - c * ring_rows;
+        const int y = y0 - 1 + rr;
+        if (y < 0 || y >= ny) continue;
+        const std::size_t at = (static_cast<std::size_t>(c) * ring_rows + rr) * nx + x0;
+        float pkv[VEC], pmv[VEC];
+        Vec<VEC>::load(dst + at, pkv);
+        Vec<VEC>::load(S + at, pmv);
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) pkv[i] = __fadd_rn(pkv[i], __fmul_rn(m, __fsub_rn(pkv[i], pmv[i])));
+        Vec<VEC>::store(dst + at, pkv);
+      }
+    };
+    const auto issue_b = [&](int z) {
+      float* dst = bslot(z);
+      for (int rr = ty; rr < TY + 1; rr += TY) {
+        const int y = y0 + rr;
+        if (y >= ny) continue;
+        copy_async<VEC>(dst + static_cast<std::size_t>(rr) * nx + x0,
+                        A.b + static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0);
+      }
+    };
+    // z on plane z (rows y0 .. y0+TY) from r of that plane and of the plane below (as k_fgp).
+    const auto primal = [&](int z) {
+      const float* Rc = rslot(z);
+      const float* Rb = rslot(z - 1);
+      const float* B = bslot(z);
+      float* Zd = zslot(z);
+      for (int it = 0; it < 2; ++it) {
+        const int rr = ty + it * TY;
+        const bool active = rr < TY + 1;
+        const int rrc = active ? rr : 0;
+        const int y = y0 + rrc;
+        const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc) * nx;
+        const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+        float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
+        Vec<VEC>::load(rz + x0, vz);
+        Vec<VEC>::load(rzb + x0, vzb);
+        Vec<VEC>::load(ry + x0, vy);
+        Vec<VEC>::load(rym + x0, vym);
+        Vec<VEC>::load(rx + x0, vx);
+        Vec<VEC>::load(B + static_cast<std::size_t>(rrc) * nx + x0, vb);
+        float left;
+        if constexpr (VEC == 4) {
+          const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
+          left = (x0 > 0 && lane == 0) ? rx[x0 - 1] : from_lane;
+        } else {
+          left = x0 > 0 ? rx[x0 - 1] : 0.0f;
+        }
+        if (!active) continue;
+        float out[VEC];
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) {
+          const int x = x0 + i;
+          float zv = 0.0f;
+          if (y < ny) {
+            float sacc = 0.0f;
+            if (z < nz - 1) sacc = __fadd_rn(sacc, vz[i]);
+            if (z > 0) sacc = __fsub_rn(sacc, vzb[i]);
+            if (y < ny - 1) sacc = __fadd_rn(sacc, vy[i]);
+            if (y > 0) sacc = __fsub_rn(sacc, vym[i]);
+            if (x < nx - 1) sacc = __fadd_rn(sacc, vx[i]);
+            if (x > 0) sacc = __fsub_rn(sacc, i == 0 ? left : vx[i > 0 ? i - 1 : 0]);
+            zv = tv_primal(vb[i], A.lambda, sacc);
+          }
+          out[i] = zv;
+        }
+        Vec<VEC>::store(Zd + static_cast<std::size_t>(rr) * nx + x0, out);
+      }
+    };
+
+    // Prologue: plane z0 - 1 (z component only) and z0 landed and converted, z0 + 1 in flight.
+    if (z0 > 0) {
+      issue_p(z0 - 1, 1);
+      copy_commit();
+      copy_wait<0>();
+      convert(z0 - 1, 1);
+    }
+    issue_p(z0, 3);
+    issue_b(z0);
+    copy_commit();
+    copy_wait<0>();
+    convert(z0, 3);
+    if (z0 + 1 <= zlast) {
+      issue_p(z0 + 1, 3);
+      issue_b(z0 + 1);
+      copy_commit();
+    }
+    __syncthreads();
+    primal(z0);
+    __syncthreads();
+
+    const int y = y0 + ty;
+    for (int z = z0; z < z1; ++z) {
+      // Plane z + 1 (copied during the previous iteration): land and convert this thread's share,
+      // then start plane z + 2 into the free ring slot and the staging plane.
+      copy_wait<0>();
+      if (z + 1 <= zlast) convert(z + 1, 3);
+      if (z + 2 <= zlast) {
+        issue_p(z + 2, 3);
+        issue_b(z + 2);
+        copy_commit();
+      }
+      __syncthreads();
+      if (z + 1 < nz) primal(z + 1);
+      __syncthreads();
+      {
+        const float* Rc = rslot(z);
+        float rv[3][VEC];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Vec<VEC>::load(Rc + (static_cast<std::size_t>(c) * ring_rows + ty + 1) * nx + x0, rv[c]);
+        const float* zcp = zslot(z) + static_cast<std::size_t>(ty) * nx;
+        float zc[VEC], zy[VEC], zz[VEC];
+        Vec<VEC>::load(zcp + x0, zc);
+        Vec<VEC>::load(zslot(z) + static_cast<std::size_t>(ty + 1) * nx + x0, zy);
+        Vec<VEC>::load(zslot(z + 1) + static_cast<std::size_t>(ty) * nx + x0, zz);
+        float right;
+        if constexpr (VEC == 4) {
+          const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
+          right = (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? zcp[x0 + VEC] : from_lane;
+        } else {
+          right = x0 + 1 < nx ? zcp[x0 + 1] : 0.0f;
+        }
+        if (y < ny) {
+          float pv[3][VEC];
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) {
+            const int x = x0 + i;
+            const float c = zc[i];
+            float g[3];
+            g[0] = z < nz - 1 ? __fsub_rn(c, zz[i]) : 0.0f;
+            g[1] = y < ny - 1 ? __fsub_rn(c, zy[i]) : 0.0f;
+            g[2] = x < nx - 1 ? __fsub_rn(c, i == VEC - 1 ? right : zc[i < VEC - 1 ? i + 1 : 0]) : 0.0f;
+            const float r[3] = {rv[0][i], rv[1][i], rv[2][i]};
+            float p[3];
+            tv_dual_project(g, A.step, r, p);
+#pragma unroll
+            for (int c2 = 0; c2 < 3; ++c2) pv[c2][i] = p[c2];
+          }
+          const std::size_t at = static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) Vec<VEC>::store(A.pout[c] + at, pv[c]);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // Final primal point x = max(b - lambda L(p), 0), VEC voxels of one row per thread, and its use.
 template <int VEC, int Mode>
 __global__ void __launch_bounds__(256)
@@ -337,7 +563,18 @@ struct FgpShape {
   int ty;
   int grid;
   std::size_t smem;
+  int variant = 0;  // 0: r stored (k_fgp), 1: r recomputed (k_fgp_p)
 };
+
+// Shared memory of the r-recomputing step: 3 ring slots + 1 staging plane of 3 components x TY + 2
+// rows, 2 primal and 2 b planes of TY + 1 rows (no staging on the first step).
+std::size_t fgp_p_smem(int nx, int ty, bool first) {
+  return ((first ? 3 : 4) * static_cast<std::size_t>(3) * (ty + 2) + 4 * static_cast<std::size_t>(ty + 1)) * nx *
+         sizeof(float);
+}
+
+// Autotuner choices: variant * 16 + rows per CTA.
+constexpr int kFgpVariantScale = 16;
 
 std::size_t fgp_smem(int nx, int ty) {
   return (3 * static_cast<std::size_t>(3) * (ty + 2) + 4 * static_cast<std::size_t>(ty + 1)) * nx * sizeof(float);
@@ -349,8 +586,11 @@ template <int VEC>
 std::vector<int> fgp_rows_candidates(int nx) {
   std::vector<int> out;
   const int tx = nx / VEC;
-  for (const int ty : {8, 4, 2, 1}) {
-    if (tx * ty <= 256 && fgp_smem(nx, ty) <= 200 * 1024) out.push_back(ty);
+  for (const int variant : {1, 0}) {
+    for (const int ty : {8, 4, 2, 1}) {
+      const std::size_t smem = variant == 1 ? fgp_p_smem(nx, ty, false) : fgp_smem(nx, ty);
+      if (tx * ty <= 256 && smem <= 200 * 1024) out.push_back(variant * kFgpVariantScale + ty);
+    }
   }
   return out;
 }
@@ -371,21 +611,40 @@ TuneKey fgp_key(int nz, int ny, int nx) {
 }
 
 template <int VEC>
-FgpShape fgp_shape_rows(int nz, int ny, int nx, int ty) {
-  const std::size_t smem = fgp_smem(nx, ty);
-  auto kernel = k_fgp<VEC, false, false>;
-  ensure_smem(kernel);
+FgpShape fgp_shape_rows(int nz, int ny, int nx, int choice) {
+  const int variant = choice / kFgpVariantScale;
+  const int ty = choice % kFgpVariantScale;
+  const std::size_t smem = variant == 1 ? fgp_p_smem(nx, ty, false) : fgp_smem(nx, ty);
   int per_sm = 0;
-  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (nx / VEC) * ty, smem), "cudaOccupancy");
+  if (variant == 1) {
+    auto kernel = k_fgp_p<VEC, false>;
+    ensure_smem(kernel);
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (nx / VEC) * ty, smem), "cudaOccupancy");
+  } else {
+    auto kernel = k_fgp<VEC, false, false>;
+    ensure_smem(kernel);
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (nx / VEC) * ty, smem), "cudaOccupancy");
+  }
   const long long slots = static_cast<long long>(sm_count()) * std::max(per_sm, 1);
   const long long units = static_cast<long long>((ny + ty - 1) / ty) * nz;
-  return {ty, static_cast<int>(std::min(slots, units)), smem};
+  FgpShape sh{ty, static_cast<int>(std::min(slots, units)), smem, variant};
+  return sh;
 }
+
+// Forced FGP form (qhk_tv_form): 0 the tuned / default one, 1 stored r, 2 recomputed r.
+std::atomic<int> g_fgp_form{0};
 
 template <int VEC>
 FgpShape fgp_shape(int nz, int ny, int nx) {
-  const int ty = tuned_choice(fgp_key<VEC>(nz, ny, nx), fgp_rows_default<VEC>(nx));
-  return fgp_shape_rows<VEC>(nz, ny, nx, ty);
+  const int form = g_fgp_form.load();
+  int choice = tuned_choice(fgp_key<VEC>(nz, ny, nx), fgp_rows_default<VEC>(nx));
+  if (form == 1 || form == 2) {
+    const int ty = choice % kFgpVariantScale;
+    choice = (form - 1) * kFgpVariantScale + ty;
+    const std::size_t smem = form == 2 ? fgp_p_smem(nx, ty, false) : fgp_smem(nx, ty);
+    if (smem > 200 * 1024) choice = (form - 1) * kFgpVariantScale + 1;
+  }
+  return fgp_shape_rows<VEC>(nz, ny, nx, choice);
 }
 
 template <int VEC, bool FIRST, bool LAST>
@@ -394,6 +653,17 @@ void launch_fgp(const FgpArgs& a, const FgpShape& sh, cudaStream_t s) {
   ensure_smem(kernel);
   const dim3 block(a.nx / VEC, sh.ty);
   kernel<<<sh.grid, block, sh.smem, s>>>(a);
+  check_launch("fgp step");
+}
+
+// The first step of the r-recomputing form needs no staging plane: its smem is smaller.
+template <int VEC, bool FIRST>
+void launch_fgp_p(const FgpPArgs& a, const FgpShape& sh, cudaStream_t s) {
+  auto kernel = k_fgp_p<VEC, FIRST>;
+  ensure_smem(kernel);
+  const dim3 block(a.nx / VEC, sh.ty);
+  const std::size_t smem = fgp_p_smem(a.nx, sh.ty, FIRST);
+  kernel<<<sh.grid, block, smem, s>>>(a);
   check_launch("fgp step");
 }
 
@@ -436,6 +706,11 @@ void launch_final(TvFinal mode, const float* b, float* const p[3], int nz, int n
 
 float fista_t(float t) { return 0.5f * (1.0f + std::sqrt(1.0f + 4.0f * t * t)); }
 
+void set_tv_form(int form) {
+  require(form >= 0 && form <= 2, "tv: form must be 0 (tuned), 1 (stored r) or 2 (recomputed r)");
+  g_fgp_form.store(form);
+}
+
 void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, int inner, TvFinal final_mode,
              float momentum, float* xprev, float* out, float nm2, float inv_k02, cudaStream_t s) {
   require(nz >= 1 && ny >= 1 && nx >= 1, "tv: empty volume");
@@ -449,33 +724,60 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
   const FgpShape sh = vec == 4 ? fgp_shape<4>(nz, ny, nx) : fgp_shape<1>(nz, ny, nx);
   const float step = 1.0f / (12.0f * lambda);
   float tk = 1.0f;
-  const int ip = t.p_index;
-  const int ia = (ip + 1) % 3;
-  int cur_r = ip;
-  for (int k = 0; k < inner; ++k) {
-    const float tn = fista_t(tk);
-    const float m = (tk - 1.0f) / tn;
-    FgpArgs a{};
-    a.b = b;
-    a.nz = nz, a.ny = ny, a.nx = nx;
-    a.ytiles = (ny + sh.ty - 1) / sh.ty;
-    a.lambda = lambda, a.step = step, a.momentum = m;
-    const int rout = k == 0 ? (ip + 2) % 3 : 3 - ia - cur_r;
-    for (int c = 0; c < 3; ++c) {
-      a.rin[c] = t.v[cur_r][c];
-      a.pin[c] = t.v[k == 0 ? ip : ia][c];
-      a.pout[c] = t.v[ia][c];
-      a.rout[c] = t.v[rout][c];
+  if (sh.variant == 1) {
+    // p_k lives in triplet (i0 + k) % 3; step k reads p_k and p_{k-1}, writes p_{k+1} over p_{k-2}.
+    const int i0 = t.p_index;
+    float m_prev = 0.0f;
+    for (int k = 0; k < inner; ++k) {
+      FgpPArgs a{};
+      a.b = b;
+      a.nz = nz, a.ny = ny, a.nx = nx;
+      a.ytiles = (ny + sh.ty - 1) / sh.ty;
+      a.lambda = lambda, a.step = step, a.momentum = m_prev;
+      for (int c = 0; c < 3; ++c) {
+        a.pk[c] = t.v[(i0 + k) % 3][c];
+        a.pkm1[c] = t.v[(i0 + k + 2) % 3][c];
+        a.pout[c] = t.v[(i0 + k + 1) % 3][c];
+      }
+      if (vec == 4) {
+        k == 0 ? launch_fgp_p<4, true>(a, sh, s) : launch_fgp_p<4, false>(a, sh, s);
+      } else {
+        k == 0 ? launch_fgp_p<1, true>(a, sh, s) : launch_fgp_p<1, false>(a, sh, s);
+      }
+      const float tn = fista_t(tk);
+      m_prev = (tk - 1.0f) / tn;
+      tk = tn;
     }
-    if (vec == 4) {
-      launch_fgp_any<4>(k == 0, k == inner - 1, a, sh, s);
-    } else {
-      launch_fgp_any<1>(k == 0, k == inner - 1, a, sh, s);
+    if (inner > 0) t.p_index = (i0 + inner) % 3;
+  } else {
+    const int ip = t.p_index;
+    const int ia = (ip + 1) % 3;
+    int cur_r = ip;
+    for (int k = 0; k < inner; ++k) {
+      const float tn = fista_t(tk);
+      const float m = (tk - 1.0f) / tn;
+      FgpArgs a{};
+      a.b = b;
+      a.nz = nz, a.ny = ny, a.nx = nx;
+      a.ytiles = (ny + sh.ty - 1) / sh.ty;
+      a.lambda = lambda, a.step = step, a.momentum = m;
+      const int rout = k == 0 ? (ip + 2) % 3 : 3 - ia - cur_r;
+      for (int c = 0; c < 3; ++c) {
+        a.rin[c] = t.v[cur_r][c];
+        a.pin[c] = t.v[k == 0 ? ip : ia][c];
+        a.pout[c] = t.v[ia][c];
+        a.rout[c] = t.v[rout][c];
+      }
+      if (vec == 4) {
+        launch_fgp_any<4>(k == 0, k == inner - 1, a, sh, s);
+      } else {
+        launch_fgp_any<1>(k == 0, k == inner - 1, a, sh, s);
+      }
+      cur_r = rout;
+      tk = tn;
     }
-    cur_r = rout;
-    tk = tn;
+    if (inner > 0) t.p_index = ia;
   }
-  if (inner > 0) t.p_index = ia;
   float* const* p = t.v[t.p_index];
   if (vec == 4) {
     launch_final<4>(final_mode, b, p, nz, ny, nx, lambda, momentum, xprev, out, nm2, inv_k02, s);
@@ -500,20 +802,35 @@ __global__ void k_fill_hash(float* p, std::size_t n, float lo, float hi, unsigne
 
 template <int VEC>
 void tune_fgp_rows(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s) {
+  // A middle step of each form: r (or p_k) from triplet 0, p (or p_{k-1}) from triplet 1, outputs
+  // into triplets 1 and 2 (the inputs each run reads are never written).
   FgpArgs a{};
   a.b = b;
   a.nz = nz, a.ny = ny, a.nx = nx;
   a.lambda = lambda, a.step = 1.0f / (12.0f * lambda), a.momentum = 0.5f;
+  FgpPArgs q{};
+  q.b = b;
+  q.nz = nz, q.ny = ny, q.nx = nx;
+  q.lambda = a.lambda, q.step = a.step, q.momentum = 0.5f;
   for (int c = 0; c < 3; ++c) {
     a.rin[c] = t.v[0][c];
     a.pin[c] = t.v[1][c];
     a.pout[c] = t.v[1][c];
     a.rout[c] = t.v[2][c];
+    q.pk[c] = t.v[0][c];
+    q.pkm1[c] = t.v[1][c];
+    q.pout[c] = t.v[2][c];
   }
   autotune(fgp_key<VEC>(nz, ny, nx), fgp_rows_candidates<VEC>(nx), fgp_rows_default<VEC>(nx),
-           [&](int ty) {
-             a.ytiles = (ny + ty - 1) / ty;
-             launch_fgp<VEC, false, false>(a, fgp_shape_rows<VEC>(nz, ny, nx, ty), s);
+           [&](int choice) {
+             const FgpShape sh = fgp_shape_rows<VEC>(nz, ny, nx, choice);
+             if (sh.variant == 1) {
+               q.ytiles = (ny + sh.ty - 1) / sh.ty;
+               launch_fgp_p<VEC, false>(q, sh, s);
+             } else {
+               a.ytiles = (ny + sh.ty - 1) / sh.ty;
+               launch_fgp<VEC, false, false>(a, sh, s);
+             }
            },
            s);
 }

@@ -53,7 +53,16 @@ def test_rfft3_and_irfft3_match_numpy(cuda, qhk, shape):
     assert rel_err(host(out), x) < 2e-6
 
 
-def test_tv_prox_bit_identical_to_reference(cuda, qhk):
+@pytest.fixture(params=[1, 2], ids=["stored_r", "recomputed_r"])
+def tv_form(request, qhk):
+    """Both FGP step forms (the extrapolated point stored between steps, or recomputed from the two
+    previous duals) must give the reference's iterates bit for bit."""
+    qhk.tv_form(request.param)
+    yield request.param
+    qhk.tv_form(0)
+
+
+def test_tv_prox_bit_identical_to_reference(cuda, qhk, tv_form):
     g = golden("tv_prox")
     nz, ny, nx = g["b"].shape
     b = dev(cuda, g["b"])
@@ -66,7 +75,7 @@ def test_tv_prox_bit_identical_to_reference(cuda, qhk):
 
 @pytest.mark.parametrize("shape,inner", [((24, 20, 36), 7), ((10, 12, 30), 5), ((9, 7, 8), 1), ((8, 8, 8), 0),
                                          ((40, 33, 64), 10)])
-def test_tv_prox_bit_identical_to_oracle(cuda, qhk, shape, inner):
+def test_tv_prox_bit_identical_to_oracle(cuda, qhk, shape, inner, tv_form):
     rng = np.random.default_rng(inner + shape[0])
     b = rng.uniform(-0.2, 1.0, shape).astype(np.float32)
     p0 = (rng.uniform(-0.6, 0.6, (3,) + shape) * (rng.uniform(size=(3,) + shape) > 0.3)).astype(np.float32)
