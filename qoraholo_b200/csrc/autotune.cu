@@ -1,6 +1,7 @@
 // Launch-shape autotuner (autotune.hpp).
 #include <algorithm>
 #include <cstdlib>
+#include <fstream>
 #include <map>
 #include <mutex>
 #include <sstream>
@@ -27,6 +28,44 @@ std::atomic<int> g_enabled{initial_enabled()};
 
 const char* family_name(TuneFamily f) { return f == TuneFamily::axis ? "axis_cols" : "fgp_rows"; }
 
+// Optional table of choices shared between runs (QHK_AUTOTUNE_FILE): one line per key, "family s0 ..
+// s5 choice". Keys found there are not timed again; new choices are appended. A profiled run can so
+// reuse the shapes a plain run of the same command chose, instead of timing them under the profiler.
+const char* table_path() {
+  const char* p = std::getenv("QHK_AUTOTUNE_FILE");
+  return (p && p[0]) ? p : nullptr;
+}
+
+bool g_table_loaded = false;  // guarded by g_tune_mutex
+
+void load_table(int device) {
+  if (g_table_loaded) return;
+  g_table_loaded = true;
+  const char* path = table_path();
+  if (!path) return;
+  std::ifstream in(path);
+  std::string fam;
+  while (in >> fam) {
+    TuneKey k;
+    k.device = device;
+    k.family = fam == "fgp_rows" ? TuneFamily::fgp : TuneFamily::axis;
+    for (long long& v : k.shape) in >> v;
+    Entry e;
+    in >> e.choice;
+    if (!in) break;
+    g_tuned.emplace(k, std::move(e));
+  }
+}
+
+void append_table(const TuneKey& k, int choice) {
+  const char* path = table_path();
+  if (!path) return;
+  std::ofstream out(path, std::ios::app);
+  out << family_name(k.family);
+  for (const long long v : k.shape) out << ' ' << v;
+  out << ' ' << choice << '\n';
+}
+
 }  // namespace
 
 bool TuneKey::operator<(const TuneKey& o) const {
@@ -46,12 +85,14 @@ TuneKey tune_key(TuneFamily family, std::array<long long, 6> shape) {
 int tuned_choice(const TuneKey& key, int fallback) {
   if (!autotune_enabled()) return fallback;
   std::lock_guard<std::mutex> lk(g_tune_mutex);
+  load_table(key.device);
   const auto it = g_tuned.find(key);
   return it == g_tuned.end() ? fallback : it->second.choice;
 }
 
 bool is_tuned(const TuneKey& key) {
   std::lock_guard<std::mutex> lk(g_tune_mutex);
+  load_table(key.device);
   return g_tuned.count(key) != 0;
 }
 
@@ -84,6 +125,7 @@ int autotune(const TuneKey& key, const std::vector<int>& candidates, int fallbac
   }
   std::lock_guard<std::mutex> lk(g_tune_mutex);
   const auto ins = g_tuned.emplace(key, std::move(e));
+  if (ins.second) append_table(key, ins.first->second.choice);
   return ins.first->second.choice;
 }
 

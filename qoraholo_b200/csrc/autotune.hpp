@@ -4,7 +4,9 @@
 // Tuning runs when a plan is built (never inside a stream capture): each candidate is launched on
 // the plan's own scratch buffers, twice to warm up and then `reps` times between CUDA events, and
 // the candidate with the smallest time wins. Kernels then read their shape from the table, falling
-// back to a fixed heuristic when a shape was never tuned (or tuning is off: QHK_AUTOTUNE=0). The
+// back to a fixed heuristic when a shape was never tuned (or tuning is off: QHK_AUTOTUNE=0). With
+// QHK_AUTOTUNE_FILE set, choices are also read from and appended to that file, so that another run
+// (a profiled one, say) uses the same shapes without timing them again. The
 // choices only change how work is tiled, never the arithmetic of any output element, so results
 // are bitwise the same whichever shape wins.
 #pragma once
