@@ -207,24 +207,22 @@ __global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
 
     const int y = y0 + ty;
     for (int z = z0; z < z1; ++z) {
-      const bool prefetch = z + 2 <= zlast;
-      if (prefetch) {
-        issue_r(z + 2, 3);
-        issue_b(z + 2);
-        copy_commit();
-      }
+      // Two barriers per plane: after the first every thread is past the previous plane's dual
+      // step, so the ring slot and b slot of plane z + 2 (those of z - 1 and z) are free for the
+      // prefetch, which then streams in during this plane's primal and dual steps.
       const std::size_t at = static_cast<std::size_t>(z) * nxy + static_cast<std::size_t>(y) * nx + x0;
       float pv[3][VEC];
       if (!FIRST && y < ny) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) Vec<VEC>::load(A.pin[c] + at, pv[c]);
       }
-      if (prefetch) {
-        copy_wait<1>();
-      } else {
-        copy_wait<0>();
-      }
+      copy_wait<0>();  // plane z + 1
       __syncthreads();
+      if (z + 2 <= zlast) {
+        issue_r(z + 2, 3);
+        issue_b(z + 2);
+        copy_commit();
+      }
       if (z + 1 < nz) primal(z + 1);
       __syncthreads();
       {
@@ -275,8 +273,8 @@ __global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
           }
         }
       }
-      __syncthreads();
     }
+    __syncthreads();  // the next march's prologue reuses the ring
   }
 }
 
