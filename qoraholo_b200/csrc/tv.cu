@@ -136,28 +136,38 @@ __global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
     // Lanes that exist in this thread's warp (the block's last warp may be partial).
     const int warp_threads = min(32, static_cast<int>(blockDim.x * blockDim.y) - (linear & ~31));
     const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
+    // One primal value from the ring: sum of the r differences in the host's order, then tv_primal.
+    const auto primal_value = [&](int z, int y, int x, float vz, float vzb, float vy, float vym, float vx,
+                                  float left, float vb) {
+      float sacc = 0.0f;
+      if (z < nz - 1) sacc = __fadd_rn(sacc, vz);
+      if (z > 0) sacc = __fsub_rn(sacc, vzb);
+      if (y < ny - 1) sacc = __fadd_rn(sacc, vy);
+      if (y > 0) sacc = __fsub_rn(sacc, vym);
+      if (x < nx - 1) sacc = __fadd_rn(sacc, vx);
+      if (x > 0) sacc = __fsub_rn(sacc, left);
+      return tv_primal(vb, A.lambda, sacc);
+    };
     const auto primal = [&](int z) {
       const float* Rc = rslot(z);
       const float* Rb = rslot(z - 1);
       const float* B = bslot(z);
       float* Zd = zslot(z);
-      for (int it = 0; it < 2; ++it) {
-        const int rr = ty + it * TY;
-        const bool active = rr < TY + 1;
-        const int rrc = active ? rr : 0;
-        const int y = y0 + rrc;
-        const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
-        const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
-        const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
-        const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rrc) * nx;
-        const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rrc + 1) * nx;
+      {  // rows y0 .. y0 + TY - 1: one row per thread row, VEC values per thread
+        const int rr = ty;
+        const int y = y0 + rr;
+        const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+        const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+        const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+        const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr) * nx;
+        const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
         float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
         Vec<VEC>::load(rz + x0, vz);
         Vec<VEC>::load(rzb + x0, vzb);
         Vec<VEC>::load(ry + x0, vy);
         Vec<VEC>::load(rym + x0, vym);
         Vec<VEC>::load(rx + x0, vx);
-        Vec<VEC>::load(B + static_cast<std::size_t>(rrc) * nx + x0, vb);
+        Vec<VEC>::load(B + static_cast<std::size_t>(rr) * nx + x0, vb);
         float left;
         if constexpr (VEC == 4) {
           const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
@@ -165,29 +175,37 @@ __global__ void __launch_bounds__(256, 3) k_fgp(FgpArgs A) {
         } else {
           left = x0 > 0 ? rx[x0 - 1] : 0.0f;
         }
-        if (!active) continue;
         float out[VEC];
 #pragma unroll
         for (int i = 0; i < VEC; ++i) {
           const int x = x0 + i;
-          float zv = 0.0f;
-          if (y < ny) {
-            float s = 0.0f;
-            if (z < nz - 1) s = __fadd_rn(s, vz[i]);
-            if (z > 0) s = __fsub_rn(s, vzb[i]);
-            if (y < ny - 1) s = __fadd_rn(s, vy[i]);
-            if (y > 0) s = __fsub_rn(s, vym[i]);
-            if (x < nx - 1) s = __fadd_rn(s, vx[i]);
-            if (x > 0) s = __fsub_rn(s, i == 0 ? left : vx[i > 0 ? i - 1 : 0]);
-            zv = tv_primal(vb[i], A.lambda, s);
-          }
-          out[i] = zv;
+          out[i] = y < ny ? primal_value(z, y, x, vz[i], vzb[i], vy[i], vym[i], vx[i],
+                                         i == 0 ? left : vx[i > 0 ? i - 1 : 0], vb[i])
+                          : 0.0f;
         }
         Vec<VEC>::store(Zd + static_cast<std::size_t>(rr) * nx + x0, out);
       }
+      {  // row y0 + TY (the next tile's first row, needed for this tile's y gradient): spread over
+         // all threads, one value each, so that no thread row waits for another.
+        const int rr = TY;
+        const int y = y0 + rr;
+        if (y < ny) {
+          const float* rz = Rc + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+          const float* rzb = Rb + (0 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+          const float* ry = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+          const float* rym = Rc + (1 * static_cast<std::size_t>(ring_rows) + rr) * nx;
+          const float* rx = Rc + (2 * static_cast<std::size_t>(ring_rows) + rr + 1) * nx;
+          const float* vb = B + static_cast<std::size_t>(rr) * nx;
+          float* out = Zd + static_cast<std::size_t>(rr) * nx;
+          const int nthreads = static_cast<int>(blockDim.x * blockDim.y);
+          for (int x = linear; x < nx; x += nthreads) {
+            out[x] = primal_value(z, y, x, rz[x], rzb[x], ry[x], rym[x], rx[x], x > 0 ? rx[x - 1] : 0.0f, vb[x]);
+          }
+        }
+      }
     };
 
-    // Prologue: planes z0 - 1 (z component only), z0 (and b) in one group, z0 + 1 in the next.
+  // Prologue: planes z0 - 1 (z component only), z0 (and b) in one group, z0 + 1 in the next.
     if (z0 > 0) issue_r(z0 - 1, 1);
     issue_r(z0, 3);
     issue_b(z0);
