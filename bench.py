@@ -76,7 +76,7 @@ def _parent_index(shapes, i):
     return n
 
 
-def phantom_fields(shapes, illum, n, pixel, device):
+def phantom_fields(shapes, illum, n, pixel, device, keep_on_device=False):
     """Rytov field ratios (count, n, n) at z = 0 of nested ellipsoids `shapes` (painter's order)
     for each illumination: the analytic first Born spectrum of each shape placed on the Ewald caps
     (an ellipsoid is an affinely scaled ball), taken as a Rytov phase -- the construction of the
@@ -115,6 +115,18 @@ def phantom_fields(shapes, illum, n, pixel, device):
         u = 1j / (4 * math.pi * nuz) * o * par / (pixel * pixel)
         u = torch.where(ok, u, torch.zeros_like(u))
         out[j] = torch.exp(torch.fft.ifft2(u)).to(torch.complex64)
+    return out if keep_on_device else out.cpu().numpy()
+
+
+def device_holograms(capi, ratio, illum, pixel, carrier, seed):
+    """Holograms (count, n, n) float32 on the host from device field ratios, synthesised on the device
+    (qhk_synthesize_holograms_device, noise sigma = NOISE)."""
+    import torch
+
+    count, n = ratio.shape[0], ratio.shape[1]
+    out = torch.empty((count, n, n), dtype=torch.float32, device=ratio.device)
+    capi.synthesize_holograms_device(ratio.data_ptr(), count, n, illum, pixel, carrier=carrier, noise=NOISE, seed=seed,
+                                     d_out=out.data_ptr())
     return out.cpu().numpy()
 
 
@@ -370,22 +382,26 @@ def serve_sample(rng, kind):
 
 
 def serving_setup(qh, stacks_per_geometry=2, seed=2024):
-    """Per mix entry: illuminations, geometry, background holograms and distinct request stacks."""
+    """Per mix entry: illuminations, geometry, background holograms and distinct request stacks
+    (field ratios and holograms computed on the device)."""
+    import torch
+
+    from qoraholo_b200 import capi
+
     rng = np.random.default_rng(seed)
     geos = []
     for idx, (name, share, count, n, hpix, out, carrier, radius, opts) in enumerate(SERVE_MIX):
         fpix = hpix * n / out
         geom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=fpix)
-        hgeom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=hpix)
         illum = qh.circular_scan(count, 0.9, geom)
         c = carrier / (n * hpix)
         stacks = []
         for k in range(stacks_per_geometry):
-            ratio = phantom_fields(serve_sample(rng, idx), illum, n, hpix, "cuda")
-            stacks.append(qh.synthesize_holograms(ratio, illum, hgeom, carrier=(c, c), noise=NOISE,
-                                                  seed=100 * idx + k + 1))
-        bg = qh.synthesize_holograms(np.ones((count, n, n), np.complex64), illum, hgeom, carrier=(c, c), noise=NOISE,
-                                     seed=100 * idx + 99)
+            ratio = phantom_fields(serve_sample(rng, idx), illum, n, hpix, "cuda", keep_on_device=True)
+            stacks.append(device_holograms(capi, ratio, illum, hpix, (c, c), seed=100 * idx + k + 1))
+        ones = torch.ones((count, n, n), dtype=torch.complex64, device="cuda")
+        bg = device_holograms(capi, ones, illum, hpix, (c, c), seed=100 * idx + 99)
+        del ones
         geos.append(dict(name=name, share=share, count=count, n=n, out=out, carrier=carrier, radius=radius,
                          opts=opts, geom=geom, illum=illum, stacks=stacks, bg=bg))
     return geos

@@ -186,6 +186,16 @@ int qhk_unwrap_batch_run(qhk_unwrap_batch* plan, const float* d_wrapped, float* 
 size_t qhk_unwrap_batch_device_bytes(const qhk_unwrap_batch* plan);
 int qhk_unwrap_batch_destroy(qhk_unwrap_batch* plan);
 
+/* Off-axis hologram synthesis on the device: synthesize_holograms (src/phantom.cpp:193-221, host-only in
+ * the reference), |R + u_in ratio|^2 + noise, R = amplitude e^{-2 pi i carrier . r}, u_in = e^{2 pi i
+ * (fy y + fx x)}. d_ratio (count, n, n) complex64 and d_out (count, n, n) float32 on the device,
+ * illuminations on the host; `pixel` is the hologram pixel. Noise-free holograms equal the host's to
+ * float rounding; the noise is N(0, noise^2) from a counter-based generator seeded by `seed` (other
+ * draws than the host's std::mt19937_64). Synchronous. */
+int qhk_synthesize_holograms_device(const void* d_ratio, int count, int n, const float* illum_fyfx, double pixel,
+                                    double carrier_y, double carrier_x, double amplitude, float noise, uint64_t seed,
+                                    float* d_out, void* stream);
+
 /* ---- Pipeline: replaces cuda::make_pipeline and Pipeline::Impl (src/backends.hpp:75-89,
  * src/cuda/pipeline.cu:12-161). Validation of the Pipeline constructor (src/pipeline.cpp:72-91). */
 typedef struct qhk_pipeline_options {

@@ -107,6 +107,8 @@ _PROTOS = {
     "qhk_unwrap_batch_run": (_I, [_VP, _VP, _VP, _I, _VP]),
     "qhk_unwrap_batch_device_bytes": (C.c_size_t, [_VP]),
     "qhk_unwrap_batch_destroy": (_I, [_VP]),
+    "qhk_synthesize_holograms_device": (_I, [_VP, _I, _I, _VP, C.c_double, C.c_double, C.c_double, C.c_double, _F,
+                                             C.c_uint64, _VP, _VP]),
     "qhk_autotune_enable": (_I, [_I]),
     "qhk_tv_form": (_I, [_I]),
     "qhk_autotune_report": (C.c_size_t, [_VP, C.c_size_t]),
@@ -239,6 +241,16 @@ def unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, stream=0):
 def autotune_enable(enabled: bool = True):
     """Plans built from now on time their launch shapes (on by default)."""
     check(lib().qhk_autotune_enable(int(bool(enabled))))
+
+
+def synthesize_holograms_device(d_ratio, count, n, illuminations, pixel, carrier=(5.0, 5.0), reference_amplitude=1.0,
+                                noise=0.0, seed=1, d_out=0, stream=0):
+    """Off-axis holograms on the device from device field ratios (count, n, n) complex64 into d_out
+    (count, n, n) float32 (qhk_synthesize_holograms_device)."""
+    il = np.ascontiguousarray(np.reshape(illuminations, (-1, 2)), np.float32)
+    check(lib().qhk_synthesize_holograms_device(_VP(d_ratio), int(count), int(n), host_ptr(il), float(pixel),
+                                                float(carrier[0]), float(carrier[1]), float(reference_amplitude),
+                                                float(noise), int(seed) & ((1 << 64) - 1), _VP(d_out), _VP(stream)))
 
 
 def tv_form(form: int):

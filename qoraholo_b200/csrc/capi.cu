@@ -18,6 +18,7 @@
 #include "odt.hpp"
 #include "pipeline.hpp"
 #include "server.hpp"
+#include "synth.hpp"
 #include "unwrap.hpp"
 
 namespace {
@@ -730,6 +731,15 @@ size_t qhk_unwrap_batch_device_bytes(const qhk_unwrap_batch* p) { return p ? p->
 
 int qhk_unwrap_batch_destroy(qhk_unwrap_batch* p) {
   return guard([&] { delete p; });
+}
+
+int qhk_synthesize_holograms_device(const void* d_ratio, int count, int n, const float* illum_fyfx, double pixel,
+                                    double carrier_y, double carrier_x, double amplitude, float noise, uint64_t seed,
+                                    float* d_out, void* stream) {
+  return guard([&] {
+    qhk::synthesize_holograms_device(static_cast<const float2*>(d_ratio), illum_fyfx, count, n, pixel, carrier_y,
+                                     carrier_x, amplitude, noise, seed, d_out, as_stream(stream));
+  });
 }
 
 struct qhk_server {

@@ -297,3 +297,37 @@ def test_phantom_generators_match_reference(qh):
     np.testing.assert_array_equal(qh.render_phantom(spheres(qh, CELL), gg, 12, 32), g["render"])
     np.testing.assert_allclose(qh.synthesize_holograms(g["rytov"], g["illum"], gg, (1.0, 1.5)), g["holo"], rtol=1e-6)
     np.testing.assert_array_equal(qh.circular_scan(49, 0.9, gg), g["scan49"])
+
+
+# ---- hologram synthesis on the device ---------------------------------------------------------
+
+
+def test_device_holograms_match_host_synthesis(qh):
+    """synthesize_holograms on the device (src/phantom.cpp:193-221): noise-free intensities equal the
+    host's to float rounding; the noise has the requested mean and spread, is reproducible for a seed
+    and changes with it."""
+    import torch
+
+    from qoraholo_b200 import capi
+
+    hg = np.array([0.532, 1.337, 1.2, 0.1], np.float32)
+    il = O.circular_scan(5, 0.9, G)
+    ratio = O.forward_fields(np.array([[0.0, 0.3, -0.2, 2.0, 1.36]], np.float32), il, hg, 96)
+    c = (30 / (96 * 0.1), 28 / (96 * 0.1))
+    host = qh.synthesize_holograms(ratio, il, geom(qh, hg), carrier=c)
+    d_ratio = torch.from_numpy(np.ascontiguousarray(ratio, np.complex64)).cuda()
+    out = torch.empty((5, 96, 96), dtype=torch.float32, device="cuda")
+
+    def run(noise, seed):
+        capi.synthesize_holograms_device(d_ratio.data_ptr(), 5, 96, il, float(hg[3]), carrier=c, noise=noise,
+                                         seed=seed, d_out=out.data_ptr())
+        return out.cpu().numpy()
+
+    clean = run(0.0, 1)
+    assert rel_err(clean, host) < 1e-6
+    noisy = run(0.02, 7)
+    d = (noisy - clean).astype(np.float64)
+    assert abs(d.mean()) < 3 * 0.02 / np.sqrt(d.size) + 1e-6
+    assert abs(d.std() - 0.02) < 0.02 * 0.02
+    assert np.array_equal(noisy, run(0.02, 7))
+    assert not np.array_equal(noisy, run(0.02, 8))
