@@ -78,7 +78,9 @@ __device__ __forceinline__ void tv_dual_step(const float g[3], float step, float
     q[a] = __fadd_rn(r[a], __fmul_rn(step, g[a]));
     norm2 = __fadd_rn(norm2, __fmul_rn(q[a], q[a]));
   }
-  const float scale = norm2 > 1.0f ? __fdiv_rn(1.0f, __fsqrt_rn(norm2)) : 1.0f;
+  // 1 / sqrt(norm2) with two roundings as the host's 1.0f / std::sqrt(norm2): the correctly rounded
+  // reciprocal of the rounded root equals the correctly rounded quotient 1 / root bit for bit.
+  const float scale = norm2 > 1.0f ? __frcp_rn(__fsqrt_rn(norm2)) : 1.0f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const float next = __fmul_rn(q[a], scale);
@@ -96,7 +98,9 @@ __device__ __forceinline__ void tv_dual_project(const float g[3], float step, co
     q[a] = __fadd_rn(r[a], __fmul_rn(step, g[a]));
     norm2 = __fadd_rn(norm2, __fmul_rn(q[a], q[a]));
   }
-  const float scale = norm2 > 1.0f ? __fdiv_rn(1.0f, __fsqrt_rn(norm2)) : 1.0f;
+  // 1 / sqrt(norm2) with two roundings as the host's 1.0f / std::sqrt(norm2): the correctly rounded
+  // reciprocal of the rounded root equals the correctly rounded quotient 1 / root bit for bit.
+  const float scale = norm2 > 1.0f ? __frcp_rn(__fsqrt_rn(norm2)) : 1.0f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) p[a] = __fmul_rn(q[a], scale);
 }
