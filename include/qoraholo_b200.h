@@ -263,7 +263,7 @@ typedef struct qhk_request_times {
 } qhk_request_times;
 
 typedef struct qhk_server_counters {
-  uint64_t submitted, completed, failed;
+  uint64_t submitted, completed, failed, cancelled;
   uint64_t workspaces_created, workspaces_evicted, graph_launches, passed_over;
   size_t budget, used, peak_used;
   int geometries, inflight, peak_inflight;
@@ -285,6 +285,9 @@ int qhk_server_submit(qhk_server* server, int geometry_id, const float* hologram
                       uint64_t* ticket);
 /* *done = 1 once the request has completed. */
 int qhk_server_done(qhk_server* server, uint64_t ticket, int* done);
+/* Withdraws a request not admitted yet (*cancelled = 1): it then completes with QHK_LOGIC_ERROR and uses
+ * no device time. *cancelled = 0 once it runs or has finished. */
+int qhk_server_cancel(qhk_server* server, uint64_t ticket, int* cancelled);
 /* Blocks until the request is done; `filled` and `times` may be NULL. Returns the request's error. */
 int qhk_server_wait(qhk_server* server, uint64_t ticket, double* filled, qhk_request_times* times);
 int qhk_server_stats(qhk_server* server, qhk_server_counters* stats);

@@ -57,7 +57,7 @@ class RequestTimes(C.Structure):
 
 
 class ServerCounters(C.Structure):
-    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64), ("cancelled", C.c_uint64),
                 ("workspaces_created", C.c_uint64), ("workspaces_evicted", C.c_uint64),
                 ("graph_launches", C.c_uint64), ("passed_over", C.c_uint64), ("budget", C.c_size_t),
                 ("used", C.c_size_t), ("peak_used", C.c_size_t), ("geometries", C.c_int), ("inflight", C.c_int),
@@ -119,6 +119,7 @@ _PROTOS = {
     "qhk_server_submit": (_I, [_VP, _I, _VP, _VP, C.POINTER(C.c_uint64)]),
     "qhk_server_done": (_I, [_VP, C.c_uint64, C.POINTER(_I)]),
     "qhk_server_wait": (_I, [_VP, C.c_uint64, C.POINTER(C.c_double), C.POINTER(RequestTimes)]),
+    "qhk_server_cancel": (_I, [_VP, C.c_uint64, C.POINTER(_I)]),
     "qhk_server_stats": (_I, [_VP, C.POINTER(ServerCounters)]),
     "qhk_server_destroy": (_I, [_VP]),
     "qhk_admission_simulate": (_I, [C.c_size_t, _I, _I, _I, _VP, _VP, _VP, _I, _VP, _VP, _VP, C.POINTER(_I)]),
@@ -470,6 +471,12 @@ class Server:
         d = _I()
         check(lib().qhk_server_done(self._h, int(ticket), C.byref(d)))
         return bool(d.value)
+
+    def cancel(self, ticket):
+        """Withdraws a request that has not started; True if it was withdrawn (its wait() then raises)."""
+        c = _I()
+        check(lib().qhk_server_cancel(self._h, int(ticket), C.byref(c)))
+        return bool(c.value)
 
     def wait(self, ticket):
         """Blocks until the request is done: (index volume, filled fraction, timings dict in ms)."""

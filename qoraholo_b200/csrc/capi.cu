@@ -794,6 +794,13 @@ int qhk_server_done(qhk_server* sv, uint64_t ticket, int* done) {
   });
 }
 
+int qhk_server_cancel(qhk_server* sv, uint64_t ticket, int* cancelled) {
+  return guard([&] {
+    qhk::require(sv && cancelled, "Server: null argument");
+    *cancelled = sv->server.cancel(ticket) ? 1 : 0;
+  });
+}
+
 int qhk_server_wait(qhk_server* sv, uint64_t ticket, double* filled, qhk_request_times* times) {
   return guard([&] {
     qhk::require(sv != nullptr, "Server: null server");
@@ -807,9 +814,10 @@ int qhk_server_stats(qhk_server* sv, qhk_server_counters* out) {
   return guard([&] {
     qhk::require(sv && out, "Server: null argument");
     const qhk::ServerStats s = sv->server.stats();
-    *out = qhk_server_counters{s.submitted, s.completed, s.failed, s.workspaces_created, s.workspaces_evicted,
-                            s.graph_launches, s.passed_over, s.budget, s.used, s.peak_used, s.geometries,
-                            s.inflight, s.peak_inflight};
+    *out = qhk_server_counters{s.submitted,          s.completed,      s.failed,         s.cancelled,
+                               s.workspaces_created, s.workspaces_evicted, s.graph_launches, s.passed_over,
+                               s.budget,             s.used,           s.peak_used,      s.geometries,
+                               s.inflight,           s.peak_inflight};
   });
 }
 

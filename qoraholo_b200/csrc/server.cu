@@ -340,6 +340,25 @@ bool Server::done(std::uint64_t ticket) {
   return it->second->done;
 }
 
+bool Server::cancel(std::uint64_t ticket) {
+  std::lock_guard<std::mutex> lk(mu_);
+  const auto it = requests_.find(ticket);
+  require(it != requests_.end(), "Server: unknown ticket");
+  const auto q = std::find(pending_.begin(), pending_.end(), ticket);
+  if (q == pending_.end()) return false;
+  pending_.erase(q);
+  Request& r = *it->second;
+  r.error = "Server: request cancelled before it ran";
+  r.error_status = kLogicError;
+  r.admitted = r.finished = Clock::now();
+  r.done = true;
+  ++stats_.cancelled;
+  kick_ = true;  // a passed-over head may be gone
+  wake_.notify_one();
+  done_.notify_all();
+  return true;
+}
+
 void Server::wait(std::uint64_t ticket, double* filled, RequestTimes* times) {
   std::unique_ptr<Request> r;
   {

@@ -106,7 +106,7 @@ struct RequestTimes {
 };
 
 struct ServerStats {
-  std::uint64_t submitted = 0, completed = 0, failed = 0;
+  std::uint64_t submitted = 0, completed = 0, failed = 0, cancelled = 0;
   std::uint64_t workspaces_created = 0, workspaces_evicted = 0, graph_launches = 0, passed_over = 0;
   std::size_t budget = 0, used = 0, peak_used = 0;
   int geometries = 0, inflight = 0, peak_inflight = 0;
@@ -135,6 +135,9 @@ class Server {
   void wait(std::uint64_t ticket, double* filled, RequestTimes* times);
   // True when the request has completed (wait() will not block).
   bool done(std::uint64_t ticket);
+  // Withdraws a request that has not been admitted yet: it completes with QHK_LOGIC_ERROR ("cancelled")
+  // and takes no device time. Returns false (and changes nothing) once it runs or has finished.
+  bool cancel(std::uint64_t ticket);
   [[nodiscard]] ServerStats stats();
   void volume_shape(int geometry, int* nz, int* n);
 

@@ -73,6 +73,25 @@ def test_synthetic_hologram_gives_forward_field(qh):
     assert np.max(np.abs(ratio - truth)) < 1e-4
 
 
+def test_noisy_hologram_stays_close(qh):
+    # Field.NoisyHologramStaysClose (tests/test_field.cpp:88-106): noise of 2 % of the mean intensity,
+    # interior rms (8-pixel margin) below 0.02.
+    hg = np.array([0.532, 1.337, 1.2, 0.055], np.float32)
+    fg = hg.copy()
+    fg[3] = hg[3] * 2
+    il = np.array([[0.0, 0.0], [0.4, -0.7]], np.float32)
+    sph = np.array([[0.0, 0.3, -0.2, 2.0, 1.36]], np.float32)
+    truth_holo = O.forward_fields(sph, il, hg, 128, "born")
+    truth = O.forward_fields(sph, il, fg, 64, "born")
+    holo = qh.synthesize_holograms(truth_holo, il, geom(qh, hg), carrier=(5.0, 5.0), noise=0.04, seed=3)
+    bg = qh.synthesize_holograms(np.ones((2, 128, 128), np.complex64), il, geom(qh, hg), carrier=(5.0, 5.0),
+                                 noise=0.04, seed=4)
+    kw = dict(center=(35.2, 35.2), radius=17.0, output_size=64)
+    ratio = qh.field_ratio(qh.extract_fields(holo, **kw), qh.extract_fields(bg, **kw))
+    d = (ratio - truth)[:, 8:-8, 8:-8]
+    assert float(np.sqrt(np.mean(np.abs(d) ** 2))) < 0.02
+
+
 def test_auto_detection_matches_explicit_centre(qh):
     # Field.AutoDetectionMatchesExplicitCentre (tests/test_field.cpp:108-119)
     hg = np.array([0.532, 1.337, 1.2, 0.055], np.float32)
@@ -176,6 +195,18 @@ def test_recovers_sphere_index_and_gp_helps(qh):
     assert rmse(gp) < 0.7 * rmse(plain)
     # Odt.TvReducesErrorAgainstGp (tests/test_odt.cpp:88-101)
     assert abs(tv[inner].mean() - 1.36) < 4e-3 and rmse(tv) < rmse(gp)
+
+
+def test_real_gp_matches_complex_gp(qh):
+    # Odt.RealGpMatchesComplexGp (tests/test_odt.cpp:66-86): R2C and C2C GP iterates agree (1e-4,
+    # measured 5e-6 by the reference) and fill exactly the same k-space voxels.
+    sph = np.array([[0.0, 0.0, 0.0, 3.0, 1.36]], np.float32)
+    il = O.circular_scan(49, 0.9, G)
+    fields = qh.rytov(O.forward_fields(sph, il, G, 64, "rytov"))
+    a, fa = qh.reconstruct(fields, il, geom(qh, G), iterations=10, return_filled=True)
+    b, fb = qh.reconstruct(fields, il, geom(qh, G), iterations=10, gp_transform="c2c", return_filled=True)
+    assert contrast_err(a, b, float(G[1])) < 1e-4
+    assert fa == fb
 
 
 def test_reconstruct_rejects_bad_arguments(qh):

@@ -269,3 +269,26 @@ def test_server_errors(workload):
     with capi.Server(hbm_budget=1 << 20, max_inflight=2) as sv:
         with pytest.raises(ValueError):
             _register(sv, {"gp64": w})
+
+
+@pytest.mark.gpu
+def test_server_cancels_queued_requests(workload):
+    """A request not admitted yet can be withdrawn: it fails with QHK_LOGIC_ERROR, takes no device
+    time, and the requests around it complete unchanged."""
+    from qoraholo_b200 import capi
+
+    w = workload["tv128"]
+    with capi.Server(hbm_budget=8 * GiB, max_inflight=1) as sv:
+        gid = _register(sv, {"tv128": w})["tv128"]
+        tickets = [sv.submit(gid, w["stacks"][k % 3]) for k in range(8)]
+        withdrawn = [t for t in tickets[4:] if sv.cancel(t)]
+        assert withdrawn  # one slot: the tail of the queue has not started yet
+        for k, t in enumerate(tickets):
+            if t in withdrawn:
+                with pytest.raises(capi.QhkError) as e:
+                    sv.wait(t)
+                assert e.value.code == capi.LOGIC_ERROR
+            else:
+                assert np.array_equal(sv.wait(t)[0], w["alone"][k % 3])
+        st = sv.stats()
+        assert st["cancelled"] == len(withdrawn) and st["completed"] == len(tickets) - len(withdrawn)
