@@ -269,6 +269,11 @@ typedef struct qhk_server_counters {
   int geometries, inflight, peak_inflight;
 } qhk_server_counters;
 
+/* The environment variable QHK_SERVER_STAGERS sets the number of host threads that stage pageable
+ * inputs and outputs through the workspaces' page-locked buffers (default 2). QHK_SERVER_EXCLUSIVE=1
+ * runs the requests' kernels one request at a time, in admission order, while their copies still
+ * overlap: a lower tail latency at moderate load, less throughput at saturation (requests that run
+ * together fill each other's idle SMs). */
 int qhk_server_create(qhk_server** server, size_t hbm_budget_bytes, int max_inflight, int use_graphs);
 /* Registers a geometry, validated as qhk_pipeline_create (`upload_chunks` is ignored), with its
  * background holograms (count, N, N) on the host. Synchronous. QHK_INVALID_ARGUMENT when its

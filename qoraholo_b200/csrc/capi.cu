@@ -2,6 +2,7 @@
 // arguments, converts exceptions into a status code and records the message for qhk_last_error().
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numbers>
@@ -749,7 +750,10 @@ struct qhk_server {
 int qhk_server_create(qhk_server** server, size_t hbm_budget_bytes, int max_inflight, int use_graphs) {
   return guard([&] {
     qhk::require(server != nullptr, "Server: null argument");
-    *server = new qhk_server{qhk::Server(hbm_budget_bytes, max_inflight, use_graphs != 0)};
+    // QHK_SERVER_STAGERS: host threads that stage pageable inputs and outputs (default 2).
+    const char* e = std::getenv("QHK_SERVER_STAGERS");
+    const int stagers = e && std::atoi(e) > 0 ? std::atoi(e) : 2;
+    *server = new qhk_server{qhk::Server(hbm_budget_bytes, max_inflight, use_graphs != 0, stagers)};
   });
 }
 

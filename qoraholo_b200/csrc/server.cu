@@ -15,6 +15,7 @@
 // Results do not depend on what runs beside them: each request computes in its own workspace with
 // the same deterministic kernels, so a request's volume is bitwise the same alone and in a mix.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 
@@ -189,6 +190,8 @@ Server::Workspace::~Workspace() {
 
 Server::Server(std::size_t hbm_budget, int max_inflight, bool use_graphs, int stagers)
     : use_graphs_(use_graphs), admission_(hbm_budget, max_inflight) {
+  const char* e = std::getenv("QHK_SERVER_EXCLUSIVE");
+  exclusive_ = e && e[0] == '1';
   require(stagers >= 1, "Server: need at least one stager thread");
   check(cudaGetDevice(&device_), "cudaGetDevice");
   stats_.budget = hbm_budget;
@@ -409,10 +412,25 @@ void Server::launch(const Request& r, Workspace& w, const Geometry& g) {
   check(cudaMemcpyAsync(w.plan->holo_buffer(), in, g.holo_floats * sizeof(float), cudaMemcpyHostToDevice, s),
         "Server: upload holograms");
   const float2* bg = g.background.get();
+  // Serialised compute (QHK_SERVER_EXCLUSIVE=1): each request's kernels wait for the previous
+  // request's kernels, in the order they are enqueued, while copies still overlap.
+  std::unique_lock<std::mutex> ck(compute_mu_, std::defer_lock);
+  const auto begin_compute = [&] {
+    if (!exclusive_) return;
+    ck.lock();
+    check(cudaStreamWaitEvent(s, compute_tail_.get(), 0), "cudaStreamWaitEvent");
+  };
+  const auto end_compute = [&] {
+    if (!exclusive_) return;
+    compute_tail_.record(s);
+    ck.unlock();
+  };
   if (!w.warmed || !use_graphs_) {
     // First request of a workspace: eager launches, which also make every lazy per-device setup
     // (twiddle tables, shared-memory limits) happen outside any capture.
+    begin_compute();
     w.plan->enqueue(w.plan->holo_buffer(), bg, w.plan->index_buffer(), s);
+    end_compute();
     w.warmed = true;
   } else {
     if (!w.graph) {
@@ -443,7 +461,9 @@ void Server::launch(const Request& r, Workspace& w, const Geometry& g) {
       g_launches.fetch_sub(kernels);
       w.graph_kernels = kernels;
     }
+    begin_compute();
     check(cudaGraphLaunch(w.graph, s), "Server: graph launch");
+    end_compute();
     g_launches.fetch_add(w.graph_kernels);
     std::lock_guard<std::mutex> lk(mu_);
     ++stats_.graph_launches;

@@ -205,6 +205,9 @@ class Server {
   std::condition_variable jobs_cv_;  // stagers
   int device_ = 0;
   bool use_graphs_;
+  bool exclusive_ = false;  // serialise the requests' kernels (copies still overlap)
+  std::mutex compute_mu_;
+  Event compute_tail_;      // recorded after the last enqueued request's kernels
   bool stop_ = false;
   bool stop_stagers_ = false;
   bool kick_ = false;  // something the scheduler acts on changed since it last looked
