@@ -481,12 +481,15 @@ def serving_leg(qh, capi, requests, rate, inflight=SERVE_INFLIGHT, plain=True):
         plain_request(qh, g, bgf[i], g["stacks"][0])
     plain_out = {}
     plain_lat = []
+    plain_ms = {}
     t0 = time.perf_counter()
     for j, (arr, gi, si) in enumerate(saturated if plain else []):
         now = time.perf_counter() - t0
         if now < arr:
             time.sleep(arr - now)
+        t_req = time.perf_counter()
         ri = plain_request(qh, geos[gi], bgf[gi], geos[gi]["stacks"][si])
+        plain_ms.setdefault(gi, []).append(1000.0 * (time.perf_counter() - t_req))
         plain_lat.append(1000.0 * (time.perf_counter() - t0 - arr))
         plain_out.setdefault((gi, si), ri)
     plain_span = time.perf_counter() - t0
@@ -517,6 +520,8 @@ def serving_leg(qh, capi, requests, rate, inflight=SERVE_INFLIGHT, plain=True):
         "saturated_p50_p99_ms": [round(statistics.median(sat_lat), 2), round(percentile(sat_lat, 0.99), 2)],
         "plain": {"value": round(plain_v, 3), "unit": UNIT, "p50_ms": round(statistics.median(pl), 2),
                   "p99_ms": round(percentile(pl, 0.99), 2),
+                  "median_request_ms": {g["name"]: round(statistics.median(plain_ms[i]), 1)
+                                        for i, g in enumerate(geos) if i in plain_ms},
                   "path": "per-call API (extract_fields, field_ratio, rytov, reconstruct) serially, numpy in/out, "
                           "same saturating arrivals (latency is queueing)"},
         "speedup": round(served_v / plain_v, 3),

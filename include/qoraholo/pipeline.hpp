@@ -54,6 +54,9 @@ class Pipeline {
   [[nodiscard]] std::span<const float> output() const;
   [[nodiscard]] double filled() const;
   [[nodiscard]] OdtResult run(const Array3<float>& holograms);
+  // The same into caller memory: holograms (count, N, N) -> index (nz, n, n), no intermediate
+  // host buffers of the caller's size (qhk_pipeline_run).
+  void run(std::span<const float> holograms, std::span<float> index);
 
   [[nodiscard]] const PipelineTimings& timings() const;
   [[nodiscard]] double setup_ms() const;

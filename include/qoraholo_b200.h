@@ -224,6 +224,15 @@ float* qhk_pipeline_input(qhk_pipeline* pipeline);
 const float* qhk_pipeline_output(const qhk_pipeline* pipeline);
 /* input -> output; QHK_LOGIC_ERROR before set_background. Synchronous. */
 int qhk_pipeline_process(qhk_pipeline* pipeline);
+/* Pipeline::run (src/pipeline.cpp:116-129, run(holograms) -> OdtResult) on caller memory:
+ * holograms (count, N, N) float32 -> index (nz, m, m) float32, both host memory, pageable or
+ * page-locked (batched pipelines: batch stacks in, batch volumes out). Synchronous; the result
+ * (filled, timings) as after process(). The staging copies run on QHK_COPY_THREADS host threads
+ * (default min(8, hardware threads)), each upload chunk's copy overlapping the transfer and field
+ * passes of the chunks before it; the pages of `index` are written (faulted in) while the device
+ * solves, then the volume is copied out part by part as it arrives. `input` and `output` are
+ * used as staging and hold this call's data afterwards. */
+int qhk_pipeline_run(qhk_pipeline* pipeline, const float* holograms, float* index);
 /* Device-resident variant: d_holo (count, N, N) and d_index (nz, m, m) on the device, asynchronous on
  * `stream`, no host copies (for serving loops and benchmarks). */
 int qhk_pipeline_process_device(qhk_pipeline* pipeline, const float* d_holo, float* d_index, void* stream);

@@ -92,6 +92,7 @@ _PROTOS = {
     "qhk_pipeline_input": (_VP, [_VP]),
     "qhk_pipeline_output": (_VP, [_VP]),
     "qhk_pipeline_process": (_I, [_VP]),
+    "qhk_pipeline_run": (_I, [_VP, _VP, _VP]),
     "qhk_pipeline_process_device": (_I, [_VP, _VP, _VP, _VP]),
     "qhk_pipeline_result": (_I, [_VP, C.POINTER(C.c_double), _VP]),
     "qhk_pipeline_filled": (_I, [_VP, _VP, C.POINTER(C.c_double)]),
@@ -371,6 +372,18 @@ class Pipeline:
 
     def process(self):
         check(lib().qhk_pipeline_process(self._h))
+
+    def run(self, holograms, out=None):
+        """qhk_pipeline_run: host holograms (input_shape) -> a new (or the given) host volume array."""
+        h = np.ascontiguousarray(holograms, np.float32)
+        if h.shape != self.input_shape:
+            raise ValueError(f"holograms must have shape {self.input_shape}")
+        if out is None:
+            out = np.empty(self.shape, np.float32)
+        elif out.shape != self.shape or out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape {self.shape}")
+        check(lib().qhk_pipeline_run(self._h, host_ptr(h), host_ptr(out)))
+        return out
 
     def process_device(self, d_holo, d_index, stream=0):
         check(lib().qhk_pipeline_process_device(self._h, _VP(d_holo), _VP(d_index), _VP(stream)))

@@ -238,20 +238,19 @@ PYBIND11_MODULE(_core, m) {
       .def(
           "run",
           [](Pipeline& p, In<float> holograms) {
-            const auto in = p.input();
-            if (static_cast<std::size_t>(holograms.size()) != in.size()) {
+            if (static_cast<std::size_t>(holograms.size()) != p.input().size() || holograms.ndim() != 3 ||
+                holograms.shape(1) != holograms.shape(2)) {
               throw std::invalid_argument("Pipeline.run: shape must be (count, N, N)");
             }
-            std::copy(holograms.data(), holograms.data() + holograms.size(), in.begin());
             const auto [nz, ny, nx] = p.output_shape();
-            Array3<float> out(nz, ny, nx);
+            py::array_t<float> out({nz, ny, nx});  // uninitialised: run() faults its pages in while the device works
+            std::span<const float> in(holograms.data(), static_cast<std::size_t>(holograms.size()));
+            std::span<float> dst(out.mutable_data(), static_cast<std::size_t>(out.size()));
             {
               py::gil_scoped_release release;
-              p.process();
-              const auto o = p.output();
-              std::copy(o.begin(), o.end(), out.data.begin());
+              p.run(in, dst);
             }
-            return to_numpy(std::move(out));
+            return out;
           },
           py::arg("holograms"))
       .def_property_readonly("filled", &Pipeline::filled)

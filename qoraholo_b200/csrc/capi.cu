@@ -465,6 +465,13 @@ int qhk_pipeline_process(qhk_pipeline* p) {
   });
 }
 
+int qhk_pipeline_run(qhk_pipeline* p, const float* holograms, float* index) {
+  return guard([&] {
+    qhk::require(p && holograms && index, "Pipeline: null argument");
+    p->plan.process_host(holograms, index);
+  });
+}
+
 int qhk_pipeline_process_device(qhk_pipeline* p, const float* d_holo, float* d_index, void* stream) {
   return guard([&] {
     qhk::require(p && d_holo && d_index, "Pipeline: null argument");

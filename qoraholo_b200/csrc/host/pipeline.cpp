@@ -91,18 +91,24 @@ std::span<const float> Pipeline::output() const {
 
 double Pipeline::filled() const { return impl_->filled; }
 
-OdtResult Pipeline::run(const Array3<float>& holograms) {
-  const auto in = input();
-  host::require(holograms.size() == in.size() && holograms.ny == holograms.nx,
-                "Pipeline::run: shape must be (count, N, N)");
-  std::copy(holograms.data.begin(), holograms.data.end(), in.begin());
-  process();
-  OdtResult r;
+void Pipeline::run(std::span<const float> holograms, std::span<float> index) {
   const auto [nz, ny, nx] = impl_->shape;
-  r.ri = Array3<float>(nz, ny, nx);
-  const auto out = output();
-  std::copy(out.begin(), out.end(), r.ri.data.begin());
-  r.filled = filled();
+  host::require(holograms.size() == impl_->input_size, "Pipeline::run: shape must be (count, N, N)");
+  host::require(index.size() == static_cast<std::size_t>(nz) * ny * nx, "Pipeline::run: output must be (nz, n, n)");
+  if (!impl_->has_background) throw std::logic_error("Pipeline: set_background() first");
+  host::check(qhk_pipeline_run(impl_->handle, holograms.data(), index.data()));
+  qhk_pipeline_timings t{};
+  host::check(qhk_pipeline_result(impl_->handle, &impl_->filled, &t));
+  impl_->timings = PipelineTimings{t.upload, t.fields, t.rytov,  t.fft2,     t.clear, t.mapping,
+                                   t.normalize, t.solve, t.finish, t.download, t.total};
+}
+
+OdtResult Pipeline::run(const Array3<float>& holograms) {
+  host::require(holograms.ny == holograms.nx, "Pipeline::run: shape must be (count, N, N)");
+  const auto [nz, ny, nx] = impl_->shape;
+  OdtResult r{Array3<float>(nz, ny, nx), 0.0};
+  run(std::span<const float>(holograms.data), std::span<float>(r.ri.data));
+  r.filled = impl_->filled;
   return r;
 }
 

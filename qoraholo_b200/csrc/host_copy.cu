@@ -1,0 +1,121 @@
+// HostCopier: persistent threads for large host copies and page pre-faulting.
+#include <unistd.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+
+#include "host_copy.hpp"
+
+namespace qhk {
+
+HostCopier::HostCopier(int threads) {
+  for (int i = 1; i < std::max(threads, 1); ++i) workers_.emplace_back([this] { worker(); });
+}
+
+HostCopier::~HostCopier() {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    stop_ = true;
+  }
+  wake_.notify_all();
+  for (auto& t : workers_) t.join();
+}
+
+HostCopier& HostCopier::shared() {
+  static HostCopier copier([] {
+    const char* e = std::getenv("QHK_COPY_THREADS");
+    if (e && std::atoi(e) > 0) return std::atoi(e);
+    return static_cast<int>(std::min(8u, std::max(1u, std::thread::hardware_concurrency())));
+  }());
+  return copier;
+}
+
+void HostCopier::drain(Job& job) {
+  for (;;) {
+    std::size_t i;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (job.next >= job.parts) return;
+      i = job.next++;
+    }
+    (*job.fn)(i);
+    std::lock_guard<std::mutex> lk(mu_);
+    if (++job.done == job.parts) finished_.notify_all();
+  }
+}
+
+void HostCopier::worker() {
+  std::uint64_t seen = 0;
+  for (;;) {
+    Job* job;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      wake_.wait(lk, [&] { return stop_ || (job_ != nullptr && generation_ != seen); });
+      if (stop_) return;
+      seen = generation_;
+      job = job_;
+      ++job->active;
+    }
+    drain(*job);
+    std::lock_guard<std::mutex> lk(mu_);
+    if (--job->active == 0) finished_.notify_all();
+  }
+}
+
+void HostCopier::run(std::size_t parts, const std::function<void(std::size_t)>& fn) {
+  if (parts == 0) return;
+  if (parts == 1 || workers_.empty()) {
+    for (std::size_t i = 0; i < parts; ++i) fn(i);
+    return;
+  }
+  std::lock_guard<std::mutex> one(job_mu_);
+  Job job;
+  job.fn = &fn;
+  job.parts = parts;
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    job_ = &job;
+    ++generation_;
+  }
+  wake_.notify_all();
+  drain(job);
+  std::unique_lock<std::mutex> lk(mu_);
+  job_ = nullptr;  // workers that have not joined yet no longer can; `job` lives until those inside leave
+  finished_.wait(lk, [&] { return job.done == job.parts && job.active == 0; });
+}
+
+void HostCopier::copy(void* dst, const void* src, std::size_t bytes) {
+  if (bytes == 0 || dst == src) return;
+  const std::size_t parts = (bytes + kPart - 1) / kPart;
+  const std::function<void(std::size_t)> fn = [&](std::size_t i) {
+    const std::size_t off = i * kPart;
+    std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, std::min(kPart, bytes - off));
+  };
+  run(parts, fn);
+}
+
+void HostCopier::touch(void* dst, std::size_t bytes) {
+  if (bytes == 0) return;
+  static const std::size_t page = [] {
+    const long p = sysconf(_SC_PAGESIZE);
+    return p > 0 ? static_cast<std::size_t>(p) : std::size_t{4096};
+  }();
+  const std::size_t parts = (bytes + kPart - 1) / kPart;
+  char* base = static_cast<char*>(dst);
+  const std::function<void(std::size_t)> fn = [&](std::size_t i) {
+    const std::size_t begin = i * kPart, end = std::min(begin + kPart, bytes);
+    // the first byte of the part, then every page boundary inside it
+    const auto addr = reinterpret_cast<std::uintptr_t>(base + begin);
+    std::size_t off = begin;
+    for (;;) {
+      *reinterpret_cast<volatile char*>(base + off) = 0;
+      const std::size_t next = ((addr - begin + off) / page + 1) * page - (addr - begin);
+      if (next >= end) break;
+      off = next;
+    }
+  };
+  run(parts, fn);
+}
+
+}  // namespace qhk

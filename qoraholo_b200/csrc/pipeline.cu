@@ -5,10 +5,14 @@
 // the field passes of each part start as soon as its copy has landed (event wait), so the copy
 // overlaps field extraction. The last field pass forms the ratio to the resident background
 // fields and its phase / log-amplitude directly; then the unwrap passes, the Rytov assembly,
-// the ODT plan, and one device -> host copy of the volume into page-locked memory. Stage times
-// are event intervals on the compute stream, read after it finishes.
+// the ODT plan, and the device -> host copy of the volume into page-locked memory in parts.
+// process_host() does the same from and into caller memory: the host copy threads fill each
+// upload chunk's staging just before its transfer, and copy each downloaded part out as it lands.
+// Stage times are event intervals on the compute stream, read after it finishes (the upload time
+// then includes the host staging of the chunks).
 #include <chrono>
 
+#include "host_copy.hpp"
 #include "pipeline.hpp"
 
 namespace qhk {
@@ -51,6 +55,7 @@ PipelinePlan::PipelinePlan(const CropPlan& crop, int count, int upload_chunks, c
   phi_.reset(b * field);
   index_.reset(b * odt_.volume());
   for (int k = 0; k < chunks_; ++k) chunk_done_.emplace_back();
+  for (int k = 0; k < kOutParts; ++k) part_done_.emplace_back();
 }
 
 std::size_t PipelinePlan::device_bytes() const {
@@ -80,7 +85,7 @@ void PipelinePlan::enqueue(const float* d_holo, const float2* bg, float* d_index
 }
 
 void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float2* bg, float* d_index, cudaStream_t s,
-                           bool marks) {
+                           bool marks, const float* host_src) {
   const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
   if (marks) clock_.mark(kStart, s);
   const int images = count_ * batch_;
@@ -91,6 +96,9 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
       const int first = k * chunk_;
       const int valid = std::min(chunk_, images - first);
       float* dst = holo_.get() + first * image;
+      if (host_src) {
+        HostCopier::shared().copy(input_.get() + first * image, host_src + first * image, valid * image * sizeof(float));
+      }
       check(cudaMemcpyAsync(dst, input_.get() + first * image, valid * image * sizeof(float), cudaMemcpyHostToDevice, c),
             "upload holograms");
       chunk_done_[k].record(c);
@@ -111,18 +119,39 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
   }
 }
 
-void PipelinePlan::process() {
+void PipelinePlan::process() { process_host(nullptr, nullptr); }
+
+void PipelinePlan::process_host(const float* holograms, float* index) {
   if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
   const auto t0 = std::chrono::steady_clock::now();
   const cudaStream_t s = compute_.get();
-  compute(nullptr, true, background_.get(), index_.get(), s, true);
-  check(cudaMemcpyAsync(output_.get(), index_.get(), batch_ * odt_.volume() * sizeof(float), cudaMemcpyDeviceToHost,
-                        s),
-        "download index");
+  compute(nullptr, true, background_.get(), index_.get(), s, true, holograms == input_.get() ? nullptr : holograms);
+  const std::size_t total = static_cast<std::size_t>(batch_) * odt_.volume();
+  const std::size_t part = (total + kOutParts - 1) / kOutParts;
+  const auto part_len = [&](int j) {
+    const std::size_t off = j * part;
+    return off < total ? std::min(part, total - off) : std::size_t{0};
+  };
+  for (int j = 0; j < kOutParts; ++j) {
+    if (part_len(j) > 0) {
+      check(cudaMemcpyAsync(output_.get() + j * part, index_.get() + j * part, part_len(j) * sizeof(float),
+                            cudaMemcpyDeviceToHost, s),
+            "download index");
+    }
+    part_done_[j].record(s);
+  }
   check(cudaMemcpyAsync(filled_host_.get(), odt_.filled(), batch_ * sizeof(unsigned long long),
                         cudaMemcpyDeviceToHost, s),
         "download filled");
   clock_.mark(kDownloaded, s);
+  if (index != nullptr && index != output_.get()) {
+    HostCopier& copier = HostCopier::shared();
+    copier.touch(index, total * sizeof(float));  // while the device works
+    for (int j = 0; j < kOutParts; ++j) {
+      part_done_[j].synchronize();
+      copier.copy(index + j * part, output_.get() + j * part, part_len(j) * sizeof(float));
+    }
+  }
   check(cudaStreamSynchronize(s), "process");
   filled_ = static_cast<double>(*filled_host_.get()) / static_cast<double>(odt_.volume());
   const int o = kRytov + 1;

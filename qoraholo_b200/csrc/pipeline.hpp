@@ -29,6 +29,14 @@ class PipelinePlan {
   [[nodiscard]] const float* output() const { return output_.get(); }
   // input() -> output(), synchronous, with stage timings.
   void process();
+  // Caller memory (pageable or page-locked) holograms (batch * count, N, N) -> caller memory
+  // volume(s) (batch, nz, n, n), synchronous, with stage timings. Each upload chunk is copied into
+  // the page-locked input by the host copy threads just before its transfer is queued, so the copy
+  // of chunk k overlaps the transfer and field passes of the chunks before it; the pages of
+  // `index` are faulted in while the solver runs, and the volume comes back in kOutParts parts,
+  // each copied out as soon as it has landed while the next part is in flight. Either pointer may
+  // be null: the input is then taken from input(), the volume left in output().
+  void process_host(const float* holograms, float* index);
   // Holograms already on the device -> index on the device, asynchronous on `s` (no host copies).
   void process_device(const float* d_holo, float* d_index, cudaStream_t s);
   // The same replayed as one CUDA graph (captured on the second call for these buffers; the first
@@ -64,8 +72,11 @@ class PipelinePlan {
 
  private:
   enum { kStart, kFields, kRytov, kDownloaded = kRytov + 1 + OdtPlan::kMarks, kMarks };
+  static constexpr int kOutParts = 8;
+  // chunked_upload: the holograms come from input_ in chunks on the copy stream, each first
+  // copied there from `host_src` when that is given.
   void compute(const float* d_holo, bool chunked_upload, const float2* bg, float* d_index, cudaStream_t s,
-               bool marks);
+               bool marks, const float* host_src = nullptr);
 
   CropPlan crop_;
   int count_;
@@ -88,6 +99,7 @@ class PipelinePlan {
   DevBuf<float> phi_;
   DevBuf<float> index_;
   std::vector<Event> chunk_done_;
+  std::vector<Event> part_done_;
   StageClock clock_;
   CapturedWork graph_;
   bool graph_warm_ = false;

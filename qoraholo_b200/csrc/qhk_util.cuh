@@ -136,6 +136,7 @@ class Event {
   Event(Event&& o) noexcept : e_(std::exchange(o.e_, nullptr)) {}
   [[nodiscard]] cudaEvent_t get() const { return e_; }
   void record(cudaStream_t s) { check(cudaEventRecord(e_, s), "cudaEventRecord"); }
+  void synchronize() const { check(cudaEventSynchronize(e_), "cudaEventSynchronize"); }
   [[nodiscard]] float since(const Event& start) const { return since_event(start.get()); }
   [[nodiscard]] float since_event(cudaEvent_t start) const {
     float ms = 0;
