@@ -216,10 +216,10 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
+def profiled_traffic(summary):
     """DRAM bytes per FGP launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture),
-    from the committed summary, or None."""
-    p = ROOT / "profiles" / "k_fgp_256cubed.md"
+    from the committed summary of that kernel, or None."""
+    p = ROOT / "profiles" / summary
     if p.exists():
         m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
         if m:
@@ -227,38 +227,56 @@ def profiled_traffic():
     return None
 
 
+def fgp_form(capi, n):
+    """The FGP form the autotuner chose for an n^3 volume: (two_step, rows per CTA)."""
+    for line in capi.autotune_report().splitlines():
+        m = re.match(rf"fgp_rows device \d+ shape {n} {n} {n} 4 0 0 -> (\d+)", line.strip())
+        if m:
+            choice = int(m.group(1))
+            return choice // 16 == 2, choice % 16
+    return False, 0
+
+
 def fgp_roofline(torch, capi, stream):
-    """Average duration of one FGP step at 256^3 (CUDA events, kernel timed alone) and its
-    algorithmic bytes: per step b, r (3), p (3) read and p (3), r (3) written (13 volumes); the first
-    step reads p as r and the last writes no r (10 volumes each)."""
+    """Average duration of one launch of the FGP kernel the TV proximal step runs at 256^3 (CUDA
+    events, kernel timed alone, on a 12-volume workspace so that the tuned form can run) and its
+    algorithmic bytes: a launch reads b, r (3), p (3) and writes p (3), r (3) (13 volumes); the first
+    reads p as r and the last writes no r (10 volumes each). The one-step form (k_fgp) does one FGP
+    step per launch, the two-step form (k_fgp2) two, so a prox of TV_INNER steps takes TV_INNER or
+    TV_INNER / 2 launches."""
     n = FIELD_N
     vol = n * n * n
     b = torch.rand((n, n, n), device="cuda")
     x = torch.empty_like(b)
-    dual = torch.zeros((9, n, n, n), device="cuda")
+    work = torch.zeros((12, n, n, n), device="cuda")
     lam = TV_WEIGHT * (2 * math.pi / WAVELENGTH) ** 2
 
     def timed(inner, reps=5):
-        capi.tv_prox_device(b.data_ptr(), x.data_ptr(), dual.data_ptr(), n, n, n, lam, inner, stream)
+        capi.tv_prox_workspace(b.data_ptr(), x.data_ptr(), work.data_ptr(), 12, n, n, n, lam, inner, stream)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
         for _ in range(reps):
-            capi.tv_prox_device(b.data_ptr(), x.data_ptr(), dual.data_ptr(), n, n, n, lam, inner, stream)
+            capi.tv_prox_workspace(b.data_ptr(), x.data_ptr(), work.data_ptr(), 12, n, n, n, lam, inner, stream)
         e.record()
         torch.cuda.synchronize()
         return s.elapsed_time(e) / reps
 
     t10, t0 = timed(TV_INNER), timed(0)
-    t_step = (t10 - t0) / TV_INNER
-    volumes = (10 + 13 * (TV_INNER - 2) + 10) / TV_INNER
+    two_step, rows = fgp_form(capi, n)
+    launches = TV_INNER // 2 if two_step else TV_INNER
+    t_launch = (t10 - t0) / launches
+    volumes = (10 + 13 * (launches - 2) + 10) / launches
     alg = volumes * vol * 4
     peak, which = measured_peaks()
-    achieved = alg / (t_step * 1e-3) / 1e9
-    del b, x, dual
-    return {"kernel": "k_fgp (one FGP step of the TV proximal operator, 256^3)", "bound": "hbm",
-            "achieved": round(achieved, 1), "peak": peak, "peak_source": f"{which} hbm_gbs (burst copy)",
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": profiled_traffic(),
-            "algorithmic_bytes_per_launch": alg, "avg_launch_ms": round(t_step, 5)}
+    achieved = alg / (t_launch * 1e-3) / 1e9
+    del b, x, work
+    kernel = (f"k_fgp2 (two FGP steps per launch, {rows} rows per CTA, 256^3)" if two_step else
+              "k_fgp (one FGP step of the TV proximal operator, 256^3)")
+    return {"kernel": kernel, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "peak_source": f"{which} hbm_gbs (burst copy)", "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": profiled_traffic("k_fgp2_256cubed.md" if two_step else "k_fgp_256cubed.md"),
+            "algorithmic_bytes_per_launch": alg, "avg_launch_ms": round(t_launch, 5),
+            "fgp_steps_per_launch": 2 if two_step else 1, "ms_per_fgp_step": round((t10 - t0) / TV_INNER, 5)}
 
 
 def reference_sample(holo, bg, illum, iterations):
@@ -773,9 +791,10 @@ def c4_leg(qh, capi, torch, reps=5):
     return out
 
 
-def kernel_case(name, reps):
+def kernel_case(name, reps, tv_form=0):
     """Small standalone launches of one kernel family for profiling (no JSON line): `fgp` runs the
-    TV proximal step at 256^3 (10 FGP steps + final primal per rep); `fft` a 256^3 rfft3 + irfft3
+    TV proximal step at 256^3 on a 12-volume workspace (10 FGP steps in the tuned form + final primal
+    per rep); `fft` a 256^3 rfft3 + irfft3
     per rep; `kspace` a 256^3 GP-4 solve from 49 random 256^2 fields per rep (the k-space step's
     row and axis passes); `pipeline` the full device pipeline on 9 x 128^2 holograms -> 64^3."""
     import torch
@@ -783,6 +802,7 @@ def kernel_case(name, reps):
     from qoraholo_b200 import capi
 
     stream = torch.cuda.current_stream().cuda_stream
+    capi.tv_form(tv_form)
     if name == "fft":
         n = FIELD_N
         x = torch.rand((n, n, n), device="cuda")
@@ -805,10 +825,10 @@ def kernel_case(name, reps):
         n = FIELD_N
         b = torch.rand((n, n, n), device="cuda")
         x = torch.empty_like(b)
-        dual = torch.zeros((9, n, n, n), device="cuda")
+        work = torch.zeros((12, n, n, n), device="cuda")
         lam = TV_WEIGHT * (2 * math.pi / WAVELENGTH) ** 2
         for _ in range(reps):
-            capi.tv_prox_device(b.data_ptr(), x.data_ptr(), dual.data_ptr(), n, n, n, lam, TV_INNER, stream)
+            capi.tv_prox_workspace(b.data_ptr(), x.data_ptr(), work.data_ptr(), 12, n, n, n, lam, TV_INNER, stream)
     else:
         import qoraholo_b200 as qh
 
@@ -836,6 +856,8 @@ def main():
     ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "serve", "bpm", "c4"], default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--tv-form", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="with --kernel-case: FGP form (0 tuned/default, 1 stored r, 2 recomputed r, 3 two steps)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
@@ -872,7 +894,7 @@ def main():
         print(json.dumps(bpm_leg(qh, torch)))
         return 0
     if args.kernel_case:
-        return kernel_case(args.kernel_case, args.reps)
+        return kernel_case(args.kernel_case, args.reps, args.tv_form)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)

@@ -106,9 +106,17 @@ int qhk_tv_prox(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int
                 void* stream);
 
 /* The same proximal step with no allocation: d_dual holds 9 volumes -- the dual p (3 volumes, warm
- * start, updated in place) followed by 6 volumes of scratch. Asynchronous on `stream`. */
+ * start, updated in place) followed by 6 volumes of scratch. Asynchronous on `stream`. With 9
+ * volumes it runs the one-step FGP forms (qhk_tv_prox, with 9 volumes of its own scratch, can run
+ * two steps per pass). */
 int qhk_tv_prox_device(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int nx, float lambda, int inner,
                        void* stream);
+
+/* The same with a caller workspace of `work_volumes` volumes: the dual p (3 volumes, warm start,
+ * updated in place) followed by 6 (work_volumes 9: the one-step FGP forms) or 9 volumes of scratch
+ * (work_volumes 12: also the two-step form). No allocation; asynchronous on `stream`. */
+int qhk_tv_prox_workspace(const float* d_b, float* d_x, float* d_work, int work_volumes, int nz, int ny, int nx,
+                          float lambda, int inner, void* stream);
 
 /* Number of kernels this library has launched since it was loaded (for launch accounting). */
 uint64_t qhk_kernel_launches(void);
@@ -164,7 +172,8 @@ int qhk_unwrap_noalloc(const float* d_wrapped, float* d_unwrapped, int count, in
 int qhk_autotune_enable(int enabled);
 /* FGP step form of tv_prox (bitwise the same results): 0 the tuned one, 1 the extrapolated point
  * stored between steps (13 volumes of traffic per step), 2 recomputed from the two previous duals
- * (10 volumes). */
+ * (10 volumes), 3 two steps per pass (13 volumes per two steps; needs rows of a multiple of 4
+ * floats and a fourth dual triplet, so qhk_tv_prox_device runs form 1 instead). */
 int qhk_tv_form(int form);
 /* The tuned choices, one line each, into `buf` (NUL-terminated, truncated to `size`); returns the
  * full length. */

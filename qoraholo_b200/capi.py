@@ -85,6 +85,7 @@ _PROTOS = {
     "qhk_irfft3": (_I, [_VP, _VP, _I, _I, _I, _F, _VP]),
     "qhk_tv_prox_device": (_I, [_VP, _VP, _VP, _I, _I, _I, _F, _I, _VP]),
     "qhk_kernel_launches": (C.c_uint64, []),
+    "qhk_tv_prox_workspace": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _F, _I, _VP]),
     "qhk_unwrap_noalloc": (_I, [_VP, _VP, _I, _I, _I, _VP]),
     "qhk_bpm_vjp": (_I, [_VP, _I, _I, _VP, _VP, _I, C.POINTER(Geometry), _I, _VP]),
     "qhk_pipeline_create": (_I, [C.POINTER(_VP), _VP, _VP, C.POINTER(Geometry)]),
@@ -233,6 +234,13 @@ def tv_prox(d_b, d_x, d_dual, nz, ny, nx, lam, inner, stream=0):
 def tv_prox_device(d_b, d_x, d_dual9, nz, ny, nx, lam, inner, stream=0):
     """No-allocation proximal step: d_dual9 holds the dual (3 volumes) and 6 volumes of scratch."""
     check(lib().qhk_tv_prox_device(_VP(d_b), _VP(d_x), _VP(d_dual9), nz, ny, nx, float(lam), int(inner), _VP(stream)))
+
+
+def tv_prox_workspace(d_b, d_x, d_work, work_volumes, nz, ny, nx, lam, inner, stream=0):
+    """No-allocation proximal step on a caller workspace of 9 or 12 volumes (the dual first); with 12
+    the two-step FGP form can run."""
+    check(lib().qhk_tv_prox_workspace(_VP(d_b), _VP(d_x), _VP(d_work), int(work_volumes), nz, ny, nx, float(lam),
+                                      int(inner), _VP(stream)))
 
 
 def unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, stream=0):

@@ -512,11 +512,11 @@ void bpm_solve(const BpmTablesHost& t, const float2* d_fields, float* d_x, int i
   float* next = y + size;
   float* grad = y + 2 * size;
   float* z = y + 3 * size;
-  DevBuf<float> dual(tv ? 9 * size : 0);
+  DevBuf<float> dual(tv ? 12 * size : 0);
   TvBuffers tvb;
   if (tv) {
     check(cudaMemsetAsync(dual.get(), 0, 3 * size * sizeof(float), s), "cudaMemset");
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 4; ++i)
       for (int c = 0; c < 3; ++c) tvb.v[i][c] = dual.get() + (3 * i + c) * size;
   }
   check(cudaMemcpyAsync(y, d_x, size * sizeof(float), cudaMemcpyDeviceToDevice, s), "copy x");

@@ -192,12 +192,11 @@ int qhk_tv_prox(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int
     qhk::require(nz >= 1 && ny >= 1 && nx >= 1 && lambda > 0 && inner >= 0, "tv_prox: invalid arguments");
     const std::size_t v = static_cast<std::size_t>(nz) * ny * nx;
     const cudaStream_t s = as_stream(stream);
-    qhk::DevBuf<float> scratch(6 * v);
+    qhk::DevBuf<float> scratch(9 * v);
     qhk::TvBuffers t;
     for (int c = 0; c < 3; ++c) {
       t.v[0][c] = d_dual + c * v;
-      t.v[1][c] = scratch.get() + c * v;
-      t.v[2][c] = scratch.get() + (3 + c) * v;
+      for (int i = 1; i < 4; ++i) t.v[i][c] = scratch.get() + (3 * (i - 1) + c) * v;
     }
     t.p_index = 0;
     qhk::tv_prox(d_b, t, nz, ny, nx, lambda, inner, qhk::TvFinal::plain, 0.0f, nullptr, d_x, 0, 0, s);
@@ -225,6 +224,28 @@ int qhk_tv_prox_device(const float* d_b, float* d_x, float* d_dual, int nz, int 
     if (t.p_index != 0) {
       qhk::check(cudaMemcpyAsync(d_dual, t.v[t.p_index][0], 3 * v * sizeof(float), cudaMemcpyDeviceToDevice, s),
                  "copy dual");
+    }
+  });
+}
+
+int qhk_tv_prox_workspace(const float* d_b, float* d_x, float* d_work, int work_volumes, int nz, int ny, int nx,
+                          float lambda, int inner, void* stream) {
+  return guard([&] {
+    qhk::require(d_b && d_x && d_work, "tv_prox: null argument");
+    qhk::require(work_volumes == 9 || work_volumes == 12, "tv_prox: work_volumes must be 9 or 12");
+    qhk::require(nz >= 1 && ny >= 1 && nx >= 1 && lambda > 0 && inner >= 0, "tv_prox: invalid arguments");
+    const std::size_t v = static_cast<std::size_t>(nz) * ny * nx;
+    const cudaStream_t s = as_stream(stream);
+    qhk::TvBuffers t;
+    for (int i = 0; i < work_volumes / 3; ++i)
+      for (int c = 0; c < 3; ++c) t.v[i][c] = d_work + (3 * i + c) * v;
+    t.p_index = 0;
+    qhk::tv_prox(d_b, t, nz, ny, nx, lambda, inner, qhk::TvFinal::plain, 0.0f, nullptr, d_x, 0, 0, s);
+    if (t.p_index != 0) {
+      for (int c = 0; c < 3; ++c) {
+        qhk::check(cudaMemcpyAsync(d_work + c * v, t.v[t.p_index][c], v * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                   "copy dual");
+      }
     }
   });
 }

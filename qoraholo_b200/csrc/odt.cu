@@ -243,8 +243,8 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
     x_.reset(b * vol_);
     if (cfg_.tv) {
       xprev_.reset(vol_);
-      dual_.reset(9 * vol_);
-      for (int i = 0; i < 3; ++i)
+      dual_.reset(12 * vol_);
+      for (int i = 0; i < 4; ++i)
         for (int c = 0; c < 3; ++c) tv_.v[i][c] = dual_.get() + (3 * i + c) * vol_;
     }
   } else {

@@ -68,9 +68,13 @@ void fft2d(float2* data, int count, int n, bool forward, float scale, cudaStream
 // step reads the previous dual r from one triplet and writes the next r to another, and the
 // first step of a call moves p to a free triplet (neighbouring CTAs still read the old p as r),
 // so the three rotate and p_index is updated by tv_prox.
+// Dual triplets (three volumes each) of the FGP iteration: p lives in v[p_index]. The fourth
+// triplet is optional; with it the two-step form (k_fgp2) can run, which reads the duals of the
+// neighbouring tiles' rows and so cannot update p or r in place.
 struct TvBuffers {
-  float* v[3][3] = {};
+  float* v[4][3] = {};
   int p_index = 0;
+  [[nodiscard]] bool has_fourth() const { return v[3][0] != nullptr; }
 };
 enum class TvFinal : int {
   plain,     // out = argmin

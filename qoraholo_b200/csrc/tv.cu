@@ -572,6 +572,383 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Two FGP steps (k and k + 1) in one pass over the volume, so that a pair of steps moves the HBM
+// traffic of one: b, r_k (3) and p_k (3) read, p_{k+2} (3) and r_{k+2} (3) written -- 13 volumes
+// for two steps (the first pair reads p_0 as r_0: 10; the last writes no r: 10). The march and the
+// split of the (y-tile, z) units over one wave of CTAs are those of k_fgp; the rows of step k are
+// widened by the halo that step k + 1 needs and recomputed by both neighbouring tiles:
+//   z_k        rows y0-1 .. y0+TY+1   from r_k rows y0-2 .. y0+TY+1 and b
+//   r_{k+1}    rows y0-1 .. y0+TY     (dual step k; p_{k+1} only on the tile's own rows)
+//   z_{k+1}    rows y0   .. y0+TY
+//   p, r_{k+2} rows y0   .. y0+TY-1   (dual step k + 1, to HBM)
+// In z the march runs three planes ahead of its output. Iteration q computes z_k of plane q+2,
+// dual step k of plane q+1, z_{k+1} of plane q+1 and dual step k+1 of plane q, while r_k and b of
+// plane q+3 stream in (cp.async). Shared memory: r_k ring (3 planes x 3 components x TY+4 rows),
+// b ring (3 x TY+3), z_k (2 x TY+3), r_{k+1} (z component of 2 planes, y and x of one, TY+2 rows
+// each), z_{k+1} (2 x TY+1): 20 TY + 61 rows of nx floats. The own rows of every phase belong to
+// one thread row each (four x values per thread), and the halo rows of z_k and of dual step k are
+// spread over all threads with the same point -> thread map in both phases, so the step-k dual
+// reads only z_k values that its own thread wrote in this iteration or that a barrier separates
+// from their writer: two barriers per plane. p_{k+1} and r_{k+1} of the thread's own points stay
+// in registers from dual step k to dual step k + 1. The per-point operations are those of k_fgp in
+// the same order, so the iterates are bit-identical.
+struct Fgp2Args {
+  const float* b;
+  const float* rin[3];  // r_k; on the first step p_0
+  const float* pin[3];  // p_k (not read on the first step)
+  float* pout[3];       // p_{k+2}
+  float* rout[3];       // r_{k+2} (not written when step k + 1 is the last)
+  int nz, ny, nx;
+  int ytiles;
+  float lambda, step;
+  float m1, m2;  // momenta of steps k and k + 1
+};
+
+// The primal point max(b - lambda L(r), 0) of one voxel from its six dual neighbours, the sum in the
+// host's order (src/common.hpp:107-153).
+__device__ __forceinline__ float fgp_primal_at(int z, int y, int x, int nz, int ny, int nx, float vz, float vzb,
+                                               float vy, float vym, float vx, float vxm, float vb, float lambda) {
+  float sacc = 0.0f;
+  if (z < nz - 1) sacc = __fadd_rn(sacc, vz);
+  if (z > 0) sacc = __fsub_rn(sacc, vzb);
+  if (y < ny - 1) sacc = __fadd_rn(sacc, vy);
+  if (y > 0) sacc = __fsub_rn(sacc, vym);
+  if (x < nx - 1) sacc = __fadd_rn(sacc, vx);
+  if (x > 0) sacc = __fsub_rn(sacc, vxm);
+  return tv_primal(vb, lambda, sacc);
+}
+
+// One dual step at a voxel from its primal value c and its +z, +y and +x neighbours.
+__device__ __forceinline__ void fgp_dual_at(float c, float cz, float cy, float cx, int z, int y, int x, int nz, int ny,
+                                            int nx, float step, float momentum, float p[3], float r[3]) {
+  float g[3];
+  g[0] = z < nz - 1 ? __fsub_rn(c, cz) : 0.0f;
+  g[1] = y < ny - 1 ? __fsub_rn(c, cy) : 0.0f;
+  g[2] = x < nx - 1 ? __fsub_rn(c, cx) : 0.0f;
+  tv_dual_step(g, step, momentum, p, r);
+}
+
+constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(ty) + 61; }
+// Threads per CTA the two-step kernel is compiled for (nx / 4 x TY must stay within it).
+constexpr int fgp2_threads(int ty) { return ty == 8 ? 512 : 256; }
+
+template <int TY, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
+  extern __shared__ __align__(16) float sm[];
+  constexpr int VEC = 4;
+  constexpr int RK_ROWS = TY + 4, B_ROWS = TY + 3, R1_ROWS = TY + 2, Z1_ROWS = TY + 1;
+  constexpr int HALO = (8 + TY - 1) / TY;     // halo points of dual step k per thread: 2 nx over nx / 4 * TY threads
+  constexpr int HALO_Z = (12 + TY - 1) / TY;  // halo points of z_k per thread: 3 nx
+  constexpr int HALO_Z1 = (4 + TY - 1) / TY;  // halo points of z_{k+1} per thread: nx
+  constexpr int COPY_R = (3 * RK_ROWS + TY - 1) / TY;  // r_k rows a thread row copies per plane
+  constexpr int COPY_B = (B_ROWS + TY - 1) / TY;
+  const int nx = A.nx, ny = A.ny, nz = A.nz;
+  const int tx = static_cast<int>(threadIdx.x);
+  const int ty = static_cast<int>(threadIdx.y);
+  const int x0 = tx * VEC;
+  const int nthreads = static_cast<int>(blockDim.x) * TY;
+  const int linear = ty * static_cast<int>(blockDim.x) + tx;
+  const int lane = linear & 31;
+  const int warp_threads = min(32, nthreads - (linear & ~31));
+  const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
+  const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
+  // Shared memory in floats: slot strides and buffer bases (32-bit offsets from sm).
+  const int RKP = RK_ROWS * nx, BP = B_ROWS * nx, R1P = R1_ROWS * nx, Z1P = Z1_ROWS * nx;
+  const int OB = 9 * RKP, OZ = OB + 3 * BP, OR = OZ + 2 * BP, OZ1 = OR + 4 * R1P;
+  // Own-row offsets within a slot: r_k row ty+2 (rows start at y0-2); b, z_k, r_{k+1} row ty+1
+  // (rows start at y0-1); z_{k+1} row ty (rows start at y0).
+  const int own_rk = (ty + 2) * nx + x0;
+  const int own_b = (ty + 1) * nx + x0;
+  const int own_z1 = ty * nx + x0;
+  // Halo points (the same point -> thread map in the z_k and dual-k phases): v = linear + j
+  // nthreads over the rows y0-1 (side 0), y0+TY (1), y0+TY+1 (2); row of z_k / b: 0, TY+1, TY+2.
+  int hz_side[HALO_Z], hz_x[HALO_Z];
+#pragma unroll
+  for (int j = 0; j < HALO_Z; ++j) {
+    const int v = linear + j * nthreads;
+    hz_side[j] = v < 3 * nx ? v / nx : -1;
+    hz_x[j] = v - max(hz_side[j], 0) * nx;
+  }
+
+  const long long units = static_cast<long long>(A.ytiles) * nz;
+  const long long u_end = units * (blockIdx.x + 1) / gridDim.x;
+  for (long long u = units * blockIdx.x / gridDim.x; u < u_end;) {
+    const int y0 = static_cast<int>(u / nz) * TY;
+    const int z0 = static_cast<int>(u % nz);
+    const int zend = static_cast<int>(min(static_cast<long long>(nz), z0 + (u_end - u)));
+    u += zend - z0;
+    const int zmax = min(zend + 1, nz - 1);  // last plane of r_k and b read
+    const int y = y0 + ty;
+    const bool own = y < ny;
+    const std::size_t own_g = static_cast<std::size_t>(y) * nx + x0;  // within a plane
+
+    // Copies of one plane into ring slot s: r_k rows y0-2 .. y0+TY+1 (row y0-2 of the y component
+    // only), b rows y0-1 .. y0+TY+1; rows outside the volume are never read and not copied.
+    const auto issue_rk = [&](int z, int s, int comps) {
+      const std::size_t po = z * nxy;
+#pragma unroll
+      for (int j = 0; j < COPY_R; ++j) {
+        const int rc = ty + j * TY;
+        const int c = rc / RK_ROWS;
+        const int i = rc - c * RK_ROWS;
+        const int yy = y0 - 2 + i;
+        if (rc < comps * RK_ROWS && yy >= 0 && yy < ny && (i != 0 || c == 1)) {
+          copy_async<VEC>(sm + (s * 3 + c) * RKP + i * nx + x0, A.rin[c] + po + static_cast<std::size_t>(yy) * nx + x0);
+        }
+      }
+    };
+    const auto issue_b = [&](int z, int s) {
+      const std::size_t po = z * nxy;
+#pragma unroll
+      for (int j = 0; j < COPY_B; ++j) {
+        const int i = ty + j * TY;
+        const int yy = y0 - 1 + i;
+        if (i < B_ROWS && yy >= 0 && yy < ny) {
+          copy_async<VEC>(sm + OB + s * BP + i * nx + x0, A.b + po + static_cast<std::size_t>(yy) * nx + x0);
+        }
+      }
+    };
+    const auto mod3 = [](int z) { return ((z % 3) + 3) % 3; };
+    // Iteration q needs r_k and b of planes up to q+2 (the z component of q+1 for z_k of q+2).
+    if (z0 >= 2) issue_rk(z0 - 2, mod3(z0 - 2), 1);
+    if (z0 >= 1) {
+      issue_rk(z0 - 1, mod3(z0 - 1), 3);
+      issue_b(z0 - 1, mod3(z0 - 1));
+    }
+    copy_commit();
+
+    float cr[3][VEC] = {}, cp[3][VEC] = {};  // r_{k+1}, p_{k+1} of this thread's points of plane q
+    float nr[3][VEC] = {}, np[3][VEC] = {};  // the same of plane q+1
+    int m0 = mod3(z0 - 3);                   // ring slot of plane q (and of q+3)
+    for (int q = z0 - 3; q < zend; ++q, m0 = m0 == 2 ? 0 : m0 + 1) {
+      const int a2 = q + 2, a1 = q + 1;
+      const int m1 = m0 == 2 ? 0 : m0 + 1;  // slot of q+1
+      const int m2 = m0 == 0 ? 2 : m0 - 1;  // slot of q+2
+      const int par = q & 1;                // parity of q (and q+2); q+1 has par ^ 1
+      const bool do_a = a2 >= 0 && a2 < nz;                  // z_k of plane a2
+      const bool do_b = a1 >= 0 && a1 >= z0 - 1 && a1 < nz;  // dual step k on plane a1
+      const bool do_c = a1 >= z0 && a1 < nz;                 // z_{k+1} of plane a1
+      const bool do_d = q >= z0;                             // dual step k+1 on plane q
+      // p_k of plane a1 (own points, then the halo points), loaded ahead of the wait.
+      float pk[3][VEC] = {};
+      float ph[HALO][3] = {};
+      if (!FIRST && do_b) {
+        const std::size_t po = a1 * nxy;
+        if (own) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) Vec<VEC>::load(A.pin[c] + po + own_g, pk[c]);
+        }
+#pragma unroll
+        for (int h = 0; h < HALO; ++h) {
+          const int side = hz_side[h];
+          const int yy = side == 0 ? y0 - 1 : y0 + TY;
+          if ((side == 0 || side == 1) && yy >= 0 && yy < ny) {
+            const std::size_t at = po + static_cast<std::size_t>(yy) * nx + hz_x[h];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ph[h][c] = A.pin[c][at];
+          }
+        }
+      }
+      copy_wait<0>();  // plane a2
+      __syncthreads();
+      if (q + 3 <= zmax) {
+        issue_rk(q + 3, m0, 3);
+        issue_b(q + 3, m0);
+      }
+      copy_commit();
+
+      if (do_a) {
+        const int a = a2;
+        const float* Rz = sm + (m2 * 3 + 0) * RKP;
+        const float* Rzb = sm + (m1 * 3 + 0) * RKP;  // plane a-1; not read on plane 0
+        const float* Ry = sm + (m2 * 3 + 1) * RKP;
+        const float* Rx = sm + (m2 * 3 + 2) * RKP;
+        const float* B = sm + OB + m2 * BP;
+        float* Z = sm + OZ + par * BP;
+        {
+          float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
+          Vec<VEC>::load(Rz + own_rk, vz);
+          Vec<VEC>::load(Rzb + own_rk, vzb);
+          Vec<VEC>::load(Ry + own_rk, vy);
+          Vec<VEC>::load(Ry + own_rk - nx, vym);
+          Vec<VEC>::load(Rx + own_rk, vx);
+          Vec<VEC>::load(B + own_b, vb);
+          const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
+          const float left = (x0 > 0 && lane == 0) ? Rx[own_rk - 1] : from_lane;
+          float out[VEC];
+#pragma unroll
+          for (int k = 0; k < VEC; ++k)
+            out[k] = own ? fgp_primal_at(a, y, x0 + k, nz, ny, nx, vz[k], vzb[k], vy[k], vym[k], vx[k],
+                                         k == 0 ? left : vx[k > 0 ? k - 1 : 0], vb[k], A.lambda)
+                         : 0.0f;
+          Vec<VEC>::store(Z + own_b, out);
+        }
+#pragma unroll
+        for (int j = 0; j < HALO_Z; ++j) {
+          const int side = hz_side[j];
+          const int x = hz_x[j];
+          const int zi = side == 0 ? 0 : TY + side;
+          const int yy = y0 - 1 + zi;
+          if (side >= 0 && yy >= 0 && yy < ny) {
+            const int i = (zi + 1) * nx + x;  // r_k row of yy
+            const float vxm = x > 0 ? Rx[i - 1] : 0.0f;
+            Z[zi * nx + x] = fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - nx], Rx[i], vxm,
+                                           B[zi * nx + x], A.lambda);
+          }
+        }
+      }
+
+      if (do_b) {
+        const int a = a1;
+        const float* Zc = sm + OZ + (par ^ 1) * BP;
+        const float* Zn = sm + OZ + par * BP;  // plane a+1; read only below plane nz-1
+        const float* R = sm + (m1 * 3) * RKP;
+        float* Rz1 = sm + OR + (par ^ 1) * R1P;
+        float* Ry1 = sm + OR + 2 * R1P;
+        float* Rx1 = sm + OR + 3 * R1P;
+        {
+          float zc[VEC], zy[VEC], zz[VEC];
+          Vec<VEC>::load(Zc + own_b, zc);
+          Vec<VEC>::load(Zc + own_b + nx, zy);
+          Vec<VEC>::load(Zn + own_b, zz);
+          const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
+          const float right =
+              (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? Zc[own_b + VEC] : from_lane;
+          float rv[3][VEC];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) Vec<VEC>::load(R + c * RKP + own_rk, rv[c]);
+          if (own) {
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) {
+              float p[3], r[3];
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                r[c] = rv[c][k];
+                p[c] = FIRST ? rv[c][k] : pk[c][k];
+              }
+              fgp_dual_at(zc[k], zz[k], zy[k], k == VEC - 1 ? right : zc[k < VEC - 1 ? k + 1 : 0], a, y, x0 + k, nz, ny,
+                          nx, A.step, A.m1, p, r);
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                np[c][k] = p[c];
+                nr[c][k] = r[c];
+              }
+            }
+            Vec<VEC>::store(Rz1 + own_b, nr[0]);
+            Vec<VEC>::store(Ry1 + own_b, nr[1]);
+            Vec<VEC>::store(Rx1 + own_b, nr[2]);
+          }
+        }
+        // halo rows y0-1 and y0+TY: the points this thread took in the z_k phase, so their z_k of
+        // plane a+1 is this thread's own write.
+#pragma unroll
+        for (int h = 0; h < HALO; ++h) {
+          const int side = hz_side[h];
+          const int x = hz_x[h];
+          const int zi = side == 0 ? 0 : TY + 1;
+          const int yy = y0 - 1 + zi;
+          if ((side == 0 || side == 1) && yy >= 0 && yy < ny) {
+            const int i = zi * nx + x;
+            const float c0 = Zc[i];
+            const float cz = a < nz - 1 ? Zn[i] : 0.0f;
+            const float cy = yy < ny - 1 ? Zc[i + nx] : 0.0f;
+            const float cx = x < nx - 1 ? Zc[i + 1] : 0.0f;
+            float p[3], r[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              r[c] = R[c * RKP + i + nx];
+              p[c] = FIRST ? r[c] : ph[h][c];
+            }
+            fgp_dual_at(c0, cz, cy, cx, a, yy, x, nz, ny, nx, A.step, A.m1, p, r);
+            Rz1[i] = r[0];
+            Ry1[i] = r[1];
+            Rx1[i] = r[2];
+          }
+        }
+      }
+      __syncthreads();  // r_{k+1} of plane a1 complete
+
+      float zn[VEC] = {};  // z_{k+1} of this thread's points of plane a1
+      if (do_c) {
+        const int a = a1;
+        const float* Rz = sm + OR + (par ^ 1) * R1P;
+        const float* Rzb = sm + OR + par * R1P;  // plane a-1; not read on plane 0
+        const float* Ry = sm + OR + 2 * R1P;
+        const float* Rx = sm + OR + 3 * R1P;
+        const float* B = sm + OB + m1 * BP;
+        float* Z = sm + OZ1 + (par ^ 1) * Z1P;
+        {
+          float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
+          Vec<VEC>::load(Rz + own_b, vz);
+          Vec<VEC>::load(Rzb + own_b, vzb);
+          Vec<VEC>::load(Ry + own_b, vy);
+          Vec<VEC>::load(Ry + own_b - nx, vym);
+          Vec<VEC>::load(Rx + own_b, vx);
+          Vec<VEC>::load(B + own_b, vb);
+          const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
+          const float left = (x0 > 0 && lane == 0) ? Rx[own_b - 1] : from_lane;
+#pragma unroll
+          for (int k = 0; k < VEC; ++k)
+            zn[k] = own ? fgp_primal_at(a, y, x0 + k, nz, ny, nx, vz[k], vzb[k], vy[k], vym[k], vx[k],
+                                        k == 0 ? left : vx[k > 0 ? k - 1 : 0], vb[k], A.lambda)
+                        : 0.0f;
+          Vec<VEC>::store(Z + own_z1, zn);
+        }
+        if (y0 + TY < ny) {  // row y0+TY, spread over all threads
+          const int yy = y0 + TY;
+#pragma unroll
+          for (int j = 0; j < HALO_Z1; ++j) {
+            const int x = linear + j * nthreads;
+            if (x < nx) {
+              const int i = (TY + 1) * nx + x;
+              const float vxm = x > 0 ? Rx[i - 1] : 0.0f;
+              Z[TY * nx + x] =
+                  fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - nx], Rx[i], vxm, B[i], A.lambda);
+            }
+          }
+        }
+      }
+
+      if (do_d) {  // own row: z_{k+1} of plane q row ty (row ty+1 below it), of plane q+1 in zn
+        const float* Zc = sm + OZ1 + par * Z1P;
+        float zc[VEC], zy[VEC];
+        Vec<VEC>::load(Zc + own_z1, zc);
+        Vec<VEC>::load(Zc + own_z1 + nx, zy);
+        const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
+        const float right = (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? Zc[own_z1 + VEC] : from_lane;
+        if (own) {
+#pragma unroll
+          for (int k = 0; k < VEC; ++k) {
+            float p[3] = {cp[0][k], cp[1][k], cp[2][k]};
+            float r[3] = {cr[0][k], cr[1][k], cr[2][k]};
+            fgp_dual_at(zc[k], zn[k], zy[k], k == VEC - 1 ? right : zc[k < VEC - 1 ? k + 1 : 0], q, y, x0 + k, nz, ny,
+                        nx, A.step, A.m2, p, r);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              cp[c][k] = p[c];
+              cr[c][k] = r[c];
+            }
+          }
+          const std::size_t at = q * nxy + own_g;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            Vec<VEC>::store(A.pout[c] + at, cp[c]);
+            if (!LAST) Vec<VEC>::store(A.rout[c] + at, cr[c]);
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          cr[c][k] = nr[c][k];
+          cp[c][k] = np[c][k];
+        }
+    }
+    __syncthreads();  // the next march's prologue reuses the rings
+  }
+}
+
 // Rows per CTA for an (nz, ny, nx) volume (TY rows of full x extent) and the grid: every CTA
 // resident at once (a partial second wave would double the time of the step), with an even share of
 // the plane units each.
@@ -579,8 +956,16 @@ struct FgpShape {
   int ty;
   int grid;
   std::size_t smem;
-  int variant = 0;  // 0: r stored (k_fgp), 1: r recomputed (k_fgp_p)
+  int variant = 0;  // 0: r stored (k_fgp), 1: r recomputed (k_fgp_p), 2: two steps per pass (k_fgp2)
 };
+
+// Shared memory of the two-step form, and the largest a CTA may take on this part.
+std::size_t fgp2_smem(int nx, int ty) { return fgp2_rows(ty) * static_cast<std::size_t>(nx) * sizeof(float); }
+constexpr std::size_t kSmemOptin = 227 * 1024;
+
+bool fgp2_fits(int nx, int ty) {
+  return nx % 4 == 0 && (nx / 4) * ty <= fgp2_threads(ty) && fgp2_smem(nx, ty) <= kSmemOptin;
+}
 
 // Shared memory of the r-recomputing step: 3 ring slots + 1 staging plane of 3 components x TY + 2
 // rows, 2 primal and 2 b planes of TY + 1 rows (no staging on the first step).
@@ -597,11 +982,17 @@ std::size_t fgp_smem(int nx, int ty) {
 }
 
 // Rows per CTA that a CTA of this volume can take: tx * ty <= 256 threads and the shared memory
-// within the SM's limit; the default is the tallest of at most 4 rows within 110 KiB.
+// within the SM's limit (the two-step form: float4 rows, 512 threads and the opt-in limit, and only
+// where the caller has the fourth dual triplet); the default is the tallest of at most 4 rows of
+// the one-step form within 110 KiB.
 template <int VEC>
-std::vector<int> fgp_rows_candidates(int nx) {
+std::vector<int> fgp_rows_candidates(int nx, bool two_step) {
   std::vector<int> out;
   const int tx = nx / VEC;
+  if (VEC == 4 && two_step) {
+    for (const int ty : {8, 4, 2})
+      if (fgp2_fits(nx, ty)) out.push_back(2 * kFgpVariantScale + ty);
+  }
   for (const int variant : {1, 0}) {
     for (const int ty : {8, 4, 2, 1}) {
       const std::size_t smem = variant == 1 ? fgp_p_smem(nx, ty, false) : fgp_smem(nx, ty);
@@ -630,9 +1021,22 @@ template <int VEC>
 FgpShape fgp_shape_rows(int nz, int ny, int nx, int choice) {
   const int variant = choice / kFgpVariantScale;
   const int ty = choice % kFgpVariantScale;
-  const std::size_t smem = variant == 1 ? fgp_p_smem(nx, ty, false) : fgp_smem(nx, ty);
+  const std::size_t smem =
+      variant == 2 ? fgp2_smem(nx, ty) : variant == 1 ? fgp_p_smem(nx, ty, false) : fgp_smem(nx, ty);
   int per_sm = 0;
-  if (variant == 1) {
+  if (variant == 2) {
+    const auto occupancy = [&](auto kernel) {
+      ensure_smem(kernel);
+      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (nx / 4) * ty, smem), "cudaOccupancy");
+    };
+    if (ty == 8) {
+      occupancy(k_fgp2<8, false, false>);
+    } else if (ty == 4) {
+      occupancy(k_fgp2<4, false, false>);
+    } else {
+      occupancy(k_fgp2<2, false, false>);
+    }
+  } else if (variant == 1) {
     auto kernel = k_fgp_p<VEC, false>;
     ensure_smem(kernel);
     check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (nx / VEC) * ty, smem), "cudaOccupancy");
@@ -647,18 +1051,33 @@ FgpShape fgp_shape_rows(int nz, int ny, int nx, int choice) {
   return sh;
 }
 
-// Forced FGP form (qhk_tv_form): 0 the tuned / default one, 1 stored r, 2 recomputed r.
+// Forced FGP form (qhk_tv_form): 0 the tuned / default one, 1 stored r, 2 recomputed r, 3 two
+// steps per pass.
 std::atomic<int> g_fgp_form{0};
 
+// The tuned (or forced) shape; the two-step form only with VEC = 4 and a fourth dual triplet, else
+// the stored-r form with its default rows.
 template <int VEC>
-FgpShape fgp_shape(int nz, int ny, int nx) {
+FgpShape fgp_shape(int nz, int ny, int nx, bool two_step) {
   const int form = g_fgp_form.load();
-  int choice = tuned_choice(fgp_key<VEC>(nz, ny, nx), fgp_rows_default<VEC>(nx));
-  if (form == 1 || form == 2) {
-    const int ty = choice % kFgpVariantScale;
+  const int fallback = fgp_rows_default<VEC>(nx);
+  int choice = tuned_choice(fgp_key<VEC>(nz, ny, nx), fallback);
+  if (form == 3) {
+    choice = fallback;
+    for (const int ty : {8, 4, 2}) {
+      if (fgp2_fits(nx, ty)) {
+        choice = 2 * kFgpVariantScale + ty;
+        break;
+      }
+    }
+  } else if (form == 1 || form == 2) {
+    const int ty = choice / kFgpVariantScale == 2 ? fallback : choice % kFgpVariantScale;
     choice = (form - 1) * kFgpVariantScale + ty;
     const std::size_t smem = form == 2 ? fgp_p_smem(nx, ty, false) : fgp_smem(nx, ty);
     if (smem > 200 * 1024) choice = (form - 1) * kFgpVariantScale + 1;
+  }
+  if (choice / kFgpVariantScale == 2 && (VEC != 4 || !two_step || !fgp2_fits(nx, choice % kFgpVariantScale))) {
+    choice = fallback;
   }
   return fgp_shape_rows<VEC>(nz, ny, nx, choice);
 }
@@ -681,6 +1100,39 @@ void launch_fgp_p(const FgpPArgs& a, const FgpShape& sh, cudaStream_t s) {
   const std::size_t smem = fgp_p_smem(a.nx, sh.ty, FIRST);
   kernel<<<sh.grid, block, smem, s>>>(a);
   check_launch("fgp step");
+}
+
+template <int TY, bool FIRST, bool LAST>
+void launch_fgp2_t(const Fgp2Args& a, int grid, cudaStream_t s) {
+  auto kernel = k_fgp2<TY, FIRST, LAST>;
+  ensure_smem(kernel);
+  kernel<<<grid, dim3(a.nx / 4, TY), fgp2_smem(a.nx, TY), s>>>(a);
+  check_launch("fgp two steps");
+}
+
+template <int TY>
+void launch_fgp2_rows(bool first, bool last, const Fgp2Args& a, int grid, cudaStream_t s) {
+  if (first && last) {
+    launch_fgp2_t<TY, true, true>(a, grid, s);
+  } else if (first) {
+    launch_fgp2_t<TY, true, false>(a, grid, s);
+  } else if (last) {
+    launch_fgp2_t<TY, false, true>(a, grid, s);
+  } else {
+    launch_fgp2_t<TY, false, false>(a, grid, s);
+  }
+}
+
+void launch_fgp2(bool first, bool last, const Fgp2Args& a, const FgpShape& sh, cudaStream_t s) {
+  require(a.nx % 4 == 0 && fgp2_fits(a.nx, sh.ty), "tv: two-step FGP shape out of range");
+  if (sh.ty == 8) {
+    launch_fgp2_rows<8>(first, last, a, sh.grid, s);
+  } else if (sh.ty == 4) {
+    launch_fgp2_rows<4>(first, last, a, sh.grid, s);
+  } else {
+    require(sh.ty == 2, "tv: two-step FGP rows must be 2, 4 or 8");
+    launch_fgp2_rows<2>(first, last, a, sh.grid, s);
+  }
 }
 
 template <int VEC>
@@ -723,7 +1175,8 @@ void launch_final(TvFinal mode, const float* b, float* const p[3], int nz, int n
 float fista_t(float t) { return 0.5f * (1.0f + std::sqrt(1.0f + 4.0f * t * t)); }
 
 void set_tv_form(int form) {
-  require(form >= 0 && form <= 2, "tv: form must be 0 (tuned), 1 (stored r) or 2 (recomputed r)");
+  require(form >= 0 && form <= 3,
+          "tv: form must be 0 (tuned), 1 (stored r), 2 (recomputed r) or 3 (two steps per pass)");
   g_fgp_form.store(form);
 }
 
@@ -736,11 +1189,78 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
                  (xprev == nullptr || reinterpret_cast<std::uintptr_t>(xprev) % 16 == 0);
   for (int i = 0; i < 3; ++i)
     for (int c = 0; c < 3; ++c) aligned = aligned && reinterpret_cast<std::uintptr_t>(t.v[i][c]) % 16 == 0;
+  if (t.has_fourth()) {
+    for (int c = 0; c < 3; ++c) aligned = aligned && reinterpret_cast<std::uintptr_t>(t.v[3][c]) % 16 == 0;
+  }
   const int vec = aligned ? 4 : 1;
-  const FgpShape sh = vec == 4 ? fgp_shape<4>(nz, ny, nx) : fgp_shape<1>(nz, ny, nx);
+  const FgpShape sh = vec == 4 ? fgp_shape<4>(nz, ny, nx, t.has_fourth()) : fgp_shape<1>(nz, ny, nx, false);
   const float step = 1.0f / (12.0f * lambda);
   float tk = 1.0f;
-  if (sh.variant == 1) {
+  if (sh.variant != 2 && t.p_index == 3) {
+    // The one-step forms rotate among the first three triplets: bring p there (only after the form
+    // changed between two calls on the same buffers).
+    const std::size_t vbytes = static_cast<std::size_t>(nz) * ny * nx * sizeof(float);
+    for (int c = 0; c < 3; ++c)
+      check(cudaMemcpyAsync(t.v[0][c], t.v[3][c], vbytes, cudaMemcpyDeviceToDevice, s), "copy dual");
+    t.p_index = 0;
+  }
+  if (sh.variant == 2) {
+    // Pairs of steps: (p, r) in two triplets -> (p, r) in two others; the first pair reads p_0 as
+    // r_0. An odd last step runs the one-step kernel (stored-r form of the same shape family).
+    int pc = t.p_index, rc = t.p_index;
+    const auto free_pair = [&](int& f0, int& f1) {
+      int n = 0;
+      for (int i = 0; i < 4 && n < 2; ++i) {
+        if (i == pc || i == rc) continue;
+        (n++ == 0 ? f0 : f1) = i;
+      }
+    };
+    int k = 0;
+    for (; k + 2 <= inner; k += 2) {
+      const float t1 = fista_t(tk);
+      const float t2 = fista_t(t1);
+      Fgp2Args a{};
+      a.b = b;
+      a.nz = nz, a.ny = ny, a.nx = nx;
+      a.ytiles = (ny + sh.ty - 1) / sh.ty;
+      a.lambda = lambda, a.step = step;
+      a.m1 = (tk - 1.0f) / t1;
+      a.m2 = (t1 - 1.0f) / t2;
+      int f0 = 0, f1 = 0;
+      free_pair(f0, f1);
+      for (int c = 0; c < 3; ++c) {
+        a.rin[c] = t.v[rc][c];
+        a.pin[c] = t.v[pc][c];
+        a.pout[c] = t.v[f0][c];
+        a.rout[c] = t.v[f1][c];
+      }
+      launch_fgp2(k == 0, k + 2 == inner, a, sh, s);
+      pc = f0, rc = f1;
+      tk = t2;
+    }
+    if (k < inner) {  // the last step alone
+      const FgpShape one = fgp_shape_rows<4>(nz, ny, nx, fgp_rows_default<4>(nx));
+      const float tn = fista_t(tk);
+      FgpArgs a{};
+      a.b = b;
+      a.nz = nz, a.ny = ny, a.nx = nx;
+      a.ytiles = (ny + one.ty - 1) / one.ty;
+      a.lambda = lambda, a.step = step, a.momentum = (tk - 1.0f) / tn;
+      int f0 = 0, f1 = 0;
+      free_pair(f0, f1);
+      const int po = k == 0 ? f0 : pc;  // the first step may not update p_0 = r_0 in place
+      for (int c = 0; c < 3; ++c) {
+        a.rin[c] = t.v[rc][c];
+        a.pin[c] = t.v[pc][c];
+        a.pout[c] = t.v[po][c];
+        a.rout[c] = t.v[f1][c];
+      }
+      launch_fgp_any<4>(k == 0, true, a, one, s);
+      pc = po;
+      tk = tn;
+    }
+    t.p_index = pc;
+  } else if (sh.variant == 1) {
     // p_k lives in triplet (i0 + k) % 3; step k reads p_k and p_{k-1}, writes p_{k+1} over p_{k-2}.
     const int i0 = t.p_index;
     float m_prev = 0.0f;
@@ -818,8 +1338,9 @@ __global__ void k_fill_hash(float* p, std::size_t n, float lo, float hi, unsigne
 
 template <int VEC>
 void tune_fgp_rows(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s) {
-  // A middle step of each form: r (or p_k) from triplet 0, p (or p_{k-1}) from triplet 1, outputs
-  // into triplets 1 and 2 (the inputs each run reads are never written).
+  // Two middle steps of each form (one launch of the two-step form, two of the others): r (or p_k)
+  // from triplet 0, p (or p_{k-1}) from triplet 1, outputs into triplets 1 and 2 (the two-step
+  // form: 2 and 3), so that the inputs each run reads are never written.
   FgpArgs a{};
   a.b = b;
   a.nz = nz, a.ny = ny, a.nx = nx;
@@ -837,14 +1358,31 @@ void tune_fgp_rows(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
     q.pkm1[c] = t.v[1][c];
     q.pout[c] = t.v[2][c];
   }
-  autotune(fgp_key<VEC>(nz, ny, nx), fgp_rows_candidates<VEC>(nx), fgp_rows_default<VEC>(nx),
+  Fgp2Args w{};
+  w.b = b;
+  w.nz = nz, w.ny = ny, w.nx = nx;
+  w.lambda = a.lambda, w.step = a.step, w.m1 = 0.5f, w.m2 = 0.5f;
+  if (t.has_fourth()) {
+    for (int c = 0; c < 3; ++c) {
+      w.rin[c] = t.v[0][c];
+      w.pin[c] = t.v[1][c];
+      w.pout[c] = t.v[2][c];
+      w.rout[c] = t.v[3][c];
+    }
+  }
+  autotune(fgp_key<VEC>(nz, ny, nx), fgp_rows_candidates<VEC>(nx, t.has_fourth()), fgp_rows_default<VEC>(nx),
            [&](int choice) {
              const FgpShape sh = fgp_shape_rows<VEC>(nz, ny, nx, choice);
-             if (sh.variant == 1) {
+             if (sh.variant == 2) {
+               w.ytiles = (ny + sh.ty - 1) / sh.ty;
+               launch_fgp2(false, false, w, sh, s);
+             } else if (sh.variant == 1) {
                q.ytiles = (ny + sh.ty - 1) / sh.ty;
+               launch_fgp_p<VEC, false>(q, sh, s);
                launch_fgp_p<VEC, false>(q, sh, s);
              } else {
                a.ytiles = (ny + sh.ty - 1) / sh.ty;
+               launch_fgp<VEC, false, false>(a, sh, s);
                launch_fgp<VEC, false, false>(a, sh, s);
              }
            },
@@ -868,7 +1406,7 @@ void tune_tv(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaS
     check(cudaMemsetAsync(t.v[1][c], 0, vol * sizeof(float), s), "cudaMemset");
   }
   bool aligned = nx % 4 == 0 && reinterpret_cast<std::uintptr_t>(b) % 16 == 0;
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < (t.has_fourth() ? 4 : 3); ++i)
     for (int c = 0; c < 3; ++c) aligned = aligned && reinterpret_cast<std::uintptr_t>(t.v[i][c]) % 16 == 0;
   if (aligned) {
     tune_fgp_rows<4>(b, t, nz, ny, nx, lambda, s);

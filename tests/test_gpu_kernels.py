@@ -53,10 +53,11 @@ def test_rfft3_and_irfft3_match_numpy(cuda, qhk, shape):
     assert rel_err(host(out), x) < 2e-6
 
 
-@pytest.fixture(params=[1, 2], ids=["stored_r", "recomputed_r"])
+@pytest.fixture(params=[1, 2, 3], ids=["stored_r", "recomputed_r", "two_step"])
 def tv_form(request, qhk):
-    """Both FGP step forms (the extrapolated point stored between steps, or recomputed from the two
-    previous duals) must give the reference's iterates bit for bit."""
+    """Every FGP step form (the extrapolated point stored between steps, recomputed from the two
+    previous duals, or two steps per pass with the halo rows recomputed) must give the reference's
+    iterates bit for bit."""
     qhk.tv_form(request.param)
     yield request.param
     qhk.tv_form(0)
@@ -74,7 +75,8 @@ def test_tv_prox_bit_identical_to_reference(cuda, qhk, tv_form):
 
 
 @pytest.mark.parametrize("shape,inner", [((24, 20, 36), 7), ((10, 12, 30), 5), ((9, 7, 8), 1), ((8, 8, 8), 0),
-                                         ((40, 33, 64), 10)])
+                                         ((40, 33, 64), 10), ((17, 29, 16), 4), ((6, 5, 4), 3), ((3, 40, 12), 2),
+                                         ((1, 16, 16), 4), ((2, 9, 8), 6), ((12, 70, 256), 4)])
 def test_tv_prox_bit_identical_to_oracle(cuda, qhk, shape, inner, tv_form):
     rng = np.random.default_rng(inner + shape[0])
     b = rng.uniform(-0.2, 1.0, shape).astype(np.float32)
