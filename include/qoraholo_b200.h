@@ -118,6 +118,12 @@ int qhk_tv_prox_device(const float* d_b, float* d_x, float* d_dual, int nz, int 
 int qhk_tv_prox_workspace(const float* d_b, float* d_x, float* d_work, int work_volumes, int nz, int ny, int nx,
                           float lambda, int inner, void* stream);
 
+/* Bounded device waits that ran out since the library was loaded: the two-step FGP kernel waits
+ * for its box loads (TMA) on mbarriers with an iteration limit, and a wait that gives up counts
+ * here and ends the kernel early (the result is then invalid). 0 in every correct run. Synchronises
+ * the device. */
+int qhk_wait_timeouts(uint64_t* count);
+
 /* Number of kernels this library has launched since it was loaded (for launch accounting). */
 uint64_t qhk_kernel_launches(void);
 

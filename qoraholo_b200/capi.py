@@ -85,6 +85,7 @@ _PROTOS = {
     "qhk_irfft3": (_I, [_VP, _VP, _I, _I, _I, _F, _VP]),
     "qhk_tv_prox_device": (_I, [_VP, _VP, _VP, _I, _I, _I, _F, _I, _VP]),
     "qhk_kernel_launches": (C.c_uint64, []),
+    "qhk_wait_timeouts": (_I, [C.POINTER(C.c_uint64)]),
     "qhk_tv_prox_workspace": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _F, _I, _VP]),
     "qhk_unwrap_noalloc": (_I, [_VP, _VP, _I, _I, _I, _VP]),
     "qhk_bpm_vjp": (_I, [_VP, _I, _I, _VP, _VP, _I, C.POINTER(Geometry), _I, _VP]),
@@ -246,6 +247,14 @@ def tv_prox_workspace(d_b, d_x, d_work, work_volumes, nz, ny, nx, lam, inner, st
 def unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, stream=0):
     """qhk_unwrap_noalloc: device in / device out, no allocation (scratch in a static device array)."""
     check(lib().qhk_unwrap_noalloc(_VP(d_wrapped), _VP(d_unwrapped), count, ny, nx, _VP(stream)))
+
+
+def wait_timeouts() -> int:
+    """Bounded device waits that ran out since the library was loaded (qhk_wait_timeouts); 0 in every
+    correct run."""
+    n = C.c_uint64()
+    check(lib().qhk_wait_timeouts(C.byref(n)))
+    return n.value
 
 
 def autotune_enable(enabled: bool = True):

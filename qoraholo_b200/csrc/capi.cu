@@ -250,6 +250,13 @@ int qhk_tv_prox_workspace(const float* d_b, float* d_x, float* d_work, int work_
   });
 }
 
+int qhk_wait_timeouts(uint64_t* count) {
+  return guard([&] {
+    qhk::require(count != nullptr, "wait_timeouts: null argument");
+    *count = qhk::tv_wait_timeouts();
+  });
+}
+
 uint64_t qhk_kernel_launches(void) { return qhk::g_launches.load(std::memory_order_relaxed); }
 
 int qhk_fft2d(void* d_data, int count, int n, int forward, float scale, void* stream) {

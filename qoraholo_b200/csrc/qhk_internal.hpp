@@ -98,5 +98,8 @@ void set_tv_form(int form);
 // Times the FGP tile heights on this volume's shape and keeps the fastest for later tv_prox calls.
 // b and all three dual triplets of t are scratch (overwritten). Never inside a stream capture.
 void tune_tv(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s);
+// Bounded waits of the FGP kernels that ran out since the library was loaded (0 unless a box load
+// never completed). Synchronises the device.
+unsigned long long tv_wait_timeouts();
 
 }  // namespace qhk

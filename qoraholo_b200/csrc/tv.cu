@@ -23,6 +23,7 @@
 
 #include "autotune.hpp"
 #include "qhk_internal.hpp"
+#include "tma.cuh"
 
 namespace qhk {
 
@@ -593,16 +594,23 @@ __global__ void __launch_bounds__(256)
 // in registers from dual step k to dual step k + 1. The per-point operations are those of k_fgp in
 // the same order, so the iterates are bit-identical.
 struct Fgp2Args {
-  const float* b;
-  const float* rin[3];  // r_k; on the first step p_0
   const float* pin[3];  // p_k (not read on the first step)
   float* pout[3];       // p_{k+2}
   float* rout[3];       // r_{k+2} (not written when step k + 1 is the last)
   int nz, ny, nx;
+  int pitch;  // shared-memory row length: nx rounded up to 32 floats (the box width)
   int ytiles;
   float lambda, step;
   float m1, m2;  // momenta of steps k and k + 1
 };
+// Box-load maps of r_k (on the first step p_0), boxes of (pitch x TY+4 rows), and of b (pitch x TY+3).
+struct Fgp2Maps {
+  CUtensorMap r[3];
+  CUtensorMap b;
+};
+
+// Waits of k_fgp2 that ran out (a box load that never completed); read by tv_wait_timeouts().
+__device__ unsigned long long g_fgp2_timeouts = 0;
 
 // The primal point max(b - lambda L(r), 0) of one voxel from its six dual neighbours, the sum in the
 // host's order (src/common.hpp:107-153).
@@ -633,15 +641,13 @@ constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(t
 constexpr int fgp2_threads(int ty) { return ty == 8 ? 512 : 256; }
 
 template <int TY, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
-  extern __shared__ __align__(16) float sm[];
+__global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const __grid_constant__ Fgp2Maps M) {
+  extern __shared__ __align__(128) float smem2[];
   constexpr int VEC = 4;
   constexpr int RK_ROWS = TY + 4, B_ROWS = TY + 3, R1_ROWS = TY + 2, Z1_ROWS = TY + 1;
   constexpr int HALO = (8 + TY - 1) / TY;     // halo points of dual step k per thread: 2 nx over nx / 4 * TY threads
   constexpr int HALO_Z = (12 + TY - 1) / TY;  // halo points of z_k per thread: 3 nx
   constexpr int HALO_Z1 = (4 + TY - 1) / TY;  // halo points of z_{k+1} per thread: nx
-  constexpr int COPY_R = (3 * RK_ROWS + TY - 1) / TY;  // r_k rows a thread row copies per plane
-  constexpr int COPY_B = (B_ROWS + TY - 1) / TY;
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   const int tx = static_cast<int>(threadIdx.x);
   const int ty = static_cast<int>(threadIdx.y);
@@ -652,14 +658,23 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
   const int warp_threads = min(32, nthreads - (linear & ~31));
   const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
   const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
-  // Shared memory in floats: slot strides and buffer bases (32-bit offsets from sm).
-  const int RKP = RK_ROWS * nx, BP = B_ROWS * nx, R1P = R1_ROWS * nx, Z1P = Z1_ROWS * nx;
+  // Shared memory in floats, rows of P = A.pitch floats (nx rounded up to 128 bytes; the columns
+  // from nx on hold the zeros the box loads fill in): slot strides and buffer bases (32-bit offsets
+  // from smem2), then the three ring-slot mbarriers.
+  const int P = A.pitch;
+  const int RKP = RK_ROWS * P, BP = B_ROWS * P, R1P = R1_ROWS * P, Z1P = Z1_ROWS * P;
   const int OB = 9 * RKP, OZ = OB + 3 * BP, OR = OZ + 2 * BP, OZ1 = OR + 4 * R1P;
+  std::uint64_t* const bars = reinterpret_cast<std::uint64_t*>(smem2 + OZ1 + 2 * Z1P);
   // Own-row offsets within a slot: r_k row ty+2 (rows start at y0-2); b, z_k, r_{k+1} row ty+1
   // (rows start at y0-1); z_{k+1} row ty (rows start at y0).
-  const int own_rk = (ty + 2) * nx + x0;
-  const int own_b = (ty + 1) * nx + x0;
-  const int own_z1 = ty * nx + x0;
+  const int own_rk = (ty + 2) * P + x0;
+  const int own_b = (ty + 1) * P + x0;
+  const int own_z1 = ty * P + x0;
+  if (linear == 0) {
+    for (int i = 0; i < 3; ++i) tma::mbar_init(bars + i, 1);
+  }
+  __syncthreads();
+  unsigned phases = 0;  // bit s: parity of the next completion of slot s's mbarrier
   // Halo points (the same point -> thread map in the z_k and dual-k phases): v = linear + j
   // nthreads over the rows y0-1 (side 0), y0+TY (1), y0+TY+1 (2); row of z_k / b: 0, TY+1, TY+2.
   int hz_side[HALO_Z], hz_x[HALO_Z];
@@ -682,40 +697,29 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
     const bool own = y < ny;
     const std::size_t own_g = static_cast<std::size_t>(y) * nx + x0;  // within a plane
 
-    // Copies of one plane into ring slot s: r_k rows y0-2 .. y0+TY+1 (row y0-2 of the y component
-    // only), b rows y0-1 .. y0+TY+1; rows outside the volume are never read and not copied.
-    const auto issue_rk = [&](int z, int s, int comps) {
-      const std::size_t po = z * nxy;
-#pragma unroll
-      for (int j = 0; j < COPY_R; ++j) {
-        const int rc = ty + j * TY;
-        const int c = rc / RK_ROWS;
-        const int i = rc - c * RK_ROWS;
-        const int yy = y0 - 2 + i;
-        if (rc < comps * RK_ROWS && yy >= 0 && yy < ny && (i != 0 || c == 1)) {
-          copy_async<VEC>(sm + (s * 3 + c) * RKP + i * nx + x0, A.rin[c] + po + static_cast<std::size_t>(yy) * nx + x0);
-        }
-      }
+    // Box loads of one plane into ring slot s by thread 0: r_k rows y0-2 .. y0+TY+1 (`comps`
+    // components) and b rows y0-1 .. y0+TY+1, counted on the slot's mbarrier. Rows outside the
+    // volume arrive as zeros and are never read.
+    const auto issue = [&](int z, int s, int comps, bool with_b) {
+      tma::fence_async_shared();
+      tma::mbar_expect(bars + s, static_cast<unsigned>((comps * RK_ROWS + (with_b ? B_ROWS : 0)) * P * 4));
+      for (int c = 0; c < comps; ++c) tma::load_3d(smem2 + (s * 3 + c) * RKP, &M.r[c], 0, y0 - 2, z, bars + s);
+      if (with_b) tma::load_3d(smem2 + OB + s * BP, &M.b, 0, y0 - 1, z, bars + s);
     };
-    const auto issue_b = [&](int z, int s) {
-      const std::size_t po = z * nxy;
-#pragma unroll
-      for (int j = 0; j < COPY_B; ++j) {
-        const int i = ty + j * TY;
-        const int yy = y0 - 1 + i;
-        if (i < B_ROWS && yy >= 0 && yy < ny) {
-          copy_async<VEC>(sm + OB + s * BP + i * nx + x0, A.b + po + static_cast<std::size_t>(yy) * nx + x0);
-        }
-      }
+    // Bounded wait for slot s (every thread), then its phase bit flips.
+    const auto wait_slot = [&](int s) {
+      const bool ok = tma::mbar_wait(bars + s, (phases >> s) & 1u, &g_fgp2_timeouts);
+      phases ^= 1u << s;
+      return ok;
     };
     const auto mod3 = [](int z) { return ((z % 3) + 3) % 3; };
     // Iteration q needs r_k and b of planes up to q+2 (the z component of q+1 for z_k of q+2).
-    if (z0 >= 2) issue_rk(z0 - 2, mod3(z0 - 2), 1);
-    if (z0 >= 1) {
-      issue_rk(z0 - 1, mod3(z0 - 1), 3);
-      issue_b(z0 - 1, mod3(z0 - 1));
+    if (linear == 0) {
+      if (z0 >= 2) issue(z0 - 2, mod3(z0 - 2), 1, false);
+      if (z0 >= 1) issue(z0 - 1, mod3(z0 - 1), 3, true);
     }
-    copy_commit();
+    bool ok = true;
+    if (z0 >= 2) ok = wait_slot(mod3(z0 - 2)) && ok;
 
     float cr[3][VEC] = {}, cp[3][VEC] = {};  // r_{k+1}, p_{k+1} of this thread's points of plane q
     float nr[3][VEC] = {}, np[3][VEC] = {};  // the same of plane q+1
@@ -749,28 +753,29 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
           }
         }
       }
-      copy_wait<0>();  // plane a2
-      __syncthreads();
-      if (q + 3 <= zmax) {
-        issue_rk(q + 3, m0, 3);
-        issue_b(q + 3, m0);
+      if (a2 >= 0 && a2 <= zmax) ok = wait_slot(m2) && ok;  // plane a2 (loaded one iteration ago)
+      if (__syncthreads_or(!ok)) {
+        // A load never completed: leave with the timeout counted (every thread takes this exit),
+        // after one more bounded wait for the load in flight.
+        if (a2 >= 0 && a2 <= zmax) tma::mbar_wait(bars + m2, ((phases >> m2) & 1u) ^ 1u, &g_fgp2_timeouts);
+        return;
       }
-      copy_commit();
+      if (linear == 0 && q + 3 <= zmax) issue(q + 3, m0, 3, true);
 
       if (do_a) {
         const int a = a2;
-        const float* Rz = sm + (m2 * 3 + 0) * RKP;
-        const float* Rzb = sm + (m1 * 3 + 0) * RKP;  // plane a-1; not read on plane 0
-        const float* Ry = sm + (m2 * 3 + 1) * RKP;
-        const float* Rx = sm + (m2 * 3 + 2) * RKP;
-        const float* B = sm + OB + m2 * BP;
-        float* Z = sm + OZ + par * BP;
+        const float* Rz = smem2 + (m2 * 3 + 0) * RKP;
+        const float* Rzb = smem2 + (m1 * 3 + 0) * RKP;  // plane a-1; not read on plane 0
+        const float* Ry = smem2 + (m2 * 3 + 1) * RKP;
+        const float* Rx = smem2 + (m2 * 3 + 2) * RKP;
+        const float* B = smem2 + OB + m2 * BP;
+        float* Z = smem2 + OZ + par * BP;
         {
           float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
           Vec<VEC>::load(Rz + own_rk, vz);
           Vec<VEC>::load(Rzb + own_rk, vzb);
           Vec<VEC>::load(Ry + own_rk, vy);
-          Vec<VEC>::load(Ry + own_rk - nx, vym);
+          Vec<VEC>::load(Ry + own_rk - P, vym);
           Vec<VEC>::load(Rx + own_rk, vx);
           Vec<VEC>::load(B + own_b, vb);
           const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
@@ -790,26 +795,26 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
           const int zi = side == 0 ? 0 : TY + side;
           const int yy = y0 - 1 + zi;
           if (side >= 0 && yy >= 0 && yy < ny) {
-            const int i = (zi + 1) * nx + x;  // r_k row of yy
+            const int i = (zi + 1) * P + x;  // r_k row of yy
             const float vxm = x > 0 ? Rx[i - 1] : 0.0f;
-            Z[zi * nx + x] = fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - nx], Rx[i], vxm,
-                                           B[zi * nx + x], A.lambda);
+            Z[zi * P + x] = fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - P], Rx[i], vxm,
+                                          B[zi * P + x], A.lambda);
           }
         }
       }
 
       if (do_b) {
         const int a = a1;
-        const float* Zc = sm + OZ + (par ^ 1) * BP;
-        const float* Zn = sm + OZ + par * BP;  // plane a+1; read only below plane nz-1
-        const float* R = sm + (m1 * 3) * RKP;
-        float* Rz1 = sm + OR + (par ^ 1) * R1P;
-        float* Ry1 = sm + OR + 2 * R1P;
-        float* Rx1 = sm + OR + 3 * R1P;
+        const float* Zc = smem2 + OZ + (par ^ 1) * BP;
+        const float* Zn = smem2 + OZ + par * BP;  // plane a+1; read only below plane nz-1
+        const float* R = smem2 + (m1 * 3) * RKP;
+        float* Rz1 = smem2 + OR + (par ^ 1) * R1P;
+        float* Ry1 = smem2 + OR + 2 * R1P;
+        float* Rx1 = smem2 + OR + 3 * R1P;
         {
           float zc[VEC], zy[VEC], zz[VEC];
           Vec<VEC>::load(Zc + own_b, zc);
-          Vec<VEC>::load(Zc + own_b + nx, zy);
+          Vec<VEC>::load(Zc + own_b + P, zy);
           Vec<VEC>::load(Zn + own_b, zz);
           const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
           const float right =
@@ -848,15 +853,15 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
           const int zi = side == 0 ? 0 : TY + 1;
           const int yy = y0 - 1 + zi;
           if ((side == 0 || side == 1) && yy >= 0 && yy < ny) {
-            const int i = zi * nx + x;
+            const int i = zi * P + x;
             const float c0 = Zc[i];
             const float cz = a < nz - 1 ? Zn[i] : 0.0f;
-            const float cy = yy < ny - 1 ? Zc[i + nx] : 0.0f;
+            const float cy = yy < ny - 1 ? Zc[i + P] : 0.0f;
             const float cx = x < nx - 1 ? Zc[i + 1] : 0.0f;
             float p[3], r[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              r[c] = R[c * RKP + i + nx];
+              r[c] = R[c * RKP + i + P];
               p[c] = FIRST ? r[c] : ph[h][c];
             }
             fgp_dual_at(c0, cz, cy, cx, a, yy, x, nz, ny, nx, A.step, A.m1, p, r);
@@ -871,18 +876,18 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
       float zn[VEC] = {};  // z_{k+1} of this thread's points of plane a1
       if (do_c) {
         const int a = a1;
-        const float* Rz = sm + OR + (par ^ 1) * R1P;
-        const float* Rzb = sm + OR + par * R1P;  // plane a-1; not read on plane 0
-        const float* Ry = sm + OR + 2 * R1P;
-        const float* Rx = sm + OR + 3 * R1P;
-        const float* B = sm + OB + m1 * BP;
-        float* Z = sm + OZ1 + (par ^ 1) * Z1P;
+        const float* Rz = smem2 + OR + (par ^ 1) * R1P;
+        const float* Rzb = smem2 + OR + par * R1P;  // plane a-1; not read on plane 0
+        const float* Ry = smem2 + OR + 2 * R1P;
+        const float* Rx = smem2 + OR + 3 * R1P;
+        const float* B = smem2 + OB + m1 * BP;
+        float* Z = smem2 + OZ1 + (par ^ 1) * Z1P;
         {
           float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
           Vec<VEC>::load(Rz + own_b, vz);
           Vec<VEC>::load(Rzb + own_b, vzb);
           Vec<VEC>::load(Ry + own_b, vy);
-          Vec<VEC>::load(Ry + own_b - nx, vym);
+          Vec<VEC>::load(Ry + own_b - P, vym);
           Vec<VEC>::load(Rx + own_b, vx);
           Vec<VEC>::load(B + own_b, vb);
           const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
@@ -900,20 +905,20 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A) {
           for (int j = 0; j < HALO_Z1; ++j) {
             const int x = linear + j * nthreads;
             if (x < nx) {
-              const int i = (TY + 1) * nx + x;
+              const int i = (TY + 1) * P + x;
               const float vxm = x > 0 ? Rx[i - 1] : 0.0f;
-              Z[TY * nx + x] =
-                  fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - nx], Rx[i], vxm, B[i], A.lambda);
+              Z[TY * P + x] =
+                  fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - P], Rx[i], vxm, B[i], A.lambda);
             }
           }
         }
       }
 
       if (do_d) {  // own row: z_{k+1} of plane q row ty (row ty+1 below it), of plane q+1 in zn
-        const float* Zc = sm + OZ1 + par * Z1P;
+        const float* Zc = smem2 + OZ1 + par * Z1P;
         float zc[VEC], zy[VEC];
         Vec<VEC>::load(Zc + own_z1, zc);
-        Vec<VEC>::load(Zc + own_z1 + nx, zy);
+        Vec<VEC>::load(Zc + own_z1 + P, zy);
         const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
         const float right = (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? Zc[own_z1 + VEC] : from_lane;
         if (own) {
@@ -959,12 +964,17 @@ struct FgpShape {
   int variant = 0;  // 0: r stored (k_fgp), 1: r recomputed (k_fgp_p), 2: two steps per pass (k_fgp2)
 };
 
-// Shared memory of the two-step form, and the largest a CTA may take on this part.
-std::size_t fgp2_smem(int nx, int ty) { return fgp2_rows(ty) * static_cast<std::size_t>(nx) * sizeof(float); }
+// Shared memory of the two-step form (rows of the 128-byte-aligned pitch, then 3 mbarriers), and
+// the largest a CTA may take on this part.
+int fgp2_pitch(int nx) { return (nx + 31) / 32 * 32; }
+std::size_t fgp2_smem(int nx, int ty) {
+  return fgp2_rows(ty) * static_cast<std::size_t>(fgp2_pitch(nx)) * sizeof(float) + 3 * sizeof(std::uint64_t);
+}
 constexpr std::size_t kSmemOptin = 227 * 1024;
 
+// Box loads take at most 256 floats per row.
 bool fgp2_fits(int nx, int ty) {
-  return nx % 4 == 0 && (nx / 4) * ty <= fgp2_threads(ty) && fgp2_smem(nx, ty) <= kSmemOptin;
+  return nx % 4 == 0 && nx <= 256 && (nx / 4) * ty <= fgp2_threads(ty) && fgp2_smem(nx, ty) <= kSmemOptin;
 }
 
 // Shared memory of the r-recomputing step: 3 ring slots + 1 staging plane of 3 components x TY + 2
@@ -1103,35 +1113,42 @@ void launch_fgp_p(const FgpPArgs& a, const FgpShape& sh, cudaStream_t s) {
 }
 
 template <int TY, bool FIRST, bool LAST>
-void launch_fgp2_t(const Fgp2Args& a, int grid, cudaStream_t s) {
+void launch_fgp2_t(const Fgp2Args& a, const float* const rin[3], const float* b, int grid, cudaStream_t s) {
   auto kernel = k_fgp2<TY, FIRST, LAST>;
   ensure_smem(kernel);
-  kernel<<<grid, dim3(a.nx / 4, TY), fgp2_smem(a.nx, TY), s>>>(a);
+  Fgp2Maps maps;
+  for (int c = 0; c < 3; ++c) maps.r[c] = volume_tensor_map(rin[c], a.nx, a.ny, a.nz, a.pitch, TY + 4);
+  maps.b = volume_tensor_map(b, a.nx, a.ny, a.nz, a.pitch, TY + 3);
+  kernel<<<grid, dim3(a.nx / 4, TY), fgp2_smem(a.nx, TY), s>>>(a, maps);
   check_launch("fgp two steps");
 }
 
 template <int TY>
-void launch_fgp2_rows(bool first, bool last, const Fgp2Args& a, int grid, cudaStream_t s) {
+void launch_fgp2_rows(bool first, bool last, const Fgp2Args& a, const float* const rin[3], const float* b, int grid,
+                      cudaStream_t s) {
   if (first && last) {
-    launch_fgp2_t<TY, true, true>(a, grid, s);
+    launch_fgp2_t<TY, true, true>(a, rin, b, grid, s);
   } else if (first) {
-    launch_fgp2_t<TY, true, false>(a, grid, s);
+    launch_fgp2_t<TY, true, false>(a, rin, b, grid, s);
   } else if (last) {
-    launch_fgp2_t<TY, false, true>(a, grid, s);
+    launch_fgp2_t<TY, false, true>(a, rin, b, grid, s);
   } else {
-    launch_fgp2_t<TY, false, false>(a, grid, s);
+    launch_fgp2_t<TY, false, false>(a, rin, b, grid, s);
   }
 }
 
-void launch_fgp2(bool first, bool last, const Fgp2Args& a, const FgpShape& sh, cudaStream_t s) {
-  require(a.nx % 4 == 0 && fgp2_fits(a.nx, sh.ty), "tv: two-step FGP shape out of range");
+// rin: r_k (p_0 on the first step), b: the point the prox is taken at.
+void launch_fgp2(bool first, bool last, Fgp2Args a, const float* const rin[3], const float* b, const FgpShape& sh,
+                 cudaStream_t s) {
+  require(fgp2_fits(a.nx, sh.ty), "tv: two-step FGP shape out of range");
+  a.pitch = fgp2_pitch(a.nx);
   if (sh.ty == 8) {
-    launch_fgp2_rows<8>(first, last, a, sh.grid, s);
+    launch_fgp2_rows<8>(first, last, a, rin, b, sh.grid, s);
   } else if (sh.ty == 4) {
-    launch_fgp2_rows<4>(first, last, a, sh.grid, s);
+    launch_fgp2_rows<4>(first, last, a, rin, b, sh.grid, s);
   } else {
     require(sh.ty == 2, "tv: two-step FGP rows must be 2, 4 or 8");
-    launch_fgp2_rows<2>(first, last, a, sh.grid, s);
+    launch_fgp2_rows<2>(first, last, a, rin, b, sh.grid, s);
   }
 }
 
@@ -1173,6 +1190,12 @@ void launch_final(TvFinal mode, const float* b, float* const p[3], int nz, int n
 }  // namespace
 
 float fista_t(float t) { return 0.5f * (1.0f + std::sqrt(1.0f + 4.0f * t * t)); }
+
+unsigned long long tv_wait_timeouts() {
+  unsigned long long n = 0;
+  check(cudaMemcpyFromSymbol(&n, g_fgp2_timeouts, sizeof(n)), "read wait timeouts");
+  return n;
+}
 
 void set_tv_form(int form) {
   require(form >= 0 && form <= 3,
@@ -1220,7 +1243,6 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
       const float t1 = fista_t(tk);
       const float t2 = fista_t(t1);
       Fgp2Args a{};
-      a.b = b;
       a.nz = nz, a.ny = ny, a.nx = nx;
       a.ytiles = (ny + sh.ty - 1) / sh.ty;
       a.lambda = lambda, a.step = step;
@@ -1228,13 +1250,14 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
       a.m2 = (t1 - 1.0f) / t2;
       int f0 = 0, f1 = 0;
       free_pair(f0, f1);
+      const float* rin[3];
       for (int c = 0; c < 3; ++c) {
-        a.rin[c] = t.v[rc][c];
+        rin[c] = t.v[rc][c];
         a.pin[c] = t.v[pc][c];
         a.pout[c] = t.v[f0][c];
         a.rout[c] = t.v[f1][c];
       }
-      launch_fgp2(k == 0, k + 2 == inner, a, sh, s);
+      launch_fgp2(k == 0, k + 2 == inner, a, rin, b, sh, s);
       pc = f0, rc = f1;
       tk = t2;
     }
@@ -1359,12 +1382,12 @@ void tune_fgp_rows(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
     q.pout[c] = t.v[2][c];
   }
   Fgp2Args w{};
-  w.b = b;
   w.nz = nz, w.ny = ny, w.nx = nx;
   w.lambda = a.lambda, w.step = a.step, w.m1 = 0.5f, w.m2 = 0.5f;
+  const float* w_rin[3] = {};
   if (t.has_fourth()) {
     for (int c = 0; c < 3; ++c) {
-      w.rin[c] = t.v[0][c];
+      w_rin[c] = t.v[0][c];
       w.pin[c] = t.v[1][c];
       w.pout[c] = t.v[2][c];
       w.rout[c] = t.v[3][c];
@@ -1375,7 +1398,7 @@ void tune_fgp_rows(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
              const FgpShape sh = fgp_shape_rows<VEC>(nz, ny, nx, choice);
              if (sh.variant == 2) {
                w.ytiles = (ny + sh.ty - 1) / sh.ty;
-               launch_fgp2(false, false, w, sh, s);
+               launch_fgp2(false, false, w, w_rin, b, sh, s);
              } else if (sh.variant == 1) {
                q.ytiles = (ny + sh.ty - 1) / sh.ty;
                launch_fgp_p<VEC, false>(q, sh, s);

@@ -88,6 +88,7 @@ def test_tv_prox_bit_identical_to_oracle(cuda, qhk, shape, inner, tv_form):
     qhk.tv_prox(tb.data_ptr(), tx.data_ptr(), td.data_ptr(), *shape, lam, inner)
     assert np.array_equal(host(tx), x_ref)
     assert np.array_equal(host(td), np.stack(p))
+    assert qhk.wait_timeouts() == 0  # no box load of the two-step form ran out of its bounded wait
 
 
 @pytest.mark.parametrize("n,nz,count", [(32, 32, 13), (48, 40, 25), (64, 64, 49), (30, 34, 7)])
