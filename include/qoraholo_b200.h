@@ -308,8 +308,8 @@ int qhk_server_add_geometry(qhk_server* server, const qhk_pipeline_options* opti
 int qhk_server_remove_geometry(qhk_server* server, int geometry_id);
 int qhk_server_volume_shape(qhk_server* server, int geometry_id, int* nz, int* n);
 /* Queues holograms (count, N, N) float32 -> index (nz, n, n) float32 into `index_out`. Host buffers,
- * pageable (staged by the calling thread) or page-locked (copied directly); `index_out` must stay
- * valid until qhk_server_wait returns. */
+ * pageable (staged by the server's threads) or page-locked (copied directly); both must stay valid
+ * until qhk_server_wait returns, and a pageable `index_out` holds unspecified values until then. */
 int qhk_server_submit(qhk_server* server, int geometry_id, const float* holograms, float* index_out,
                       uint64_t* ticket);
 /* *done = 1 once the request has completed. */

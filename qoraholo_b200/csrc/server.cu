@@ -155,29 +155,6 @@ std::vector<int> Admission::make_room(std::size_t bytes) {
 
 namespace {
 
-// memcpy split over a few threads: staging copies of large hologram stacks are host-bandwidth
-// bound, and one core reaches a fraction of it.
-void parallel_copy(void* dst, const void* src, std::size_t bytes) {
-  constexpr std::size_t kPerThread = std::size_t{16} << 20;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const std::size_t parts = std::min<std::size_t>(std::min<std::size_t>(hw, 8), (bytes + kPerThread - 1) / kPerThread);
-  if (parts <= 1) {
-    std::memcpy(dst, src, bytes);
-    return;
-  }
-  const std::size_t step = (bytes / parts + 63) & ~std::size_t{63};
-  std::vector<std::thread> workers;
-  for (std::size_t p = 1; p < parts; ++p) {
-    const std::size_t off = p * step;
-    if (off >= bytes) break;
-    workers.emplace_back([=] {
-      std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, std::min(step, bytes - off));
-    });
-  }
-  std::memcpy(dst, src, std::min(step, bytes));
-  for (auto& t : workers) t.join();
-}
-
 double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
@@ -196,7 +173,11 @@ Server::Server(std::size_t hbm_budget, int max_inflight, bool use_graphs, int st
   check(cudaGetDevice(&device_), "cudaGetDevice");
   stats_.budget = hbm_budget;
   thread_ = std::thread([this] { loop(); });
-  for (int i = 0; i < stagers; ++i) stagers_.emplace_back([this] { stager(); });
+  // Each stager copies with its own threads (the staging copies are host-bandwidth bound and one core
+  // reaches a fraction of it), so two stagers' copies proceed side by side.
+  const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+  for (int i = 0; i < stagers; ++i) copiers_.push_back(std::make_unique<HostCopier>(std::clamp(hw / stagers, 1, 8)));
+  for (int i = 0; i < stagers; ++i) stagers_.emplace_back([this, i] { stager(*copiers_[i]); });
 }
 
 Server::~Server() {
@@ -496,7 +477,7 @@ void Server::fail_request(Request& r, const std::string& error, Status status) {
 
 // Stager: stage the input into the workspace (pageable callers), allocate the workspace if it is
 // new, and enqueue the request's device work.
-void Server::start_request(std::uint64_t ticket) {
+void Server::start_request(std::uint64_t ticket, HostCopier& copier) {
   Request* r = nullptr;
   Workspace* w = nullptr;
   const Geometry* g = nullptr;
@@ -515,7 +496,7 @@ void Server::start_request(std::uint64_t ticket) {
     }
     if (!r->in_pinned) {
       if (!w->in.get()) w->in = PinnedBuf<float>(g->holo_floats);
-      parallel_copy(w->in.get(), r->caller_in, g->holo_floats * sizeof(float));
+      copier.copy(w->in.get(), r->caller_in, g->holo_floats * sizeof(float));
     }
     if (!r->out_pinned && !w->out.get()) w->out = PinnedBuf<float>(g->volume);
     if (fresh) {
@@ -524,6 +505,14 @@ void Server::start_request(std::uint64_t ticket) {
       ++stats_.workspaces_created;
     }
     launch(*r, *w, *g);
+    // While the device works: the page faults of a fresh output buffer (its contents are unspecified
+    // until wait returns) are taken now instead of during the copy out, which waits for this.
+    if (!r->out_pinned) copier.touch(r->caller_out, g->volume * sizeof(float));
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      r->started = true;
+    }
+    started_.notify_all();
   } catch (const std::exception& e) {
     std::unique_ptr<Workspace> failed;
     {
@@ -534,7 +523,9 @@ void Server::start_request(std::uint64_t ticket) {
       }
       const auto* qe = dynamic_cast<const Error*>(&e);
       fail_request(*r, e.what(), qe ? qe->status : kInternal);
+      r->started = true;  // no drain may wait on it
     }
+    started_.notify_all();
     // Freeing device memory waits for the device, including other requests' completion callbacks,
     // which take the lock: it is released first.
     failed.reset();
@@ -543,17 +534,18 @@ void Server::start_request(std::uint64_t ticket) {
 
 // Stager: copy a finished request's volume out of the workspace's staging buffer, then release the
 // workspace.
-void Server::drain_request(std::uint64_t ticket) {
+void Server::drain_request(std::uint64_t ticket, HostCopier& copier) {
   Request* r = nullptr;
   const Workspace* w = nullptr;
   std::size_t bytes = 0;
   {
-    std::lock_guard<std::mutex> lk(mu_);
+    std::unique_lock<std::mutex> lk(mu_);
     r = requests_.at(ticket).get();
     w = workspaces_.at(r->workspace).get();
     bytes = geoms_[r->geometry]->volume * sizeof(float);
+    started_.wait(lk, [r] { return r->started; });  // the start job may still be faulting caller_out in
   }
-  parallel_copy(r->caller_out, w->out.get(), bytes);
+  copier.copy(r->caller_out, w->out.get(), bytes);
   std::lock_guard<std::mutex> lk(mu_);
   r->finished = Clock::now();
   r->done = true;
@@ -564,7 +556,7 @@ void Server::drain_request(std::uint64_t ticket) {
   done_.notify_all();
 }
 
-void Server::stager() {
+void Server::stager(HostCopier& copier) {
   cudaSetDevice(device_);
   std::unique_lock<std::mutex> lk(mu_);
   for (;;) {
@@ -574,9 +566,9 @@ void Server::stager() {
     jobs_.pop_front();
     lk.unlock();
     if (job.kind == Job::start) {
-      start_request(job.ticket);
+      start_request(job.ticket, copier);
     } else {
-      drain_request(job.ticket);
+      drain_request(job.ticket, copier);
     }
     lk.lock();
   }

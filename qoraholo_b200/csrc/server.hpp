@@ -3,6 +3,8 @@
 // form is one Pipeline per geometry used by one caller at a time (src/cuda/pipeline.cu:12-147).
 #pragma once
 
+#include "host_copy.hpp"
+
 #include <chrono>
 #include <condition_variable>
 #include <cstddef>
@@ -128,8 +130,9 @@ class Server {
   void remove_geometry(int geometry);
   // Queues one request: holograms (count, N, N) on the host -> index (nz, n, n) into `host_out`.
   // Both may be pageable (staged through the workspace's page-locked buffers by the server's stager
-  // threads) or page-locked (copied directly). Both must stay valid until wait() returns. Returns a
-  // ticket.
+  // threads) or page-locked (copied directly). Both must stay valid until wait() returns; the contents
+  // of a pageable `host_out` are unspecified until then (its pages are faulted in while the request
+  // runs). Returns a ticket.
   std::uint64_t submit(int geometry, const float* host_holo, float* host_out);
   // Blocks until the request is done; its filled fraction and timings. Throws the request's error.
   void wait(std::uint64_t ticket, double* filled, RequestTimes* times);
@@ -169,6 +172,7 @@ class Server {
     const float* caller_in = nullptr;
     float* caller_out = nullptr;
     bool in_pinned = false, out_pinned = false;
+    bool started = false;  // the start job is done with caller_out (its pages faulted in): drain may copy
     Clock::time_point submitted, admitted, finished;
     int workspace = -1;
     bool fresh_workspace = false;  // admitted with a workspace still to be allocated
@@ -191,9 +195,9 @@ class Server {
 
   static void CUDART_CB on_complete(void* data);
   void loop();
-  void stager();
-  void start_request(std::uint64_t ticket);
-  void drain_request(std::uint64_t ticket);
+  void stager(HostCopier& copier);
+  void start_request(std::uint64_t ticket, HostCopier& copier);
+  void drain_request(std::uint64_t ticket, HostCopier& copier);
   void launch(const Request& r, Workspace& w, const Geometry& g);
   void fail_request(Request& r, const std::string& error, Status status);
   static std::unique_ptr<Workspace> make_workspace(const Geometry& g);
@@ -203,6 +207,7 @@ class Server {
   std::condition_variable wake_;   // scheduler: submissions, completions, released workspaces, stop
   std::condition_variable done_;   // waiters
   std::condition_variable jobs_cv_;  // stagers
+  std::condition_variable started_;  // drains waiting for their request's start job
   int device_ = 0;
   bool use_graphs_;
   bool exclusive_ = false;  // serialise the requests' kernels (copies still overlap)
@@ -222,6 +227,7 @@ class Server {
   std::uint64_t next_ticket_ = 1;
   ServerStats stats_;
   std::thread thread_;
+  std::vector<std::unique_ptr<HostCopier>> copiers_;  // one per stager
   std::vector<std::thread> stagers_;
 };
 
