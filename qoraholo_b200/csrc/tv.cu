@@ -583,10 +583,13 @@ __global__ void __launch_bounds__(256)
 //   z_{k+1}    rows y0   .. y0+TY
 //   p, r_{k+2} rows y0   .. y0+TY-1   (dual step k + 1, to HBM)
 // In z the march runs three planes ahead of its output. Iteration q computes z_k of plane q+2,
-// dual step k of plane q+1, z_{k+1} of plane q+1 and dual step k+1 of plane q, while r_k and b of
-// plane q+3 stream in (cp.async). Shared memory: r_k ring (3 planes x 3 components x TY+4 rows),
-// b ring (3 x TY+3), z_k (2 x TY+3), r_{k+1} (z component of 2 planes, y and x of one, TY+2 rows
-// each), z_{k+1} (2 x TY+1): 20 TY + 61 rows of nx floats. The own rows of every phase belong to
+// dual step k of plane q+1, z_{k+1} of plane q+1 and dual step k+1 of plane q. The inputs arrive as
+// TMA box loads issued after the iteration's second barrier, when the slots they go to have been
+// read: r_k and b of plane q+3 (used from the next iteration on) and p_k of plane q+2 (used by the
+// next iteration's dual step k). Shared memory, in rows of the pitch (nx rounded up to 32 floats):
+// r_k (2 planes x 3 components x TY+4 rows), b ring (3 x TY+3), z_k (2 x TY+3), r_{k+1} (z
+// component of 2 planes, y and x of one, TY+2 rows each), z_{k+1} (2 x TY+1), p_k (3 x TY+2):
+// 20 TY + 55 rows. The own rows of every phase belong to
 // one thread row each (four x values per thread), and the halo rows of z_k and of dual step k are
 // spread over all threads with the same point -> thread map in both phases, so the step-k dual
 // reads only z_k values that its own thread wrote in this iteration or that a barrier separates
@@ -607,6 +610,7 @@ struct Fgp2Args {
 struct Fgp2Maps {
   CUtensorMap r[3];
   CUtensorMap b;
+  CUtensorMap p[3];  // p_k, boxes of (pitch x TY+2 rows); not read on the first step
 };
 
 // Waits of k_fgp2 that ran out (a box load that never completed); read by tv_wait_timeouts().
@@ -636,7 +640,7 @@ __device__ __forceinline__ void fgp_dual_at(float c, float cz, float cy, float c
   tv_dual_step(g, step, momentum, p, r);
 }
 
-constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(ty) + 61; }
+constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(ty) + 55; }
 // Threads per CTA the two-step kernel is compiled for (nx / 4 x TY must stay within it).
 constexpr int fgp2_threads(int ty) { return ty == 8 ? 512 : 256; }
 
@@ -663,8 +667,9 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   // from smem2), then the three ring-slot mbarriers.
   const int P = A.pitch;
   const int RKP = RK_ROWS * P, BP = B_ROWS * P, R1P = R1_ROWS * P, Z1P = Z1_ROWS * P;
-  const int OB = 9 * RKP, OZ = OB + 3 * BP, OR = OZ + 2 * BP, OZ1 = OR + 4 * R1P;
-  std::uint64_t* const bars = reinterpret_cast<std::uint64_t*>(smem2 + OZ1 + 2 * Z1P);
+  const int OB = 6 * RKP, OZ = OB + 3 * BP, OR = OZ + 2 * BP, OZ1 = OR + 4 * R1P, OPK = OZ1 + 2 * Z1P;
+  // mbarriers: 0 and 1 for the plane loads (r_k and b) of even and odd planes, 2 for p_k.
+  std::uint64_t* const bars = reinterpret_cast<std::uint64_t*>(smem2 + OPK + 3 * R1P);
   // Own-row offsets within a slot: r_k row ty+2 (rows start at y0-2); b, z_k, r_{k+1} row ty+1
   // (rows start at y0-1); z_{k+1} row ty (rows start at y0).
   const int own_rk = (ty + 2) * P + x0;
@@ -674,7 +679,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
     for (int i = 0; i < 3; ++i) tma::mbar_init(bars + i, 1);
   }
   __syncthreads();
-  unsigned phases = 0;  // bit s: parity of the next completion of slot s's mbarrier
+  unsigned phases = 0;  // bit i: parity of the next completion of mbarrier i
   // Halo points (the same point -> thread map in the z_k and dual-k phases): v = linear + j
   // nthreads over the rows y0-1 (side 0), y0+TY (1), y0+TY+1 (2); row of z_k / b: 0, TY+1, TY+2.
   int hz_side[HALO_Z], hz_x[HALO_Z];
@@ -697,20 +702,27 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
     const bool own = y < ny;
     const std::size_t own_g = static_cast<std::size_t>(y) * nx + x0;  // within a plane
 
-    // Box loads of one plane into ring slot s by thread 0: r_k rows y0-2 .. y0+TY+1 (`comps`
-    // components) and b rows y0-1 .. y0+TY+1, counted on the slot's mbarrier. Rows outside the
-    // volume arrive as zeros and are never read.
-    const auto issue = [&](int z, int s, int comps, bool with_b) {
+    // Box loads by thread 0, counted on an mbarrier. A plane z: r_k rows y0-2 .. y0+TY+1 (`comps`
+    // components) into r_k slot z&1 and b rows y0-1 .. y0+TY+1 into b slot `sb`, on mbarrier z&1;
+    // p_k of plane z, rows y0-1 .. y0+TY, into the p_k slot on mbarrier 2. Rows outside the volume
+    // arrive as zeros and are never read.
+    const auto issue = [&](int z, int sb, int comps, bool with_b) {
       tma::fence_async_shared();
-      tma::mbar_expect(bars + s, static_cast<unsigned>((comps * RK_ROWS + (with_b ? B_ROWS : 0)) * P * 4));
-      for (int c = 0; c < comps; ++c) tma::load_3d(smem2 + (s * 3 + c) * RKP, &M.r[c], 0, y0 - 2, z, bars + s);
-      if (with_b) tma::load_3d(smem2 + OB + s * BP, &M.b, 0, y0 - 1, z, bars + s);
+      std::uint64_t* bar = bars + (z & 1);
+      tma::mbar_expect(bar, static_cast<unsigned>((comps * RK_ROWS + (with_b ? B_ROWS : 0)) * P * 4));
+      for (int c = 0; c < comps; ++c) tma::load_3d(smem2 + ((z & 1) * 3 + c) * RKP, &M.r[c], 0, y0 - 2, z, bar);
+      if (with_b) tma::load_3d(smem2 + OB + sb * BP, &M.b, 0, y0 - 1, z, bar);
     };
-    // Bounded wait for slot s (every thread), then its phase bit flips.
-    const auto wait_slot = [&](int s) {
-      const bool ok = tma::mbar_wait(bars + s, (phases >> s) & 1u, &g_fgp2_timeouts);
-      phases ^= 1u << s;
-      return ok;
+    const auto issue_pk = [&](int z) {
+      tma::fence_async_shared();
+      tma::mbar_expect(bars + 2, static_cast<unsigned>(3 * R1_ROWS * P * 4));
+      for (int c = 0; c < 3; ++c) tma::load_3d(smem2 + OPK + c * R1P, &M.p[c], 0, y0 - 1, z, bars + 2);
+    };
+    // Bounded wait on mbarrier i (every thread), then its phase bit flips.
+    const auto wait_bar = [&](int i) {
+      const bool done = tma::mbar_wait(bars + i, (phases >> i) & 1u, &g_fgp2_timeouts);
+      phases ^= 1u << i;
+      return done;
     };
     const auto mod3 = [](int z) { return ((z % 3) + 3) % 3; };
     // Iteration q needs r_k and b of planes up to q+2 (the z component of q+1 for z_k of q+2).
@@ -719,55 +731,35 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
       if (z0 >= 1) issue(z0 - 1, mod3(z0 - 1), 3, true);
     }
     bool ok = true;
-    if (z0 >= 2) ok = wait_slot(mod3(z0 - 2)) && ok;
+    if (z0 >= 2) ok = wait_bar((z0 - 2) & 1) && ok;
 
     float cr[3][VEC] = {}, cp[3][VEC] = {};  // r_{k+1}, p_{k+1} of this thread's points of plane q
     float nr[3][VEC] = {}, np[3][VEC] = {};  // the same of plane q+1
-    int m0 = mod3(z0 - 3);                   // ring slot of plane q (and of q+3)
+    int m0 = mod3(z0 - 3);                   // b slot of plane q (and of q+3)
     for (int q = z0 - 3; q < zend; ++q, m0 = m0 == 2 ? 0 : m0 + 1) {
       const int a2 = q + 2, a1 = q + 1;
-      const int m1 = m0 == 2 ? 0 : m0 + 1;  // slot of q+1
-      const int m2 = m0 == 0 ? 2 : m0 - 1;  // slot of q+2
-      const int par = q & 1;                // parity of q (and q+2); q+1 has par ^ 1
+      const int m1 = m0 == 2 ? 0 : m0 + 1;  // b slot of q+1
+      const int m2 = m0 == 0 ? 2 : m0 - 1;  // b slot of q+2
+      const int par = q & 1;                // parity of q and q+2 (r_k slot, z_k, z_{k+1}); q+1 has par ^ 1
       const bool do_a = a2 >= 0 && a2 < nz;                  // z_k of plane a2
       const bool do_b = a1 >= 0 && a1 >= z0 - 1 && a1 < nz;  // dual step k on plane a1
       const bool do_c = a1 >= z0 && a1 < nz;                 // z_{k+1} of plane a1
       const bool do_d = q >= z0;                             // dual step k+1 on plane q
-      // p_k of plane a1 (own points, then the halo points), loaded ahead of the wait.
-      float pk[3][VEC] = {};
-      float ph[HALO][3] = {};
-      if (!FIRST && do_b) {
-        const std::size_t po = a1 * nxy;
-        if (own) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) Vec<VEC>::load(A.pin[c] + po + own_g, pk[c]);
-        }
-#pragma unroll
-        for (int h = 0; h < HALO; ++h) {
-          const int side = hz_side[h];
-          const int yy = side == 0 ? y0 - 1 : y0 + TY;
-          if ((side == 0 || side == 1) && yy >= 0 && yy < ny) {
-            const std::size_t at = po + static_cast<std::size_t>(yy) * nx + hz_x[h];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) ph[h][c] = A.pin[c][at];
-          }
-        }
-      }
-      if (a2 >= 0 && a2 <= zmax) ok = wait_slot(m2) && ok;  // plane a2 (loaded one iteration ago)
+      const bool wait_plane = a2 >= 0 && a2 <= zmax;  // plane a2, loaded one iteration ago
+      if (wait_plane) ok = wait_bar(par) && ok;
       if (__syncthreads_or(!ok)) {
         // A load never completed: leave with the timeout counted (every thread takes this exit),
         // after one more bounded wait for the load in flight.
-        if (a2 >= 0 && a2 <= zmax) tma::mbar_wait(bars + m2, ((phases >> m2) & 1u) ^ 1u, &g_fgp2_timeouts);
+        if (wait_plane) tma::mbar_wait(bars + par, ((phases >> par) & 1u) ^ 1u, &g_fgp2_timeouts);
         return;
       }
-      if (linear == 0 && q + 3 <= zmax) issue(q + 3, m0, 3, true);
 
       if (do_a) {
         const int a = a2;
-        const float* Rz = smem2 + (m2 * 3 + 0) * RKP;
-        const float* Rzb = smem2 + (m1 * 3 + 0) * RKP;  // plane a-1; not read on plane 0
-        const float* Ry = smem2 + (m2 * 3 + 1) * RKP;
-        const float* Rx = smem2 + (m2 * 3 + 2) * RKP;
+        const float* Rz = smem2 + (par * 3 + 0) * RKP;
+        const float* Rzb = smem2 + ((par ^ 1) * 3 + 0) * RKP;  // plane a-1; not read on plane 0
+        const float* Ry = smem2 + (par * 3 + 1) * RKP;
+        const float* Rx = smem2 + (par * 3 + 2) * RKP;
         const float* B = smem2 + OB + m2 * BP;
         float* Z = smem2 + OZ + par * BP;
         {
@@ -803,11 +795,15 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
         }
       }
 
+      // p_k of plane a1, loaded during the previous iteration.
+      const bool wait_pk = !FIRST && do_b;
+      if (wait_pk) ok = wait_bar(2) && ok;
+      const float* PK = smem2 + OPK;
       if (do_b) {
         const int a = a1;
         const float* Zc = smem2 + OZ + (par ^ 1) * BP;
         const float* Zn = smem2 + OZ + par * BP;  // plane a+1; read only below plane nz-1
-        const float* R = smem2 + (m1 * 3) * RKP;
+        const float* R = smem2 + ((par ^ 1) * 3) * RKP;
         float* Rz1 = smem2 + OR + (par ^ 1) * R1P;
         float* Ry1 = smem2 + OR + 2 * R1P;
         float* Rx1 = smem2 + OR + 3 * R1P;
@@ -819,9 +815,12 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
           const float right =
               (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? Zc[own_b + VEC] : from_lane;
-          float rv[3][VEC];
+          float rv[3][VEC], pk[3][VEC];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) Vec<VEC>::load(R + c * RKP + own_rk, rv[c]);
+          for (int c = 0; c < 3; ++c) {
+            Vec<VEC>::load(R + c * RKP + own_rk, rv[c]);
+            if (!FIRST) Vec<VEC>::load(PK + c * R1P + own_b, pk[c]);
+          }
           if (own) {
 #pragma unroll
             for (int k = 0; k < VEC; ++k) {
@@ -862,7 +861,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
               r[c] = R[c * RKP + i + P];
-              p[c] = FIRST ? r[c] : ph[h][c];
+              p[c] = FIRST ? r[c] : PK[c * R1P + i];
             }
             fgp_dual_at(c0, cz, cy, cx, a, yy, x, nz, ny, nx, A.step, A.m1, p, r);
             Rz1[i] = r[0];
@@ -871,7 +870,18 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           }
         }
       }
-      __syncthreads();  // r_{k+1} of plane a1 complete
+      if (__syncthreads_or(!ok)) {  // r_{k+1} of plane a1 complete
+        if (wait_pk) tma::mbar_wait(bars + 2, ((phases >> 2) & 1u) ^ 1u, &g_fgp2_timeouts);
+        return;
+      }
+      // Every thread is past z_k of a2 and dual step k of a1: r_k of a1 (slot par ^ 1) and p_k are
+      // free for plane q+3 and p_k of a2; b of q+3 goes into the slot of b of q (last read one
+      // iteration ago).
+      if (linear == 0) {
+        if (q + 3 <= zmax) issue(q + 3, m0, 3, true);
+        // exactly the planes whose dual step k the next iteration runs (and waits for): do_b of q+1
+        if (!FIRST && a2 >= 0 && a2 >= z0 - 1 && a2 < nz && a2 <= zend) issue_pk(a2);
+      }
 
       float zn[VEC] = {};  // z_{k+1} of this thread's points of plane a1
       if (do_c) {
@@ -1119,6 +1129,7 @@ void launch_fgp2_t(const Fgp2Args& a, const float* const rin[3], const float* b,
   Fgp2Maps maps;
   for (int c = 0; c < 3; ++c) maps.r[c] = volume_tensor_map(rin[c], a.nx, a.ny, a.nz, a.pitch, TY + 4);
   maps.b = volume_tensor_map(b, a.nx, a.ny, a.nz, a.pitch, TY + 3);
+  for (int c = 0; c < 3; ++c) maps.p[c] = FIRST ? maps.r[c] : volume_tensor_map(a.pin[c], a.nx, a.ny, a.nz, a.pitch, TY + 2);
   kernel<<<grid, dim3(a.nx / 4, TY), fgp2_smem(a.nx, TY), s>>>(a, maps);
   check_launch("fgp two steps");
 }
