@@ -604,7 +604,8 @@ struct Fgp2Args {
   int pitch;  // shared-memory row length: nx rounded up to 32 floats (the box width)
   int ytiles;
   float lambda, step;
-  float m1, m2;  // momenta of steps k and k + 1
+  float m1, m2;     // momenta of steps k and k + 1
+  float neg_zero;  // -0.0f, the addend of the packed products (a value the compiler cannot see)
 };
 // Box-load maps of r_k (on the first step p_0), boxes of (pitch x TY+4 rows), and of b (pitch x TY+3).
 struct Fgp2Maps {
@@ -638,6 +639,87 @@ __device__ __forceinline__ void fgp_dual_at(float c, float cz, float cy, float c
   g[1] = y < ny - 1 ? __fsub_rn(c, cy) : 0.0f;
   g[2] = x < nx - 1 ? __fsub_rn(c, cx) : 0.0f;
   tv_dual_step(g, step, momentum, p, r);
+}
+
+// The same two operations on a pair of neighbouring x points with Blackwell's packed FP32 add and
+// multiply (two correctly rounded operations per instruction, each as the scalar __fadd_rn /
+// __fmul_rn). A term a guard drops is added as -0.0 or subtracted as +0.0 instead, which leaves
+// every value (signed zeros included) unchanged, so the pair results equal the scalar ones bit for
+// bit. z and y guards are the same for both points; x guards come as the points' own flags.
+//
+// Products must round on their own: ptxas contracts a packed multiply followed by a packed add into
+// one FMA even when both carry explicit rounding modes, and also when the product is written as an
+// FMA with a literal -0.0 addend (it folds that back into a multiply); measured on this toolkit, it
+// changes results in the last bit. So a product is an FMA whose -0.0 addend (`nz`) comes from a
+// kernel argument: RN(a b + -0) = RN(a b) for every a b, signed zeros included, and an FMA result
+// is never fused into a later add.
+__device__ __forceinline__ unsigned long long pack2(float2 a) {
+  unsigned long long v;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(a.x), "f"(a.y));
+  return v;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long v) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(v));
+  return a;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)));
+  return unpack2(d);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return add2(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b, float2 nz) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)), "l"(pack2(nz)));
+  return unpack2(d);
+}
+
+// Primal points of x and x+1: vxm is the x component of the dual at x-1 and x (dropped where the
+// point is x = 0); last_x1 marks x+1 = nx-1 (its +x term dropped).
+__device__ __forceinline__ float2 fgp_primal_pair(bool zhi, bool zlo, bool yhi, bool ylo, bool first_x0,
+                                                  bool last_x1, float2 vz, float2 vzb, float2 vy, float2 vym,
+                                                  float2 vx, float2 vxm, float2 vb, float lambda, float2 nz) {
+  float2 sacc = make_float2(0.0f, 0.0f);
+  if (zhi) sacc = add2(sacc, vz);   // z < nz - 1
+  if (zlo) sacc = sub2(sacc, vzb);  // z > 0
+  if (yhi) sacc = add2(sacc, vy);   // y < ny - 1
+  if (ylo) sacc = sub2(sacc, vym);  // y > 0
+  if (last_x1) vx.y = -0.0f;        // x + 1 == nx - 1
+  sacc = add2(sacc, vx);
+  if (first_x0) vxm.x = 0.0f;  // x == 0
+  sacc = sub2(sacc, vxm);
+  const float2 t = sub2(vb, mul2(make_float2(lambda, lambda), sacc, nz));
+  return make_float2(t.x > 0.0f ? t.x : 0.0f, t.y > 0.0f ? t.y : 0.0f);
+}
+
+// Dual steps at x and x+1 (tv_dual_step on each point, the same operations).
+__device__ __forceinline__ void fgp_dual_pair(float2 c, float2 cz, float2 cy, float2 cx, bool zhi, bool yhi,
+                                              bool last_x1, float step, float momentum, float2 p[3], float2 r[3],
+                                              float2 nz) {
+  float2 g[3];
+  g[0] = zhi ? sub2(c, cz) : make_float2(0.0f, 0.0f);
+  g[1] = yhi ? sub2(c, cy) : make_float2(0.0f, 0.0f);
+  g[2] = sub2(c, cx);
+  if (last_x1) g[2].y = 0.0f;
+  const float2 st = make_float2(step, step);
+  float2 q[3];
+  float2 norm2 = make_float2(0.0f, 0.0f);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    q[a] = add2(r[a], mul2(st, g[a], nz));
+    norm2 = add2(norm2, mul2(q[a], q[a], nz));
+  }
+  // 1 / sqrt(norm2) per point, as tv_dual_step.
+  const float2 scale = make_float2(norm2.x > 1.0f ? __frcp_rn(__fsqrt_rn(norm2.x)) : 1.0f,
+                                   norm2.y > 1.0f ? __frcp_rn(__fsqrt_rn(norm2.y)) : 1.0f);
+  const float2 m = make_float2(momentum, momentum);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float2 next = mul2(q[a], scale, nz);
+    r[a] = add2(next, mul2(m, sub2(next, p[a]), nz));
+    p[a] = next;
+  }
 }
 
 constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(ty) + 55; }
@@ -675,6 +757,47 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   const int own_rk = (ty + 2) * P + x0;
   const int own_b = (ty + 1) * P + x0;
   const int own_z1 = ty * P + x0;
+  // The thread's four own points run as two pairs of packed operations; x guards per point.
+  const bool x_first = x0 == 0;       // point 0 is x = 0
+  const bool x_last = x0 + VEC == nx;  // point 3 is x = nx - 1
+  const auto f2 = [](float a, float b) { return make_float2(a, b); };
+  const float2 nzero = make_float2(A.neg_zero, A.neg_zero);
+  // Primal points of the own row of plane z (y given); left = x component of the dual at x0-1.
+  const auto primal4 = [&](int z, int yy, const float* vz, const float* vzb, const float* vy, const float* vym,
+                           const float* vx, float left, const float* vb, float* out) {
+    const bool zhi = z < nz - 1, zlo = z > 0, yhi = yy < ny - 1, ylo = yy > 0;
+    const float2 o0 = fgp_primal_pair(zhi, zlo, yhi, ylo, x_first, false, f2(vz[0], vz[1]), f2(vzb[0], vzb[1]),
+                                      f2(vy[0], vy[1]), f2(vym[0], vym[1]), f2(vx[0], vx[1]), f2(left, vx[0]),
+                                      f2(vb[0], vb[1]), A.lambda, nzero);
+    const float2 o1 = fgp_primal_pair(zhi, zlo, yhi, ylo, false, x_last, f2(vz[2], vz[3]), f2(vzb[2], vzb[3]),
+                                      f2(vy[2], vy[3]), f2(vym[2], vym[3]), f2(vx[2], vx[3]), f2(vx[1], vx[2]),
+                                      f2(vb[2], vb[3]), A.lambda, nzero);
+    out[0] = o0.x, out[1] = o0.y, out[2] = o1.x, out[3] = o1.y;
+  };
+  // Dual steps of the own points (row yy) of plane z from primal values c, +z (cz), +y (cy) and the
+  // primal value right of the last point; p and r updated in place.
+  const auto dual4 = [&](int z, int yy, const float* c, const float* cz, const float* cy, float right,
+                         float momentum, float (*pv)[VEC], float (*rv)[VEC]) {
+    const bool zhi = z < nz - 1, yhi = yy < ny - 1;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k0 = 2 * h;
+      float2 pp[3], rr[3];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        pp[cc] = f2(pv[cc][k0], pv[cc][k0 + 1]);
+        rr[cc] = f2(rv[cc][k0], rv[cc][k0 + 1]);
+      }
+      fgp_dual_pair(f2(c[k0], c[k0 + 1]), f2(cz[k0], cz[k0 + 1]), f2(cy[k0], cy[k0 + 1]),
+                    f2(c[k0 + 1], h == 0 ? c[2] : right), zhi, yhi, h == 1 && x_last, A.step, momentum, pp, rr,
+                    nzero);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        pv[cc][k0] = pp[cc].x, pv[cc][k0 + 1] = pp[cc].y;
+        rv[cc][k0] = rr[cc].x, rv[cc][k0 + 1] = rr[cc].y;
+      }
+    }
+  };
   if (linear == 0) {
     for (int i = 0; i < 3; ++i) tma::mbar_init(bars + i, 1);
   }
@@ -772,12 +895,8 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           Vec<VEC>::load(B + own_b, vb);
           const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
           const float left = (x0 > 0 && lane == 0) ? Rx[own_rk - 1] : from_lane;
-          float out[VEC];
-#pragma unroll
-          for (int k = 0; k < VEC; ++k)
-            out[k] = own ? fgp_primal_at(a, y, x0 + k, nz, ny, nx, vz[k], vzb[k], vy[k], vym[k], vx[k],
-                                         k == 0 ? left : vx[k > 0 ? k - 1 : 0], vb[k], A.lambda)
-                         : 0.0f;
+          float out[VEC] = {};
+          if (own) primal4(a, y, vz, vzb, vy, vym, vx, left, vb, out);
           Vec<VEC>::store(Z + own_b, out);
         }
 #pragma unroll
@@ -823,21 +942,13 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           }
           if (own) {
 #pragma unroll
-            for (int k = 0; k < VEC; ++k) {
-              float p[3], r[3];
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-              for (int c = 0; c < 3; ++c) {
-                r[c] = rv[c][k];
-                p[c] = FIRST ? rv[c][k] : pk[c][k];
+              for (int k = 0; k < VEC; ++k) {
+                nr[c][k] = rv[c][k];
+                np[c][k] = FIRST ? rv[c][k] : pk[c][k];
               }
-              fgp_dual_at(zc[k], zz[k], zy[k], k == VEC - 1 ? right : zc[k < VEC - 1 ? k + 1 : 0], a, y, x0 + k, nz, ny,
-                          nx, A.step, A.m1, p, r);
-#pragma unroll
-              for (int c = 0; c < 3; ++c) {
-                np[c][k] = p[c];
-                nr[c][k] = r[c];
-              }
-            }
+            dual4(a, y, zc, zz, zy, right, A.m1, np, nr);
             Vec<VEC>::store(Rz1 + own_b, nr[0]);
             Vec<VEC>::store(Ry1 + own_b, nr[1]);
             Vec<VEC>::store(Rx1 + own_b, nr[2]);
@@ -902,11 +1013,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           Vec<VEC>::load(B + own_b, vb);
           const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
           const float left = (x0 > 0 && lane == 0) ? Rx[own_b - 1] : from_lane;
-#pragma unroll
-          for (int k = 0; k < VEC; ++k)
-            zn[k] = own ? fgp_primal_at(a, y, x0 + k, nz, ny, nx, vz[k], vzb[k], vy[k], vym[k], vx[k],
-                                        k == 0 ? left : vx[k > 0 ? k - 1 : 0], vb[k], A.lambda)
-                        : 0.0f;
+          if (own) primal4(a, y, vz, vzb, vy, vym, vx, left, vb, zn);
           Vec<VEC>::store(Z + own_z1, zn);
         }
         if (y0 + TY < ny) {  // row y0+TY, spread over all threads
@@ -932,18 +1039,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
         const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
         const float right = (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? Zc[own_z1 + VEC] : from_lane;
         if (own) {
-#pragma unroll
-          for (int k = 0; k < VEC; ++k) {
-            float p[3] = {cp[0][k], cp[1][k], cp[2][k]};
-            float r[3] = {cr[0][k], cr[1][k], cr[2][k]};
-            fgp_dual_at(zc[k], zn[k], zy[k], k == VEC - 1 ? right : zc[k < VEC - 1 ? k + 1 : 0], q, y, x0 + k, nz, ny,
-                        nx, A.step, A.m2, p, r);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              cp[c][k] = p[c];
-              cr[c][k] = r[c];
-            }
-          }
+          dual4(q, y, zc, zn, zy, right, A.m2, cp, cr);
           const std::size_t at = q * nxy + own_g;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
@@ -1153,6 +1249,7 @@ void launch_fgp2(bool first, bool last, Fgp2Args a, const float* const rin[3], c
                  cudaStream_t s) {
   require(fgp2_fits(a.nx, sh.ty), "tv: two-step FGP shape out of range");
   a.pitch = fgp2_pitch(a.nx);
+  a.neg_zero = -0.0f;
   if (sh.ty == 8) {
     launch_fgp2_rows<8>(first, last, a, rin, b, sh.grid, s);
   } else if (sh.ty == 4) {
