@@ -731,9 +731,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   extern __shared__ __align__(128) float smem2[];
   constexpr int VEC = 4;
   constexpr int RK_ROWS = TY + 4, B_ROWS = TY + 3, R1_ROWS = TY + 2, Z1_ROWS = TY + 1;
-  constexpr int HALO = (8 + TY - 1) / TY;     // halo points of dual step k per thread: 2 nx over nx / 4 * TY threads
-  constexpr int HALO_Z = (12 + TY - 1) / TY;  // halo points of z_k per thread: 3 nx
-  constexpr int HALO_Z1 = (4 + TY - 1) / TY;  // halo points of z_{k+1} per thread: nx
+  constexpr int HALO = (8 + TY - 1) / TY;  // halo pair slots per thread: 2 nx over nx / 4 * TY threads
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   const int tx = static_cast<int>(threadIdx.x);
   const int ty = static_cast<int>(threadIdx.y);
@@ -803,15 +801,20 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   }
   __syncthreads();
   unsigned phases = 0;  // bit i: parity of the next completion of mbarrier i
-  // Halo points (the same point -> thread map in the z_k and dual-k phases): v = linear + j
-  // nthreads over the rows y0-1 (side 0), y0+TY (1), y0+TY+1 (2); row of z_k / b: 0, TY+1, TY+2.
-  int hz_side[HALO_Z], hz_x[HALO_Z];
+  // Halo rows as pairs of points (x, x+1), x even: 2 nx pair slots, slot u = linear + j nthreads.
+  // Slots below 3 nx / 2 are the z_k halo rows y0-1 (side 0), y0+TY (1), y0+TY+1 (2) -- z_k / b row
+  // 0, TY+1, TY+2 -- of which those below nx are also the dual-k halo rows, so each such pair's z_k is
+  // its own thread's write; the rest (side 3) are row y0+TY of z_{k+1}.
+  const int half = nx / 2;
+  int hz_side[HALO], hz_x[HALO];
 #pragma unroll
-  for (int j = 0; j < HALO_Z; ++j) {
-    const int v = linear + j * nthreads;
-    hz_side[j] = v < 3 * nx ? v / nx : -1;
-    hz_x[j] = v - max(hz_side[j], 0) * nx;
+  for (int j = 0; j < HALO; ++j) {
+    const int u = linear + j * nthreads;
+    hz_side[j] = u < 2 * nx ? u / half : -1;
+    hz_x[j] = 2 * (u - max(hz_side[j], 0) * half);
   }
+  const auto ld2 = [](const float* p) { return *reinterpret_cast<const float2*>(p); };
+  const auto st2 = [](float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; };
 
   const long long units = static_cast<long long>(A.ytiles) * nz;
   const long long u_end = units * (blockIdx.x + 1) / gridDim.x;
@@ -900,16 +903,18 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           Vec<VEC>::store(Z + own_b, out);
         }
 #pragma unroll
-        for (int j = 0; j < HALO_Z; ++j) {
+        for (int j = 0; j < HALO; ++j) {
           const int side = hz_side[j];
           const int x = hz_x[j];
           const int zi = side == 0 ? 0 : TY + side;
           const int yy = y0 - 1 + zi;
-          if (side >= 0 && yy >= 0 && yy < ny) {
+          if (side >= 0 && side <= 2 && yy >= 0 && yy < ny) {
             const int i = (zi + 1) * P + x;  // r_k row of yy
-            const float vxm = x > 0 ? Rx[i - 1] : 0.0f;
-            Z[zi * P + x] = fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - P], Rx[i], vxm,
-                                          B[zi * P + x], A.lambda);
+            const float2 vx = ld2(Rx + i);
+            const float2 o = fgp_primal_pair(a < nz - 1, a > 0, yy < ny - 1, yy > 0, x == 0, x + 1 == nx - 1,
+                                             ld2(Rz + i), ld2(Rzb + i), ld2(Ry + i), ld2(Ry + i - P), vx,
+                                             f2(x > 0 ? Rx[i - 1] : 0.0f, vx.x), ld2(B + zi * P + x), A.lambda, nzero);
+            st2(Z + zi * P + x, o);
           }
         }
       }
@@ -964,20 +969,20 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           const int yy = y0 - 1 + zi;
           if ((side == 0 || side == 1) && yy >= 0 && yy < ny) {
             const int i = zi * P + x;
-            const float c0 = Zc[i];
-            const float cz = a < nz - 1 ? Zn[i] : 0.0f;
-            const float cy = yy < ny - 1 ? Zc[i + P] : 0.0f;
-            const float cx = x < nx - 1 ? Zc[i + 1] : 0.0f;
-            float p[3], r[3];
+            const float2 c0 = ld2(Zc + i);
+            const float2 cz = a < nz - 1 ? ld2(Zn + i) : f2(0.0f, 0.0f);
+            const float2 cy = yy < ny - 1 ? ld2(Zc + i + P) : f2(0.0f, 0.0f);
+            const float2 cx = f2(c0.y, x + 2 < nx ? Zc[i + 2] : 0.0f);
+            float2 p[3], r[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              r[c] = R[c * RKP + i + P];
-              p[c] = FIRST ? r[c] : PK[c * R1P + i];
+              r[c] = ld2(R + c * RKP + i + P);
+              p[c] = FIRST ? r[c] : ld2(PK + c * R1P + i);
             }
-            fgp_dual_at(c0, cz, cy, cx, a, yy, x, nz, ny, nx, A.step, A.m1, p, r);
-            Rz1[i] = r[0];
-            Ry1[i] = r[1];
-            Rx1[i] = r[2];
+            fgp_dual_pair(c0, cz, cy, cx, a < nz - 1, yy < ny - 1, x + 1 == nx - 1, A.step, A.m1, p, r, nzero);
+            st2(Rz1 + i, r[0]);
+            st2(Ry1 + i, r[1]);
+            st2(Rx1 + i, r[2]);
           }
         }
       }
@@ -1016,16 +1021,18 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           if (own) primal4(a, y, vz, vzb, vy, vym, vx, left, vb, zn);
           Vec<VEC>::store(Z + own_z1, zn);
         }
-        if (y0 + TY < ny) {  // row y0+TY, spread over all threads
+        if (y0 + TY < ny) {  // row y0+TY: the pair slots of side 3
           const int yy = y0 + TY;
 #pragma unroll
-          for (int j = 0; j < HALO_Z1; ++j) {
-            const int x = linear + j * nthreads;
-            if (x < nx) {
+          for (int j = 0; j < HALO; ++j) {
+            const int x = hz_x[j];
+            if (hz_side[j] == 3) {
               const int i = (TY + 1) * P + x;
-              const float vxm = x > 0 ? Rx[i - 1] : 0.0f;
-              Z[TY * P + x] =
-                  fgp_primal_at(a, yy, x, nz, ny, nx, Rz[i], Rzb[i], Ry[i], Ry[i - P], Rx[i], vxm, B[i], A.lambda);
+              const float2 vx = ld2(Rx + i);
+              const float2 o = fgp_primal_pair(a < nz - 1, a > 0, yy < ny - 1, yy > 0, x == 0, x + 1 == nx - 1,
+                                               ld2(Rz + i), ld2(Rzb + i), ld2(Ry + i), ld2(Ry + i - P), vx,
+                                               f2(x > 0 ? Rx[i - 1] : 0.0f, vx.x), ld2(B + i), A.lambda, nzero);
+              st2(Z + TY * P + x, o);
             }
           }
         }
