@@ -856,8 +856,9 @@ def main():
     ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "serve", "bpm", "c4"], default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--tv-form", type=int, default=0, choices=[0, 1, 2, 3],
-                    help="with --kernel-case: FGP form (0 tuned/default, 1 stored r, 2 recomputed r, 3 two steps)")
+    ap.add_argument("--tv-form", type=int, default=0, choices=[0, 1, 2, 3, 18, 20, 24],
+                    help="with --kernel-case: FGP form (0 tuned/default, 1 stored r, 2 recomputed r, 3 two steps, "
+                         "16 + rows two steps with that many rows per CTA)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)

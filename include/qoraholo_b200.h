@@ -179,7 +179,8 @@ int qhk_autotune_enable(int enabled);
 /* FGP step form of tv_prox (bitwise the same results): 0 the tuned one, 1 the extrapolated point
  * stored between steps (13 volumes of traffic per step), 2 recomputed from the two previous duals
  * (10 volumes), 3 two steps per pass (13 volumes per two steps; needs rows of a multiple of 4
- * floats and a fourth dual triplet, so qhk_tv_prox_device runs form 1 instead). */
+ * floats, at most 256, and a fourth dual triplet, so qhk_tv_prox_device runs form 1 instead),
+ * 16 + rows: two steps per pass with 2, 4 or 8 rows per CTA (where the volume allows it). */
 int qhk_tv_form(int form);
 /* The tuned choices, one line each, into `buf` (NUL-terminated, truncated to `size`); returns the
  * full length. */

@@ -1175,7 +1175,7 @@ FgpShape fgp_shape_rows(int nz, int ny, int nx, int choice) {
 }
 
 // Forced FGP form (qhk_tv_form): 0 the tuned / default one, 1 stored r, 2 recomputed r, 3 two
-// steps per pass.
+// steps per pass, 16 + rows two steps per pass with that many rows per CTA (2, 4 or 8).
 std::atomic<int> g_fgp_form{0};
 
 // The tuned (or forced) shape; the two-step form only with VEC = 4 and a fourth dual triplet, else
@@ -1193,6 +1193,8 @@ FgpShape fgp_shape(int nz, int ny, int nx, bool two_step) {
         break;
       }
     }
+  } else if (form >= 16) {  // two steps per pass with form - 16 rows, where that fits
+    choice = fgp2_fits(nx, form - 16) ? 2 * kFgpVariantScale + (form - 16) : fallback;
   } else if (form == 1 || form == 2) {
     const int ty = choice / kFgpVariantScale == 2 ? fallback : choice % kFgpVariantScale;
     choice = (form - 1) * kFgpVariantScale + ty;
@@ -1313,8 +1315,9 @@ unsigned long long tv_wait_timeouts() {
 }
 
 void set_tv_form(int form) {
-  require(form >= 0 && form <= 3,
-          "tv: form must be 0 (tuned), 1 (stored r), 2 (recomputed r) or 3 (two steps per pass)");
+  require((form >= 0 && form <= 3) || form == 18 || form == 20 || form == 24,
+          "tv: form must be 0 (tuned), 1 (stored r), 2 (recomputed r), 3 (two steps per pass) or 16 + rows "
+          "(two steps per pass with 2, 4 or 8 rows per CTA)");
   g_fgp_form.store(form);
 }
 

@@ -53,11 +53,12 @@ def test_rfft3_and_irfft3_match_numpy(cuda, qhk, shape):
     assert rel_err(host(out), x) < 2e-6
 
 
-@pytest.fixture(params=[1, 2, 3], ids=["stored_r", "recomputed_r", "two_step"])
+@pytest.fixture(params=[1, 2, 3, 20, 18], ids=["stored_r", "recomputed_r", "two_step", "two_step_4_rows",
+                                                 "two_step_2_rows"])
 def tv_form(request, qhk):
     """Every FGP step form (the extrapolated point stored between steps, recomputed from the two
-    previous duals, or two steps per pass with the halo rows recomputed) must give the reference's
-    iterates bit for bit."""
+    previous duals, or two steps per pass with the halo rows recomputed, at each tile height the
+    autotuner may pick) must give the reference's iterates bit for bit."""
     qhk.tv_form(request.param)
     yield request.param
     qhk.tv_form(0)
