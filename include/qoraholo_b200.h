@@ -118,6 +118,12 @@ int qhk_tv_prox_device(const float* d_b, float* d_x, float* d_dual, int nz, int 
 int qhk_tv_prox_workspace(const float* d_b, float* d_x, float* d_work, int work_volumes, int nz, int ny, int nx,
                           float lambda, int inner, void* stream);
 
+/* Page-locked host memory (no counterpart in the reference): qhk_pipeline_run transfers page-locked
+ * holograms and volumes directly, without staging copies, so callers that reuse buffers across runs
+ * can allocate them here. */
+int qhk_pinned_alloc(size_t bytes, void** ptr);
+int qhk_pinned_free(void* ptr);
+
 /* Bounded device waits that ran out since the library was loaded: the two-step FGP kernel waits
  * for its box loads (TMA) on mbarriers with an iteration limit, and a wait that gives up counts
  * here and ends the kernel early (the result is then invalid). 0 in every correct run. Synchronises
@@ -246,8 +252,9 @@ int qhk_pipeline_process(qhk_pipeline* pipeline);
  * (filled, timings) as after process(). The staging copies run on QHK_COPY_THREADS host threads
  * (default min(8, hardware threads)), each upload chunk's copy overlapping the transfer and field
  * passes of the chunks before it; the pages of `index` are written (faulted in) while the device
- * solves, then the volume is copied out part by part as it arrives. `input` and `output` are
- * used as staging and hold this call's data afterwards. */
+ * solves, then the volume is copied out part by part as it arrives. Page-locked buffers (such as
+ * qhk_pinned_alloc's) are transferred directly instead, without staging or host copies. `input` and
+ * `output` serve as the staging for pageable buffers and then hold this call's data. */
 int qhk_pipeline_run(qhk_pipeline* pipeline, const float* holograms, float* index);
 /* Device-resident variant: d_holo (count, N, N) and d_index (nz, m, m) on the device, asynchronous on
  * `stream`, no host copies (for serving loops and benchmarks). */

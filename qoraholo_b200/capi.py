@@ -86,6 +86,8 @@ _PROTOS = {
     "qhk_tv_prox_device": (_I, [_VP, _VP, _VP, _I, _I, _I, _F, _I, _VP]),
     "qhk_kernel_launches": (C.c_uint64, []),
     "qhk_wait_timeouts": (_I, [C.POINTER(C.c_uint64)]),
+    "qhk_pinned_alloc": (_I, [C.c_size_t, C.POINTER(_VP)]),
+    "qhk_pinned_free": (_I, [_VP]),
     "qhk_tv_prox_workspace": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _F, _I, _VP]),
     "qhk_unwrap_noalloc": (_I, [_VP, _VP, _I, _I, _I, _VP]),
     "qhk_bpm_vjp": (_I, [_VP, _I, _I, _VP, _VP, _I, C.POINTER(Geometry), _I, _VP]),
@@ -247,6 +249,21 @@ def tv_prox_workspace(d_b, d_x, d_work, work_volumes, nz, ny, nx, lam, inner, st
 def unwrap_noalloc(d_wrapped, d_unwrapped, count, ny, nx, stream=0):
     """qhk_unwrap_noalloc: device in / device out, no allocation (scratch in a static device array)."""
     check(lib().qhk_unwrap_noalloc(_VP(d_wrapped), _VP(d_unwrapped), count, ny, nx, _VP(stream)))
+
+
+def pinned_array(shape, dtype=np.float32) -> np.ndarray:
+    """A numpy array in page-locked host memory (qhk_pinned_alloc), freed when the array is released:
+    qhk_pipeline_run transfers such buffers directly, without staging copies."""
+    import weakref
+
+    dtype = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dtype.itemsize
+    ptr = _VP()
+    check(lib().qhk_pinned_alloc(nbytes, C.byref(ptr)))
+    raw = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(nbytes,))
+    arr = raw.view(dtype).reshape(shape)
+    weakref.finalize(arr, lib().qhk_pinned_free, _VP(ptr.value))
+    return arr
 
 
 def wait_timeouts() -> int:

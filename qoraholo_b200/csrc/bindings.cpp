@@ -7,12 +7,15 @@
 #include <pybind11/stl.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <optional>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "qoraholo/qoraholo.hpp"
+#include "qoraholo_b200.h"
 
 namespace py = pybind11;
 using namespace qoraholo;
@@ -28,6 +31,53 @@ Array3<T> to_array(const In<T>& a) {
   Array3<T> out(static_cast<int>(a.shape(0)), static_cast<int>(a.shape(1)), static_cast<int>(a.shape(2)));
   std::copy(a.data(), a.data() + a.size(), out.data.begin());
   return out;
+}
+
+// Page-locked buffers for Pipeline.run results, recycled when their arrays are released (a couple of
+// free buffers per size are kept; the rest are freed). Never destroyed: at exit the CUDA runtime may
+// already be gone.
+struct PooledBuffer {
+  float* data;
+  std::size_t size;
+};
+
+class PinnedPool {
+ public:
+  float* take(std::size_t n) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto& v = free_[n];
+      if (!v.empty()) {
+        float* p = v.back();
+        v.pop_back();
+        return p;
+      }
+    }
+    void* p = nullptr;
+    if (qhk_pinned_alloc(n * sizeof(float), &p) != QHK_OK) throw std::runtime_error(qhk_last_error());
+    return static_cast<float*>(p);
+  }
+  void give(float* p, std::size_t n) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto& v = free_[n];
+      if (v.size() < kKeep) {
+        v.push_back(p);
+        return;
+      }
+    }
+    qhk_pinned_free(p);
+  }
+
+ private:
+  static constexpr std::size_t kKeep = 2;
+  std::mutex mu_;
+  std::map<std::size_t, std::vector<float*>> free_;
+};
+
+PinnedPool& pinned_pool() {
+  static auto* pool = new PinnedPool;
+  return *pool;
 }
 
 template <class T>
@@ -243,9 +293,18 @@ PYBIND11_MODULE(_core, m) {
               throw std::invalid_argument("Pipeline.run: shape must be (count, N, N)");
             }
             const auto [nz, ny, nx] = p.output_shape();
-            py::array_t<float> out({nz, ny, nx});  // uninitialised: run() faults its pages in while the device works
+            // The result lives in a page-locked buffer of the pool, so the device writes it directly;
+            // the buffer goes back to the pool when the array is released.
+            const std::size_t n = static_cast<std::size_t>(nz) * ny * nx;
+            auto* owner = new PooledBuffer{pinned_pool().take(n), n};
+            py::capsule release_buffer(owner, [](void* o) {
+              auto* b = static_cast<PooledBuffer*>(o);
+              pinned_pool().give(b->data, b->size);
+              delete b;
+            });
+            py::array_t<float> out({nz, ny, nx}, owner->data, release_buffer);
             std::span<const float> in(holograms.data(), static_cast<std::size_t>(holograms.size()));
-            std::span<float> dst(out.mutable_data(), static_cast<std::size_t>(out.size()));
+            std::span<float> dst(owner->data, n);
             {
               py::gil_scoped_release release;
               p.run(in, dst);

@@ -250,6 +250,20 @@ int qhk_tv_prox_workspace(const float* d_b, float* d_x, float* d_work, int work_
   });
 }
 
+int qhk_pinned_alloc(size_t bytes, void** ptr) {
+  return guard([&] {
+    qhk::require(ptr != nullptr && bytes > 0, "pinned_alloc: null pointer or zero size");
+    *ptr = nullptr;
+    qhk::check(cudaMallocHost(ptr, bytes), "cudaMallocHost");
+  });
+}
+
+int qhk_pinned_free(void* ptr) {
+  return guard([&] {
+    if (ptr) qhk::check(cudaFreeHost(ptr), "cudaFreeHost");
+  });
+}
+
 int qhk_wait_timeouts(uint64_t* count) {
   return guard([&] {
     qhk::require(count != nullptr, "wait_timeouts: null argument");

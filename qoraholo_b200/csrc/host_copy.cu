@@ -5,9 +5,29 @@
 #include <cstdlib>
 #include <cstring>
 
+#include <cuda_runtime.h>
+
 #include "host_copy.hpp"
 
 namespace qhk {
+
+namespace {
+
+bool locked(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // not a pointer the runtime knows: pageable
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+bool is_page_locked(const void* p, std::size_t bytes) {
+  if (p == nullptr || bytes == 0) return false;
+  return locked(p) && locked(static_cast<const char*>(p) + bytes - 1);
+}
 
 HostCopier::HostCopier(int threads) {
   for (int i = 1; i < std::max(threads, 1); ++i) workers_.emplace_back([this] { worker(); });

@@ -14,6 +14,10 @@
 
 namespace qhk {
 
+// Whether [p, p + bytes) is page-locked host memory (both ends lie in page-locked allocations, so
+// the device can transfer it directly without a staging copy).
+bool is_page_locked(const void* p, std::size_t bytes);
+
 class HostCopier {
  public:
   // `threads` in total, the calling thread included (so threads - 1 workers).

@@ -85,7 +85,7 @@ void PipelinePlan::enqueue(const float* d_holo, const float2* bg, float* d_index
 }
 
 void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float2* bg, float* d_index, cudaStream_t s,
-                           bool marks, const float* host_src) {
+                           bool marks, const float* host_src, bool host_src_locked) {
   const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
   if (marks) clock_.mark(kStart, s);
   const int images = count_ * batch_;
@@ -96,11 +96,13 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
       const int first = k * chunk_;
       const int valid = std::min(chunk_, images - first);
       float* dst = holo_.get() + first * image;
-      if (host_src) {
+      const float* src = input_.get() + first * image;
+      if (host_src && host_src_locked) {
+        src = host_src + first * image;  // page-locked caller memory: transferred directly
+      } else if (host_src) {
         HostCopier::shared().copy(input_.get() + first * image, host_src + first * image, valid * image * sizeof(float));
       }
-      check(cudaMemcpyAsync(dst, input_.get() + first * image, valid * image * sizeof(float), cudaMemcpyHostToDevice, c),
-            "upload holograms");
+      check(cudaMemcpyAsync(dst, src, valid * image * sizeof(float), cudaMemcpyHostToDevice, c), "upload holograms");
       chunk_done_[k].record(c);
       check(cudaStreamWaitEvent(s, chunk_done_[k].get(), 0), "cudaStreamWaitEvent");
       field_.spectra(dst, first, valid, s);
@@ -125,8 +127,14 @@ void PipelinePlan::process_host(const float* holograms, float* index) {
   if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
   const auto t0 = std::chrono::steady_clock::now();
   const cudaStream_t s = compute_.get();
-  compute(nullptr, true, background_.get(), index_.get(), s, true, holograms == input_.get() ? nullptr : holograms);
+  const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
+  const float* src = holograms == input_.get() ? nullptr : holograms;
+  const bool src_locked = src && is_page_locked(src, static_cast<std::size_t>(batch_) * count_ * image * sizeof(float));
+  compute(nullptr, true, background_.get(), index_.get(), s, true, src, src_locked);
   const std::size_t total = static_cast<std::size_t>(batch_) * odt_.volume();
+  // Page-locked caller output: the device writes it directly (no staging, no host copy).
+  const bool dst_locked = index && index != output_.get() && is_page_locked(index, total * sizeof(float));
+  float* const down = dst_locked ? index : output_.get();
   const std::size_t part = (total + kOutParts - 1) / kOutParts;
   const auto part_len = [&](int j) {
     const std::size_t off = j * part;
@@ -134,7 +142,7 @@ void PipelinePlan::process_host(const float* holograms, float* index) {
   };
   for (int j = 0; j < kOutParts; ++j) {
     if (part_len(j) > 0) {
-      check(cudaMemcpyAsync(output_.get() + j * part, index_.get() + j * part, part_len(j) * sizeof(float),
+      check(cudaMemcpyAsync(down + j * part, index_.get() + j * part, part_len(j) * sizeof(float),
                             cudaMemcpyDeviceToHost, s),
             "download index");
     }
@@ -144,7 +152,7 @@ void PipelinePlan::process_host(const float* holograms, float* index) {
                         cudaMemcpyDeviceToHost, s),
         "download filled");
   clock_.mark(kDownloaded, s);
-  if (index != nullptr && index != output_.get()) {
+  if (index != nullptr && index != output_.get() && !dst_locked) {
     HostCopier& copier = HostCopier::shared();
     copier.touch(index, total * sizeof(float));  // while the device works
     for (int j = 0; j < kOutParts; ++j) {

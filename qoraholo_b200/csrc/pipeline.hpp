@@ -34,8 +34,9 @@ class PipelinePlan {
   // the page-locked input by the host copy threads just before its transfer is queued, so the copy
   // of chunk k overlaps the transfer and field passes of the chunks before it; the pages of
   // `index` are faulted in while the solver runs, and the volume comes back in kOutParts parts,
-  // each copied out as soon as it has landed while the next part is in flight. Either pointer may
-  // be null: the input is then taken from input(), the volume left in output().
+  // each copied out as soon as it has landed while the next part is in flight. Page-locked caller
+  // buffers are transferred directly, without staging or host copies. Either pointer may be null:
+  // the input is then taken from input(), the volume left in output().
   void process_host(const float* holograms, float* index);
   // Holograms already on the device -> index on the device, asynchronous on `s` (no host copies).
   void process_device(const float* d_holo, float* d_index, cudaStream_t s);
@@ -74,9 +75,10 @@ class PipelinePlan {
   enum { kStart, kFields, kRytov, kDownloaded = kRytov + 1 + OdtPlan::kMarks, kMarks };
   static constexpr int kOutParts = 8;
   // chunked_upload: the holograms come from input_ in chunks on the copy stream, each first
-  // copied there from `host_src` when that is given.
+  // copied there from `host_src` when that is given (or transferred straight from it when it is
+  // page-locked).
   void compute(const float* d_holo, bool chunked_upload, const float2* bg, float* d_index, cudaStream_t s,
-               bool marks, const float* host_src = nullptr);
+               bool marks, const float* host_src = nullptr, bool host_src_locked = false);
 
   CropPlan crop_;
   int count_;

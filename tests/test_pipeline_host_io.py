@@ -1,8 +1,9 @@
 """Pipeline runs on caller host memory (qhk_pipeline_run, qoraholo.Pipeline.run): the holograms are
 staged by the host copy threads chunk by chunk and the volume copied out part by part, and the
 volume is bitwise the one process() leaves in the pipeline's own page-locked output -- for any
-number of upload chunks, batched pipelines, caller buffers that are not page aligned, and the
-pipeline's own buffers passed as source and destination."""
+number of upload chunks, batched pipelines, caller buffers that are not page aligned, page-locked
+caller buffers (transferred directly), and the pipeline's own buffers passed as source and
+destination."""
 
 from __future__ import annotations
 
@@ -121,3 +122,38 @@ def test_public_pipeline_run_equals_process(cuda):
         assert np.array_equal(got, want) and api.filled == filled
         assert api.timings["total"] > 0
     ref.close()
+
+
+def test_run_on_page_locked_buffers_equals_process(cuda):
+    """Page-locked holograms and volume (qhk_pinned_alloc) are transferred directly."""
+    from qoraholo_b200 import capi
+
+    il, bg, stacks = _stacks(2)
+    p = _pipeline(capi, il, bg, iterations=3, solver="tv", tv_inner=4, upload_chunks=4)
+    holo = capi.pinned_array(stacks[0].shape)
+    out = capi.pinned_array(p.shape)
+    for h in stacks:
+        want, _ = _processed(p, h)
+        holo[...] = h
+        out[...] = -1.0
+        assert p.run(holo, out=out) is out and np.array_equal(out, want)
+    p.close()
+
+
+def test_public_results_stay_valid_across_runs(cuda):
+    """Pipeline.run returns arrays in recycled page-locked buffers: a result that is still held is
+    never written by later runs, and released ones are reused."""
+    import qoraholo_b200 as qh
+    from qoraholo_b200 import capi
+
+    il, bg, stacks = _stacks(3)
+    geom = qh.Geometry(wavelength=float(G[0]), n_medium=float(G[1]), na=float(G[2]), pixel=float(G[3]))
+    api = qh.Pipeline(9, 64, (18, 18), il, geom, radius=14.0, output_size=34, iterations=2)
+    api.set_background(bg)
+    held = [api.run(h) for h in stacks]  # three live results
+    copies = [r.copy() for r in held]
+    for _ in range(3):
+        api.run(stacks[0])  # released at once, its buffer reused by the next run
+    for r, c in zip(held, copies):
+        assert np.array_equal(r, c)
+    assert not np.array_equal(held[0], held[1])
