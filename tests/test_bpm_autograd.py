@@ -120,7 +120,7 @@ def test_gradient_descent_through_autograd_reduces_the_misfit(torch):
         loss = 0.5 * (model(x) - data).abs().pow(2).sum()
         loss.backward()
         opt.step()
-        losses.append(float(loss))
+        losses.append(loss.item())
     assert all(b <= a for a, b in zip(losses, losses[1:]))
     assert losses[-1] < 0.5 * losses[0]
 
