@@ -584,17 +584,18 @@ __global__ void __launch_bounds__(256)
 //   p, r_{k+2} rows y0   .. y0+TY-1   (dual step k + 1, to HBM)
 // In z the march runs three planes ahead of its output. Iteration q computes z_k of plane q+2,
 // dual step k of plane q+1, z_{k+1} of plane q+1 and dual step k+1 of plane q. The inputs arrive as
-// TMA box loads issued after the iteration's second barrier, when the slots they go to have been
-// read: r_k and b of plane q+3 (used from the next iteration on) and p_k of plane q+2 (used by the
+// TMA box loads: r_k and b of plane q+3 into the ring slot of plane q at the iteration's first
+// barrier (a whole plane ahead of their use), p_k of plane q+2 at its second barrier (used by the
 // next iteration's dual step k). Shared memory, in rows of the pitch (nx rounded up to 32 floats):
-// r_k (2 planes x 3 components x TY+4 rows), b ring (3 x TY+3), z_k (2 x TY+3), r_{k+1} (z
-// component of 2 planes, y and x of one, TY+2 rows each), z_{k+1} (2 x TY+1), p_k (3 x TY+2):
-// 20 TY + 55 rows. The own rows of every phase belong to
-// one thread row each (four x values per thread), and the halo rows of z_k and of dual step k are
-// spread over all threads with the same point -> thread map in both phases, so the step-k dual
-// reads only z_k values that its own thread wrote in this iteration or that a barrier separates
-// from their writer: two barriers per plane. p_{k+1} and r_{k+1} of the thread's own points stay
-// in registers from dual step k to dual step k + 1. The per-point operations are those of k_fgp in
+// r_k ring (3 planes x 3 components x TY+4 rows), b ring (3 x TY+3), z_k (2 x TY+3), the parts of
+// r_{k+1} that other threads read (its y component, TY+2 rows; its z component of row y0+TY for
+// two planes and its x component of that row; each thread's last own x value), z_{k+1}
+// (2 x TY+1), p_k (3 x TY+2): 20 TY + 64 rows and ceil(threads / pitch) rows. The own rows of
+// every phase belong to one thread row each (four x values per thread), and the halo rows of z_k
+// and of dual step k are spread over all threads with the same point -> thread map in both phases,
+// so the step-k dual reads only z_k values that its own thread wrote in this iteration or that a
+// barrier separates from their writer: two barriers per plane. p_{k+1} and r_{k+1} of the thread's
+// own points stay in registers from dual step k to the z_{k+1} phase and dual step k + 1. The per-point operations are those of k_fgp in
 // the same order, so the iterates are bit-identical.
 struct Fgp2Args {
   const float* pin[3];  // p_k (not read on the first step)
@@ -616,30 +617,6 @@ struct Fgp2Maps {
 
 // Waits of k_fgp2 that ran out (a box load that never completed); read by tv_wait_timeouts().
 __device__ unsigned long long g_fgp2_timeouts = 0;
-
-// The primal point max(b - lambda L(r), 0) of one voxel from its six dual neighbours, the sum in the
-// host's order (src/common.hpp:107-153).
-__device__ __forceinline__ float fgp_primal_at(int z, int y, int x, int nz, int ny, int nx, float vz, float vzb,
-                                               float vy, float vym, float vx, float vxm, float vb, float lambda) {
-  float sacc = 0.0f;
-  if (z < nz - 1) sacc = __fadd_rn(sacc, vz);
-  if (z > 0) sacc = __fsub_rn(sacc, vzb);
-  if (y < ny - 1) sacc = __fadd_rn(sacc, vy);
-  if (y > 0) sacc = __fsub_rn(sacc, vym);
-  if (x < nx - 1) sacc = __fadd_rn(sacc, vx);
-  if (x > 0) sacc = __fsub_rn(sacc, vxm);
-  return tv_primal(vb, lambda, sacc);
-}
-
-// One dual step at a voxel from its primal value c and its +z, +y and +x neighbours.
-__device__ __forceinline__ void fgp_dual_at(float c, float cz, float cy, float cx, int z, int y, int x, int nz, int ny,
-                                            int nx, float step, float momentum, float p[3], float r[3]) {
-  float g[3];
-  g[0] = z < nz - 1 ? __fsub_rn(c, cz) : 0.0f;
-  g[1] = y < ny - 1 ? __fsub_rn(c, cy) : 0.0f;
-  g[2] = x < nx - 1 ? __fsub_rn(c, cx) : 0.0f;
-  tv_dual_step(g, step, momentum, p, r);
-}
 
 // The same two operations on a pair of neighbouring x points with Blackwell's packed FP32 add and
 // multiply (two correctly rounded operations per instruction, each as the scalar __fadd_rn /
@@ -722,7 +699,9 @@ __device__ __forceinline__ void fgp_dual_pair(float2 c, float2 cz, float2 cy, fl
   }
 }
 
-constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(ty) + 55; }
+// Rows of the two-step kernel's shared memory, apart from the rows that hold each thread's last own
+// x value (ceil(threads / pitch)).
+constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(ty) + 64; }
 // Threads per CTA the two-step kernel is compiled for (nx / 4 x TY must stay within it).
 constexpr int fgp2_threads(int ty) { return ty == 8 ? 512 : 256; }
 
@@ -744,11 +723,16 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
   // Shared memory in floats, rows of P = A.pitch floats (nx rounded up to 128 bytes; the columns
   // from nx on hold the zeros the box loads fill in): slot strides and buffer bases (32-bit offsets
-  // from smem2), then the three ring-slot mbarriers.
+  // from smem2), then the mbarriers. r_{k+1} keeps in shared memory only what other threads read:
+  // its y component (rows y0-1 .. y0+TY), its z component of row y0+TY for two planes, its x
+  // component of row y0+TY, and each thread's last own x value (the left neighbour of the next
+  // thread's first point); the rest the z_{k+1} phase takes from the registers of its own thread.
   const int P = A.pitch;
   const int RKP = RK_ROWS * P, BP = B_ROWS * P, R1P = R1_ROWS * P, Z1P = Z1_ROWS * P;
-  const int OB = 6 * RKP, OZ = OB + 3 * BP, OR = OZ + 2 * BP, OZ1 = OR + 4 * R1P, OPK = OZ1 + 2 * Z1P;
-  // mbarriers: 0 and 1 for the plane loads (r_k and b) of even and odd planes, 2 for p_k.
+  const int EDGE_ROWS = (nthreads + P - 1) / P;
+  const int OB = 9 * RKP, OZ = OB + 3 * BP, ORY = OZ + 2 * BP, ORZH = ORY + R1P, ORXH = ORZH + 2 * P,
+            OEDGE = ORXH + P, OZ1 = OEDGE + EDGE_ROWS * P, OPK = OZ1 + 2 * Z1P;
+  // mbarriers: 0-2 for the plane loads (r_k and b) into ring slots 0-2, 3 for p_k.
   std::uint64_t* const bars = reinterpret_cast<std::uint64_t*>(smem2 + OPK + 3 * R1P);
   // Own-row offsets within a slot: r_k row ty+2 (rows start at y0-2); b, z_k, r_{k+1} row ty+1
   // (rows start at y0-1); z_{k+1} row ty (rows start at y0).
@@ -797,7 +781,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
     }
   };
   if (linear == 0) {
-    for (int i = 0; i < 3; ++i) tma::mbar_init(bars + i, 1);
+    for (int i = 0; i < 4; ++i) tma::mbar_init(bars + i, 1);
   }
   __syncthreads();
   unsigned phases = 0;  // bit i: parity of the next completion of mbarrier i
@@ -828,21 +812,21 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
     const bool own = y < ny;
     const std::size_t own_g = static_cast<std::size_t>(y) * nx + x0;  // within a plane
 
-    // Box loads by thread 0, counted on an mbarrier. A plane z: r_k rows y0-2 .. y0+TY+1 (`comps`
-    // components) into r_k slot z&1 and b rows y0-1 .. y0+TY+1 into b slot `sb`, on mbarrier z&1;
-    // p_k of plane z, rows y0-1 .. y0+TY, into the p_k slot on mbarrier 2. Rows outside the volume
-    // arrive as zeros and are never read.
-    const auto issue = [&](int z, int sb, int comps, bool with_b) {
+    // Box loads by thread 0, counted on an mbarrier. A plane z into ring slot s (z mod 3): r_k rows
+    // y0-2 .. y0+TY+1 (`comps` components) and b rows y0-1 .. y0+TY+1, on mbarrier s; p_k of plane
+    // z, rows y0-1 .. y0+TY, into the p_k slot on mbarrier 3. Rows outside the volume arrive as
+    // zeros and are never read.
+    const auto issue = [&](int z, int s, int comps, bool with_b) {
       tma::fence_async_shared();
-      std::uint64_t* bar = bars + (z & 1);
+      std::uint64_t* bar = bars + s;
       tma::mbar_expect(bar, static_cast<unsigned>((comps * RK_ROWS + (with_b ? B_ROWS : 0)) * P * 4));
-      for (int c = 0; c < comps; ++c) tma::load_3d(smem2 + ((z & 1) * 3 + c) * RKP, &M.r[c], 0, y0 - 2, z, bar);
-      if (with_b) tma::load_3d(smem2 + OB + sb * BP, &M.b, 0, y0 - 1, z, bar);
+      for (int c = 0; c < comps; ++c) tma::load_3d(smem2 + (s * 3 + c) * RKP, &M.r[c], 0, y0 - 2, z, bar);
+      if (with_b) tma::load_3d(smem2 + OB + s * BP, &M.b, 0, y0 - 1, z, bar);
     };
     const auto issue_pk = [&](int z) {
       tma::fence_async_shared();
-      tma::mbar_expect(bars + 2, static_cast<unsigned>(3 * R1_ROWS * P * 4));
-      for (int c = 0; c < 3; ++c) tma::load_3d(smem2 + OPK + c * R1P, &M.p[c], 0, y0 - 1, z, bars + 2);
+      tma::mbar_expect(bars + 3, static_cast<unsigned>(3 * R1_ROWS * P * 4));
+      for (int c = 0; c < 3; ++c) tma::load_3d(smem2 + OPK + c * R1P, &M.p[c], 0, y0 - 1, z, bars + 3);
     };
     // Bounded wait on mbarrier i (every thread), then its phase bit flips.
     const auto wait_bar = [&](int i) {
@@ -857,35 +841,37 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
       if (z0 >= 1) issue(z0 - 1, mod3(z0 - 1), 3, true);
     }
     bool ok = true;
-    if (z0 >= 2) ok = wait_bar((z0 - 2) & 1) && ok;
+    if (z0 >= 2) ok = wait_bar(mod3(z0 - 2)) && ok;
 
     float cr[3][VEC] = {}, cp[3][VEC] = {};  // r_{k+1}, p_{k+1} of this thread's points of plane q
     float nr[3][VEC] = {}, np[3][VEC] = {};  // the same of plane q+1
-    int m0 = mod3(z0 - 3);                   // b slot of plane q (and of q+3)
+    int m0 = mod3(z0 - 3);                   // ring slot of plane q (and of q+3)
     for (int q = z0 - 3; q < zend; ++q, m0 = m0 == 2 ? 0 : m0 + 1) {
       const int a2 = q + 2, a1 = q + 1;
-      const int m1 = m0 == 2 ? 0 : m0 + 1;  // b slot of q+1
-      const int m2 = m0 == 0 ? 2 : m0 - 1;  // b slot of q+2
-      const int par = q & 1;                // parity of q and q+2 (r_k slot, z_k, z_{k+1}); q+1 has par ^ 1
+      const int m1 = m0 == 2 ? 0 : m0 + 1;  // ring slot of q+1
+      const int m2 = m0 == 0 ? 2 : m0 - 1;  // ring slot of q+2
+      const int par = q & 1;                // parity of q and q+2 (z_k, z_{k+1}, r_{k+1} row); q+1 has par ^ 1
       const bool do_a = a2 >= 0 && a2 < nz;                  // z_k of plane a2
       const bool do_b = a1 >= 0 && a1 >= z0 - 1 && a1 < nz;  // dual step k on plane a1
       const bool do_c = a1 >= z0 && a1 < nz;                 // z_{k+1} of plane a1
       const bool do_d = q >= z0;                             // dual step k+1 on plane q
       const bool wait_plane = a2 >= 0 && a2 <= zmax;  // plane a2, loaded one iteration ago
-      if (wait_plane) ok = wait_bar(par) && ok;
+      if (wait_plane) ok = wait_bar(m2) && ok;
       if (__syncthreads_or(!ok)) {
         // A load never completed: leave with the timeout counted (every thread takes this exit),
         // after one more bounded wait for the load in flight.
-        if (wait_plane) tma::mbar_wait(bars + par, ((phases >> par) & 1u) ^ 1u, &g_fgp2_timeouts);
+        if (wait_plane) tma::mbar_wait(bars + m2, ((phases >> m2) & 1u) ^ 1u, &g_fgp2_timeouts);
         return;
       }
+      // Slot m0 held plane q, last read one iteration ago: plane q+3 streams in for a whole plane.
+      if (linear == 0 && q + 3 <= zmax) issue(q + 3, m0, 3, true);
 
       if (do_a) {
         const int a = a2;
-        const float* Rz = smem2 + (par * 3 + 0) * RKP;
-        const float* Rzb = smem2 + ((par ^ 1) * 3 + 0) * RKP;  // plane a-1; not read on plane 0
-        const float* Ry = smem2 + (par * 3 + 1) * RKP;
-        const float* Rx = smem2 + (par * 3 + 2) * RKP;
+        const float* Rz = smem2 + (m2 * 3 + 0) * RKP;
+        const float* Rzb = smem2 + (m1 * 3 + 0) * RKP;  // plane a-1; not read on plane 0
+        const float* Ry = smem2 + (m2 * 3 + 1) * RKP;
+        const float* Rx = smem2 + (m2 * 3 + 2) * RKP;
         const float* B = smem2 + OB + m2 * BP;
         float* Z = smem2 + OZ + par * BP;
         {
@@ -921,16 +907,16 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
 
       // p_k of plane a1, loaded during the previous iteration.
       const bool wait_pk = !FIRST && do_b;
-      if (wait_pk) ok = wait_bar(2) && ok;
+      if (wait_pk) ok = wait_bar(3) && ok;
       const float* PK = smem2 + OPK;
       if (do_b) {
         const int a = a1;
         const float* Zc = smem2 + OZ + (par ^ 1) * BP;
         const float* Zn = smem2 + OZ + par * BP;  // plane a+1; read only below plane nz-1
-        const float* R = smem2 + ((par ^ 1) * 3) * RKP;
-        float* Rz1 = smem2 + OR + (par ^ 1) * R1P;
-        float* Ry1 = smem2 + OR + 2 * R1P;
-        float* Rx1 = smem2 + OR + 3 * R1P;
+        const float* R = smem2 + (m1 * 3) * RKP;
+        float* Ry1 = smem2 + ORY;
+        float* RzH = smem2 + ORZH + (par ^ 1) * P;  // z component of row y0+TY, plane a1
+        float* RxH = smem2 + ORXH;                  // x component of row y0+TY
         {
           float zc[VEC], zy[VEC], zz[VEC];
           Vec<VEC>::load(Zc + own_b, zc);
@@ -954,10 +940,9 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
                 np[c][k] = FIRST ? rv[c][k] : pk[c][k];
               }
             dual4(a, y, zc, zz, zy, right, A.m1, np, nr);
-            Vec<VEC>::store(Rz1 + own_b, nr[0]);
             Vec<VEC>::store(Ry1 + own_b, nr[1]);
-            Vec<VEC>::store(Rx1 + own_b, nr[2]);
           }
+          smem2[OEDGE + linear] = nr[2][3];  // the left neighbour of the next thread's first point
         }
         // halo rows y0-1 and y0+TY: the points this thread took in the z_k phase, so their z_k of
         // plane a+1 is this thread's own write.
@@ -980,45 +965,41 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
               p[c] = FIRST ? r[c] : ld2(PK + c * R1P + i);
             }
             fgp_dual_pair(c0, cz, cy, cx, a < nz - 1, yy < ny - 1, x + 1 == nx - 1, A.step, A.m1, p, r, nzero);
-            st2(Rz1 + i, r[0]);
             st2(Ry1 + i, r[1]);
-            st2(Rx1 + i, r[2]);
+            if (side == 1) {
+              st2(RzH + x, r[0]);
+              st2(RxH + x, r[2]);
+            }
           }
         }
       }
       if (__syncthreads_or(!ok)) {  // r_{k+1} of plane a1 complete
-        if (wait_pk) tma::mbar_wait(bars + 2, ((phases >> 2) & 1u) ^ 1u, &g_fgp2_timeouts);
+        if (wait_pk) tma::mbar_wait(bars + 3, ((phases >> 3) & 1u) ^ 1u, &g_fgp2_timeouts);
         return;
       }
-      // Every thread is past z_k of a2 and dual step k of a1: r_k of a1 (slot par ^ 1) and p_k are
-      // free for plane q+3 and p_k of a2; b of q+3 goes into the slot of b of q (last read one
-      // iteration ago).
-      if (linear == 0) {
-        if (q + 3 <= zmax) issue(q + 3, m0, 3, true);
-        // exactly the planes whose dual step k the next iteration runs (and waits for): do_b of q+1
-        if (!FIRST && a2 >= 0 && a2 >= z0 - 1 && a2 < nz && a2 <= zend) issue_pk(a2);
-      }
+      // Every thread is past dual step k of a1: the p_k slot is free for p_k of a2, exactly the
+      // planes whose dual step k the next iteration runs (and waits for): do_b of q+1.
+      if (linear == 0 && !FIRST && a2 >= 0 && a2 >= z0 - 1 && a2 < nz && a2 <= zend) issue_pk(a2);
 
       float zn[VEC] = {};  // z_{k+1} of this thread's points of plane a1
       if (do_c) {
         const int a = a1;
-        const float* Rz = smem2 + OR + (par ^ 1) * R1P;
-        const float* Rzb = smem2 + OR + par * R1P;  // plane a-1; not read on plane 0
-        const float* Ry = smem2 + OR + 2 * R1P;
-        const float* Rx = smem2 + OR + 3 * R1P;
+        const float* RzH = smem2 + ORZH + (par ^ 1) * P;  // row y0+TY, plane a
+        const float* RzbH = smem2 + ORZH + par * P;       // row y0+TY, plane a-1; not read on plane 0
+        const float* Ry = smem2 + ORY;
+        const float* RxH = smem2 + ORXH;
         const float* B = smem2 + OB + m1 * BP;
         float* Z = smem2 + OZ1 + (par ^ 1) * Z1P;
         {
-          float vz[VEC], vzb[VEC], vy[VEC], vym[VEC], vx[VEC], vb[VEC];
-          Vec<VEC>::load(Rz + own_b, vz);
-          Vec<VEC>::load(Rzb + own_b, vzb);
-          Vec<VEC>::load(Ry + own_b, vy);
+          // Own points: r_{k+1} of planes a (nr) and a-1 (cr, before the dual step k+1 below
+          // updates it) from this thread's registers; the y component of the row below and the x
+          // component left of the first point from shared memory.
+          float vym[VEC], vb[VEC];
           Vec<VEC>::load(Ry + own_b - P, vym);
-          Vec<VEC>::load(Rx + own_b, vx);
           Vec<VEC>::load(B + own_b, vb);
-          const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
-          const float left = (x0 > 0 && lane == 0) ? Rx[own_b - 1] : from_lane;
-          if (own) primal4(a, y, vz, vzb, vy, vym, vx, left, vb, zn);
+          const float from_lane = __shfl_up_sync(lanes, nr[2][3], 1);
+          const float left = (x0 > 0 && lane == 0) ? smem2[OEDGE + linear - 1] : from_lane;
+          if (own) primal4(a, y, nr[0], cr[0], nr[1], vym, nr[2], left, vb, zn);
           Vec<VEC>::store(Z + own_z1, zn);
         }
         if (y0 + TY < ny) {  // row y0+TY: the pair slots of side 3
@@ -1028,10 +1009,10 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
             const int x = hz_x[j];
             if (hz_side[j] == 3) {
               const int i = (TY + 1) * P + x;
-              const float2 vx = ld2(Rx + i);
+              const float2 vx = ld2(RxH + x);
               const float2 o = fgp_primal_pair(a < nz - 1, a > 0, yy < ny - 1, yy > 0, x == 0, x + 1 == nx - 1,
-                                               ld2(Rz + i), ld2(Rzb + i), ld2(Ry + i), ld2(Ry + i - P), vx,
-                                               f2(x > 0 ? Rx[i - 1] : 0.0f, vx.x), ld2(B + i), A.lambda, nzero);
+                                               ld2(RzH + x), ld2(RzbH + x), ld2(Ry + i), ld2(Ry + i - P), vx,
+                                               f2(x > 0 ? RxH[x - 1] : 0.0f, vx.x), ld2(B + i), A.lambda, nzero);
               st2(Z + TY * P + x, o);
             }
           }
@@ -1081,7 +1062,9 @@ struct FgpShape {
 // the largest a CTA may take on this part.
 int fgp2_pitch(int nx) { return (nx + 31) / 32 * 32; }
 std::size_t fgp2_smem(int nx, int ty) {
-  return fgp2_rows(ty) * static_cast<std::size_t>(fgp2_pitch(nx)) * sizeof(float) + 3 * sizeof(std::uint64_t);
+  const std::size_t pitch = fgp2_pitch(nx);
+  const std::size_t edge_rows = ((nx / 4) * static_cast<std::size_t>(ty) + pitch - 1) / pitch;
+  return (fgp2_rows(ty) + edge_rows) * pitch * sizeof(float) + 4 * sizeof(std::uint64_t);
 }
 constexpr std::size_t kSmemOptin = 227 * 1024;
 
