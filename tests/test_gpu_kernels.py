@@ -170,3 +170,30 @@ def test_odt_plan_runs_are_deterministic(cuda, qhk):
     assert np.array_equal(out[0], out[1])
     assert plan.device_bytes > 0
     assert 0 < plan.filled() < 1
+
+
+@pytest.mark.parametrize("shape", [(256, 256, 256), (130, 250, 256)])
+def test_two_step_fgp_equals_one_step_at_full_size(cuda, qhk, shape):
+    """At the bench's 256^3 (and a ragged 130 x 250 x 256) every CTA of the two-step kernel marches
+    through several tiles and z segments; its prox must still equal the one-step kernel's (which
+    the tests above pin to the oracle) bit for bit, dual included."""
+    rng = np.random.default_rng(21)
+    b = dev(cuda, rng.uniform(-0.2, 1.0, shape).astype(np.float32))
+    p0 = (rng.uniform(-0.6, 0.6, (3,) + shape) * (rng.uniform(size=(3,) + shape) > 0.3)).astype(np.float32)
+    lam, inner = 0.04, 10
+    results = []
+    for form in (1, 3):
+        qhk.tv_form(form)
+        try:
+            x = cuda.zeros(shape, dtype=cuda.float32, device="cuda")
+            work = cuda.zeros((12,) + shape, dtype=cuda.float32, device="cuda")
+            work[:3] = dev(cuda, p0)
+            qhk.tv_prox_workspace(b.data_ptr(), x.data_ptr(), work.data_ptr(), 12, *shape, lam, inner)
+            cuda.cuda.synchronize()
+            results.append((host(x), host(work[:3])))
+        finally:
+            qhk.tv_form(0)
+        del work
+    assert np.array_equal(results[0][0], results[1][0])
+    assert np.array_equal(results[0][1], results[1][1])
+    assert qhk.wait_timeouts() == 0
