@@ -16,6 +16,7 @@
 
 #include "qoraholo/qoraholo.hpp"
 #include "qoraholo_b200.h"
+#include "host/raw.hpp"
 
 namespace py = pybind11;
 using namespace qoraholo;
@@ -24,6 +25,13 @@ namespace {
 
 template <class T>
 using In = py::array_t<T, py::array::c_style | py::array::forcecast>;
+
+// (count, ny, nx) of a 3D array, as to_array validates it.
+template <class T>
+std::array<int, 3> dims3(const In<T>& a) {
+  if (a.ndim() != 3) throw std::invalid_argument("expected a 3D array (count, ny, nx)");
+  return {static_cast<int>(a.shape(0)), static_cast<int>(a.shape(1)), static_cast<int>(a.shape(2))};
+}
 
 template <class T>
 Array3<T> to_array(const In<T>& a) {
@@ -169,12 +177,14 @@ PYBIND11_MODULE(_core, m) {
       .def_readonly("x", &Sideband::x)
       .def_readonly("magnitude", &Sideband::magnitude);
 
+  // The per-call functions run on the numpy buffers themselves (raw.hpp): no copies into owning
+  // arrays, outputs allocated uninitialised and written by the device transfer.
   m.def(
       "find_sideband",
       [](In<float> holograms, float dc_exclusion) {
-        auto h = to_array(holograms);
+        const auto [nz, ny, nx] = dims3(holograms);
         py::gil_scoped_release release;
-        return find_sideband(h, dc_exclusion);
+        return raw::find_sideband(holograms.data(), nz, ny, nx, dc_exclusion);
       },
       py::arg("holograms"), py::arg("dc_exclusion") = 0.0f);
 
@@ -182,15 +192,20 @@ PYBIND11_MODULE(_core, m) {
       "extract_fields",
       [](In<float> holograms, std::optional<std::array<float, 2>> center, float radius, float dc_exclusion,
          int output_size, const std::string& backend) {
-        auto h = to_array(holograms);
+        const auto [nz, ny, nx] = dims3(holograms);
         const FieldOptions opt{center, radius, dc_exclusion, output_size};
         const Backend b = parse_backend(backend);
-        Array3<cfloat> out;
+        raw::FieldCall call;
         {
           py::gil_scoped_release release;
-          out = extract_fields(h, opt, b);
+          call = raw::extract_fields_check(holograms.data(), nz, ny, nx, opt, b);
         }
-        return to_numpy(std::move(out));
+        py::array_t<cfloat> out({nz, call.out, call.out});
+        {
+          py::gil_scoped_release release;
+          raw::extract_fields_run(holograms.data(), nz, nx, opt, call, out.mutable_data());
+        }
+        return out;
       },
       py::arg("holograms"), py::arg("center") = py::none(), py::arg("radius") = 0.0f, py::arg("dc_exclusion") = 0.0f,
       py::arg("output_size") = 0, py::arg("backend") = "cuda");
@@ -198,42 +213,43 @@ PYBIND11_MODULE(_core, m) {
   m.def(
       "field_ratio",
       [](In<cfloat> sample, In<cfloat> background) {
-        auto s = to_array(sample);
-        auto b = to_array(background);
-        Array3<cfloat> out;
+        const auto [nz, ny, nx] = dims3(sample);
+        const auto [bz, by, bx] = dims3(background);
+        raw::field_ratio_check(nz, ny, nx, bz, by, bx);
+        py::array_t<cfloat> out({nz, ny, nx});
         {
           py::gil_scoped_release release;
-          out = field_ratio(s, b);
+          raw::field_ratio_run(sample.data(), nz, ny, nx, background.data(), bz, out.mutable_data());
         }
-        return to_numpy(std::move(out));
+        return out;
       },
       py::arg("sample"), py::arg("background"));
 
   m.def(
       "unwrap",
       [](In<float> wrapped, const std::string& backend) {
-        auto w = to_array(wrapped);
-        const Backend b = parse_backend(backend);
-        Array3<float> out;
+        const auto [nz, ny, nx] = dims3(wrapped);
+        raw::unwrap_check(ny, nx, parse_backend(backend));
+        py::array_t<float> out({nz, ny, nx});
         {
           py::gil_scoped_release release;
-          out = unwrap(w, b);
+          raw::unwrap_run(wrapped.data(), nz, ny, nx, out.mutable_data());
         }
-        return to_numpy(std::move(out));
+        return out;
       },
       py::arg("wrapped"), py::arg("backend") = "cuda");
 
   m.def(
       "rytov",
       [](In<cfloat> ratio, const std::string& backend) {
-        auto r = to_array(ratio);
-        const Backend b = parse_backend(backend);
-        Array3<cfloat> out;
+        const auto [nz, ny, nx] = dims3(ratio);
+        raw::rytov_check(ny, nx, parse_backend(backend));
+        py::array_t<cfloat> out({nz, ny, nx});
         {
           py::gil_scoped_release release;
-          out = rytov(r, b);
+          raw::rytov_run(ratio.data(), nz, ny, nx, out.mutable_data());
         }
-        return to_numpy(std::move(out));
+        return out;
       },
       py::arg("ratio"), py::arg("backend") = "cuda");
 
@@ -242,15 +258,17 @@ PYBIND11_MODULE(_core, m) {
       [](In<cfloat> fields, In<float> illuminations, const Geometry& geometry, int nz, int iterations,
          const std::string& solver, const std::string& gp_transform, float tv_weight, int tv_inner,
          const std::string& mapping, const std::string& backend) {
-        auto f = to_array(fields);
+        const auto [count, ny, nx] = dims3(fields);
         const auto il = to_illum(illuminations);
         const OdtOptions opt = odt_options(nz, iterations, solver, gp_transform, tv_weight, tv_inner, mapping, backend);
-        OdtResult r;
+        const int depth = raw::reconstruct_check(count, ny, nx, il, geometry, opt);
+        py::array_t<float> out({depth, nx, nx});
+        double filled = 0;
         {
           py::gil_scoped_release release;
-          r = reconstruct(f, il, geometry, opt);
+          filled = raw::reconstruct_run(fields.data(), count, nx, il, geometry, opt, out.mutable_data());
         }
-        return py::make_tuple(to_numpy(std::move(r.ri)), r.filled);
+        return py::make_tuple(out, filled);
       },
       py::arg("fields"), py::arg("illuminations"), py::arg("geometry"), py::arg("nz") = 0, py::arg("iterations") = 0,
       py::arg("solver") = "gp", py::arg("gp_transform") = "r2c", py::arg("tv_weight") = OdtOptions{}.tv_weight,

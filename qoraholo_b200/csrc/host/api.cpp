@@ -6,6 +6,7 @@
 #include <string>
 
 #include "host_common.hpp"
+#include "raw.hpp"
 #include "qoraholo/qoraholo.hpp"
 
 namespace qoraholo {
@@ -15,14 +16,21 @@ using host::require;
 
 bool cuda_available() { return qhk_device_present() != 0; }
 
-Sideband find_sideband(const Array3<float>& holograms, float dc_exclusion) {
-  const int n = holograms.nx;
-  require(holograms.nz >= 1 && n == holograms.ny && n % 2 == 0 && n >= 4,
-          "find_sideband: holograms must be square with an even side");
+namespace raw {
+
+Sideband find_sideband(const float* holograms, int count, int ny, int nx, float dc_exclusion) {
+  const int n = nx;
+  require(count >= 1 && n == ny && n % 2 == 0 && n >= 4, "find_sideband: holograms must be square with an even side");
   host::require_cuda(Backend::cuda);
   Sideband s;
-  check(qhk_find_sideband(holograms.data.data(), n, dc_exclusion, &s.iy, &s.ix, &s.y, &s.x, &s.magnitude));
+  check(qhk_find_sideband(holograms, n, dc_exclusion, &s.iy, &s.ix, &s.y, &s.x, &s.magnitude));
   return s;
+}
+
+}  // namespace raw
+
+Sideband find_sideband(const Array3<float>& holograms, float dc_exclusion) {
+  return raw::find_sideband(holograms.data.data(), holograms.nz, holograms.ny, holograms.nx, dc_exclusion);
 }
 
 namespace {
@@ -40,54 +48,92 @@ int checked_output(const FieldOptions& o, std::array<float, 2> c, int n) {
 
 }  // namespace
 
-Array3<cfloat> extract_fields(const Array3<float>& holograms, const FieldOptions& options, Backend backend) {
-  host::require_even_square(holograms.ny, holograms.nx, "extract_fields");
-  require(holograms.nz >= 1, "extract_fields: empty stack");
+namespace raw {
+
+FieldCall extract_fields_check(const float* holograms, int count, int ny, int nx, const FieldOptions& options,
+                               Backend backend) {
+  host::require_even_square(ny, nx, "extract_fields");
+  require(count >= 1, "extract_fields: empty stack");
   host::require_cuda(backend);
-  std::array<float, 2> c{};
+  FieldCall call;
   if (options.center) {
-    c = *options.center;
+    call.center = *options.center;
   } else {
-    const Sideband s = find_sideband(holograms, options.dc_exclusion);
-    c = {static_cast<float>(s.iy), static_cast<float>(s.ix)};
+    const Sideband s = find_sideband(holograms, count, ny, nx, options.dc_exclusion);
+    call.center = {static_cast<float>(s.iy), static_cast<float>(s.ix)};
   }
-  const int m = checked_output(options, c, holograms.nx);
-  Array3<cfloat> out(holograms.nz, m, m);
-  check(qhk_extract_fields(holograms.data.data(), holograms.nz, holograms.nx, c[0], c[1], options.radius,
-                           options.output_size, out.data.data()));
+  call.out = checked_output(options, call.center, nx);
+  return call;
+}
+
+void extract_fields_run(const float* holograms, int count, int n, const FieldOptions& options, const FieldCall& call,
+                        cfloat* out) {
+  check(qhk_extract_fields(holograms, count, n, call.center[0], call.center[1], options.radius, options.output_size,
+                           out));
+}
+
+void field_ratio_check(int count, int ny, int nx, int bcount, int bny, int bnx) {
+  if (ny != bny || nx != bnx || (bcount != 1 && bcount != count)) {
+    throw std::invalid_argument("field_ratio: background shape does not match");
+  }
+  host::require_cuda(Backend::cuda);
+}
+
+void field_ratio_run(const cfloat* sample, int count, int ny, int nx, const cfloat* background, int bcount,
+                     cfloat* out) {
+  if (static_cast<std::size_t>(count) * ny * nx == 0) return;
+  check(qhk_field_ratio(sample, count, ny, nx, background, bcount, out));
+}
+
+void unwrap_check(int ny, int nx, Backend backend) {
+  require(ny % 2 == 0 && nx % 2 == 0 && ny >= 2 && nx >= 2, "unwrap: image sides must be even");
+  host::require_cuda(backend);
+}
+
+void unwrap_run(const float* wrapped, int count, int ny, int nx, float* out) {
+  if (count == 0) return;
+  check(qhk_unwrap(wrapped, count, ny, nx, out));
+}
+
+void rytov_check(int ny, int nx, Backend backend) {
+  require(ny % 2 == 0 && nx % 2 == 0 && ny >= 4 && nx >= 4, "rytov: image sides must be even");
+  host::require_cuda(backend);
+}
+
+void rytov_run(const cfloat* ratio, int count, int ny, int nx, cfloat* out) {
+  if (count == 0) return;
+  check(qhk_rytov(ratio, count, ny, nx, out));
+}
+
+}  // namespace raw
+
+Array3<cfloat> extract_fields(const Array3<float>& holograms, const FieldOptions& options, Backend backend) {
+  const raw::FieldCall call =
+      raw::extract_fields_check(holograms.data.data(), holograms.nz, holograms.ny, holograms.nx, options, backend);
+  Array3<cfloat> out(holograms.nz, call.out, call.out);
+  raw::extract_fields_run(holograms.data.data(), holograms.nz, holograms.nx, options, call, out.data.data());
   return out;
 }
 
 Array3<cfloat> field_ratio(const Array3<cfloat>& sample, const Array3<cfloat>& background) {
-  if (sample.ny != background.ny || sample.nx != background.nx ||
-      (background.nz != 1 && background.nz != sample.nz)) {
-    throw std::invalid_argument("field_ratio: background shape does not match");
-  }
-  host::require_cuda(Backend::cuda);
+  raw::field_ratio_check(sample.nz, sample.ny, sample.nx, background.nz, background.ny, background.nx);
   Array3<cfloat> out(sample.nz, sample.ny, sample.nx);
-  if (sample.size() == 0) return out;
-  check(qhk_field_ratio(sample.data.data(), sample.nz, sample.ny, sample.nx, background.data.data(), background.nz,
-                        out.data.data()));
+  raw::field_ratio_run(sample.data.data(), sample.nz, sample.ny, sample.nx, background.data.data(), background.nz,
+                       out.data.data());
   return out;
 }
 
 Array3<float> unwrap(const Array3<float>& wrapped, Backend backend) {
-  require(wrapped.ny % 2 == 0 && wrapped.nx % 2 == 0 && wrapped.ny >= 2 && wrapped.nx >= 2,
-          "unwrap: image sides must be even");
-  host::require_cuda(backend);
+  raw::unwrap_check(wrapped.ny, wrapped.nx, backend);
   Array3<float> out(wrapped.nz, wrapped.ny, wrapped.nx);
-  if (wrapped.nz == 0) return out;
-  check(qhk_unwrap(wrapped.data.data(), wrapped.nz, wrapped.ny, wrapped.nx, out.data.data()));
+  raw::unwrap_run(wrapped.data.data(), wrapped.nz, wrapped.ny, wrapped.nx, out.data.data());
   return out;
 }
 
 Array3<cfloat> rytov(const Array3<cfloat>& ratio, Backend backend) {
-  require(ratio.ny % 2 == 0 && ratio.nx % 2 == 0 && ratio.ny >= 4 && ratio.nx >= 4,
-          "rytov: image sides must be even");
-  host::require_cuda(backend);
+  raw::rytov_check(ratio.ny, ratio.nx, backend);
   Array3<cfloat> out(ratio.nz, ratio.ny, ratio.nx);
-  if (ratio.nz == 0) return out;
-  check(qhk_rytov(ratio.data.data(), ratio.nz, ratio.ny, ratio.nx, out.data.data()));
+  raw::rytov_run(ratio.data.data(), ratio.nz, ratio.ny, ratio.nx, out.data.data());
   return out;
 }
 
@@ -121,17 +167,34 @@ int checked_odt(int n, int count, std::span<const Illumination> il, const Geomet
 
 }  // namespace host
 
-OdtResult reconstruct(const Array3<cfloat>& rytov_fields, std::span<const Illumination> illuminations,
-                      const Geometry& geometry, const OdtOptions& options) {
-  require(rytov_fields.ny == rytov_fields.nx, "reconstruct: images must be square");
-  const int n = rytov_fields.nx;
-  const int nz = host::checked_odt(n, rytov_fields.nz, illuminations, geometry, options);
+namespace raw {
+
+int reconstruct_check(int count, int ny, int nx, std::span<const Illumination> illuminations, const Geometry& geometry,
+                      const OdtOptions& options) {
+  require(ny == nx, "reconstruct: images must be square");
+  return host::checked_odt(nx, count, illuminations, geometry, options);
+}
+
+double reconstruct_run(const cfloat* fields, int count, int n, std::span<const Illumination> illuminations,
+                       const Geometry& geometry, const OdtOptions& options, float* out) {
   const qhk_geometry g{geometry.wavelength, geometry.n_medium, geometry.na, geometry.pixel};
   const qhk_odt_options o = host::odt_options(options);
+  double filled = 0;
+  check(qhk_reconstruct(fields, count, n, reinterpret_cast<const float*>(illuminations.data()), &g, &o, out, &filled));
+  return filled;
+}
+
+}  // namespace raw
+
+OdtResult reconstruct(const Array3<cfloat>& rytov_fields, std::span<const Illumination> illuminations,
+                      const Geometry& geometry, const OdtOptions& options) {
+  const int nz =
+      raw::reconstruct_check(rytov_fields.nz, rytov_fields.ny, rytov_fields.nx, illuminations, geometry, options);
+  const int n = rytov_fields.nx;
   OdtResult r;
   r.ri = Array3<float>(nz, n, n);
-  check(qhk_reconstruct(rytov_fields.data.data(), rytov_fields.nz, n,
-                        reinterpret_cast<const float*>(illuminations.data()), &g, &o, r.ri.data.data(), &r.filled));
+  r.filled = raw::reconstruct_run(rytov_fields.data.data(), rytov_fields.nz, n, illuminations, geometry, options,
+                                  r.ri.data.data());
   return r;
 }
 
