@@ -150,12 +150,9 @@ int qhk_reconstruct(const void* fields, int count, int n, const float* illum_fyf
     const std::size_t nf = static_cast<std::size_t>(count) * n * n;
     qhk::DevBuf<float2> d_fields(nf);
     qhk::DevBuf<float> d_index(plan.volume());
-    qhk::check(cudaMemcpyAsync(d_fields.get(), fields, nf * sizeof(float2), cudaMemcpyHostToDevice, stream.get()),
-               "upload fields");
+    qhk::upload(d_fields.get(), fields, nf * sizeof(float2), stream.get());
     plan.run(d_fields.get(), d_index.get(), stream.get());
-    qhk::check(cudaMemcpyAsync(out, d_index.get(), plan.volume() * sizeof(float), cudaMemcpyDeviceToHost,
-                               stream.get()),
-               "download index");
+    qhk::download(out, d_index.get(), plan.volume() * sizeof(float), stream.get());
     unsigned long long v = 0;
     qhk::check(cudaMemcpyAsync(&v, plan.filled(), sizeof v, cudaMemcpyDeviceToHost, stream.get()), "download filled");
     qhk::check(cudaStreamSynchronize(stream.get()), "reconstruct");
@@ -319,12 +316,9 @@ int qhk_extract_fields(const float* holo, int count, int n, float cy, float cx, 
     const std::size_t nout = static_cast<std::size_t>(count) * crop.out * crop.out;
     qhk::DevBuf<float> d_holo(nin);
     qhk::DevBuf<float2> d_out(nout);
-    qhk::check(cudaMemcpyAsync(d_holo.get(), holo, nin * sizeof(float), cudaMemcpyHostToDevice, stream.get()),
-               "upload holograms");
+    qhk::upload(d_holo.get(), holo, nin * sizeof(float), stream.get());
     plan.fields(d_holo.get(), d_out.get(), stream.get());
-    qhk::check(cudaMemcpyAsync(out, d_out.get(), nout * sizeof(float2), cudaMemcpyDeviceToHost, stream.get()),
-               "download fields");
-    qhk::check(cudaStreamSynchronize(stream.get()), "extract_fields");
+    qhk::download(out, d_out.get(), nout * sizeof(float2), stream.get());
   });
 }
 
@@ -338,11 +332,10 @@ int qhk_field_ratio(const void* sample, int count, int ny, int nx, const void* b
     const std::size_t plane = static_cast<std::size_t>(ny) * nx;
     const std::size_t total = plane * count;
     qhk::DevBuf<float2> ds(total), db(plane * bcount);
-    qhk::check(cudaMemcpyAsync(ds.get(), sample, ds.bytes(), cudaMemcpyHostToDevice, s), "upload sample");
-    qhk::check(cudaMemcpyAsync(db.get(), background, db.bytes(), cudaMemcpyHostToDevice, s), "upload background");
+    qhk::upload(ds.get(), sample, ds.bytes(), s);
+    qhk::upload(db.get(), background, db.bytes(), s);
     qhk::field_ratio(ds.get(), db.get(), plane, bcount == count && count > 1, total, ds.get(), s);
-    qhk::check(cudaMemcpyAsync(out, ds.get(), ds.bytes(), cudaMemcpyDeviceToHost, s), "download ratio");
-    qhk::check(cudaStreamSynchronize(s), "field_ratio");
+    qhk::download(out, ds.get(), ds.bytes(), s);
   });
 }
 
@@ -406,12 +399,9 @@ int qhk_unwrap(const float* wrapped, int count, int ny, int nx, float* out) {
     qhk::Stream stream;
     const std::size_t total = static_cast<std::size_t>(count) * ny * nx;
     qhk::DevBuf<float> psi(total), phi(total);
-    qhk::check(cudaMemcpyAsync(psi.get(), wrapped, total * sizeof(float), cudaMemcpyHostToDevice, stream.get()),
-               "upload phase");
+    qhk::upload(psi.get(), wrapped, total * sizeof(float), stream.get());
     plan.unwrap(psi.get(), phi.get(), stream.get());
-    qhk::check(cudaMemcpyAsync(out, phi.get(), total * sizeof(float), cudaMemcpyDeviceToHost, stream.get()),
-               "download phase");
-    qhk::check(cudaStreamSynchronize(stream.get()), "unwrap");
+    qhk::download(out, phi.get(), total * sizeof(float), stream.get());
   });
 }
 
@@ -429,11 +419,10 @@ int qhk_rytov(const void* ratio, int count, int ny, int nx, void* out) {
     const std::size_t total = static_cast<std::size_t>(count) * ny * nx;
     qhk::DevBuf<float2> r(total);
     qhk::DevBuf<float> psi(total), logamp(total), phi(total);
-    qhk::check(cudaMemcpyAsync(r.get(), ratio, total * sizeof(float2), cudaMemcpyHostToDevice, s), "upload ratio");
+    qhk::upload(r.get(), ratio, total * sizeof(float2), s);
     qhk::split_ratio(r.get(), total, psi.get(), logamp.get(), s);
     plan.rytov(psi.get(), logamp.get(), phi.get(), r.get(), s);
-    qhk::check(cudaMemcpyAsync(out, r.get(), total * sizeof(float2), cudaMemcpyDeviceToHost, s), "download rytov");
-    qhk::check(cudaStreamSynchronize(s), "rytov");
+    qhk::download(out, r.get(), total * sizeof(float2), s);
   });
 }
 

@@ -4,6 +4,9 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <string>
+#include <stdexcept>
+#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -27,6 +30,102 @@ bool locked(const void* p) {
 bool is_page_locked(const void* p, std::size_t bytes) {
   if (p == nullptr || bytes == 0) return false;
   return locked(p) && locked(static_cast<const char*>(p) + bytes - 1);
+}
+
+namespace {
+
+constexpr std::size_t kChunk = std::size_t{32} << 20;
+
+// Two page-locked staging buffers and their "transfer done" events, created on first use and kept
+// for the process (never freed: at exit the CUDA runtime may already be gone).
+struct Staging {
+  std::mutex mu;
+  void* buf[2] = {};
+  cudaEvent_t done[2] = {};
+  int device = -1;
+};
+
+Staging& staging() {
+  static auto* st = new Staging;
+  return *st;
+}
+
+// Buffers of the current device (recreated if the calling thread's device changed).
+void ensure_staging(Staging& st) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("transfer: cudaGetDevice failed");
+  if (st.device == dev && st.buf[0]) return;
+  for (int i = 0; i < 2; ++i) {
+    if (!st.buf[i] && cudaMallocHost(&st.buf[i], kChunk) != cudaSuccess) {
+      throw std::runtime_error("transfer: cudaMallocHost failed");
+    }
+    if (st.done[i]) cudaEventDestroy(st.done[i]);
+    if (cudaEventCreateWithFlags(&st.done[i], cudaEventDisableTiming) != cudaSuccess) {
+      throw std::runtime_error("transfer: cudaEventCreate failed");
+    }
+  }
+  st.device = dev;
+}
+
+void ok(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+void upload(void* d_dst, const void* host_src, std::size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  if (is_page_locked(host_src, bytes)) {
+    ok(cudaMemcpyAsync(d_dst, host_src, bytes, cudaMemcpyHostToDevice, s), "upload");
+    ok(cudaStreamSynchronize(s), "upload");
+    return;
+  }
+  Staging& st = staging();
+  std::lock_guard<std::mutex> lk(st.mu);
+  ensure_staging(st);
+  HostCopier& copier = HostCopier::shared();
+  for (std::size_t off = 0, k = 0; off < bytes; off += kChunk, ++k) {
+    const int b = static_cast<int>(k & 1);
+    const std::size_t len = std::min(kChunk, bytes - off);
+    if (k >= 2) ok(cudaEventSynchronize(st.done[b]), "upload");  // buffer b's previous transfer
+    copier.copy(st.buf[b], static_cast<const char*>(host_src) + off, len);
+    ok(cudaMemcpyAsync(static_cast<char*>(d_dst) + off, st.buf[b], len, cudaMemcpyHostToDevice, s), "upload");
+    ok(cudaEventRecord(st.done[b], s), "upload");
+  }
+  ok(cudaStreamSynchronize(s), "upload");
+}
+
+void download(void* host_dst, const void* d_src, std::size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  if (is_page_locked(host_dst, bytes)) {
+    ok(cudaMemcpyAsync(host_dst, d_src, bytes, cudaMemcpyDeviceToHost, s), "download");
+    ok(cudaStreamSynchronize(s), "download");
+    return;
+  }
+  Staging& st = staging();
+  std::lock_guard<std::mutex> lk(st.mu);
+  ensure_staging(st);
+  HostCopier& copier = HostCopier::shared();
+  const std::size_t chunks = (bytes + kChunk - 1) / kChunk;
+  const auto issue = [&](std::size_t k) {
+    const int b = static_cast<int>(k & 1);
+    const std::size_t off = k * kChunk;
+    ok(cudaMemcpyAsync(st.buf[b], static_cast<const char*>(d_src) + off, std::min(kChunk, bytes - off),
+                       cudaMemcpyDeviceToHost, s),
+       "download");
+    ok(cudaEventRecord(st.done[b], s), "download");
+  };
+  issue(0);
+  // The destination's page faults (a fresh array) are taken while the device finishes the work
+  // queued before this call and the first chunk is in flight.
+  copier.touch(host_dst, bytes);
+  for (std::size_t k = 0; k < chunks; ++k) {
+    const int b = static_cast<int>(k & 1);
+    ok(cudaEventSynchronize(st.done[b]), "download");
+    if (k + 1 < chunks) issue(k + 1);  // the next chunk lands while this one is copied out
+    const std::size_t off = k * kChunk;
+    copier.copy(static_cast<char*>(host_dst) + off, st.buf[b], std::min(kChunk, bytes - off));
+  }
 }
 
 HostCopier::HostCopier(int threads) {

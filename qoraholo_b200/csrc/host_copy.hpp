@@ -12,11 +12,23 @@
 #include <thread>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 namespace qhk {
 
 // Whether [p, p + bytes) is page-locked host memory (both ends lie in page-locked allocations, so
 // the device can transfer it directly without a staging copy).
 bool is_page_locked(const void* p, std::size_t bytes);
+
+// Host <-> device transfers of caller memory for one-shot calls: page-locked memory goes directly;
+// pageable memory streams through two page-locked staging buffers of kChunk bytes (kept for the
+// process), the host copy of one chunk overlapping the transfer of the other, on the shared copy
+// threads (a download writes every page of its destination first: its contents are unspecified
+// until it returns). Synchronous with respect to the host buffer: upload returns when the source may be
+// reused, download when the destination holds the data (both wait for `s`). One transfer at a time
+// per process (a mutex); the device side is ordered on `s`.
+void upload(void* d_dst, const void* host_src, std::size_t bytes, cudaStream_t s);
+void download(void* host_dst, const void* d_src, std::size_t bytes, cudaStream_t s);
 
 class HostCopier {
  public:
