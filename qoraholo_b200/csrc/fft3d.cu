@@ -313,6 +313,75 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// One boundary between two Gerchberg-Papoulis steps on rows, in place: the C2R of the half spectra,
+// the real-space constraint max(x, 0) and the R2C of the constrained rows, without the real rows
+// going through HBM. The operations are those of k_rows_c2r (store) followed by k_rows_r2c (Clamp)
+// on the same values, so the half spectra are bitwise the same. Each CTA reads all its rows before
+// it writes any, so `e` is updated in place.
+template <int COLS, int MC>
+__global__ void __launch_bounds__(kThreads)
+    k_rows_c2r_r2c(float2* __restrict__ e, std::size_t rows, FftLen Lm, const float2* __restrict__ twn) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  const int M = MC > 0 ? MC : Lm.n;
+  const int h = M + 1;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(h) * cp;
+  const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
+  const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
+  const int tid = static_cast<int>(threadIdx.x);
+  const int nth = static_cast<int>(blockDim.x);
+
+  for (int idx = tid; idx < h * COLS; idx += nth) {
+    const int row = idx / h;
+    const int k = idx - row * h;
+    A[k * cp + row] = row < nr ? e[(r0 + row) * h + k] : make_float2(0.0f, 0.0f);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < M * COLS; idx += nth) {
+    const int k = idx / COLS;
+    const int row = idx - k * COLS;
+    float2 xk = A[k * cp + row];
+    float2 xm = A[(M - k) * cp + row];
+    if (k == 0) {  // a real signal has real bins 0 and M; their imaginary parts drop out
+      xk.y = 0.0f;
+      xm.y = 0.0f;
+    }
+    const float2 sv = make_float2(xk.x + xm.x, xk.y - xm.y);  // xk + conj(xm)
+    const float2 d = make_float2(xk.x - xm.x, xk.y + xm.y);   // xk - conj(xm)
+    const float2 w = __ldg(twn + k);
+    const float2 t = cmulc(d, w);                              // d * e^{+2 pi i k / nx}
+    B[k * cp + row] = make_float2(sv.x - t.y, sv.y + t.x);     // sv + i t
+  }
+  __syncthreads();
+  float2* real = row_fft<false, COLS, MC>(B, A, cp, Lm, tid, nth);  // real samples 2m, 2m+1 of each row
+  for (int idx = tid; idx < M * COLS; idx += nth) {
+    const int row = idx / M;
+    const int m = idx - row * M;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (row < nr) {
+      v = real[m * cp + row];
+      v = make_float2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
+    }
+    real[m * cp + row] = v;
+  }
+  __syncthreads();
+  const float2* res = row_fft<true, COLS, MC>(real, real == A ? B : A, cp, Lm, tid, nth);
+
+  for (int idx = tid; idx < h * COLS; idx += nth) {
+    const int row = idx / h;
+    const int k = idx - row * h;
+    if (row >= nr) continue;
+    const float2 zk = res[(k == M ? 0 : k) * cp + row];
+    const float2 zm = res[(k == 0 ? 0 : M - k) * cp + row];
+    const float2 ev = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
+    const float2 od = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
+    const float2 w = __ldg(twn + k);
+    e[(r0 + row) * h + k] = cadd(ev, cmul(w, od));
+  }
+}
+
 // ---- complex rows -----------------------------------------------------------------------------------
 
 template <bool Fwd, int Mode, int COLS, int NC>
@@ -389,6 +458,18 @@ void launch_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp,
     k_rows_r2c<false, COLS, MC><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
   }
   check_launch("rows r2c");
+}
+
+template <int COLS, int MC>
+void launch_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s) {
+  const int M = nx / 2;
+  const FftLen& Lm = fft_len(M);
+  const FftLen& Ln = fft_len(nx);
+  const std::size_t smem = 2 * static_cast<std::size_t>(M + 1) * (COLS + 1) * sizeof(float2);
+  const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
+  allow_smem(k_rows_c2r_r2c<COLS, MC>, smem);
+  k_rows_c2r_r2c<COLS, MC><<<grid, kThreads, smem, s>>>(e, rows, Lm, Ln.tw);
+  check_launch("rows c2r r2c");
 }
 
 template <int COLS, int MC>
@@ -572,6 +653,26 @@ void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode,
     case 4: launch_c2r<4, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
     case 2: launch_c2r<2, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
     default: launch_c2r<1, 0>(e, x, rows, nx, mode, nm2, inv_k02, s); break;
+  }
+}
+
+void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s) {
+  require(nx >= 2 && nx % 2 == 0, "rfft: row length must be even");
+  switch (nx / 2) {
+#define QHK_C2R_R2C(M)                                    \
+  case M:                                                 \
+    launch_c2r_r2c<rows_per_cta(M), M>(e, rows, nx, s);   \
+    return;
+    QHK_FIXED_LENGTHS(QHK_C2R_R2C)
+#undef QHK_C2R_R2C
+    default: break;
+  }
+  switch (rows_per_cta(nx / 2)) {
+    case 16: launch_c2r_r2c<16, 0>(e, rows, nx, s); break;
+    case 8: launch_c2r_r2c<8, 0>(e, rows, nx, s); break;
+    case 4: launch_c2r_r2c<4, 0>(e, rows, nx, s); break;
+    case 2: launch_c2r_r2c<2, 0>(e, rows, nx, s); break;
+    default: launch_c2r_r2c<1, 0>(e, rows, nx, s); break;
   }
 }
 

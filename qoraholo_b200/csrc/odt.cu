@@ -240,8 +240,8 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
     a_.reset(b * half_);
     hits_.reset(b * half_);
     e_.reset(b * half_);
-    x_.reset(b * vol_);
-    if (cfg_.tv) {
+    if (cfg_.tv) {  // GP keeps its real rows on chip (rows_c2r_r2c)
+      x_.reset(b * vol_);
       xprev_.reset(vol_);
       dual_.reset(12 * vol_);
       for (int i = 0; i < 4; ++i)
@@ -350,6 +350,18 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
   // E = a * inv, inverse along z, then y, then C2R along x.
   axis_pass(e, n, h, nz, nh, h, false, AxisMode::from_data, inv, aux, s, b, half_);
   axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+  if (!cfg_.tv) {
+    // GP: x = C2R(E); each step clamps x, R2C, y, z restore, y, C2R. The C2R, the clamp and the next
+    // R2C run as one row pass, so x stays on chip between steps; the last C2R writes the index.
+    for (int it = 0; it < cfg_.iterations; ++it) {
+      rows_c2r_r2c(e, rows, n, s);
+      axis_pass(e, b * nz, nh, n, h, h, true, AxisMode::plain, 1.0f, AxisAux{}, s);
+      axis_pass(e, n, h, nz, nh, h, true, AxisMode::restore_half, inv, aux, s, b, half_);
+      axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+    }
+    rows_c2r(e, index, rows, n, C2rMode::index, cfg_.nm2, cfg_.inv_k02, s);
+    return;
+  }
   rows_c2r(e, x_.get(), rows, n, C2rMode::store, cfg_.nm2, cfg_.inv_k02, s);
   const auto kspace_step = [&](const float* in, bool clamp, float* out, C2rMode mode) {
     rows_r2c(in, e, rows, n, clamp, s);
@@ -358,13 +370,6 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
     axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
     rows_c2r(e, out, rows, n, mode, cfg_.nm2, cfg_.inv_k02, s);
   };
-  if (!cfg_.tv) {
-    for (int it = 0; it < cfg_.iterations; ++it) {
-      const bool last = it == cfg_.iterations - 1;
-      kspace_step(x_.get(), true, last ? index : x_.get(), last ? C2rMode::index : C2rMode::store);
-    }
-    return;
-  }
   // FISTA-TV: y lives in x_ (it is also b, the C2R output), x_prev in xprev_, the dual in dual_.
   const std::size_t vbytes = vol_ * sizeof(float);
   check(cudaMemcpyAsync(xprev_.get(), x_.get(), vbytes, cudaMemcpyDeviceToDevice, s), "copy x");

@@ -50,6 +50,9 @@ void rows_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, c
 enum class C2rMode : int { store, index };
 void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
               cudaStream_t s);
+// rows_c2r (store) then the real-space constraint max(x, 0) and rows_r2c of the constrained rows, in
+// place on the half spectra `e`, the real rows never written out (one GP step boundary).
+void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s);
 
 // Complex rows of length nx (dense). Modes for the complex Gerchberg-Papoulis loop.
 enum class RowMode : int {
