@@ -57,6 +57,9 @@ class Pipeline {
   // The same into caller memory: holograms (count, N, N) -> index (nz, n, n), no intermediate
   // host buffers of the caller's size (qhk_pipeline_run).
   void run(std::span<const float> holograms, std::span<float> index);
+  // `items` stacks back to back -> `items` volumes back to back, the transfers of one stack
+  // overlapping the solve of the next (qhk_pipeline_run_stream). filled() is the last stack's.
+  void run_stream(std::span<const float> holograms, std::span<float> index, int items);
 
   [[nodiscard]] const PipelineTimings& timings() const;
   [[nodiscard]] double setup_ms() const;

@@ -256,6 +256,13 @@ int qhk_pipeline_process(qhk_pipeline* pipeline);
  * qhk_pinned_alloc's) are transferred directly instead, without staging or host copies. `input` and
  * `output` serve as the staging for pageable buffers and then hold this call's data. */
 int qhk_pipeline_run(qhk_pipeline* pipeline, const float* holograms, float* index);
+/* A stream of `items` runs (no counterpart in the reference, which reconstructs one stack per
+ * Pipeline::run): holograms (items, count, N, N) -> index (items, nz, m, m), host memory as for
+ * qhk_pipeline_run, synchronous. The upload of stack i + 1 and the download of volume i - 1 overlap
+ * the solve of stack i, so a stream costs about the device time of its stacks rather than that plus
+ * the transfers; each volume is bitwise what qhk_pipeline_run gives for its stack. Afterwards
+ * `filled` is that of the last stack and the timings hold only `total`. One more device volume. */
+int qhk_pipeline_run_stream(qhk_pipeline* pipeline, const float* holograms, int items, float* index);
 /* Device-resident variant: d_holo (count, N, N) and d_index (nz, m, m) on the device, asynchronous on
  * `stream`, no host copies (for serving loops and benchmarks). */
 int qhk_pipeline_process_device(qhk_pipeline* pipeline, const float* d_holo, float* d_index, void* stream);

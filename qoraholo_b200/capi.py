@@ -97,6 +97,7 @@ _PROTOS = {
     "qhk_pipeline_output": (_VP, [_VP]),
     "qhk_pipeline_process": (_I, [_VP]),
     "qhk_pipeline_run": (_I, [_VP, _VP, _VP]),
+    "qhk_pipeline_run_stream": (_I, [_VP, _VP, C.c_int, _VP]),
     "qhk_pipeline_process_device": (_I, [_VP, _VP, _VP, _VP]),
     "qhk_pipeline_result": (_I, [_VP, C.POINTER(C.c_double), _VP]),
     "qhk_pipeline_filled": (_I, [_VP, _VP, C.POINTER(C.c_double)]),
@@ -417,6 +418,20 @@ class Pipeline:
         elif out.shape != self.shape or out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
             raise ValueError(f"out must be a C-contiguous float32 array of shape {self.shape}")
         check(lib().qhk_pipeline_run(self._h, host_ptr(h), host_ptr(out)))
+        return out
+
+    def run_stream(self, holograms, out=None):
+        """qhk_pipeline_run_stream: host holograms (items, *input_shape) -> (items, *shape), the
+        transfers of each stack overlapping the solve of the next."""
+        h = np.ascontiguousarray(holograms, np.float32)
+        if h.ndim != 1 + len(self.input_shape) or h.shape[1:] != self.input_shape or h.shape[0] < 1:
+            raise ValueError(f"holograms must have shape (items, {', '.join(map(str, self.input_shape))})")
+        shape = (h.shape[0],) + tuple(self.shape)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        elif out.shape != shape or out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape {shape}")
+        check(lib().qhk_pipeline_run_stream(self._h, host_ptr(h), int(h.shape[0]), host_ptr(out)))
         return out
 
     def process_device(self, d_holo, d_index, stream=0):

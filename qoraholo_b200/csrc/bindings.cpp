@@ -330,6 +330,33 @@ PYBIND11_MODULE(_core, m) {
             return out;
           },
           py::arg("holograms"))
+      .def(
+          "run_stream",
+          [](Pipeline& p, In<float> holograms) {
+            if (holograms.ndim() != 4 || holograms.shape(0) < 1 ||
+                static_cast<std::size_t>(holograms.size()) != holograms.shape(0) * p.input().size() ||
+                holograms.shape(2) != holograms.shape(3)) {
+              throw std::invalid_argument("Pipeline.run_stream: shape must be (items, count, N, N)");
+            }
+            const auto [nz, ny, nx] = p.output_shape();
+            const int items = static_cast<int>(holograms.shape(0));
+            const std::size_t n = static_cast<std::size_t>(items) * nz * ny * nx;
+            auto* owner = new PooledBuffer{pinned_pool().take(n), n};
+            py::capsule release_buffer(owner, [](void* o) {
+              auto* b = static_cast<PooledBuffer*>(o);
+              pinned_pool().give(b->data, b->size);
+              delete b;
+            });
+            py::array_t<float> out({items, nz, ny, nx}, owner->data, release_buffer);
+            std::span<const float> in(holograms.data(), static_cast<std::size_t>(holograms.size()));
+            std::span<float> dst(owner->data, n);
+            {
+              py::gil_scoped_release release;
+              p.run_stream(in, dst, items);
+            }
+            return out;
+          },
+          py::arg("holograms"))
       .def_property_readonly("filled", &Pipeline::filled)
       .def_property_readonly("setup_ms", &Pipeline::setup_ms)
       .def_property_readonly("device_bytes", &Pipeline::device_bytes)

@@ -503,6 +503,13 @@ int qhk_pipeline_run(qhk_pipeline* p, const float* holograms, float* index) {
   });
 }
 
+int qhk_pipeline_run_stream(qhk_pipeline* p, const float* holograms, int items, float* index) {
+  return guard([&] {
+    qhk::require(p && holograms && index, "Pipeline: null argument");
+    p->plan.process_stream(holograms, index, items);
+  });
+}
+
 int qhk_pipeline_process_device(qhk_pipeline* p, const float* d_holo, float* d_index, void* stream) {
   return guard([&] {
     qhk::require(p && d_holo && d_index, "Pipeline: null argument");

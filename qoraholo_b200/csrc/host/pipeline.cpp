@@ -103,6 +103,20 @@ void Pipeline::run(std::span<const float> holograms, std::span<float> index) {
                                    t.normalize, t.solve, t.finish, t.download, t.total};
 }
 
+void Pipeline::run_stream(std::span<const float> holograms, std::span<float> index, int items) {
+  const auto [nz, ny, nx] = impl_->shape;
+  const std::size_t volume = static_cast<std::size_t>(nz) * ny * nx;
+  host::require(items >= 1 && holograms.size() == items * impl_->input_size,
+                "Pipeline::run_stream: shape must be (items, count, N, N)");
+  host::require(index.size() == items * volume, "Pipeline::run_stream: output must be (items, nz, n, n)");
+  if (!impl_->has_background) throw std::logic_error("Pipeline: set_background() first");
+  host::check(qhk_pipeline_run_stream(impl_->handle, holograms.data(), items, index.data()));
+  qhk_pipeline_timings t{};
+  host::check(qhk_pipeline_result(impl_->handle, &impl_->filled, &t));
+  impl_->timings = PipelineTimings{t.upload, t.fields, t.rytov,  t.fft2,     t.clear, t.mapping,
+                                   t.normalize, t.solve, t.finish, t.download, t.total};
+}
+
 OdtResult Pipeline::run(const Array3<float>& holograms) {
   host::require(holograms.ny == holograms.nx, "Pipeline::run: shape must be (count, N, N)");
   const auto [nz, ny, nx] = impl_->shape;

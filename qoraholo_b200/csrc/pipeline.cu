@@ -91,7 +91,8 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
   const int images = count_ * batch_;
   if (chunked_upload) {
     const cudaStream_t c = copy_.get();
-    check(cudaStreamWaitEvent(c, clock_.event(kStart), 0), "cudaStreamWaitEvent");
+    // holo_ is free once the field passes of the previous input have read it.
+    check(cudaStreamWaitEvent(c, holo_free_.get(), 0), "cudaStreamWaitEvent");
     for (int k = 0; k < chunks_; ++k) {
       const int first = k * chunk_;
       const int valid = std::min(chunk_, images - first);
@@ -100,6 +101,7 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
       if (host_src && host_src_locked) {
         src = host_src + first * image;  // page-locked caller memory: transferred directly
       } else if (host_src) {
+        chunk_done_[k].synchronize();  // the previous input's transfer out of this staging chunk
         HostCopier::shared().copy(input_.get() + first * image, host_src + first * image, valid * image * sizeof(float));
       }
       check(cudaMemcpyAsync(dst, src, valid * image * sizeof(float), cudaMemcpyHostToDevice, c), "upload holograms");
@@ -107,6 +109,7 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
       check(cudaStreamWaitEvent(s, chunk_done_[k].get(), 0), "cudaStreamWaitEvent");
       field_.spectra(dst, first, valid, s);
     }
+    holo_free_.record(s);
   } else {
     field_.spectra(d_holo, 0, images, s);
   }
@@ -173,6 +176,67 @@ void PipelinePlan::process_host(const float* holograms, float* index) {
   timings_.solve = clock_.ms(o + OdtPlan::kMarkNormalize, o + OdtPlan::kMarkSolve);
   timings_.finish = clock_.ms(o + OdtPlan::kMarkSolve, o + OdtPlan::kMarkFinish);
   timings_.download = clock_.ms(o + OdtPlan::kMarkFinish, kDownloaded);
+  timings_.total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void PipelinePlan::process_stream(const float* holograms, float* index, int items) {
+  if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
+  require(input_.get() != nullptr, "Pipeline: serving workspaces have no host stream");
+  require(holograms != nullptr && index != nullptr && items >= 1, "Pipeline: stream needs inputs and outputs");
+  const auto t0 = std::chrono::steady_clock::now();
+  const cudaStream_t s = compute_.get();
+  const cudaStream_t d = down_.get();
+  const std::size_t in_item = static_cast<std::size_t>(batch_) * count_ * crop_.n * crop_.n;
+  const std::size_t out_item = static_cast<std::size_t>(batch_) * odt_.volume();
+  const bool src_locked = is_page_locked(holograms, items * in_item * sizeof(float));
+  const bool dst_locked = is_page_locked(index, items * out_item * sizeof(float));
+  if (index_alt_.get() == nullptr) index_alt_.reset(out_item);
+  float* const slot[2] = {index_.get(), index_alt_.get()};
+  const std::size_t part = (out_item + kOutParts - 1) / kOutParts;
+  const auto part_len = [&](int j) {
+    const std::size_t off = j * part;
+    return off < out_item ? std::min(part, out_item - off) : std::size_t{0};
+  };
+  HostCopier& copier = HostCopier::shared();
+  // Output i from the page-locked staging into the caller's memory, part by part as each lands.
+  const auto collect = [&](int i) {
+    if (dst_locked) return;
+    float* const dst = index + i * out_item;
+    for (int j = 0; j < kOutParts; ++j) {
+      part_done_[j].synchronize();
+      copier.copy(dst + j * part, output_.get() + j * part, part_len(j) * sizeof(float));
+    }
+  };
+  for (int i = 0; i < items; ++i) {
+    const int k = i % 2;
+    // Slot k was last read back by the download of output i - 2.
+    if (i >= 2) check(cudaStreamWaitEvent(s, downloaded_[k].get(), 0), "cudaStreamWaitEvent");
+    compute(nullptr, true, background_.get(), slot[k], s, false, holograms + i * in_item, src_locked);
+    check(cudaMemcpyAsync(filled_host_.get(), odt_.filled(), batch_ * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, s),
+          "download filled");
+    solved_[k].record(s);
+    // While the device solves input i: the host copies out output i - 1 (downloaded meanwhile), and
+    // faults in the pages of output i. Output i's download reuses the staging only after that.
+    if (i >= 1) collect(i - 1);
+    if (!dst_locked) copier.touch(index + i * out_item, out_item * sizeof(float));
+    check(cudaStreamWaitEvent(d, solved_[k].get(), 0), "cudaStreamWaitEvent");
+    float* const down = dst_locked ? index + i * out_item : output_.get();
+    for (int j = 0; j < kOutParts; ++j) {
+      if (part_len(j) > 0) {
+        check(cudaMemcpyAsync(down + j * part, slot[k] + j * part, part_len(j) * sizeof(float),
+                              cudaMemcpyDeviceToHost, d),
+              "download index");
+      }
+      part_done_[j].record(d);
+    }
+    downloaded_[k].record(d);
+  }
+  collect(items - 1);
+  check(cudaStreamSynchronize(d), "stream download");
+  check(cudaStreamSynchronize(s), "stream");
+  filled_ = static_cast<double>(*filled_host_.get()) / static_cast<double>(odt_.volume());
+  timings_ = PipelineTimes{};
   timings_.total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 

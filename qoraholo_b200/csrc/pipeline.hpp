@@ -38,6 +38,12 @@ class PipelinePlan {
   // buffers are transferred directly, without staging or host copies. Either pointer may be null:
   // the input is then taken from input(), the volume left in output().
   void process_host(const float* holograms, float* index);
+  // `items` inputs of process_host back to back -> `items` outputs back to back, caller memory,
+  // synchronous. Streamed: the upload of input i + 1 and the download of output i - 1 run while
+  // input i is solved (two device volumes alternate, the downloads on their own stream), and the host
+  // stages the next input and copies out the previous output meanwhile. Each output is bitwise that
+  // of process_host on its input; timings() then holds only the total.
+  void process_stream(const float* holograms, float* index, int items);
   // Holograms already on the device -> index on the device, asynchronous on `s` (no host copies).
   void process_device(const float* d_holo, float* d_index, cudaStream_t s);
   // The same replayed as one CUDA graph (captured on the second call for these buffers; the first
@@ -100,6 +106,11 @@ class PipelinePlan {
   DevBuf<float> logamp_;
   DevBuf<float> phi_;
   DevBuf<float> index_;
+  DevBuf<float> index_alt_;  // the second device volume of process_stream, allocated by its first call
+  Stream down_;              // process_stream's downloads
+  Event holo_free_;          // on compute_: the field passes have read holo_ (the next upload may start)
+  Event solved_[2];          // process_stream: volume slot k written
+  Event downloaded_[2];      // process_stream: volume slot k read back
   std::vector<Event> chunk_done_;
   std::vector<Event> part_done_;
   StageClock clock_;

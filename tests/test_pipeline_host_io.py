@@ -157,3 +157,97 @@ def test_public_results_stay_valid_across_runs(cuda):
     for r, c in zip(held, copies):
         assert np.array_equal(r, c)
     assert not np.array_equal(held[0], held[1])
+
+
+@pytest.mark.parametrize("odt", [dict(iterations=3, solver="tv", tv_inner=4, nz=26),
+                                 dict(iterations=4, solver="gp")])
+@pytest.mark.parametrize("items,chunks", [(1, 1), (2, 4), (5, 3)])
+def test_stream_equals_runs(cuda, odt, items, chunks):
+    """qhk_pipeline_run_stream over `items` different stacks gives, volume by volume, bitwise what
+    qhk_pipeline_run gives for each stack (the two device volumes alternate, the transfers overlap
+    the solves), into a new array or a caller array that is not page aligned; filled is the last
+    stack's; a single run afterwards is unaffected."""
+    from qoraholo_b200 import capi
+
+    il, bg, stacks = _stacks(items, seed=11)
+    p = _pipeline(capi, il, bg, upload_chunks=chunks, **odt)
+    want, filled = [], []
+    for h in stacks:
+        want.append(p.run(h))
+        filled.append(p.result()[0])
+    holo = np.stack(stacks)
+    got = p.run_stream(holo)
+    assert got.shape == (items,) + tuple(p.shape)
+    for i in range(items):
+        assert np.array_equal(got[i], want[i]), i
+    assert p.result()[0] == filled[-1] and p.result()[1]["total"] > 0
+    raw = np.empty(got.size + 1, np.float32)
+    dst = raw[1:].reshape(got.shape)
+    assert p.run_stream(holo, out=dst) is dst and np.array_equal(dst, got)
+    assert np.array_equal(p.run(stacks[0]), want[0])
+    p.close()
+
+
+def test_stream_on_page_locked_buffers(cuda):
+    """Page-locked holograms and volumes go straight between the caller's buffers and the device."""
+    from qoraholo_b200 import capi
+
+    il, bg, stacks = _stacks(3, seed=12)
+    p = _pipeline(capi, il, bg, iterations=3, solver="tv", tv_inner=4, upload_chunks=4)
+    want = [p.run(h) for h in stacks]
+    holo = capi.pinned_array((3,) + stacks[0].shape)
+    out = capi.pinned_array((3,) + tuple(p.shape))
+    holo[...] = np.stack(stacks)
+    out[...] = -1.0
+    assert p.run_stream(holo, out=out) is out
+    for i in range(3):
+        assert np.array_equal(out[i], want[i]), i
+    p.close()
+
+
+def test_batched_stream_equals_batched_runs(cuda):
+    from qoraholo_b200 import capi
+
+    B, items = 2, 3
+    il, bg, stacks = _stacks(B * items, seed=13)
+    p = _pipeline(capi, il, bg, iterations=3, solver="gp", batch=B)
+    inputs = [np.concatenate(stacks[B * i:B * (i + 1)]) for i in range(items)]
+    want = [p.run(h) for h in inputs]
+    got = p.run_stream(np.stack(inputs))
+    assert got.shape == (items, B) + tuple(p.shape[1:])
+    for i in range(items):
+        assert np.array_equal(got[i], want[i]), i
+    p.close()
+
+
+def test_public_pipeline_run_stream(cuda):
+    """qoraholo_b200.Pipeline.run_stream ((items, count, N, N) numpy in, (items, nz, n, n) out) equals
+    Pipeline.run per stack, and rejects inputs of the wrong shape."""
+    import qoraholo_b200 as qh
+
+    il, bg, stacks = _stacks(3, seed=14)
+    geom = qh.Geometry(wavelength=float(G[0]), n_medium=float(G[1]), na=float(G[2]), pixel=float(G[3]))
+    api = qh.Pipeline(9, 64, (18, 18), il, geom, radius=14.0, output_size=34, upload_chunks=3, iterations=3,
+                      solver="tv", tv_inner=4)
+    api.set_background(bg)
+    want = [api.run(h).copy() for h in stacks]
+    got = api.run_stream(np.stack(stacks))
+    assert got.shape == (3,) + want[0].shape
+    for i in range(3):
+        assert np.array_equal(got[i], want[i]), i
+    with pytest.raises(ValueError):
+        api.run_stream(stacks[0])
+    with pytest.raises(ValueError):
+        api.run_stream(np.stack(stacks)[:, :8])
+
+
+def test_stream_rejects_wrong_shapes(cuda):
+    from qoraholo_b200 import capi
+
+    il, bg, stacks = _stacks(1)
+    p = _pipeline(capi, il, bg, iterations=1, solver="gp")
+    with pytest.raises(ValueError):
+        p.run_stream(stacks[0])
+    with pytest.raises(ValueError):
+        p.run_stream(stacks[0][None], out=np.empty((1, 3, 3), np.float32))
+    p.close()
