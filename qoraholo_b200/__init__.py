@@ -137,6 +137,12 @@ class Pipeline:
         """Sample holograms (count, N, N) to the index volume (nz, n, n)."""
         return self._p.run(np.ascontiguousarray(holograms, dtype=np.float32))
 
+    def run_stream(self, holograms):
+        """A stream of stacks (items, count, N, N) to volumes (items, nz, n, n): each stack's upload
+        and each volume's download overlap the solve of its neighbour; each volume is bitwise what
+        ``run`` gives for its stack. ``filled`` is then the last stack's."""
+        return self._p.run_stream(np.ascontiguousarray(holograms, dtype=np.float32))
+
     @property
     def filled(self) -> float:
         return self._p.filled

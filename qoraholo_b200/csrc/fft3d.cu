@@ -382,6 +382,86 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// The end of one FISTA-TV iteration and the start of the next on rows: the final primal of the
+// proximal step x = max(b - lambda div p, 0) (as k_tv_final: the same additions in the same order),
+// the FISTA point y = x + m (x - xprev), xprev <- x, and the R2C of y's rows into the half spectra e,
+// y itself never written to HBM. Each row r = z * ny + y of the volume (dense (nz, ny, 2M)) is one
+// column of the tile; its divergence reads p_z of plane z - 1 and p_y of row y - 1 from HBM (L2).
+template <int COLS, int MC>
+__global__ void __launch_bounds__(kThreads)
+    k_rows_tv_final_r2c(const float* __restrict__ b, const float* __restrict__ pz, const float* __restrict__ py,
+                        const float* __restrict__ px, int nz, int ny, float lambda, float momentum,
+                        float* __restrict__ xprev, float2* __restrict__ e, std::size_t rows, FftLen Lm,
+                        const float2* __restrict__ twn) {
+  extern __shared__ float2 sm[];
+  constexpr int cp = COLS + 1;
+  const int M = MC > 0 ? MC : Lm.n;
+  const int h = M + 1;
+  const int nx = 2 * M;
+  const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
+  float2* A = sm;
+  float2* B = sm + static_cast<std::size_t>(h) * cp;
+  const std::size_t r0 = static_cast<std::size_t>(blockIdx.x) * COLS;
+  const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
+  const int tid = static_cast<int>(threadIdx.x);
+  const int nth = static_cast<int>(blockDim.x);
+
+  for (int idx = tid; idx < M * COLS; idx += nth) {
+    const int row = idx / M;
+    const int m = idx - row * M;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (row < nr) {
+      const std::size_t r = r0 + row;
+      const int y = static_cast<int>(r % static_cast<std::size_t>(ny));
+      const int z = static_cast<int>(r / static_cast<std::size_t>(ny));
+      const std::size_t i0 = r * nx + 2 * m;
+      const float2 bv = *reinterpret_cast<const float2*>(b + i0);
+      const float2 cz = *reinterpret_cast<const float2*>(pz + i0);
+      const float2 cy = *reinterpret_cast<const float2*>(py + i0);
+      const float2 cx = *reinterpret_cast<const float2*>(px + i0);
+      const float2 pv = *reinterpret_cast<const float2*>(xprev + i0);
+      float2 bz = make_float2(0.0f, 0.0f), by = make_float2(0.0f, 0.0f);
+      if (z > 0) bz = *reinterpret_cast<const float2*>(pz + i0 - nxy);
+      if (y > 0) by = *reinterpret_cast<const float2*>(py + i0 - nx);
+      const float left = m > 0 ? px[i0 - 1] : 0.0f;
+      const float bb[2] = {bv.x, bv.y}, czz[2] = {cz.x, cz.y}, cyy[2] = {cy.x, cy.y}, cxx[2] = {cx.x, cx.y};
+      const float bzz[2] = {bz.x, bz.y}, byy[2] = {by.x, by.y}, pvv[2] = {pv.x, pv.y};
+      float xv[2], yv[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int x = 2 * m + i;
+        float sdiv = 0.0f;
+        if (z < nz - 1) sdiv = __fadd_rn(sdiv, czz[i]);
+        if (z > 0) sdiv = __fsub_rn(sdiv, bzz[i]);
+        if (y < ny - 1) sdiv = __fadd_rn(sdiv, cyy[i]);
+        if (y > 0) sdiv = __fsub_rn(sdiv, byy[i]);
+        if (x < nx - 1) sdiv = __fadd_rn(sdiv, cxx[i]);
+        if (x > 0) sdiv = __fsub_rn(sdiv, i == 0 ? left : cxx[0]);
+        xv[i] = tv_primal(bb[i], lambda, sdiv);
+        yv[i] = __fadd_rn(xv[i], __fmul_rn(momentum, __fsub_rn(xv[i], pvv[i])));
+      }
+      *reinterpret_cast<float2*>(xprev + i0) = make_float2(xv[0], xv[1]);
+      v = make_float2(yv[0], yv[1]);
+    }
+    A[m * cp + row] = v;
+  }
+  __syncthreads();
+  const float2* res = row_fft<true, COLS, MC>(A, B, cp, Lm, tid, nth);
+
+  for (int idx = tid; idx < h * COLS; idx += nth) {
+    const int row = idx / h;
+    const int k = idx - row * h;
+    if (row >= nr) continue;
+    const float2 zk = res[(k == M ? 0 : k) * cp + row];
+    const float2 zm = res[(k == 0 ? 0 : M - k) * cp + row];
+    const float2 ev = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    const float2 d = make_float2(zk.x - zm.x, zk.y + zm.y);  // zk - conj(zm)
+    const float2 od = make_float2(0.5f * d.y, -0.5f * d.x);   // d / (2i)
+    const float2 w = __ldg(twn + k);
+    e[(r0 + row) * h + k] = cadd(ev, cmul(w, od));
+  }
+}
+
 // ---- complex rows -----------------------------------------------------------------------------------
 
 template <bool Fwd, int Mode, int COLS, int NC>
@@ -458,6 +538,21 @@ void launch_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp,
     k_rows_r2c<false, COLS, MC><<<grid, kThreads, smem, s>>>(x, e, rows, nx, Lm, Ln.tw);
   }
   check_launch("rows r2c");
+}
+
+template <int COLS, int MC>
+void launch_tv_final_r2c(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda,
+                         float momentum, float* xprev, float2* e, cudaStream_t s) {
+  const int M = nx / 2;
+  const FftLen& Lm = fft_len(M);
+  const FftLen& Ln = fft_len(nx);
+  const std::size_t rows = static_cast<std::size_t>(nz) * ny;
+  const std::size_t smem = 2 * static_cast<std::size_t>(M + 1) * (COLS + 1) * sizeof(float2);
+  const unsigned grid = static_cast<unsigned>((rows + COLS - 1) / COLS);
+  allow_smem(k_rows_tv_final_r2c<COLS, MC>, smem);
+  k_rows_tv_final_r2c<COLS, MC><<<grid, kThreads, smem, s>>>(b, p[0], p[1], p[2], nz, ny, lambda, momentum, xprev,
+                                                              e, rows, Lm, Ln.tw);
+  check_launch("rows tv final r2c");
 }
 
 template <int COLS, int MC>
@@ -673,6 +768,27 @@ void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s) {
     case 4: launch_c2r_r2c<4, 0>(e, rows, nx, s); break;
     case 2: launch_c2r_r2c<2, 0>(e, rows, nx, s); break;
     default: launch_c2r_r2c<1, 0>(e, rows, nx, s); break;
+  }
+}
+
+void rows_tv_final_r2c(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda, float momentum,
+                       float* xprev, float2* e, cudaStream_t s) {
+  require(nx >= 2 && nx % 2 == 0 && nz >= 1 && ny >= 1, "rfft: row length must be even");
+  switch (nx / 2) {
+#define QHK_TVF_R2C(M)                                                                           \
+  case M:                                                                                        \
+    launch_tv_final_r2c<rows_per_cta(M), M>(b, p, nz, ny, nx, lambda, momentum, xprev, e, s);    \
+    return;
+    QHK_FIXED_LENGTHS(QHK_TVF_R2C)
+#undef QHK_TVF_R2C
+    default: break;
+  }
+  switch (rows_per_cta(nx / 2)) {
+    case 16: launch_tv_final_r2c<16, 0>(b, p, nz, ny, nx, lambda, momentum, xprev, e, s); break;
+    case 8: launch_tv_final_r2c<8, 0>(b, p, nz, ny, nx, lambda, momentum, xprev, e, s); break;
+    case 4: launch_tv_final_r2c<4, 0>(b, p, nz, ny, nx, lambda, momentum, xprev, e, s); break;
+    case 2: launch_tv_final_r2c<2, 0>(b, p, nz, ny, nx, lambda, momentum, xprev, e, s); break;
+    default: launch_tv_final_r2c<1, 0>(b, p, nz, ny, nx, lambda, momentum, xprev, e, s); break;
   }
 }
 

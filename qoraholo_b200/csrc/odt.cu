@@ -376,13 +376,28 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
   check(cudaMemsetAsync(dual_.get(), 0, 3 * vbytes, s), "cudaMemset");
   tv_.p_index = 0;
   float t = 1.0f;
+  // Between iterations the final primal, the momentum point y and y's R2C run as one row pass
+  // (rows_tv_final_r2c), so y is never written: the next k-space step starts from its spectra.
   for (int it = 0; it < cfg_.iterations; ++it) {
     const bool last = it == cfg_.iterations - 1;
-    kspace_step(x_.get(), false, x_.get(), C2rMode::store);
+    if (it == 0) {
+      kspace_step(x_.get(), false, x_.get(), C2rMode::store);
+    } else {
+      axis_pass(e, b * nz, nh, n, h, h, true, AxisMode::plain, 1.0f, AxisAux{}, s);
+      axis_pass(e, n, h, nz, nh, h, true, AxisMode::restore_half, inv, aux, s, b, half_);
+      axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
+      rows_c2r(e, x_.get(), rows, n, C2rMode::store, cfg_.nm2, cfg_.inv_k02, s);
+    }
     const float tn = fista_t(t);
     const float m = (t - 1.0f) / tn;
-    tv_prox(x_.get(), tv_, nz, n, n, cfg_.lambda, cfg_.tv_inner, last ? TvFinal::index : TvFinal::momentum, m,
-            xprev_.get(), last ? index : x_.get(), cfg_.nm2, cfg_.inv_k02, s);
+    if (last) {
+      tv_prox(x_.get(), tv_, nz, n, n, cfg_.lambda, cfg_.tv_inner, TvFinal::index, m, xprev_.get(), index,
+              cfg_.nm2, cfg_.inv_k02, s);
+    } else {
+      tv_prox(x_.get(), tv_, nz, n, n, cfg_.lambda, cfg_.tv_inner, TvFinal::none, m, xprev_.get(), x_.get(),
+              cfg_.nm2, cfg_.inv_k02, s);
+      rows_tv_final_r2c(x_.get(), tv_.v[tv_.p_index], nz, n, n, cfg_.lambda, m, xprev_.get(), e, s);
+    }
     t = tn;
   }
 }

@@ -53,6 +53,11 @@ void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode,
 // rows_c2r (store) then the real-space constraint max(x, 0) and rows_r2c of the constrained rows, in
 // place on the half spectra `e`, the real rows never written out (one GP step boundary).
 void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s);
+// The final primal of a proximal TV step with FISTA momentum (tv_prox's TvFinal::momentum on dual p),
+// then rows_r2c (no clamp) of the extrapolated point into `e`, without writing it: xprev <- x,
+// e <- R2C(x + momentum (x - xprev)). Volumes dense (nz, ny, nx), nx even, 8-byte aligned.
+void rows_tv_final_r2c(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda, float momentum,
+                       float* xprev, float2* e, cudaStream_t s);
 
 // Complex rows of length nx (dense). Modes for the complex Gerchberg-Papoulis loop.
 enum class RowMode : int {
@@ -83,6 +88,7 @@ enum class TvFinal : int {
   plain,     // out = argmin
   momentum,  // x = argmin; y = x + m (x - xprev); xprev <- x; out <- y
   index,     // out = refractive index of argmin
+  none,      // no primal: the dual is left in t.v[t.p_index] (rows_tv_final_r2c takes it from there)
 };
 // `inner` FGP steps on the dual started from p, then the final primal. b and all volumes are dense
 // (nz, ny, nx). For `momentum` the primal goes to xprev (in place) and the extrapolated point to out

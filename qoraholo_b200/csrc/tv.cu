@@ -1438,6 +1438,7 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
     }
     if (inner > 0) t.p_index = ia;
   }
+  if (final_mode == TvFinal::none) return;
   float* const* p = t.v[t.p_index];
   if (vec == 4) {
     launch_final<4>(final_mode, b, p, nz, ny, nx, lambda, momentum, xprev, out, nm2, inv_k02, s);
