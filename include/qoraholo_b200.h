@@ -124,10 +124,17 @@ int qhk_tv_prox_workspace(const float* d_b, float* d_x, float* d_work, int work_
 int qhk_pinned_alloc(size_t bytes, void** ptr);
 int qhk_pinned_free(void* ptr);
 
-/* Bounded device waits that ran out since the library was loaded: the two-step FGP kernel waits
- * for its box loads (TMA) on mbarriers with an iteration limit, and a wait that gives up counts
- * here and ends the kernel early (the result is then invalid). 0 in every correct run. Synchronises
- * the device. */
+/* Bounded device waits (no counterpart in the reference, whose kernels have no device-side waits):
+ * the two-step FGP kernel waits for its box loads (TMA) on mbarriers with an iteration limit; a wait
+ * that gives up is counted and ends the kernel early, after a bounded wait for every load it still
+ * has in flight, so the context stays usable but that result is invalid. Pipelines, ODT plans, the
+ * server and qhk_tv_prox count in a counter of their own and turn a wait that ran out into
+ * QHK_TIMEOUT (std::runtime_error in C++, RuntimeError in Python) from the call that synchronises
+ * on the work: qhk_pipeline_process / run / run_stream, qhk_reconstruct, qhk_tv_prox, the server's
+ * result, and for device-form runs qhk_pipeline_filled / filled_batch / check_waits and
+ * qhk_odt_filled, qhk_bpm_reconstruct. qhk_wait_timeouts returns the count of the calls that have no
+ * counter of their own (qhk_tv_prox_device, qhk_tv_prox_workspace): 0 in every correct run. It reads
+ * the counter without waiting for work queued on other streams. */
 int qhk_wait_timeouts(uint64_t* count);
 
 /* Number of kernels this library has launched since it was loaded (for launch accounting). */
@@ -168,12 +175,15 @@ int qhk_rytov(const void* ratio, int count, int ny, int nx, void* out);
  * whose device memory is already reserved by its own allocator or HBM budget (where a library
  * allocation would fail or evict cached state), and real-time loops that must not pay for, or
  * synchronise on, allocation and release. All scratch lives in one static device array of about
- * 17.8 MB that every GPU loading the library holds until exit. Limits: even sides, ny and nx <= 1024,
- * count <= 4096, count * ny * nx <= 4194304 pixels; larger requests return QHK_INVALID_ARGUMENT.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress) for that
- * device; make that first call before any stream capture. Every call writes all the scratch it reads
- * (nothing must start at zero), asynchronously on `stream`; calls that overlap on the GPU share the
- * array and race, so serialise them (one stream, or events). */
+ * 17.8 MB that a GPU holds from the moment the library's module is loaded on it until exit. With lazy
+ * module loading (CUDA's default) that moment can be the first qhk_unwrap_noalloc call on the device,
+ * so a caller that sizes its own reservation to what is left should first make one warm-up call (or
+ * set CUDA_MODULE_LOADING=EAGER), and make that first call before any stream capture. Every call looks
+ * up the array's address on the current device (cudaGetSymbolAddress, which allocates nothing), so the
+ * function stays usable after a device reset. Limits: even sides, ny and nx <= 1024, count <= 4096,
+ * count * ny * nx <= 4194304 pixels; larger requests return QHK_INVALID_ARGUMENT. Every call writes
+ * all the scratch it reads (nothing must start at zero), asynchronously on `stream`; calls that overlap
+ * on the GPU share the array and race, so serialise them (one stream, or events). */
 int qhk_unwrap_noalloc(const float* d_wrapped, float* d_unwrapped, int count, int ny, int nx, void* stream);
 
 /* ---- Launch-shape autotuner (no counterpart in the reference, which uses cuFFT plans and fixed
@@ -217,6 +227,20 @@ int qhk_unwrap_batch_destroy(qhk_unwrap_batch* plan);
 int qhk_synthesize_holograms_device(const void* d_ratio, int count, int n, const float* illum_fyfx, double pixel,
                                     double carrier_y, double carrier_x, double amplitude, float noise, uint64_t seed,
                                     float* d_out, void* stream);
+
+/* Fixture generators of include/qoraholo/phantom.hpp, computed on the device (the reference computes
+ * them on the host: render_phantom src/phantom.cpp:84-100, forward_fields src/phantom.cpp:102-191).
+ * `spheres` are k rows of (z, y, x, radius, index) floats, micrometres from the volume centre, painted
+ * in order (each entirely inside or outside every earlier one). Host in, host out, synchronous.
+ * qhk_render_phantom: the index at the voxel centres of an (nz, n, n) volume of the geometry's pixel,
+ * bitwise the reference's double-precision evaluation. qhk_forward_fields: field ratios
+ * (count, n, n) complex64 at z = 0 for each illumination, model QHK_MODEL_BORN (1 + v),
+ * QHK_MODEL_RYTOV (e^v) or QHK_MODEL_EXACT (the scalar partial-wave solution of exactly one sphere,
+ * 1 + v); errors as the reference's (std::invalid_argument). */
+enum { QHK_MODEL_BORN = 0, QHK_MODEL_RYTOV = 1, QHK_MODEL_EXACT = 2 }; /* qoraholo::ScatteringModel */
+int qhk_render_phantom(const float* spheres, int k, const qhk_geometry* geometry, int nz, int n, float* out);
+int qhk_forward_fields(const float* spheres, int k, const float* illum_fyfx, int count, const qhk_geometry* geometry,
+                       int n, int model, void* out);
 
 /* ---- Pipeline: replaces cuda::make_pipeline and Pipeline::Impl (src/backends.hpp:75-89,
  * src/cuda/pipeline.cu:12-161). Validation of the Pipeline constructor (src/pipeline.cpp:72-91). */
@@ -268,8 +292,17 @@ int qhk_pipeline_run_stream(qhk_pipeline* pipeline, const float* holograms, int 
 int qhk_pipeline_process_device(qhk_pipeline* pipeline, const float* d_holo, float* d_index, void* stream);
 /* filled fraction and stage timings of the last process(). */
 int qhk_pipeline_result(const qhk_pipeline* pipeline, double* filled, qhk_pipeline_timings* timings);
-/* Filled fraction after process_device (waits for `stream`). */
+/* Filled fraction after process_device (waits for `stream`); QHK_TIMEOUT if a bounded device wait of
+ * the pipeline ran out since its last check (qhk_wait_timeouts). */
 int qhk_pipeline_filled(qhk_pipeline* pipeline, void* stream, double* filled);
+/* Waits for `stream` and returns QHK_TIMEOUT if a bounded device wait of the pipeline ran out since
+ * its last check (after device-form runs, which cannot report it themselves). */
+int qhk_pipeline_check_waits(qhk_pipeline* pipeline, void* stream);
+/* Test hook of the timeout path: one bounded wait (`polls` polls, 1 .. 2^20) on an mbarrier that
+ * nothing arrives at -- the form of the FGP kernel's waits -- counted in the pipeline's counter, on
+ * the pipeline's own stream; returns QHK_TIMEOUT as a run whose wait ran out does. No load is in
+ * flight, so the pipeline stays usable. */
+int qhk_pipeline_wait_probe(qhk_pipeline* pipeline, int polls);
 int qhk_pipeline_shape(const qhk_pipeline* pipeline, int* nz, int* ny, int* nx);
 /* Batched pipeline (no counterpart in the reference): `batch` requests of this geometry per run, each
  * pass one launch for all of them. Input (batch * count, N, N), output (batch, nz, m, m); the

@@ -185,6 +185,67 @@ int ref_reconstruct(const void* fields, int count, int n, const float* il, const
   });
 }
 
+// The Ewald mapping of cpu::reconstruct (src/cpu/odt.cpp:137-171) on given spectra, followed by the
+// Hermitian half data of src/cpu/odt.cpp:37-62: the grid from the reference's make_grid
+// (src/api.cpp:32-42), every bin from its detail::ewald_target, the sign from detail::parity, and
+// the half data from detail::hermitian_data and detail::negative_bin (src/common.hpp), so the
+// indices, hit counts and sums are the reference's own. The loop is the reference's (one k_z column
+// per iteration, illuminations in order, fiz in float). Outputs: a (nz, n, n/2+1) complex, hits
+// (nz, n, n/2+1) in {0, 1, 2}, and the filled-voxel count.
+int ref_ewald_half(const void* spectra, int count, int n, int nz, const float* il, const float* geom, void* a_out,
+                   unsigned char* hits_out, long long* filled) {
+  return guard([&] {
+    const Geometry gm = geometry(geom);
+    const detail::OdtGrid g = make_grid(n, nz, gm);
+    const auto ill = illum(il, count);
+    const auto* s = static_cast<const cfloat*>(spectra);
+    const std::size_t plane = static_cast<std::size_t>(n) * n;
+    std::vector<float> fiz(count);
+    for (int a = 0; a < count; ++a) {
+      fiz[a] = std::sqrt(g.fm2 - ill[a].fy * ill[a].fy - ill[a].fx * ill[a].fx);
+    }
+    std::vector<cfloat> pot(static_cast<std::size_t>(nz) * plane);
+    std::vector<float> weight(pot.size(), 0.0f);
+    for (int col = 0; col < static_cast<int>(plane); ++col) {
+      const int ky = col / n;
+      const int kx = col % n;
+      for (int a = 0; a < count; ++a) {
+        detail::EwaldTarget t{};
+        if (!detail::ewald_target(g, ky, kx, ill[a].fy, ill[a].fx, fiz[a], t)) continue;
+        const cfloat v = cfloat(0.0f, -g.gain * t.nuz) * s[a * plane + col];
+        const std::size_t i = t.kz * plane + col;
+        pot[i] += detail::parity(t.kz) * v;
+        weight[i] += 1.0f;
+      }
+    }
+    long long count_filled = 0;
+    for (std::size_t i = 0; i < pot.size(); ++i) {
+      if (weight[i] > 0) {
+        pot[i] /= weight[i];
+        ++count_filled;
+      }
+    }
+    const int h = n / 2 + 1;
+    auto* a = static_cast<cfloat*>(a_out);
+    for (int kz = 0; kz < nz; ++kz) {
+      const int mz = detail::negative_bin(kz, nz);
+      for (int ky = 0; ky < n; ++ky) {
+        const int my = detail::negative_bin(ky, n);
+        for (int kx = 0; kx < h; ++kx) {
+          const std::size_t i = (std::size_t(kz) * n + ky) * n + kx;
+          const std::size_t j = (std::size_t(mz) * n + my) * n + detail::negative_bin(kx, n);
+          const std::size_t o = (std::size_t(kz) * n + ky) * h + kx;
+          float re = 0, im = 0;
+          detail::hermitian_data(pot[i].real(), pot[i].imag(), pot[j].real(), pot[j].imag(), re, im);
+          a[o] = {re, im};
+          hits_out[o] = static_cast<unsigned char>((weight[i] > 0) + (weight[j] > 0));
+        }
+      }
+    }
+    *filled = count_filled;
+  });
+}
+
 int ref_tv_prox(const float* b, float* x, float* dual_p, int nz, int ny, int nx, float lambda,
                 int inner) {
   return guard([&] {

@@ -279,3 +279,18 @@ def pipeline_errors(count, n, illuminations, geom):
     codes = np.zeros(2, np.int32)
     lib().ref_pipeline_errors(C.c_int(count), C.c_int(n), _p(il), _p(_geom(geom)), _p(codes))
     return int(codes[0]), int(codes[1])
+
+
+def ewald_half(spectra, illuminations, geom, nz=0):
+    """The reference's Ewald mapping and Hermitian half data (ref_ewald_half) on spectra (count, n, n)
+    complex64: returns (a (nz, n, n/2+1) complex64, hits uint8, filled voxel count)."""
+    s = _c64(spectra)
+    count, n = s.shape[0], s.shape[2]
+    nzz = nz if nz > 0 else n
+    il = _illum(illuminations)
+    a = np.zeros((nzz, n, n // 2 + 1), np.complex64)
+    hits = np.zeros(a.shape, np.uint8)
+    filled = C.c_longlong()
+    _check(lib().ref_ewald_half(_p(s), C.c_int(count), C.c_int(n), C.c_int(nzz), _p(il), _p(_geom(geom)), _p(a),
+                                _p(hits), C.byref(filled)))
+    return a, hits, int(filled.value)

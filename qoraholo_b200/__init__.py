@@ -1,13 +1,14 @@
-"""Holotomography (optical diffraction tomography) reconstruction on NVIDIA B200.
+"""Optical diffraction tomography -- holograms to refractive index -- on NVIDIA B200.
 
-Drop-in for the ``qoraholo`` Python package: the same functions, arguments and return values
-(python/qoraholo/__init__.py of QoraHolo), computed by hand-written sm_100a CUDA kernels behind
-the C ABI of ``libqhk.so`` (include/qoraholo_b200.h). ``backend`` defaults to ``"cuda"``, the only
-backend of this build; ``"cpu"`` raises.
+A drop-in for the ``qoraholo`` Python package: every public name, argument, default and return form
+follows python/qoraholo/__init__.py of QoraHolo, and the work runs in this project's sm_100a kernels
+behind the C ABI of ``libqhk.so`` (include/qoraholo_b200.h). ``backend`` is accepted everywhere and
+defaults to ``"cuda"``; this build has no host implementation, so ``"cpu"`` raises.
 
-Arrays are numpy, centre-origin, square with even sides. Functions that work on images accept a
-single 2D image or a 3D stack (count, n, n) and return the same rank. Lengths are micrometres,
-spatial frequencies cycles per micrometre.
+Conventions: numpy arrays; images square with an even side and their origin at pixel n/2; image
+functions take one image (2D) or a stack (count, n, n) and answer with the rank they were given;
+lengths in micrometres, spatial frequencies in cycles per micrometre; illuminations as (count, 2)
+pairs (fy, fx).
 """
 
 from __future__ import annotations
@@ -16,7 +17,7 @@ import numpy as np
 
 try:
     from . import _core  # noqa: E402
-except ImportError as e:  # fail loudly: there is no fallback implementation
+except ImportError as e:  # no fallback: without the native libraries nothing here can run
     raise ImportError(
         "qoraholo_b200 native extension is not built; run `python qoraholo_b200/_build.py`"
     ) from e
@@ -44,158 +45,176 @@ __all__ = [
 ]
 
 
-def _stack(a, dtype):
-    a = np.ascontiguousarray(a, dtype=dtype)
-    if a.ndim == 2:
-        return a[None], True
-    if a.ndim != 3:
-        raise ValueError(f"expected a 2D image or a 3D stack, got {a.ndim} dimensions")
-    return a, False
+class _Images:
+    """A C-contiguous 3D stack of `dtype` made from an image or a stack, remembering which it was,
+    so that results go back in the caller's rank."""
+
+    def __init__(self, a, dtype):
+        arr = np.ascontiguousarray(a, dtype=dtype)
+        if arr.ndim not in (2, 3):
+            raise ValueError(f"expected a 2D image or a 3D stack, got {arr.ndim} dimensions")
+        self.was_image = arr.ndim == 2
+        self.stack = arr[np.newaxis] if self.was_image else arr
+
+    def give_back(self, result):
+        return result[0] if self.was_image else result
 
 
-def _unstack(a, single):
-    return a[0] if single else a
+def _views(illuminations):
+    """Illumination frequencies as a contiguous (count, 2) float32 array."""
+    return np.ascontiguousarray(np.asarray(illuminations, dtype=np.float32).reshape(-1, 2))
 
 
-def _illum(illuminations):
-    return np.ascontiguousarray(np.reshape(illuminations, (-1, 2)), dtype=np.float32)
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
 
 
 def find_sideband(hologram, dc_exclusion: float = 0.0) -> Sideband:
-    """Peak of the +1 sideband (x > 0 half plane) of the first hologram, in pixels from DC."""
-    h, _ = _stack(hologram, np.float32)
-    return _core.find_sideband(h, dc_exclusion)
+    """Locate the +1 diffraction order in the spectrum of the (first) hologram: the strongest bin of
+    the right half plane outside a disc of radius ``dc_exclusion`` around DC (N/8 when 0), refined to
+    a fraction of a bin; positions in pixels relative to DC."""
+    return _core.find_sideband(_Images(hologram, np.float32).stack, dc_exclusion)
 
 
 def extract_fields(holograms, center=None, radius: float = 0.0, dc_exclusion: float = 0.0, output_size: int = 0,
                    backend: str = "cuda"):
-    """Off-axis hologram(s) to complex field(s).
-
-    ``center`` is the sideband centre (y, x) in pixels from DC; detected when omitted. ``radius``
-    defaults to |center| / 3, ``output_size`` to the hologram side.
-    """
-    h, single = _stack(holograms, np.float32)
-    return _unstack(_core.extract_fields(h, center, radius, dc_exclusion, output_size, backend), single)
+    """Demodulate off-axis holograms into complex fields: the sideband at ``center`` (y, x pixels from
+    DC; searched for with ``find_sideband`` when None) is cut out with a disc of ``radius`` (|center| / 3
+    when 0), moved to the origin and transformed back on an ``output_size`` grid (the hologram's size
+    when 0)."""
+    h = _Images(holograms, np.float32)
+    return h.give_back(_core.extract_fields(h.stack, center, radius, dc_exclusion, output_size, backend))
 
 
 def field_ratio(sample, background):
-    """sample / background; background is one field or one per sample field."""
-    s, single = _stack(sample, np.complex64)
-    b, _ = _stack(background, np.complex64)
-    return _unstack(_core.field_ratio(s, b), single)
+    """Divide sample fields by background fields (a single background applies to every sample)."""
+    s = _Images(sample, np.complex64)
+    return s.give_back(_core.field_ratio(s.stack, _Images(background, np.complex64).stack))
 
 
 def unwrap(phase, backend: str = "cuda"):
-    """Least-squares unwrapping (Ghiglia & Romero 1994), congruent to the input mod 2 pi."""
-    p, single = _stack(phase, np.float32)
-    return _unstack(_core.unwrap(p, backend), single)
+    """Unwrap phase images in the least-squares sense (the Neumann Poisson problem solved by cosine
+    transforms), then add the constant that makes the result agree with the input modulo 2 pi."""
+    p = _Images(phase, np.float32)
+    return p.give_back(_core.unwrap(p.stack, backend))
 
 
 def rytov(ratio, backend: str = "cuda"):
-    """log|r| + i unwrap(arg r), with the mean phase on the image border in (-pi, pi]."""
-    r, single = _stack(ratio, np.complex64)
-    return _unstack(_core.rytov(r, backend), single)
+    """Complex Rytov phase of field ratios: log-amplitude plus i times the unwrapped phase, shifted by
+    a multiple of 2 pi so that its mean over the image border lies in (-pi, pi]."""
+    r = _Images(ratio, np.complex64)
+    return r.give_back(_core.rytov(r.stack, backend))
 
 
 def reconstruct(fields, illuminations, geometry: Geometry, nz: int = 0, iterations: int = 0, solver: str = "gp",
                 gp_transform: str = "r2c", tv_weight: float = 1e-2, tv_inner: int = 10, mapping: str = "gather",
                 backend: str = "cuda", return_filled: bool = False):
-    """Rytov fields (count, n, n) to a refractive-index volume (nz, n, n).
+    """Refractive-index volume (nz, n, n) from Rytov fields (count, n, n), one per illumination.
 
-    ``solver="gp"``: Gerchberg-Papoulis with n >= n_medium (``gp_transform`` "r2c" half spectra or
-    "c2c"); ``solver="tv"``: FISTA with a TV term of weight ``tv_weight`` on n^2 - n_medium^2 and
-    ``tv_inner`` FGP steps per iteration. ``return_filled`` also returns the fraction of k-space
-    voxels that received data.
+    The fields' spectra are placed on their Ewald caps; ``iterations`` = 0 inverts that directly.
+    Otherwise ``solver="gp"`` alternates the measured k-space data with a non-negative potential
+    (Gerchberg-Papoulis; ``gp_transform`` "r2c" on half spectra or "c2c" on full ones) and
+    ``solver="tv"`` runs FISTA with an isotropic total-variation penalty of weight ``tv_weight``,
+    ``tv_inner`` dual steps per proximal step. ``nz`` (the field side when 0) must be even.
+    ``return_filled`` adds the fraction of k-space voxels that data reached.
     """
-    f, _ = _stack(fields, np.complex64)
-    ri, filled = _core.reconstruct(f, _illum(illuminations), geometry, nz, iterations, solver, gp_transform,
-                                   tv_weight, tv_inner, mapping, backend)
+    ri, filled = _core.reconstruct(_Images(fields, np.complex64).stack, _views(illuminations), geometry, nz,
+                                   iterations, solver, gp_transform, tv_weight, tv_inner, mapping, backend)
     return (ri, filled) if return_filled else ri
 
 
 class Pipeline:
-    """Holograms to refractive index with device state allocated once.
-
-    The background fields stay on the device; each ``run`` does one upload of the sample holograms
-    and one download of the volume, from page-locked buffers. ``upload_chunks`` splits the upload
-    so field extraction overlaps it.
+    """The whole hologram-to-index chain for a fixed geometry, with everything it needs kept on the
+    device between runs: plans, the background fields (from ``set_background``) and the k-space
+    constants. A ``run`` moves the sample holograms in and the volume out once; ``upload_chunks``
+    lets field extraction start on the first chunk while the rest are still in transfer.
     """
 
     def __init__(self, count: int, hologram_size: int, center, illuminations, geometry: Geometry,
                  radius: float = 0.0, output_size: int = 0, nz: int = 0, iterations: int = 0, solver: str = "gp",
                  gp_transform: str = "r2c", tv_weight: float = 1e-2, tv_inner: int = 10, mapping: str = "gather",
                  backend: str = "cuda", upload_chunks: int = 1):
-        self._p = _core.Pipeline(count, hologram_size, tuple(center), radius, output_size, _illum(illuminations),
+        self._p = _core.Pipeline(count, hologram_size, tuple(center), radius, output_size, _views(illuminations),
                                  geometry, nz, iterations, solver, gp_transform, tv_weight, tv_inner, mapping, backend,
                                  upload_chunks)
 
     def set_background(self, backgrounds) -> None:
-        """Background holograms (count, N, N); their fields are extracted once and kept."""
-        self._p.set_background(np.ascontiguousarray(backgrounds, dtype=np.float32))
+        """Take the background holograms (count, N, N); their fields are computed now and kept."""
+        self._p.set_background(_f32(backgrounds))
 
     def run(self, holograms):
-        """Sample holograms (count, N, N) to the index volume (nz, n, n)."""
-        return self._p.run(np.ascontiguousarray(holograms, dtype=np.float32))
+        """Reconstruct one stack of sample holograms (count, N, N); returns the volume (nz, n, n)."""
+        return self._p.run(_f32(holograms))
 
     def run_stream(self, holograms):
-        """A stream of stacks (items, count, N, N) to volumes (items, nz, n, n): each stack's upload
-        and each volume's download overlap the solve of its neighbour; each volume is bitwise what
-        ``run`` gives for its stack. ``filled`` is then the last stack's."""
-        return self._p.run_stream(np.ascontiguousarray(holograms, dtype=np.float32))
+        """Reconstruct many stacks (items, count, N, N) into (items, nz, n, n). Transfers of one stack
+        hide behind the solve of the next, and every volume is bitwise what ``run`` returns for its
+        stack; ``filled`` afterwards refers to the last one."""
+        return self._p.run_stream(_f32(holograms))
 
     @property
     def filled(self) -> float:
+        """Fraction of k-space voxels that the last run's data reached."""
         return self._p.filled
 
     @property
     def timings(self) -> dict[str, float]:
-        """Milliseconds per stage of the last run (device event intervals; ``total`` is host time)."""
+        """Stage times of the last run in milliseconds: device event intervals, ``total`` on the host."""
         return self._p.timings
 
     @property
     def setup_ms(self) -> float:
+        """Time taken to build the pipeline, in milliseconds."""
         return self._p.setup_ms
 
     @property
     def device_bytes(self) -> int:
+        """Device memory the pipeline holds."""
         return self._p.device_bytes
 
 
 def circular_scan(count: int, na_illumination: float, geometry: Geometry):
-    """Normal incidence, then count - 1 directions evenly spaced on a circle: (count, 2)."""
+    """Illumination frequencies (count, 2): the first view on axis, the others at equal steps around a
+    cone of numerical aperture ``na_illumination``."""
     return _core.circular_scan(count, na_illumination, geometry)[0]
 
 
 def render_phantom(spheres, geometry: Geometry, nz: int, n: int):
-    """Refractive index of the spheres at voxel centres, (nz, n, n)."""
+    """Sample the spheres' refractive index at the voxel centres of an (nz, n, n) grid of the
+    geometry's pixel, the volume centred on the origin; later spheres paint over earlier ones."""
     return _core.render_phantom(list(spheres), geometry, nz, n)
 
 
 def forward_fields(spheres, illuminations, geometry: Geometry, n: int, model: str = "rytov"):
-    """Field ratios u / u_in at z = 0, (count, n, n), band-limited to the detection NA."""
-    return _core.forward_fields(list(spheres), _illum(illuminations), geometry, n, model)
+    """Simulated field ratios u / u_in at the central plane (count, n, n), limited to the detection
+    aperture: first Born (``"born"``), its Rytov form (``"rytov"``), or the exact scalar solution of a
+    single sphere (``"exact"``)."""
+    return _core.forward_fields(list(spheres), _views(illuminations), geometry, n, model)
 
 
 def bpm_forward(ri, illuminations, geometry: Geometry, obliquity: bool = True, backend: str = "cuda"):
-    """Refractive index (nz, n, n) to field ratios (count, n, n) by multi-slice beam propagation."""
-    return _core.bpm_forward(np.ascontiguousarray(ri, dtype=np.float32), _illum(illuminations), geometry, obliquity,
-                             backend)
+    """Field ratios (count, n, n) that the multi-slice beam-propagation model predicts for an index
+    volume (nz, n, n)."""
+    return _core.bpm_forward(_f32(ri), _views(illuminations), geometry, obliquity, backend)
 
 
 def bpm_reconstruct(fields, illuminations, geometry: Geometry, initial, iterations: int = 20, batch: int = 0,
                     step: float = 1.0, tv_weight: float = 0.0, tv_inner: int = 10, obliquity: bool = True,
                     backend: str = "cuda", return_loss: bool = False):
-    """Field ratios (count, n, n) to refractive index by gradient descent on the BPM."""
-    ri, loss = _core.bpm_reconstruct(np.ascontiguousarray(fields, dtype=np.complex64), _illum(illuminations), geometry,
-                                     np.ascontiguousarray(initial, dtype=np.float32), iterations, batch, step,
-                                     tv_weight, tv_inner, obliquity, backend)
+    """Fit an index volume to measured field ratios through the beam-propagation model, starting from
+    ``initial``: proximal gradient steps over all views (FISTA) or over batches of ``batch`` views,
+    optionally with a total-variation term. ``return_loss`` adds the data misfit of every iteration."""
+    ri, loss = _core.bpm_reconstruct(np.ascontiguousarray(fields, dtype=np.complex64), _views(illuminations),
+                                     geometry, _f32(initial), iterations, batch, step, tv_weight, tv_inner, obliquity,
+                                     backend)
     return (ri, np.asarray(loss)) if return_loss else ri
 
 
 def synthesize_holograms(ratio, illuminations, geometry: Geometry, carrier=(5.0, 5.0),
                          reference_amplitude: float = 1.0, noise: float = 0.0, seed: int = 1):
-    """|R + u_in * ratio|^2 + Gaussian noise, with R = a exp(-2 pi i carrier . r)."""
-    r, single = _stack(ratio, np.complex64)
-    out = _core.synthesize_holograms(r, _illum(illuminations), geometry, tuple(carrier), reference_amplitude, noise,
-                                     seed)
-    return _unstack(out, single)
+    """Off-axis holograms of field ratios: the intensity of a tilted reference wave (amplitude
+    ``reference_amplitude``, spatial frequency ``carrier``) plus the illuminated sample field, with
+    additive Gaussian noise of standard deviation ``noise`` drawn from a generator seeded by ``seed``."""
+    r = _Images(ratio, np.complex64)
+    return r.give_back(_core.synthesize_holograms(r.stack, _views(illuminations), geometry, tuple(carrier),
+                                                  reference_amplitude, noise, seed))

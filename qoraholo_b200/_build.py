@@ -41,6 +41,18 @@ def _headers():
     return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list(INCLUDE.rglob("*.h*"))
 
 
+def _stale(obj: Path, src: Path) -> bool:
+    """True when obj must be rebuilt: it or its dependency list (obj.d, written by the compiler's -MD
+    -MF) is missing, or the source or any header it included is newer."""
+    dep = obj.with_suffix(".d")
+    if not obj.exists() or not dep.exists():
+        return True
+    text = dep.read_text().replace("\\\n", " ")
+    files = [Path(t) for t in text.partition(":")[2].split()]
+    built = obj.stat().st_mtime
+    return any(not f.exists() or f.stat().st_mtime > built for f in [src, *files])
+
+
 def _run(cmd):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -56,13 +68,12 @@ def _compile_many(jobs):
 def build_qhk(force=False) -> Path:
     sources = sorted(CSRC.glob("*.cu"))
     BUILD.mkdir(exist_ok=True)
-    hdr_time = _newest(_headers())
     jobs, objs = [], []
     for src in sources:
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)
-        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_time):
-            jobs.append([NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+        if force or _stale(obj, src):
+            jobs.append([NVCC, *NVCC_FLAGS, "-MD", "-MF", str(obj.with_suffix(".d")), "-c", str(src), "-o", str(obj)])
     _compile_many(jobs)
     if force or jobs or not LIB_QHK.exists() or LIB_QHK.stat().st_mtime < _newest(objs):
         _run([NVCC, *ARCH, "-shared", "-o", str(LIB_QHK), *map(str, objs)])
@@ -75,13 +86,12 @@ def build_host(force=False) -> Path | None:
     if not sources:
         return None
     BUILD.mkdir(exist_ok=True)
-    hdr_time = max(_newest(_headers()), _newest(host_dir.glob("*.hpp")))
     jobs, objs = [], []
     for src in sources:
         obj = BUILD / ("host_" + src.stem + ".o")
         objs.append(obj)
-        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_time):
-            jobs.append(["g++", *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
+        if force or _stale(obj, src):
+            jobs.append(["g++", *CXX_FLAGS, "-MD", "-MF", str(obj.with_suffix(".d")), "-c", str(src), "-o", str(obj)])
     _compile_many(jobs)
     if force or jobs or not LIB_HOST.exists() or LIB_HOST.stat().st_mtime < max(_newest(objs), LIB_QHK.stat().st_mtime):
         _run(["g++", "-shared", "-o", str(LIB_HOST), *map(str, objs), f"-L{PKG}", "-lqhk", "-Wl,-rpath,$ORIGIN"])

@@ -101,6 +101,8 @@ _PROTOS = {
     "qhk_pipeline_process_device": (_I, [_VP, _VP, _VP, _VP]),
     "qhk_pipeline_result": (_I, [_VP, C.POINTER(C.c_double), _VP]),
     "qhk_pipeline_filled": (_I, [_VP, _VP, C.POINTER(C.c_double)]),
+    "qhk_pipeline_check_waits": (_I, [_VP, _VP]),
+    "qhk_pipeline_wait_probe": (_I, [_VP, _I]),
     "qhk_pipeline_shape": (_I, [_VP, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "qhk_pipeline_device_bytes": (C.c_size_t, [_VP]),
     "qhk_pipeline_destroy": (_I, [_VP]),
@@ -456,6 +458,16 @@ class Pipeline:
         v = C.c_double()
         check(lib().qhk_pipeline_filled(self._h, _VP(stream), C.byref(v)))
         return v.value
+
+    def check_waits(self, stream=0):
+        """Waits for `stream`; raises QhkError (TIMEOUT) if a bounded device wait of this pipeline ran
+        out since the last check (device-form runs cannot report it themselves)."""
+        check(lib().qhk_pipeline_check_waits(self._h, _VP(stream)))
+
+    def wait_probe(self, polls=1000):
+        """Test hook of the timeout path: one bounded wait that nothing completes, counted in this
+        pipeline's counter; raises QhkError (TIMEOUT) as a run whose wait ran out does."""
+        check(lib().qhk_pipeline_wait_probe(self._h, int(polls)))
 
     @property
     def device_bytes(self):

@@ -238,52 +238,65 @@ int rows_cols(int n) {
 
 }  // namespace
 
+// Per-view tables of the multi-slice model (the quantities of src/bpm.cpp:10-60), on the lateral DFT
+// grid in transform order. For a scattered plane wave of lateral frequency (fy, fx) = bin + illumination
+// that propagates in the medium (fy^2 + fx^2 < fm^2), with axial frequency nu = sqrt(fm^2 - fy^2 - fx^2):
+//   step  e^{i 2 pi (nu - fiz) dz}: one slice of propagation of the envelope (the carrier e^{i 2 pi fiz z}
+//         of the illumination factored out), dz = pixel;
+//   last  e^{i 2 pi (nu - fiz) z_back}: from the last slice back to the volume's central plane, where the
+//         fields are recorded, kept only inside the pupil (fy^2 + fx^2 <= fna^2);
+//   q     the obliquity fm / nu of the thin-screen update, with nu bounded below by
+//         sqrt(max(fm^2 - fna^2, fm^2 / 100)); 1 without obliquity and for evanescent bins.
+// Evanescent bins propagate nothing (step = last = 0). The Lipschitz constant of the data term's
+// gradient is nz (k0 dz)^2 times the mean over views of q^2 at the view's own direction (bin 0).
+// Computed in double, stored in float.
 BpmTablesHost bpm_tables(int n, int nz, const float* il, int count, float wavelength, float n_medium, float na,
                          float pixel, bool obliquity) {
-  constexpr double kPi = std::numbers::pi;
-  const double lambda = wavelength;
-  const double fm = n_medium / lambda;
-  const double fna = na / lambda;
-  const double d = pixel;
-  const double df = 1.0 / (n * d);
-  const double nuz_min = std::sqrt(std::max(fm * fm - fna * fna, 0.01 * fm * fm));
-  const double back = -(nz - 1 - nz / 2) * d;
+  const double two_pi = 2.0 * std::numbers::pi;
+  const double fm2 = (double(n_medium) / wavelength) * (double(n_medium) / wavelength);
+  const double fna2 = (double(na) / wavelength) * (double(na) / wavelength);
+  const double dz = pixel;
+  const double df = 1.0 / (n * dz);
+  const double nu_floor = std::sqrt(std::max(fm2 - fna2, 0.01 * fm2));
+  const double z_back = -(nz - 1 - nz / 2) * dz;  // central plane, seen from the last slice
+  const auto unit = [](double angle) {
+    const std::complex<double> w = std::exp(std::complex<double>(0.0, angle));
+    return make_float2(static_cast<float>(w.real()), static_cast<float>(w.imag()));
+  };
+  const auto obliquity_of = [&](double nu) { return obliquity ? std::sqrt(fm2) / std::max(nu, nu_floor) : 1.0; };
+
   BpmTablesHost t;
   t.n = n;
   t.nz = nz;
   t.count = count;
-  t.phase = static_cast<float>(2.0 * kPi / lambda * d);
+  t.phase = static_cast<float>(two_pi / wavelength * dz);
   const std::size_t plane = static_cast<std::size_t>(n) * n;
   t.step.assign(plane * count, make_float2(0, 0));
   t.last.assign(plane * count, make_float2(0, 0));
   t.q.assign(plane * count, 1.0f);
-  double q0 = 0;
+  double mean_q2 = 0;
   for (int a = 0; a < count; ++a) {
     const double fiy = il[2 * a], fix = il[2 * a + 1];
-    const double fiz = std::sqrt(fm * fm - fiy * fiy - fix * fix);
+    const double fiz = std::sqrt(fm2 - fiy * fiy - fix * fix);
+    float2* step = t.step.data() + a * plane;
+    float2* last = t.last.data() + a * plane;
+    float* q = t.q.data() + a * plane;
     for (int ky = 0; ky < n; ++ky) {
+      const double fy = signed_bin(ky, n) * df + fiy;
       for (int kx = 0; kx < n; ++kx) {
-        const std::size_t i = a * plane + static_cast<std::size_t>(ky) * n + kx;
-        const double fy = signed_bin(ky, n) * df + fiy;
         const double fx = signed_bin(kx, n) * df + fix;
         const double rho2 = fy * fy + fx * fx;
-        double q = 1;
-        if (rho2 < fm * fm) {
-          const double nuz = std::sqrt(fm * fm - rho2);
-          const auto c = std::polar(1.0, 2.0 * kPi * (nuz - fiz) * d);
-          t.step[i] = make_float2(static_cast<float>(c.real()), static_cast<float>(c.imag()));
-          if (rho2 <= fna * fna) {
-            const auto l = std::polar(1.0, 2.0 * kPi * (nuz - fiz) * back);
-            t.last[i] = make_float2(static_cast<float>(l.real()), static_cast<float>(l.imag()));
-          }
-          if (obliquity) q = fm / std::max(nuz, nuz_min);
-        }
-        t.q[i] = static_cast<float>(q);
+        if (rho2 >= fm2) continue;  // evanescent
+        const std::size_t b = static_cast<std::size_t>(ky) * n + kx;
+        const double nu = std::sqrt(fm2 - rho2);
+        step[b] = unit(two_pi * (nu - fiz) * dz);
+        if (rho2 <= fna2) last[b] = unit(two_pi * (nu - fiz) * z_back);
+        q[b] = static_cast<float>(obliquity_of(nu));
       }
     }
-    q0 += static_cast<double>(t.q[a * plane]) * t.q[a * plane];
+    mean_q2 += static_cast<double>(q[0]) * q[0] / count;
   }
-  t.lipschitz = static_cast<float>(nz * static_cast<double>(t.phase) * t.phase * q0 / count);
+  t.lipschitz = static_cast<float>(nz * static_cast<double>(t.phase) * t.phase * mean_q2);
   return t;
 }
 
@@ -499,7 +512,7 @@ void add_medium(const float* x, float n_medium, std::size_t total, float* ri, cu
 }
 
 void bpm_solve(const BpmTablesHost& t, const float2* d_fields, float* d_x, int iterations, int batch, float step,
-               float tv_weight, int tv_inner, double* d_loss, cudaStream_t s) {
+               float tv_weight, int tv_inner, double* d_loss, cudaStream_t s, unsigned long long* d_waits) {
   const int count = t.count;
   batch = batch <= 0 || batch >= count ? count : batch;
   const bool fista = batch == count;
@@ -514,6 +527,7 @@ void bpm_solve(const BpmTablesHost& t, const float2* d_fields, float* d_x, int i
   float* z = y + 3 * size;
   DevBuf<float> dual(tv ? 12 * size : 0);
   TvBuffers tvb;
+  tvb.wait_status = d_waits;
   if (tv) {
     check(cudaMemsetAsync(dual.get(), 0, 3 * size * sizeof(float), s), "cudaMemset");
     for (int i = 0; i < 4; ++i)

@@ -66,8 +66,10 @@ void add_medium(const float* x, float n_medium, std::size_t total, float* ri, cu
 
 // Proximal gradient inversion (FISTA over all illuminations, or passes over batches) of the
 // contrast d_x (device, updated in place); d_loss[it] receives sum |bpm(x) - fields|^2 of each
-// iteration (unscaled). Synchronises the stream.
+// iteration (unscaled); bounded device waits of its TV steps that run out are counted in the device
+// word *d_waits (may be null: the library-wide counter). Synchronises the stream.
 void bpm_solve(const BpmTablesHost& t, const float2* d_fields, float* d_x, int iterations, int batch, float step,
-               float tv_weight, int tv_inner, double* d_loss, cudaStream_t s);
+               float tv_weight, int tv_inner, double* d_loss, cudaStream_t s,
+               unsigned long long* d_waits = nullptr);
 
 }  // namespace qhk

@@ -80,10 +80,23 @@ qhk::OdtConfig odt_config(int n, int count, const float* il, const qhk_geometry*
   return c;
 }
 
+// Reads an ODT plan's wait counter after the work queued on `s` (synchronises `s`) and fails with a
+// timeout status if a bounded device wait of the plan ran out since `seen`.
+void check_plan_waits(const qhk::OdtPlan& plan, unsigned long long& seen, cudaStream_t s, const char* what) {
+  unsigned long long n = 0;
+  qhk::check(cudaMemcpyAsync(&n, plan.wait_count(), sizeof n, cudaMemcpyDeviceToHost, s), "download wait count");
+  qhk::check(cudaStreamSynchronize(s), what);
+  if (n != seen) {
+    seen = n;
+    qhk::fail(qhk::kTimeout, qhk::wait_timeout_message(what));
+  }
+}
+
 }  // namespace
 
 struct qhk_odt {
   qhk::OdtPlan plan;
+  unsigned long long waits_seen = 0;  // the plan's wait counter at the last check
 };
 
 struct qhk_pipeline {
@@ -121,7 +134,7 @@ int qhk_odt_filled(qhk_odt* plan, void* stream, double* filled) {
     unsigned long long v = 0;
     qhk::check(cudaMemcpyAsync(&v, plan->plan.filled(), sizeof v, cudaMemcpyDeviceToHost, as_stream(stream)),
                "download filled");
-    qhk::check(cudaStreamSynchronize(as_stream(stream)), "qhk_odt_filled");
+    check_plan_waits(plan->plan, plan->waits_seen, as_stream(stream), "qhk_odt_filled");
     *filled = static_cast<double>(v) / static_cast<double>(plan->plan.volume());
   });
 }
@@ -155,7 +168,8 @@ int qhk_reconstruct(const void* fields, int count, int n, const float* illum_fyf
     qhk::download(out, d_index.get(), plan.volume() * sizeof(float), stream.get());
     unsigned long long v = 0;
     qhk::check(cudaMemcpyAsync(&v, plan.filled(), sizeof v, cudaMemcpyDeviceToHost, stream.get()), "download filled");
-    qhk::check(cudaStreamSynchronize(stream.get()), "reconstruct");
+    unsigned long long waits = 0;
+    check_plan_waits(plan, waits, stream.get(), "reconstruct");
     if (filled) *filled = static_cast<double>(v) / static_cast<double>(plan.volume());
   });
 }
@@ -190,19 +204,25 @@ int qhk_tv_prox(const float* d_b, float* d_x, float* d_dual, int nz, int ny, int
     const std::size_t v = static_cast<std::size_t>(nz) * ny * nx;
     const cudaStream_t s = as_stream(stream);
     qhk::DevBuf<float> scratch(9 * v);
+    qhk::DevBuf<unsigned long long> waits(1);
+    qhk::check(cudaMemsetAsync(waits.get(), 0, sizeof(unsigned long long), s), "cudaMemset");
     qhk::TvBuffers t;
     for (int c = 0; c < 3; ++c) {
       t.v[0][c] = d_dual + c * v;
       for (int i = 1; i < 4; ++i) t.v[i][c] = scratch.get() + (3 * (i - 1) + c) * v;
     }
     t.p_index = 0;
+    t.wait_status = waits.get();
     qhk::tv_prox(d_b, t, nz, ny, nx, lambda, inner, qhk::TvFinal::plain, 0.0f, nullptr, d_x, 0, 0, s);
     if (t.p_index != 0) {
       qhk::check(cudaMemcpyAsync(d_dual, t.v[t.p_index][0], 3 * v * sizeof(float), cudaMemcpyDeviceToDevice, s),
                  "copy dual");
     }
     // The scratch buffer is freed on return; wait for the kernels that use it.
+    unsigned long long n = 0;
+    qhk::check(cudaMemcpyAsync(&n, waits.get(), sizeof n, cudaMemcpyDeviceToHost, s), "download wait count");
     qhk::check(cudaStreamSynchronize(s), "tv_prox");
+    if (n != 0) qhk::fail(qhk::kTimeout, qhk::wait_timeout_message("tv_prox"));
   });
 }
 
@@ -474,7 +494,7 @@ int qhk_pipeline_filled_batch(qhk_pipeline* p, void* stream, double* filled) {
     qhk::check(cudaMemcpyAsync(v.data(), p->plan.odt().filled(), b * sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, as_stream(stream)),
                "download filled");
-    qhk::check(cudaStreamSynchronize(as_stream(stream)), "qhk_pipeline_filled_batch");
+    p->plan.check_device_waits(as_stream(stream));
     for (int i = 0; i < b; ++i) filled[i] = static_cast<double>(v[i]) / static_cast<double>(p->plan.odt().volume());
   });
 }
@@ -535,8 +555,22 @@ int qhk_pipeline_filled(qhk_pipeline* p, void* stream, double* filled) {
     unsigned long long v = 0;
     qhk::check(cudaMemcpyAsync(&v, p->plan.odt().filled(), sizeof v, cudaMemcpyDeviceToHost, as_stream(stream)),
                "download filled");
-    qhk::check(cudaStreamSynchronize(as_stream(stream)), "Pipeline filled");
+    p->plan.check_device_waits(as_stream(stream));
     *filled = static_cast<double>(v) / static_cast<double>(p->plan.odt().volume());
+  });
+}
+
+int qhk_pipeline_check_waits(qhk_pipeline* p, void* stream) {
+  return guard([&] {
+    qhk::require(p != nullptr, "Pipeline: null pipeline");
+    p->plan.check_device_waits(as_stream(stream));
+  });
+}
+
+int qhk_pipeline_wait_probe(qhk_pipeline* p, int polls) {
+  return guard([&] {
+    qhk::require(p != nullptr, "Pipeline: null pipeline");
+    p->plan.wait_probe(polls);
   });
 }
 
@@ -708,19 +742,24 @@ int qhk_bpm_reconstruct(const void* fields, int count, int n, const float* illum
     qhk::DevBuf<float> d_ri(vol), d_x(vol);
     qhk::DevBuf<float2> d_f(nf);
     qhk::DevBuf<double> d_loss(std::max(o->iterations, 1));
+    qhk::DevBuf<unsigned long long> d_waits(1);
+    qhk::check(cudaMemsetAsync(d_waits.get(), 0, sizeof(unsigned long long), s), "cudaMemset");
     qhk::check(cudaMemcpyAsync(d_ri.get(), initial, vol * sizeof(float), cudaMemcpyHostToDevice, s), "upload");
     qhk::check(cudaMemcpyAsync(d_f.get(), fields, nf * sizeof(float2), cudaMemcpyHostToDevice, s), "upload");
     qhk::check(cudaMemsetAsync(d_loss.get(), 0, d_loss.bytes(), s), "cudaMemset");
     qhk::contrast(d_ri.get(), geometry->n_medium, vol, d_x.get(), true, s);
     qhk::bpm_solve(t, d_f.get(), d_x.get(), o->iterations, o->batch, o->step, o->tv_weight, o->tv_inner, d_loss.get(),
-                   s);
+                   s, d_waits.get());
     qhk::add_medium(d_x.get(), geometry->n_medium, vol, d_ri.get(), s);
     qhk::check(cudaMemcpyAsync(out, d_ri.get(), vol * sizeof(float), cudaMemcpyDeviceToHost, s), "download");
     if (o->iterations > 0) {
       qhk::check(cudaMemcpyAsync(loss, d_loss.get(), o->iterations * sizeof(double), cudaMemcpyDeviceToHost, s),
                  "download loss");
     }
+    unsigned long long waits = 0;
+    qhk::check(cudaMemcpyAsync(&waits, d_waits.get(), sizeof waits, cudaMemcpyDeviceToHost, s), "download wait count");
     qhk::check(cudaStreamSynchronize(s), "bpm_reconstruct");
+    if (waits != 0) qhk::fail(qhk::kTimeout, qhk::wait_timeout_message("bpm_reconstruct"));
     for (int i = 0; i < o->iterations; ++i) loss[i] *= 0.5 / count;
   });
 }
@@ -785,6 +824,33 @@ int qhk_synthesize_holograms_device(const void* d_ratio, int count, int n, const
   return guard([&] {
     qhk::synthesize_holograms_device(static_cast<const float2*>(d_ratio), illum_fyfx, count, n, pixel, carrier_y,
                                      carrier_x, amplitude, noise, seed, d_out, as_stream(stream));
+  });
+}
+
+int qhk_render_phantom(const float* spheres, int k, const qhk_geometry* geometry, int nz, int n, float* out) {
+  return guard([&] {
+    qhk::require(geometry && out, "render_phantom: null argument");
+    qhk::require(nz >= 1 && n >= 1, "render_phantom: empty shape");
+    qhk::Stream stream;
+    const std::size_t total = static_cast<std::size_t>(nz) * n * n;
+    qhk::DevBuf<float> d(total);
+    qhk::render_spheres_device(spheres, k, geometry->n_medium, geometry->pixel, nz, n, d.get(), stream.get());
+    qhk::download(out, d.get(), total * sizeof(float), stream.get());
+    qhk::check(cudaStreamSynchronize(stream.get()), "render_phantom");
+  });
+}
+
+int qhk_forward_fields(const float* spheres, int k, const float* illum_fyfx, int count, const qhk_geometry* geometry,
+                       int n, int model, void* out) {
+  return guard([&] {
+    qhk::require(geometry && out, "forward_fields: null argument");
+    qhk::Stream stream;
+    const std::size_t total = static_cast<std::size_t>(std::max(count, 0)) * n * n;
+    qhk::DevBuf<float2> d(std::max<std::size_t>(total, 1));
+    qhk::sphere_fields_device(spheres, k, illum_fyfx, count, geometry->wavelength, geometry->n_medium, geometry->na,
+                              geometry->pixel, n, model, d.get(), stream.get());
+    qhk::download(out, d.get(), total * sizeof(float2), stream.get());
+    qhk::check(cudaStreamSynchronize(stream.get()), "forward_fields");
   });
 }
 

@@ -1,8 +1,8 @@
-// Fixture generators of the public API (include/qoraholo/phantom.hpp): spheres rendered at voxel
-// centres, analytic scattered fields (first Born / Rytov sphere spectra on the Ewald caps, or the
-// exact scalar partial-wave solution for one sphere), and off-axis holograms with Gaussian noise.
-// Host code in double precision, like the reference's generators (src/phantom.cpp); the final
-// inverse 2D FFT of forward_fields runs on the device.
+// Fixture generators of the public API (include/qoraholo/phantom.hpp). The rendered phantom and the
+// analytic fields are computed on the device (qhk_render_phantom, qhk_forward_fields; csrc/synth.cu).
+// Hologram synthesis stays on the host because its noise must be the reference's stream: draws of
+// std::normal_distribution<float> from one std::mt19937_64 seeded with `seed`, taken view by view and
+// row by row (src/phantom.cpp:193-221), so that seeded inputs are the reference's inputs.
 #include <cmath>
 #include <complex>
 #include <numbers>
@@ -16,146 +16,54 @@ namespace qoraholo {
 
 namespace {
 
-constexpr double kPi = std::numbers::pi;
+qhk_geometry c_geometry(const Geometry& g) { return {g.wavelength, g.n_medium, g.na, g.pixel}; }
 
-// Index under painter's order of the first `count` spheres at (z, y, x).
-double index_at(std::span<const Sphere> spheres, std::size_t count, double n_medium, double z, double y, double x) {
-  double n = n_medium;
-  for (std::size_t i = 0; i < count; ++i) {
-    const Sphere& s = spheres[i];
-    const double dz = z - s.z, dy = y - s.y, dx = x - s.x;
-    if (dz * dz + dy * dy + dx * dx <= double(s.radius) * s.radius) n = s.n;
-  }
-  return n;
+std::vector<float> sphere_rows(std::span<const Sphere> spheres) {
+  std::vector<float> rows;
+  rows.reserve(5 * spheres.size());
+  for (const Sphere& s : spheres) rows.insert(rows.end(), {s.z, s.y, s.x, s.radius, s.n});
+  return rows;
 }
 
-// Fourier transform of the unit ball normalised to 1 at q = 0: 3 (sin x - x cos x) / x^3.
-double ball(double x) {
-  return x < 1e-3 ? 1.0 - x * x / 10.0 : 3.0 * (std::sin(x) - x * std::cos(x)) / (x * x * x);
-}
-
-// Scattering coefficients c_l of a homogeneous sphere (scalar Helmholtz, size parameter x = k R,
-// relative index m): continuity of u and du/dr at r = R with spherical Bessel / Hankel functions,
-// ratios j_l / j_{l-1} from a downward continued fraction for stability.
-std::vector<std::complex<double>> sphere_coefficients(double x, double m) {
-  const int lmax = static_cast<int>(x + 4.0 * std::cbrt(x) + 10.0);
-  const auto ratios = [&](double z) {
-    std::vector<double> rho(lmax + 1);
-    double r = 0;
-    for (int l = lmax + 60; l >= 1; --l) {
-      r = 1.0 / ((2.0 * l + 1.0) / z - r);
-      if (l <= lmax) rho[l] = r;
-    }
-    return rho;
-  };
-  const auto rx = ratios(x);
-  const auto rm = ratios(m * x);
-  std::vector<std::complex<double>> c(lmax + 1);
-  double jm1 = std::cos(x) / x, j = std::sin(x) / x;
-  double ym1 = std::sin(x) / x, y = -std::cos(x) / x;
-  for (int l = 0; l <= lmax; ++l) {
-    if (l > 0) {
-      const double yn = (2.0 * l - 1.0) / x * y - ym1;
-      ym1 = y;
-      y = yn;
-      jm1 = j;
-      j = rx[l] * j;
-    }
-    const std::complex<double> h(j, y), hm1(jm1, ym1);
-    const double dj = jm1 - (l + 1.0) / x * j;
-    const std::complex<double> dh = hm1 - (l + 1.0) / x * h;
-    const double d = (l == 0 ? 1.0 / std::tan(m * x) : 1.0 / rm[l]) - (l + 1.0) / (m * x);
-    c[l] = (m * d * j - dj) / (dh - m * d * h);
-  }
-  return c;
+// e^{i 2 pi f r_j} for the centred coordinates r_j = (j - n / 2) * pixel of one axis.
+std::vector<std::complex<double>> axis_phases(double f, int n, double pixel) {
+  std::vector<std::complex<double>> w(n);
+  for (int j = 0; j < n; ++j) w[j] = std::polar(1.0, 2.0 * std::numbers::pi * f * ((j - n / 2) * pixel));
+  return w;
 }
 
 }  // namespace
 
 Array3<float> render_phantom(std::span<const Sphere> spheres, const Geometry& geometry, int nz, int n) {
-  if (nz < 1 || n < 1) throw std::invalid_argument("render_phantom: empty shape");
+  host::require(nz >= 1 && n >= 1, "render_phantom: empty shape");
+  host::require_cuda(Backend::cuda);
   Array3<float> out(nz, n, n);
-  const double d = geometry.pixel;
-  for (int k = 0; k < nz; ++k)
-    for (int j = 0; j < n; ++j)
-      for (int i = 0; i < n; ++i)
-        out(k, j, i) = static_cast<float>(
-            index_at(spheres, spheres.size(), geometry.n_medium, (k - nz / 2) * d, (j - n / 2) * d, (i - n / 2) * d));
+  const auto rows = sphere_rows(spheres);
+  const qhk_geometry g = c_geometry(geometry);
+  host::check(qhk_render_phantom(rows.data(), static_cast<int>(spheres.size()), &g, nz, n, out.data.data()));
   return out;
 }
 
 Array3<cfloat> forward_fields(std::span<const Sphere> spheres, std::span<const Illumination> illuminations,
                               const Geometry& geometry, int n, ScatteringModel model) {
-  if (n < 4 || n % 2 != 0) throw std::invalid_argument("forward_fields: n must be even");
-  if (model == ScatteringModel::exact && spheres.size() != 1) {
-    throw std::invalid_argument("forward_fields: the exact model takes exactly one sphere");
-  }
-  const double k0 = 2.0 * kPi / geometry.wavelength;
-  const double nm = geometry.n_medium;
-  const double fm2 = nm * nm / (double(geometry.wavelength) * geometry.wavelength);
-  const double fna2 = double(geometry.na) * geometry.na / (double(geometry.wavelength) * geometry.wavelength);
-  const double d = geometry.pixel;
-  const double df = 1.0 / (n * d);
-  const double km = k0 * nm;
-  const auto waves = model == ScatteringModel::exact ? sphere_coefficients(km * spheres[0].radius, spheres[0].n / nm)
-                                                     : std::vector<std::complex<double>>{};
-  // Potential step of each sphere over the index it is painted on, times its volume.
-  std::vector<double> step(spheres.size());
-  for (std::size_t i = 0; i < spheres.size(); ++i) {
-    const Sphere& s = spheres[i];
-    const double parent = index_at(spheres, i, nm, s.z, s.y, s.x);
-    step[i] = k0 * k0 * (double(s.n) * s.n - parent * parent) * (4.0 / 3.0 * kPi * double(s.radius) * s.radius * s.radius);
-  }
+  host::require(n >= 4 && n % 2 == 0, "forward_fields: n must be even");
+  host::require(model != ScatteringModel::exact || spheres.size() == 1,
+                "forward_fields: the exact model takes exactly one sphere");
+  host::require_cuda(Backend::cuda);
   const int count = static_cast<int>(illuminations.size());
   Array3<cfloat> out(count, n, n);
-  for (int a = 0; a < count; ++a) {
-    const double fiy = illuminations[a].fy, fix = illuminations[a].fx;
-    if (fiy * fiy + fix * fix >= fm2) {
-      throw std::invalid_argument("forward_fields: illumination beyond n_medium / wavelength");
-    }
-    const double fiz = std::sqrt(fm2 - fiy * fiy - fix * fix);
-    for (int ky = 0; ky < n; ++ky) {
-      for (int kx = 0; kx < n; ++kx) {
-        const double my = (ky < n / 2 ? ky : ky - n) * df;
-        const double mx = (kx < n / 2 ? kx : kx - n) * df;
-        const double fy = my + fiy, fx = mx + fix;
-        const double rho2 = fy * fy + fx * fx;
-        std::complex<double> u = 0;
-        if (rho2 <= fna2 && rho2 < fm2) {
-          const double nuz = std::sqrt(fm2 - rho2);
-          const double qz = nuz - fiz;
-          std::complex<double> o = 0;  // 3D spectrum of the scattering potential at q
-          if (model == ScatteringModel::exact) {
-            const Sphere& s = spheres[0];
-            const double ct = (fy * fiy + fx * fix + nuz * fiz) / fm2;
-            std::complex<double> sum = 0;
-            double pm1 = 0, p = 1;  // Legendre P_{l-1}, P_l
-            for (std::size_t l = 0; l < waves.size(); ++l) {
-              const double w = 2.0 * double(l) + 1.0;
-              sum += w * waves[l] * p;
-              const double pn = (w * ct * p - double(l) * pm1) / (double(l) + 1.0);
-              pm1 = p;
-              p = pn;
-            }
-            o = 4.0 * kPi * std::complex<double>(0.0, -1.0 / km) * sum *
-                std::polar(1.0, -2.0 * kPi * (qz * s.z + my * s.y + mx * s.x));
-          } else {
-            const double q = 2.0 * kPi * std::sqrt(qz * qz + my * my + mx * mx);
-            for (std::size_t i = 0; i < spheres.size(); ++i) {
-              const Sphere& s = spheres[i];
-              o += step[i] * ball(q * s.radius) * std::polar(1.0, -2.0 * kPi * (qz * s.z + my * s.y + mx * s.x));
-            }
-          }
-          // Fourier diffraction theorem U = i o / (4 pi nu_z); centre-origin DFT: (-1)^(ky+kx) / d^2.
-          u = std::complex<double>(0.0, 1.0 / (4.0 * kPi * nuz)) * o * (((ky + kx) & 1) ? -1.0 : 1.0) / (d * d);
-        }
-        out(a, ky, kx) = cfloat(u);
-      }
-    }
+  if (count == 0) return out;
+  std::vector<float> il(2 * illuminations.size());
+  for (std::size_t a = 0; a < illuminations.size(); ++a) {
+    il[2 * a] = illuminations[a].fy;
+    il[2 * a + 1] = illuminations[a].fx;
   }
-  host::require_cuda(Backend::cuda);
-  host::check(qhk_fft2d_host(out.data.data(), count, n, 0, 1.0f / static_cast<float>(n * n)));
-  for (auto& v : out.data) v = model == ScatteringModel::rytov ? std::exp(v) : 1.0f + v;
+  const auto rows = sphere_rows(spheres);
+  const qhk_geometry g = c_geometry(geometry);
+  const int m = model == ScatteringModel::born ? QHK_MODEL_BORN : model == ScatteringModel::rytov ? QHK_MODEL_RYTOV
+                                                                                                   : QHK_MODEL_EXACT;
+  host::check(qhk_forward_fields(rows.data(), static_cast<int>(spheres.size()), il.data(), count, &g, n, m,
+                                 out.data.data()));
   return out;
 }
 
@@ -164,18 +72,22 @@ Array3<float> synthesize_holograms(const Array3<cfloat>& ratio, std::span<const 
   if (static_cast<std::size_t>(ratio.nz) != illuminations.size()) {
     throw std::invalid_argument("synthesize_holograms: need one illumination per field");
   }
+  // |R + u_in r|^2 = A^2 + |r|^2 + 2 A Re(e^{i 2 pi ((fy + cy) y + (fx + cx) x)} r) with the reference wave
+  // R = A e^{-i 2 pi (cy y + cx x)} and the incident wave u_in = e^{i 2 pi (fy y + fx x)}: the phase
+  // factor separates into one row and one column factor per view.
   Array3<float> out(ratio.nz, ratio.ny, ratio.nx);
   std::mt19937_64 rng(options.seed);
   std::normal_distribution<float> noise(0.0f, options.noise);
-  const double d = geometry.pixel;
+  const double amp = options.reference_amplitude;
+  const double pixel = geometry.pixel;
   for (int a = 0; a < ratio.nz; ++a) {
+    const auto wy = axis_phases(double(illuminations[a].fy) + options.carrier[0], ratio.ny, pixel);
+    const auto wx = axis_phases(double(illuminations[a].fx) + options.carrier[1], ratio.nx, pixel);
     for (int y = 0; y < ratio.ny; ++y) {
       for (int x = 0; x < ratio.nx; ++x) {
-        const double ry = (y - ratio.ny / 2) * d, rx = (x - ratio.nx / 2) * d;
-        const auto incident = std::polar(1.0, 2.0 * kPi * (illuminations[a].fy * ry + illuminations[a].fx * rx));
-        const auto reference = std::polar(double(options.reference_amplitude),
-                                          -2.0 * kPi * (options.carrier[0] * ry + options.carrier[1] * rx));
-        float v = static_cast<float>(std::norm(reference + incident * std::complex<double>(ratio(a, y, x))));
+        const std::complex<double> r(ratio(a, y, x));
+        const double cross = (wy[y] * wx[x] * r).real();
+        float v = static_cast<float>(amp * amp + std::norm(r) + 2.0 * amp * cross);
         if (options.noise > 0) v += noise(rng);
         out(a, y, x) = v;
       }

@@ -53,71 +53,127 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
   return v;
 }
 
-__global__ void __launch_bounds__(256)
+// Half-spectrum mapping, one warp per lateral column (ky, kx) of the half spectrum (kx <= n/2), kMapCols
+// columns per block, consecutive in the flattened (ky, kx) order, so that the block's output rows are
+// contiguous. Lane l owns the K axial bins [l K, l K + K) of its warp's column (32 K >= nz). The
+// column's Ewald targets are computed once each: lane l takes illuminations l, l + 32, ..., for the
+// column itself (side P) and for its mirror (-ky, -kx) (side N, whose bin kz lands on -kz here). They
+// are then broadcast with warp shuffles in illumination order, and the owner of the target bin adds
+// the mapped value to its registers -- every bin's sums in the CPU's order, no atomics. The block
+// stages a, hits of its columns in shared memory and writes them out coalesced.
+constexpr int kMapCols = 16;  // columns (warps) per block
+
+template <int K>
+__device__ __forceinline__ void accumulate_k(float (&re)[K], float (&im)[K], float (&w)[K], int slot, float vr,
+                                             float vi) {
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    if (slot == i) {
+      re[i] = __fadd_rn(re[i], vr);
+      im[i] = __fadd_rn(im[i], vi);
+      w[i] = __fadd_rn(w[i], 1.0f);
+    }
+  }
+}
+
+template <int K>
+__global__ void __launch_bounds__(32 * kMapCols)
     k_map_half(const float2* __restrict__ spectra, const float4* __restrict__ illum, int count, Grid g,
                float2* __restrict__ a, std::uint8_t* __restrict__ hits, unsigned long long* __restrict__ filled) {
+  extern __shared__ __align__(16) unsigned char map_smem[];
   const int n = g.n, nz = g.nz, h = n / 2 + 1;
+  const std::size_t plane = static_cast<std::size_t>(n) * n;  // one spectrum
+  const std::size_t hplane = static_cast<std::size_t>(n) * h;  // one kz plane of the half spectrum
   {  // volume blockIdx.y of a batch: its own spectra, k-space arrays and filled count
     const std::size_t v = blockIdx.y;
-    spectra += v * count * static_cast<std::size_t>(n) * n;
-    a += v * nz * static_cast<std::size_t>(n) * h;
-    hits += v * nz * static_cast<std::size_t>(n) * h;
+    spectra += v * count * plane;
+    a += v * nz * hplane;
+    hits += v * nz * hplane;
     filled += v;
   }
-  const int chunks = (nz + kMapK - 1) / kMapK;
-  const std::size_t total = static_cast<std::size_t>(chunks) * n * h;
-  const std::size_t t = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x;
+  auto* a_tile = reinterpret_cast<float2*>(map_smem);                    // [nz][kMapCols]
+  auto* h_tile = reinterpret_cast<std::uint8_t*>(a_tile + nz * kMapCols);  // [nz][kMapCols]
+  const int lane = static_cast<int>(threadIdx.x) & 31;
+  const int warp = static_cast<int>(threadIdx.x) >> 5;
+  const std::size_t col0 = static_cast<std::size_t>(blockIdx.x) * kMapCols;
+  const std::size_t col = col0 + warp;
   unsigned long long cnt = 0;
-  if (t < total) {
-    const int kx = static_cast<int>(t % h);
-    const std::size_t rest = t / h;
-    const int ky = static_cast<int>(rest % n);
-    const int k0 = static_cast<int>(rest / n) * kMapK;
+  if (col < hplane) {
+    const int ky = static_cast<int>(col / h);
+    const int kx = static_cast<int>(col - static_cast<std::size_t>(ky) * h);
     const int myk = negative_bin(ky, n);
     const int mkx = negative_bin(kx, n);
-    const std::size_t plane = static_cast<std::size_t>(n) * n;
-    float pre[kMapK] = {}, pim[kMapK] = {}, pw[kMapK] = {};
-    float nre[kMapK] = {}, nim[kMapK] = {}, nw[kMapK] = {};
-    for (int ai = 0; ai < count; ++ai) {
-      const float4 il = __ldg(illum + ai);
-      int kz;
-      float nuz;
-      if (ewald_target(g, ky, kx, il.x, il.y, il.z, kz, nuz) && kz >= k0 && kz < k0 + kMapK) {
-        float vr, vi;
-        mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(ky) * n + kx], vr, vi);
-        accumulate(pre, pim, pw, kz - k0, vr, vi);
+    const int k0 = lane * K;
+    float pre[K] = {}, pim[K] = {}, pw[K] = {};
+    float nre[K] = {}, nim[K] = {}, nw[K] = {};
+    for (int base = 0; base < count; base += 32) {
+      const int ai = base + lane;
+      int kp = -1, kn = -1;  // target bins of side P (own column) and N (mirror, already negated)
+      float pr = 0.0f, pi = 0.0f, qr = 0.0f, qi = 0.0f;
+      if (ai < count) {
+        const float4 il = __ldg(illum + ai);
+        int kz;
+        float nuz;
+        if (ewald_target(g, ky, kx, il.x, il.y, il.z, kz, nuz)) {
+          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(ky) * n + kx], pr, pi);
+          kp = kz;
+        }
+        if (ewald_target(g, myk, mkx, il.x, il.y, il.z, kz, nuz)) {
+          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(myk) * n + mkx], qr, qi);
+          kn = negative_bin(kz, nz);
+        }
       }
-      if (ewald_target(g, myk, mkx, il.x, il.y, il.z, kz, nuz)) {
-        const int km = negative_bin(kz, nz);
-        if (km >= k0 && km < k0 + kMapK) {
-          float vr, vi;
-          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(myk) * n + mkx], vr, vi);
-          accumulate(nre, nim, nw, km - k0, vr, vi);
+      const unsigned has_p = __ballot_sync(0xffffffffu, kp >= 0);
+      const unsigned has_n = __ballot_sync(0xffffffffu, kn >= 0);
+      const int last = min(32, count - base);
+      for (int src = 0; src < last; ++src) {  // illumination base + src, in order
+        if ((has_p >> src) & 1u) {
+          const int kz = __shfl_sync(0xffffffffu, kp, src);
+          const float vr = __shfl_sync(0xffffffffu, pr, src);
+          const float vi = __shfl_sync(0xffffffffu, pi, src);
+          if (kz >= k0 && kz < k0 + K) accumulate_k<K>(pre, pim, pw, kz - k0, vr, vi);
+        }
+        if ((has_n >> src) & 1u) {
+          const int kz = __shfl_sync(0xffffffffu, kn, src);
+          const float vr = __shfl_sync(0xffffffffu, qr, src);
+          const float vi = __shfl_sync(0xffffffffu, qi, src);
+          if (kz >= k0 && kz < k0 + K) accumulate_k<K>(nre, nim, nw, kz - k0, vr, vi);
         }
       }
     }
     const bool mirror_is_full_only = kx >= 1 && kx <= n / 2 - 1;
 #pragma unroll
-    for (int i = 0; i < kMapK; ++i) {
+    for (int i = 0; i < K; ++i) {
       const int kz = k0 + i;
-      if (kz >= nz) break;
-      float pr = pre[i], pi = pim[i], mr = nre[i], mi = nim[i];
-      if (pw[i] > 0.0f) {
-        pr = __fdiv_rn(pr, pw[i]);
-        pi = __fdiv_rn(pi, pw[i]);
+      if (kz < nz) {
+        float pr = pre[i], pi = pim[i], mr = nre[i], mi = nim[i];
+        if (pw[i] > 0.0f) {
+          pr = __fdiv_rn(pr, pw[i]);
+          pi = __fdiv_rn(pi, pw[i]);
+        }
+        if (nw[i] > 0.0f) {
+          mr = __fdiv_rn(mr, nw[i]);
+          mi = __fdiv_rn(mi, nw[i]);
+        }
+        a_tile[kz * kMapCols + warp] = make_float2(__fmul_rn(0.5f, __fadd_rn(pr, mr)), __fmul_rn(0.5f, __fsub_rn(pi, mi)));
+        h_tile[kz * kMapCols + warp] = static_cast<std::uint8_t>((pw[i] > 0.0f) + (nw[i] > 0.0f));
+        cnt += (pw[i] > 0.0f) + (mirror_is_full_only && nw[i] > 0.0f);
       }
-      if (nw[i] > 0.0f) {
-        mr = __fdiv_rn(mr, nw[i]);
-        mi = __fdiv_rn(mi, nw[i]);
-      }
-      const std::size_t o = (static_cast<std::size_t>(kz) * n + ky) * h + kx;
-      a[o] = make_float2(__fmul_rn(0.5f, __fadd_rn(pr, mr)), __fmul_rn(0.5f, __fsub_rn(pi, mi)));
-      hits[o] = static_cast<std::uint8_t>((pw[i] > 0.0f) + (nw[i] > 0.0f));
-      cnt += (pw[i] > 0.0f) + (mirror_is_full_only && nw[i] > 0.0f);
+    }
+  }
+  __syncthreads();
+  // Out: kz rows of the block's columns, consecutive threads on consecutive columns.
+  const int ncols = static_cast<int>(min(static_cast<std::size_t>(kMapCols), hplane - min(col0, hplane)));
+  for (int i = static_cast<int>(threadIdx.x); i < nz * kMapCols; i += 32 * kMapCols) {
+    const int kz = i / kMapCols, c = i - kz * kMapCols;
+    if (c < ncols) {
+      const std::size_t o = kz * hplane + col0 + c;
+      a[o] = a_tile[i];
+      hits[o] = h_tile[i];
     }
   }
   cnt = warp_sum(cnt);
-  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(filled, cnt);
+  if (lane == 0 && cnt) atomicAdd(filled, cnt);
 }
 
 // Full complex potential (normalised) and the measured mask, for the complex solver and the plain
@@ -182,9 +238,29 @@ __global__ void __launch_bounds__(256)
 void map_half(const float2* spectra, const float4* illum, int count, const Grid& g, float2* a, std::uint8_t* hits,
               unsigned long long* filled, cudaStream_t s, int batch) {
   require(batch >= 1 && batch <= 65535, "ewald mapping: invalid batch");
-  const int chunks = (g.nz + kMapK - 1) / kMapK;
-  const std::size_t threads = static_cast<std::size_t>(chunks) * g.n * (g.n / 2 + 1);
-  k_map_half<<<dim3(blocks_for(threads, 256), batch), 256, 0, s>>>(spectra, illum, count, g, a, hits, filled);
+  require(g.nz >= 1 && g.nz <= 32 * 16, "ewald mapping: nz must be at most 512");
+  const std::size_t columns = static_cast<std::size_t>(g.n) * (g.n / 2 + 1);
+  const dim3 grid(blocks_for(columns, kMapCols), batch);
+  const std::size_t smem = static_cast<std::size_t>(g.nz) * kMapCols * (sizeof(float2) + 1);
+  const int per_lane = (g.nz + 31) / 32;
+  const auto launch = [&](auto kernel) {
+    if (smem > 48 * 1024) {
+      check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+            "cudaFuncSetAttribute");
+    }
+    kernel<<<grid, 32 * kMapCols, smem, s>>>(spectra, illum, count, g, a, hits, filled);
+  };
+  if (per_lane <= 2) {
+    launch(k_map_half<2>);
+  } else if (per_lane <= 4) {
+    launch(k_map_half<4>);
+  } else if (per_lane <= 8) {
+    launch(k_map_half<8>);
+  } else if (per_lane <= 12) {
+    launch(k_map_half<12>);
+  } else {
+    launch(k_map_half<16>);
+  }
   check_launch("ewald mapping");
 }
 
@@ -236,6 +312,9 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
   illum_.reset(cfg_.count);
   check(cudaMemcpy(illum_.get(), il.data(), il.size() * sizeof(float4), cudaMemcpyHostToDevice), "upload illuminations");
   filled_.reset(b);
+  waits_.reset(1);
+  check(cudaMemset(waits_.get(), 0, waits_.bytes()), "cudaMemset");
+  tv_.wait_status = waits_.get();
   if (real_) {
     a_.reset(b * half_);
     hits_.reset(b * half_);

@@ -66,6 +66,9 @@ class OdtPlan {
 
   // Voxels that received data in the last run, on the device (one count per volume of the batch).
   [[nodiscard]] const unsigned long long* filled() const { return filled_.get(); }
+  // Device counter of the plan's bounded waits that ran out, over its whole life (never reset):
+  // a caller compares it before and after its runs.
+  [[nodiscard]] const unsigned long long* wait_count() const { return waits_.get(); }
   [[nodiscard]] std::size_t volume() const { return vol_; }  // of one reconstruction
   [[nodiscard]] std::size_t device_bytes() const;
   [[nodiscard]] const OdtConfig& config() const { return cfg_; }
@@ -83,6 +86,7 @@ class OdtPlan {
   int first_mark_ = 0;
   DevBuf<float4> illum_;
   DevBuf<unsigned long long> filled_;
+  DevBuf<unsigned long long> waits_;
   DevBuf<float2> a_;
   DevBuf<std::uint8_t> hits_;
   DevBuf<float2> e_;

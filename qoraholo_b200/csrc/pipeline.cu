@@ -11,6 +11,7 @@
 // Stage times are event intervals on the compute stream, read after it finishes (the upload time
 // then includes the host staging of the chunks).
 #include <chrono>
+#include <exception>
 
 #include "host_copy.hpp"
 #include "pipeline.hpp"
@@ -24,6 +25,28 @@ int checked_chunk(int count, int upload_chunks) {
   require(upload_chunks >= 1 && upload_chunks <= count, "Pipeline: upload_chunks must be between 1 and count");
   return (count + upload_chunks - 1) / upload_chunks;
 }
+
+// Waits for every stream of a host-buffer run when an exception leaves the run, so that no transfer
+// queued into or out of caller memory or the page-locked staging is still in flight once the caller
+// gets control back (and may free or reuse that memory). Errors of the waits themselves are dropped:
+// the exception in flight already reports the failure.
+class DrainOnThrow {
+ public:
+  DrainOnThrow(cudaStream_t a, cudaStream_t b, cudaStream_t c)
+      : streams_{a, b, c}, pending_(std::uncaught_exceptions()) {}
+  DrainOnThrow(const DrainOnThrow&) = delete;
+  DrainOnThrow& operator=(const DrainOnThrow&) = delete;
+  ~DrainOnThrow() {
+    if (std::uncaught_exceptions() <= pending_) return;
+    for (cudaStream_t st : streams_) {
+      if (st != nullptr) (void)cudaStreamSynchronize(st);
+    }
+  }
+
+ private:
+  cudaStream_t streams_[3];
+  int pending_;
+};
 
 }  // namespace
 
@@ -45,7 +68,7 @@ PipelinePlan::PipelinePlan(const CropPlan& crop, int count, int upload_chunks, c
   if (own_io) {
     input_ = PinnedBuf<float>(b * count * image);
     output_ = PinnedBuf<float>(b * odt_.volume());
-    filled_host_ = PinnedBuf<unsigned long long>(b);
+    filled_host_ = PinnedBuf<unsigned long long>(b + 1);
     background_.reset(field);
   }
   holo_.reset(b * count * image);
@@ -130,6 +153,7 @@ void PipelinePlan::process_host(const float* holograms, float* index) {
   if (!has_background_) fail(kLogicError, "Pipeline: set_background() first");
   const auto t0 = std::chrono::steady_clock::now();
   const cudaStream_t s = compute_.get();
+  const DrainOnThrow drain(copy_.get(), s, down_.get());
   const std::size_t image = static_cast<std::size_t>(crop_.n) * crop_.n;
   const float* src = holograms == input_.get() ? nullptr : holograms;
   const bool src_locked = src && is_page_locked(src, static_cast<std::size_t>(batch_) * count_ * image * sizeof(float));
@@ -154,6 +178,9 @@ void PipelinePlan::process_host(const float* holograms, float* index) {
   check(cudaMemcpyAsync(filled_host_.get(), odt_.filled(), batch_ * sizeof(unsigned long long),
                         cudaMemcpyDeviceToHost, s),
         "download filled");
+  check(cudaMemcpyAsync(filled_host_.get() + batch_, odt_.wait_count(), sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, s),
+        "download wait count");
   clock_.mark(kDownloaded, s);
   if (index != nullptr && index != output_.get() && !dst_locked) {
     HostCopier& copier = HostCopier::shared();
@@ -164,6 +191,10 @@ void PipelinePlan::process_host(const float* holograms, float* index) {
     }
   }
   check(cudaStreamSynchronize(s), "process");
+  if (filled_host_.get()[batch_] != waits_seen_) {
+    waits_seen_ = filled_host_.get()[batch_];
+    fail(kTimeout, wait_timeout_message("Pipeline"));
+  }
   filled_ = static_cast<double>(*filled_host_.get()) / static_cast<double>(odt_.volume());
   const int o = kRytov + 1;
   timings_.upload = chunk_done_.back().since_event(clock_.event(kStart));
@@ -186,6 +217,7 @@ void PipelinePlan::process_stream(const float* holograms, float* index, int item
   const auto t0 = std::chrono::steady_clock::now();
   const cudaStream_t s = compute_.get();
   const cudaStream_t d = down_.get();
+  const DrainOnThrow drain(copy_.get(), s, d);
   const std::size_t in_item = static_cast<std::size_t>(batch_) * count_ * crop_.n * crop_.n;
   const std::size_t out_item = static_cast<std::size_t>(batch_) * odt_.volume();
   const bool src_locked = is_page_locked(holograms, items * in_item * sizeof(float));
@@ -232,12 +264,35 @@ void PipelinePlan::process_stream(const float* holograms, float* index, int item
     }
     downloaded_[k].record(d);
   }
+  check(cudaMemcpyAsync(filled_host_.get() + batch_, odt_.wait_count(), sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, s),
+        "download wait count");
   collect(items - 1);
   check(cudaStreamSynchronize(d), "stream download");
   check(cudaStreamSynchronize(s), "stream");
+  if (filled_host_.get()[batch_] != waits_seen_) {
+    waits_seen_ = filled_host_.get()[batch_];
+    fail(kTimeout, wait_timeout_message("Pipeline stream"));
+  }
   filled_ = static_cast<double>(*filled_host_.get()) / static_cast<double>(odt_.volume());
   timings_ = PipelineTimes{};
   timings_.total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void PipelinePlan::check_device_waits(cudaStream_t s) {
+  unsigned long long n = 0;
+  check(cudaMemcpyAsync(&n, odt_.wait_count(), sizeof n, cudaMemcpyDeviceToHost, s), "download wait count");
+  check(cudaStreamSynchronize(s), "wait count");
+  if (n != waits_seen_) {
+    waits_seen_ = n;
+    fail(kTimeout, wait_timeout_message("Pipeline"));
+  }
+}
+
+void PipelinePlan::wait_probe(int polls) {
+  require(polls >= 1 && polls <= (1 << 20), "wait_probe: polls must be between 1 and 2^20");
+  bounded_wait_probe(const_cast<unsigned long long*>(odt_.wait_count()), polls, compute_.get());
+  check_device_waits(compute_.get());
 }
 
 void PipelinePlan::process_device(const float* d_holo, float* d_index, cudaStream_t s) {

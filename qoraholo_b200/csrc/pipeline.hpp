@@ -67,6 +67,13 @@ class PipelinePlan {
   [[nodiscard]] std::size_t field_elems() const { return static_cast<std::size_t>(count_) * crop_.out * crop_.out; }
 
   [[nodiscard]] double filled() const { return filled_; }
+  // Fails with kTimeout if a bounded device wait of this plan ran out since the last check (reads
+  // the plan's wait counter; synchronises `s`). The host runs check after their own synchronise;
+  // callers of the device forms call this when they want to know.
+  void check_device_waits(cudaStream_t s);
+  // Test hook: a bounded wait that nothing completes, counted in this plan's wait counter on its
+  // own stream (the form of every wait of the two-step FGP kernel), then check_device_waits.
+  void wait_probe(int polls);
   [[nodiscard]] const PipelineTimes& timings() const { return timings_; }
   [[nodiscard]] std::size_t device_bytes() const;
   [[nodiscard]] bool has_background() const { return has_background_; }
@@ -98,7 +105,8 @@ class PipelinePlan {
   OdtPlan odt_;
   PinnedBuf<float> input_;
   PinnedBuf<float> output_;
-  PinnedBuf<unsigned long long> filled_host_;
+  PinnedBuf<unsigned long long> filled_host_;  // batch_ filled counts, then the plan's wait counter
+  unsigned long long waits_seen_ = 0;            // the wait counter at the last check
   DevBuf<float> holo_;
   DevBuf<float2> background_;
   DevBuf<float2> fields_;

@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "fft_engine.cuh"
@@ -82,6 +83,9 @@ void fft2d(float2* data, int count, int n, bool forward, float scale, cudaStream
 struct TvBuffers {
   float* v[4][3] = {};
   int p_index = 0;
+  // Device counter of this caller's bounded waits that ran out (a TMA box load of the two-step FGP
+  // kernel that never completed); null counts them in the library-wide counter (tv_wait_timeouts).
+  unsigned long long* wait_status = nullptr;
   [[nodiscard]] bool has_fourth() const { return v[3][0] != nullptr; }
 };
 enum class TvFinal : int {
@@ -107,8 +111,12 @@ void set_tv_form(int form);
 // Times the FGP tile heights on this volume's shape and keeps the fastest for later tv_prox calls.
 // b and all three dual triplets of t are scratch (overwritten). Never inside a stream capture.
 void tune_tv(float* b, TvBuffers& t, int nz, int ny, int nx, float lambda, cudaStream_t s);
-// Bounded waits of the FGP kernels that ran out since the library was loaded (0 unless a box load
-// never completed). Synchronises the device.
+// Bounded waits of the FGP kernels that ran out since the library was loaded, in calls whose
+// TvBuffers carry no wait_status of their own (0 unless a box load never completed).
 unsigned long long tv_wait_timeouts();
+// Message of the error raised when a bounded device wait ran out in `what`.
+std::string wait_timeout_message(const char* what);
+// One bounded mbarrier wait that nothing completes, counted in the device word *counter (tma.cu).
+void bounded_wait_probe(unsigned long long* counter, int polls, cudaStream_t s);
 
 }  // namespace qhk

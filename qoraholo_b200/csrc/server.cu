@@ -454,6 +454,9 @@ void Server::launch(const Request& r, Workspace& w, const Geometry& g) {
   check(cudaMemcpyAsync(w.filled.get(), w.plan->odt().filled(), sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                         s),
         "Server: download filled");
+  check(cudaMemcpyAsync(w.filled.get() + 1, w.plan->odt().wait_count(), sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, s),
+        "Server: download wait count");
   w.stop.record(s);
   auto* c = new Completion{this, r.ticket};
   const cudaError_t e = cudaLaunchHostFunc(s, &Server::on_complete, c);
@@ -589,6 +592,11 @@ void Server::loop() {
         r.gpu_ms = 0;
       }
       r.filled = static_cast<double>(*w.filled.get()) / static_cast<double>(geoms_[r.geometry]->volume);
+      if (w.filled.get()[1] != w.waits_seen) {  // a bounded device wait ran out: the volume is not valid
+        w.waits_seen = w.filled.get()[1];
+        fail_request(r, wait_timeout_message("Server"), kTimeout);
+        continue;
+      }
       if (r.out_pinned) {
         r.finished = Clock::now();
         r.done = true;

@@ -162,7 +162,8 @@ class Server {
     std::uint64_t graph_kernels = 0;
     bool warmed = false;
     Event start, stop;
-    PinnedBuf<unsigned long long> filled{1};
+    PinnedBuf<unsigned long long> filled{2};  // the filled count, then the plan's wait counter
+    unsigned long long waits_seen = 0;         // the wait counter after the previous request
     PinnedBuf<float> in, out;  // staging for pageable callers, allocated on first use
     ~Workspace();
   };

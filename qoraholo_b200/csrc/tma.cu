@@ -28,7 +28,22 @@ EncodeTiled encoder() {
   return fn;
 }
 
+// One thread waits on an mbarrier that nothing arrives at, with the bounded wait of the TMA
+// kernels: the wait runs out after `polls` polls and is counted in *counter. No load is in flight,
+// so the CTA can leave at once.
+__global__ void k_wait_probe(unsigned long long* counter, int polls) {
+  __shared__ __align__(8) std::uint64_t bar;
+  tma::mbar_init(&bar, 1);
+  tma::mbar_wait(&bar, 0, counter, polls);
+}
+
 }  // namespace
+
+void bounded_wait_probe(unsigned long long* counter, int polls, cudaStream_t s) {
+  require(counter != nullptr && polls >= 1, "wait_probe: invalid arguments");
+  k_wait_probe<<<1, 1, 0, s>>>(counter, polls);
+  check_launch("wait probe");
+}
 
 CUtensorMap volume_tensor_map(const float* base, int nx, int ny, int nz, int box_x, int box_y) {
   require(base != nullptr && reinterpret_cast<std::uintptr_t>(base) % 16 == 0, "tma: volume must be 16-byte aligned");

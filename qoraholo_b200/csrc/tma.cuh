@@ -59,11 +59,12 @@ __device__ __forceinline__ bool mbar_try_wait(std::uint64_t* bar, unsigned parit
 }
 
 // Bounded wait for the phase `parity` of `bar`: false, and *timeouts incremented, if it has not
-// completed after kWaitLimit polls (each suspends the thread for at most a short hardware-defined
+// completed after `limit` polls (each suspends the thread for at most a short hardware-defined
 // time), so that a load that never lands ends the wait with an error the host can read.
 constexpr int kWaitLimit = 1 << 20;
-__device__ __forceinline__ bool mbar_wait(std::uint64_t* bar, unsigned parity, unsigned long long* timeouts) {
-  for (int i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(std::uint64_t* bar, unsigned parity, unsigned long long* timeouts,
+                                          int limit = kWaitLimit) {
+  for (int i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
   }
   atomicAdd(timeouts, 1ull);

@@ -607,6 +607,7 @@ struct Fgp2Args {
   float lambda, step;
   float m1, m2;     // momenta of steps k and k + 1
   float neg_zero;  // -0.0f, the addend of the packed products (a value the compiler cannot see)
+  unsigned long long* timeouts;  // bounded waits that ran out are counted here (null: g_fgp2_timeouts)
 };
 // Box-load maps of r_k (on the first step p_0), boxes of (pitch x TY+4 rows), and of b (pitch x TY+3).
 struct Fgp2Maps {
@@ -615,7 +616,8 @@ struct Fgp2Maps {
   CUtensorMap p[3];  // p_k, boxes of (pitch x TY+2 rows); not read on the first step
 };
 
-// Waits of k_fgp2 that ran out (a box load that never completed); read by tv_wait_timeouts().
+// Waits of k_fgp2 that ran out (a box load that never completed) in calls that pass no counter of
+// their own; read by tv_wait_timeouts().
 __device__ unsigned long long g_fgp2_timeouts = 0;
 
 // The same two operations on a pair of neighbouring x points with Blackwell's packed FP32 add and
@@ -784,7 +786,22 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
     for (int i = 0; i < 4; ++i) tma::mbar_init(bars + i, 1);
   }
   __syncthreads();
+  unsigned long long* const timeouts = A.timeouts != nullptr ? A.timeouts : &g_fgp2_timeouts;
   unsigned phases = 0;  // bit i: parity of the next completion of mbarrier i
+  // Thread 0 (the only issuer): bit i of `armed` is set while mbarrier i has a load in flight whose
+  // completion no wait has seen yet; bit i of `armed_par` is that completion's parity. An early exit
+  // waits for those loads (bounded) before the CTA's shared memory can be handed to another CTA.
+  unsigned armed = 0, armed_par = 0;
+  const auto arm = [&](int i) {
+    armed |= 1u << i;
+    armed_par = (armed_par & ~(1u << i)) | (phases & (1u << i));
+  };
+  const auto drain = [&]() {
+    if (linear != 0) return;
+    for (int i = 0; i < 4; ++i) {
+      if ((armed >> i) & 1u) tma::mbar_wait(bars + i, (armed_par >> i) & 1u, timeouts);
+    }
+  };
   // Halo rows as pairs of points (x, x+1), x even: 2 nx pair slots, slot u = linear + j nthreads.
   // Slots below 3 nx / 2 are the z_k halo rows y0-1 (side 0), y0+TY (1), y0+TY+1 (2) -- z_k / b row
   // 0, TY+1, TY+2 -- of which those below nx are also the dual-k halo rows, so each such pair's z_k is
@@ -819,18 +836,21 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
     const auto issue = [&](int z, int s, int comps, bool with_b) {
       tma::fence_async_shared();
       std::uint64_t* bar = bars + s;
+      arm(s);
       tma::mbar_expect(bar, static_cast<unsigned>((comps * RK_ROWS + (with_b ? B_ROWS : 0)) * P * 4));
       for (int c = 0; c < comps; ++c) tma::load_3d(smem2 + (s * 3 + c) * RKP, &M.r[c], 0, y0 - 2, z, bar);
       if (with_b) tma::load_3d(smem2 + OB + s * BP, &M.b, 0, y0 - 1, z, bar);
     };
     const auto issue_pk = [&](int z) {
       tma::fence_async_shared();
+      arm(3);
       tma::mbar_expect(bars + 3, static_cast<unsigned>(3 * R1_ROWS * P * 4));
       for (int c = 0; c < 3; ++c) tma::load_3d(smem2 + OPK + c * R1P, &M.p[c], 0, y0 - 1, z, bars + 3);
     };
     // Bounded wait on mbarrier i (every thread), then its phase bit flips.
     const auto wait_bar = [&](int i) {
-      const bool done = tma::mbar_wait(bars + i, (phases >> i) & 1u, &g_fgp2_timeouts);
+      const bool done = tma::mbar_wait(bars + i, (phases >> i) & 1u, timeouts);
+      if (done) armed &= ~(1u << i);
       phases ^= 1u << i;
       return done;
     };
@@ -859,8 +879,8 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
       if (wait_plane) ok = wait_bar(m2) && ok;
       if (__syncthreads_or(!ok)) {
         // A load never completed: leave with the timeout counted (every thread takes this exit),
-        // after one more bounded wait for the load in flight.
-        if (wait_plane) tma::mbar_wait(bars + m2, ((phases >> m2) & 1u) ^ 1u, &g_fgp2_timeouts);
+        // after a bounded wait for each load still in flight (the plane of slot m2, p_k of a1).
+        drain();
         return;
       }
       // Slot m0 held plane q, last read one iteration ago: plane q+3 streams in for a whole plane.
@@ -974,7 +994,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
         }
       }
       if (__syncthreads_or(!ok)) {  // r_{k+1} of plane a1 complete
-        if (wait_pk) tma::mbar_wait(bars + 3, ((phases >> 3) & 1u) ^ 1u, &g_fgp2_timeouts);
+        drain();  // p_k of a1 if its wait ran out, and plane q+3 issued into slot m0 above
         return;
       }
       // Every thread is past dual step k of a1: the p_k slot is free for p_k of a2, exactly the
@@ -1297,6 +1317,12 @@ unsigned long long tv_wait_timeouts() {
   return n;
 }
 
+std::string wait_timeout_message(const char* what) {
+  return std::string(what) +
+         ": a bounded device wait ran out (a TMA load of the two-step FGP kernel never completed); "
+         "the result is not valid";
+}
+
 void set_tv_form(int form) {
   require((form >= 0 && form <= 3) || form == 18 || form == 20 || form == 24,
           "tv: form must be 0 (tuned), 1 (stored r), 2 (recomputed r), 3 (two steps per pass) or 16 + rows "
@@ -1344,6 +1370,7 @@ void tv_prox(const float* b, TvBuffers& t, int nz, int ny, int nx, float lambda,
       const float t1 = fista_t(tk);
       const float t2 = fista_t(t1);
       Fgp2Args a{};
+      a.timeouts = t.wait_status;
       a.nz = nz, a.ny = ny, a.nx = nx;
       a.ytiles = (ny + sh.ty - 1) / sh.ty;
       a.lambda = lambda, a.step = step;

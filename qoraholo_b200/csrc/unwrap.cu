@@ -14,7 +14,6 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
-#include <mutex>
 #include <numbers>
 #include <vector>
 
@@ -328,6 +327,15 @@ int rows_per_cta(int len, std::size_t extra_per_row) {
   return c;
 }
 
+// 2 cos(pi k / n) of the Neumann eigenvalue (src/common.hpp:28-31): the argument in float as the
+// reference forms it, its cosine evaluated in double and rounded once to float -- the correctly
+// rounded value in all but vanishingly rare cases, so that host-built and device-built tables agree
+// (the C library's single-precision cosine is off by an ulp for about 1 % of these arguments).
+float eigen_cos2(int k, int n) {
+  const float a = kPiF * static_cast<float>(k) / static_cast<float>(n);
+  return 2.0f * static_cast<float>(std::cos(static_cast<double>(a)));
+}
+
 unsigned grid_for(std::size_t total) {
   return static_cast<unsigned>(std::min<std::size_t>((total + kThreads - 1) / kThreads, 148u * 32u));
 }
@@ -345,10 +353,9 @@ UnwrapPlan::UnwrapPlan(int count, int ny, int nx) : count_(count), ny_(ny), nx_(
     }
     return w;
   };
-  // 2 cos(pi k / n) in float as the host's neumann_eigenvalue evaluates it.
   const auto cos_table = [](int n) {
     std::vector<float> c(n);
-    for (int k = 0; k < n; ++k) c[k] = 2.0f * std::cos(kPiF * static_cast<float>(k) / static_cast<float>(n));
+    for (int k = 0; k < n; ++k) c[k] = eigen_cos2(k, n);
     return c;
   };
   const auto up = [](auto& buf, const auto& host) {
@@ -607,7 +614,7 @@ UnwrapBatchPlan::UnwrapBatchPlan(const int* ny, const int* nx, int count) {
     for (int k = 0; k < n; ++k) {
       const double a = -std::numbers::pi * k / (2.0 * n);
       w[k] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
-      c[k] = 2.0f * std::cos(kPiF * static_cast<float>(k) / static_cast<float>(n));
+      c[k] = eigen_cos2(k, n);
     }
     dtw_.emplace_back(n);
     cos_.emplace_back(n);
@@ -767,21 +774,15 @@ static __device__ __align__(256) float g_unwrap_scratch[kNoAllocFloats];
 
 namespace {
 
-// Per-device address of g_unwrap_scratch (host code must not pass the symbol itself to a kernel).
-std::mutex g_scratch_mutex;
-float* g_scratch_ptr[64] = {};
-
+// The current device's address of g_unwrap_scratch. In host code the array's name is only a
+// host-side stand-in, so kernels get this address instead. It is looked up on every call (a cheap
+// query that allocates nothing) rather than cached, so that a device or primary-context reset
+// cannot leave a stale address behind. The first lookup on a device is the one that may load this
+// file's module there (lazy module loading) and with it reserve the array.
 float* scratch_base() {
-  int dev = 0;
-  check(cudaGetDevice(&dev), "cudaGetDevice");
-  require(dev >= 0 && dev < 64, "unwrap_noalloc: device index out of range");
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    check(cudaGetSymbolAddress(&p, g_unwrap_scratch), "cudaGetSymbolAddress");
-    g_scratch_ptr[dev] = static_cast<float*>(p);
-  }
-  return g_scratch_ptr[dev];
+  void* p = nullptr;
+  check(cudaGetSymbolAddress(&p, g_unwrap_scratch), "cudaGetSymbolAddress");
+  return static_cast<float*>(p);
 }
 
 // DCT twiddles e^{-i pi k / 2n}, 2 cos(pi k / n) and FFT twiddles e^{-2 pi i k / n} for one side.
@@ -790,7 +791,8 @@ __global__ void k_side_tables(int n, float2* dtw, float* cos2, float2* fftw) {
     double s, c;
     sincos(-3.141592653589793238462643 * k / (2.0 * n), &s, &c);
     dtw[k] = make_float2(static_cast<float>(c), static_cast<float>(s));
-    cos2[k] = 2.0f * cosf(kPiF * static_cast<float>(k) / static_cast<float>(n));
+    // The host tables' value (eigen_cos2): the float argument, its cosine in double, rounded once.
+    cos2[k] = 2.0f * static_cast<float>(cos(static_cast<double>(kPiF * static_cast<float>(k) / static_cast<float>(n))));
     sincos(6.283185307179586476925287 * k / n, &s, &c);
     fftw[k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
   }

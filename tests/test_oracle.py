@@ -126,3 +126,24 @@ def test_oracle_against_reference_library_random_cases():
     xr, pr = refimpl.tv_prox(b0, p0, 0.07, 5)
     p = [p0[a].copy() for a in range(3)]
     assert np.array_equal(O.tv_prox(b0, p, 0.07, 5), xr) and np.array_equal(np.stack(p), pr)
+
+
+@pytest.mark.parametrize("n,nz,pixel", [(64, 64, 0.25), (256, 256, 0.11)])
+def test_ewald_mapping_equals_the_reference_bitwise(n, nz, pixel):
+    """The numpy mapping and Hermitian half data against the reference's own mapping (oracle/_ref's
+    ref_ewald_half: its ewald_target, parity and hermitian_data), 49 views, up to the C2 size."""
+    if not refimpl.available():
+        pytest.skip("oracle/_ref not built")
+    geom = np.array([0.532, 1.337, 1.2, pixel], np.float32)
+    il = O.circular_scan(49, 0.9, geom)
+    rng = np.random.default_rng(n)
+    sp = (rng.standard_normal((49, n, n)) + 1j * rng.standard_normal((49, n, n))).astype(np.complex64)
+    a_ref, hits_ref, filled_ref = refimpl.ewald_half(sp, il, geom, nz)
+    pre, pim, w = O.ewald_map(sp, il, O.make_grid(n, nz, geom))
+    f = w > 0
+    pre = np.where(f, pre / np.where(f, w, 1), pre).astype(np.float32)
+    pim = np.where(f, pim / np.where(f, w, 1), pim).astype(np.float32)
+    a, hits = O.hermitian_half(pre, pim, w)
+    assert np.array_equal(hits, hits_ref)
+    assert np.array_equal(a, a_ref)
+    assert int(np.count_nonzero(f)) == filled_ref
