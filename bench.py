@@ -361,6 +361,34 @@ def cpu_baseline(holo, bg, illum, runs=2):
     return base, ri, filled
 
 
+def reference_cuda_leg(holo, bg, illum, ref_cpu, runs=3):
+    """The reference's own CUDA backend (oracle/_ref/libqhref_cuda.so: its src/cuda/*.cu built
+    unmodified for sm_100a with cuFFT) on the same workload through its public Pipeline::run on this
+    B200: milliseconds of the last of `runs` runs (the earlier ones warm cuFFT plans), and its
+    error against the reference CPU result. The per-kernel comparison with ours comes from a launch
+    list of `--kernel-case refcuda`."""
+    from oracle import fp64, refimpl
+
+    if not refimpl.cuda_available():
+        return {"unavailable": "oracle/_ref/libqhref_cuda.so is not built"}
+    try:
+        refimpl.select(cuda=True)
+        ri, filled, ms = refimpl.pipeline(holo, bg, (CARRIER_PX, CARRIER_PX), RADIUS, FIELD_N, illum, geom_tuple(),
+                                          iterations=ITERATIONS, solver="tv", tv_weight=TV_WEIGHT,
+                                          tv_inner=TV_INNER, runs=runs)
+    finally:
+        refimpl.select(cuda=False)
+    out = {"ms_per_recon": round(ms["run"], 2), "recons_per_s": round(1000.0 / ms["run"], 3),
+           "stage_ms": {k: round(float(ms[k]), 2) for k in ("fields", "rytov", "fft2", "mapping", "normalize",
+                                                             "solve", "finish")},
+           "filled": filled,
+           "path": "reference Pipeline::run (host holograms in, host volume out) with its CUDA backend, "
+                   f"last of {runs} runs, its own host-clock timing"}
+    if ref_cpu is not None:
+        out["rel_err_vs_reference_cpu"] = fp64.rel_contrast_err(ri, ref_cpu, N_MEDIUM)
+    return out
+
+
 def parity_report(ours, ours_filled, ref, ref_filled, holo, bg, illum):
     """Our volume against the reference CPU volume of the same inputs (index-contrast error, the
     measure of the reference's tests/test_cuda.cpp:92-97, and the filled fraction), both against an
@@ -908,7 +936,10 @@ def c4_leg(qh, capi, torch, reps=5):
 
 
 def kernel_case(name, reps, tv_form=0):
-    """Small standalone launches of one kernel family for profiling (no JSON line): `fgp` runs the
+    """Small standalone launches of one kernel family for profiling (no JSON line): `c2` runs the C2
+    reconstruction (the bench workload, device-resident) `reps` times after a warm-up run, each inside
+    the NVTX range "c2_step"; `refcuda` the reference's CUDA Pipeline::run on the same workload (`reps`
+    runs); `unwrapbatch` the C4 batch of 512 uneven unwraps (`reps` runs, no graph); `fgp` runs the
     TV proximal step at 256^3 on a 12-volume workspace (10 FGP steps in the tuned form + final primal
     per rep); `fft` a 256^3 rfft3 + irfft3
     per rep; `kspace` a 256^3 GP-4 solve from 49 random 256^2 fields per rep (the k-space step's
@@ -937,6 +968,44 @@ def kernel_case(name, reps, tv_form=0):
         index = torch.empty(plan.shape, dtype=torch.float32, device="cuda")
         for _ in range(reps):
             plan.run(fields.data_ptr(), index.data_ptr(), stream)
+    elif name == "c2":
+        import qoraholo_b200 as qh
+
+        illum, holo, bg = make_inputs()
+        pipe = capi.Pipeline(COUNT, HOLO_N, (CARRIER_PX, CARRIER_PX), illum, geom_tuple(), radius=RADIUS,
+                             output_size=FIELD_N, iterations=ITERATIONS, solver="tv", tv_weight=TV_WEIGHT,
+                             tv_inner=TV_INNER)
+        pipe.set_background(bg)
+        d_holo = torch.from_numpy(holo).cuda()
+        d_index = torch.empty(pipe.shape, dtype=torch.float32, device="cuda")
+        pipe.process_device(d_holo.data_ptr(), d_index.data_ptr(), stream)  # warm (plans, tuning)
+        torch.cuda.synchronize()
+        for _ in range(reps):  # ncu --nvtx --nvtx-include "c2_step/" captures exactly these launches
+            torch.cuda.nvtx.range_push("c2_step")
+            pipe.process_device(d_holo.data_ptr(), d_index.data_ptr(), stream)
+            torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        pipe.check_waits(stream)
+    elif name == "unwrapbatch":
+        rng = np.random.default_rng(5)
+        shapes = [(int(v), int(v)) for v in rng.choice(C4_SIDES, C4_UNWRAP)]
+        maps = phase_maps(torch, shapes)
+        plan = capi.UnwrapBatch(shapes)
+        d_in = torch.cat([m.reshape(-1) for m in maps])
+        d_out = torch.empty_like(d_in)
+        del maps
+        for _ in range(reps):
+            plan.run(d_in.data_ptr(), d_out.data_ptr(), stream, graph=False)
+    elif name == "refcuda":
+        from oracle import refimpl
+
+        illum, holo, bg = make_inputs()
+        refimpl.select(cuda=True)
+        _, _, ms = refimpl.pipeline(holo, bg, (CARRIER_PX, CARRIER_PX), RADIUS, FIELD_N, illum, geom_tuple(),
+                                    iterations=ITERATIONS, solver="tv", tv_weight=TV_WEIGHT, tv_inner=TV_INNER,
+                                    runs=reps)
+        refimpl.select(cuda=False)
+        print(f"reference CUDA Pipeline::run: {ms['run']:.1f} ms (last of {reps})")
     elif name == "fgp":
         n = FIELD_N
         b = torch.rand((n, n, n), device="cuda")
@@ -969,7 +1038,9 @@ def kernel_case(name, reps, tv_form=0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "serve", "bpm", "c4"], default=None,
+    ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "c2", "refcuda", "unwrapbatch",
+                                              "serve", "bpm", "c4"],
+                    default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--tv-form", type=int, default=0, choices=[0, 1, 2, 3, 18, 20, 24],
@@ -1114,13 +1185,19 @@ def main():
 
     cpu = None
     parity = None
+    ref_cuda = None
     if rank == 0 and world == 1:
+        ref = None
         try:
             cpu, ref, ref_filled = cpu_baseline(holo, bg, illum)
             parity = parity_report(ours, filled, ref, ref_filled, holo, bg, illum)
         except Exception as e:  # noqa: BLE001
             cpu = cpu or {"value": None, "unit": UNIT, "cores": None, "kind": "reference", "sample": f"failed: {e}"}
             parity = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            ref_cuda = reference_cuda_leg(holo, bg, illum, ref)
+        except Exception as e:  # noqa: BLE001
+            ref_cuda = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         lat = sorted(step_ms)
@@ -1141,6 +1218,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "parity": parity,
+            "reference_cuda": ref_cuda,
             "rel_err_vs_reference_cpu": (parity or {}).get("rel_err_vs_reference_cpu"),
             "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(holo.nbytes),
                     "d2h_bytes_per_step": int(FIELD_N ** 3 * 4),

@@ -74,9 +74,14 @@ std::vector<Sphere> spheres(const float* s, int k) {
   return out;
 }
 
+// Backend of the ODT options built below: the CPU one, or the reference's CUDA backend in the
+// library built with it (ref_use_cuda).
+Backend g_backend = Backend::cpu;
+
 OdtOptions odt_options(int nz, int iterations, int solver, int gp_transform, float tv_weight,
                        int tv_inner) {
   OdtOptions o;
+  o.backend = g_backend;
   o.nz = nz;
   o.iterations = iterations;
   o.solver = solver ? Solver::tv : Solver::gerchberg_papoulis;
@@ -89,6 +94,19 @@ OdtOptions odt_options(int nz, int iterations, int solver, int gp_transform, flo
 }  // namespace
 
 extern "C" {
+
+// Selects the reference's CUDA backend (1) or its CPU backend (0) for reconstruct and the Pipeline;
+// error 2 when this library was built without the CUDA backend.
+int ref_use_cuda(int on) {
+  return guard([&] {
+#ifdef QORAHOLO_HAS_CUDA
+    g_backend = on ? Backend::cuda : Backend::cpu;
+#else
+    if (on) throw std::runtime_error("reference built without its CUDA backend");
+    g_backend = Backend::cpu;
+#endif
+  });
+}
 
 const char* ref_last_error() { return g_error.c_str(); }
 

@@ -15,7 +15,9 @@ from pathlib import Path
 import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "_ref" / "libqhref.so"
+LIB_CUDA_PATH = Path(__file__).resolve().parent / "_ref" / "libqhref_cuda.so"
 _lib = None
+_path = LIB_PATH
 
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: RuntimeError}
 
@@ -28,12 +30,27 @@ def available() -> bool:
     return LIB_PATH.exists()
 
 
+def cuda_available() -> bool:
+    """The reference built with its CUDA backend (oracle/build_ref.py build_cuda) is present."""
+    return LIB_CUDA_PATH.exists()
+
+
+def select(cuda: bool = False):
+    """Routes every call of this module to the reference's CUDA backend (reconstruct and the Pipeline
+    on the GPU, src/cuda/*) or back to its CPU backend."""
+    global _lib, _path
+    path = LIB_CUDA_PATH if cuda else LIB_PATH
+    if path != _path:
+        _lib, _path = None, path
+    _check(lib().ref_use_cuda(C.c_int(1 if cuda else 0)))
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
-            raise FileNotFoundError(f"{LIB_PATH} is not built; run python oracle/build_ref.py")
-        _lib = C.CDLL(str(LIB_PATH))
+        if not _path.exists():
+            raise FileNotFoundError(f"{_path} is not built; run python oracle/build_ref.py")
+        _lib = C.CDLL(str(_path))
         _lib.ref_last_error.restype = C.c_char_p
     return _lib
 

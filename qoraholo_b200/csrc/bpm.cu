@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "bpm.hpp"
+#include "nvtx.hpp"
 
 namespace qhk {
 
@@ -384,6 +385,7 @@ void BpmPlan::fft2(const float2* src, float2* dst, bool forward, int nb, int mod
 }
 
 void BpmPlan::forward(const float* x, int first, int nb, cudaStream_t s) {
+  const NvtxRange r("qhk:bpm_forward");
   const int nz = t_.nz;
   const std::size_t total = plane_ * nb;
   const std::size_t off = plane_ * first;
@@ -420,6 +422,7 @@ void BpmPlan::forward(const float* x, int first, int nb, cudaStream_t s) {
 
 void BpmPlan::adjoint(const float* x, const float2* residual_or_null, int first, int nb, float gscale, float* grad,
                       cudaStream_t s) {
+  const NvtxRange r("qhk:bpm_adjoint");
   const int nz = t_.nz;
   const std::size_t total = plane_ * nb;
   const std::size_t off = plane_ * first;

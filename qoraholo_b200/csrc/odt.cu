@@ -19,6 +19,7 @@
 
 #include "autotune.hpp"
 #include "odt.hpp"
+#include "nvtx.hpp"
 
 namespace qhk {
 
@@ -394,19 +395,25 @@ void OdtPlan::run(float2* fields, float* index, cudaStream_t s, StageClock* cloc
   const std::size_t nn = static_cast<std::size_t>(n) * n;
   const float inv = 1.0f / (static_cast<float>(nz) * static_cast<float>(n) * static_cast<float>(n));
 
-  fft2d(fields, cfg_.count * cfg_.batch, n, true, 1.0f, s);
+  {
+    const NvtxRange r("qhk:fft2");
+    fft2d(fields, cfg_.count * cfg_.batch, n, true, 1.0f, s);
+  }
   mark(clock, kMarkFft2, s);
   check(cudaMemsetAsync(filled_.get(), 0, filled_.bytes(), s), "cudaMemset");
   mark(clock, kMarkClear, s);
   if (real_) {
+    const NvtxRange r("qhk:mapping");
     map_half(fields, illum_.get(), cfg_.count, g, a_.get(), hits_.get(), filled_.get(), s, cfg_.batch);
   } else {
+    const NvtxRange r("qhk:mapping");
     map_full(fields, illum_.get(), cfg_.count, g, pot_.get(), measured_.get(), mask_.get(), filled_.get(), s,
              cfg_.batch);
   }
   mark(clock, kMarkMapping, s);
   mark(clock, kMarkNormalize, s);
 
+  const NvtxRange r("qhk:solve");
   if (real_) {
     solve_real(index, inv, s);
   } else {
@@ -460,8 +467,10 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
   for (int it = 0; it < cfg_.iterations; ++it) {
     const bool last = it == cfg_.iterations - 1;
     if (it == 0) {
+      const NvtxRange r("qhk:kspace");
       kspace_step(x_.get(), false, x_.get(), C2rMode::store);
     } else {
+      const NvtxRange r("qhk:kspace");
       axis_pass(e, b * nz, nh, n, h, h, true, AxisMode::plain, 1.0f, AxisAux{}, s);
       axis_pass(e, n, h, nz, nh, h, true, AxisMode::restore_half, inv, aux, s, b, half_);
       axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
@@ -469,6 +478,7 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
     }
     const float tn = fista_t(t);
     const float m = (t - 1.0f) / tn;
+    const NvtxRange r("qhk:tv_prox");
     if (last) {
       tv_prox(x_.get(), tv_, nz, n, n, cfg_.lambda, cfg_.tv_inner, TvFinal::index, m, xprev_.get(), index,
               cfg_.nm2, cfg_.inv_k02, s);

@@ -15,6 +15,7 @@
 
 #include "host_copy.hpp"
 #include "pipeline.hpp"
+#include "nvtx.hpp"
 
 namespace qhk {
 
@@ -136,9 +137,15 @@ void PipelinePlan::compute(const float* d_holo, bool chunked_upload, const float
   } else {
     field_.spectra(d_holo, 0, images, s);
   }
-  field_.finish(1, nullptr, bg, psi_.get(), logamp_.get(), s, count_);
+  {
+    const NvtxRange r("qhk:fields");
+    field_.finish(1, nullptr, bg, psi_.get(), logamp_.get(), s, count_);
+  }
   if (marks) clock_.mark(kFields, s);
-  unwrap_.rytov(psi_.get(), logamp_.get(), phi_.get(), fields_.get(), s);
+  {
+    const NvtxRange r("qhk:rytov");
+    unwrap_.rytov(psi_.get(), logamp_.get(), phi_.get(), fields_.get(), s);
+  }
   if (marks) clock_.mark(kRytov, s);
   if (marks) {
     odt_.run_marked(fields_.get(), d_index, s, &clock_, kRytov + 1);

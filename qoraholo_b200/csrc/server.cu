@@ -19,6 +19,7 @@
 #include <cstring>
 #include <thread>
 
+#include "nvtx.hpp"
 #include "server.hpp"
 
 namespace qhk {
@@ -481,6 +482,7 @@ void Server::fail_request(Request& r, const std::string& error, Status status) {
 // Stager: stage the input into the workspace (pageable callers), allocate the workspace if it is
 // new, and enqueue the request's device work.
 void Server::start_request(std::uint64_t ticket, HostCopier& copier) {
+  const NvtxRange range("qhk:serve_request");
   Request* r = nullptr;
   Workspace* w = nullptr;
   const Geometry* g = nullptr;

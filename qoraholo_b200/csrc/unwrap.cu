@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "unwrap.hpp"
+#include "nvtx.hpp"
 
 namespace qhk {
 
@@ -705,6 +706,7 @@ std::size_t UnwrapBatchPlan::device_bytes() const {
 }
 
 void UnwrapBatchPlan::unwrap(const float* psi, float* phi, cudaStream_t s) {
+  const NvtxRange r("qhk:unwrap_batch");
   const auto* imgs = reinterpret_cast<const BatchImage*>(images_.get());
   int* q = counters_.get();
   const auto items = [&](int p) { return static_cast<const int2*>(pass_[p].items); };
