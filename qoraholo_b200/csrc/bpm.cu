@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "bpm.hpp"
+#include "fft_reg.cuh"
 #include "nvtx.hpp"
 
 namespace qhk {
@@ -122,6 +123,113 @@ __global__ void __launch_bounds__(kThreads) k_cols(ColArgs a, FftLen L) {
       a.s[g] = make_float2((1.0f - q) * ure, (1.0f - q) * uim);
     }
   }
+}
+
+// The same two passes on the register-resident engine (fft_reg.cuh) for n = 64, 128, 256: rows with
+// R = 256 / T rows per CTA, T threads per row; columns with COLS = 256 / T columns per CTA, T threads
+// per column, the epilogue of k_cols applied to the positions each thread holds.
+template <bool Fwd, int T, int V>
+__global__ void __launch_bounds__(kThreads)
+    k_rows_reg(const float2* __restrict__ src, float2* __restrict__ dst, std::size_t rows, const float2* tw) {
+  using Tile = regfft::RowTile<T>;
+  constexpr int N = T * V;
+  extern __shared__ float2 sm[];
+  const int t = static_cast<int>(threadIdx.x) % T, r = static_cast<int>(threadIdx.x) / T;
+  const std::size_t row = static_cast<std::size_t>(blockIdx.x) * Tile::R + r;
+  const bool live = row < rows;
+  float2 v[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) v[j] = live ? src[row * N + t + T * j] : make_float2(0.f, 0.f);
+  regfft::line_fft<T, V, Fwd>(v, t, sm + r, Tile::A, Tile::B, tw);  // every row read before any write
+  if (live) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) dst[row * N + t + T * j] = v[j];
+  }
+}
+
+template <bool Fwd, int Mode, int T, int V>
+__global__ void __launch_bounds__(kThreads) k_cols_reg(ColArgs a, const float2* tw) {
+  constexpr int N = T * V, COLS = kThreads / T;
+  extern __shared__ float2 sm[];
+  const int c = static_cast<int>(threadIdx.x) % COLS, t = static_cast<int>(threadIdx.x) / COLS;
+  const int col = static_cast<int>(blockIdx.x) * COLS + c;
+  const bool live = col < N;
+  const std::size_t base = static_cast<std::size_t>(blockIdx.y) * N * N + (live ? col : 0);
+  float2 v[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) v[j] = live ? a.data[base + static_cast<std::size_t>(t + T * j) * N] : make_float2(0.f, 0.f);
+  regfft::line_fft<T, V, Fwd>(v, t, sm + c, T * COLS, COLS, tw);
+  if (!live) return;
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    const int pos = t + T * j;
+    const std::size_t g = base + static_cast<std::size_t>(pos) * N;
+    const float2 vv = v[j];
+    if constexpr (Mode == kScreen) {
+      const float2 w = cscale(vv, a.inv);
+      if (a.store) a.store[g] = w;
+      float sn, cs;
+      sincosf(a.phase * a.x[static_cast<std::size_t>(pos) * N + col], &sn, &cs);
+      a.data[g] = cmul(make_float2(cs, sn), w);
+    } else if constexpr (Mode == kPropagate) {
+      const float2 cc = a.coef[g];
+      const float q = a.q[g];
+      const float2 sv = a.s[g];
+      const float tre = q * vv.x + (1.0f - q) * sv.x;
+      const float tim = q * vv.y + (1.0f - q) * sv.y;
+      a.s[g] = make_float2(cc.x * tre - cc.y * tim, cc.x * tim + cc.y * tre);
+    } else if constexpr (Mode == kScale) {
+      a.data[g] = cscale(vv, a.inv);
+    } else {
+      float2 gi = a.s[g];
+      if (a.has_back) gi = cadd(gi, vv);
+      else gi = vv;
+      const float2 cc = a.coef[g];
+      const float q = a.q[g];
+      const float ure = cc.x * gi.x + cc.y * gi.y;
+      const float uim = cc.x * gi.y - cc.y * gi.x;
+      a.data[g] = make_float2(q * ure, q * uim);
+      a.s[g] = make_float2((1.0f - q) * ure, (1.0f - q) * uim);
+    }
+  }
+}
+
+template <int T, int V>
+void fft2_reg(const float2* src, float2* dst, bool forward, int nb, int mode, const ColArgs& args, cudaStream_t s) {
+  constexpr int N = T * V;
+  const float2* tw = fft_len(N).tw;
+  const std::size_t rows = static_cast<std::size_t>(nb) * N;
+  {
+    using Tile = regfft::RowTile<T>;
+    const std::size_t smem = static_cast<std::size_t>(V) * Tile::A * sizeof(float2);
+    const unsigned grid = static_cast<unsigned>((rows + Tile::R - 1) / Tile::R);
+    const auto launch = [&](auto kernel) {
+      ensure_smem(kernel);
+      kernel<<<grid, kThreads, smem, s>>>(src, dst, rows, tw);
+    };
+    if (forward) {
+      launch(k_rows_reg<true, T, V>);
+    } else {
+      launch(k_rows_reg<false, T, V>);
+    }
+    check_launch("bpm rows");
+  }
+  ColArgs a = args;
+  a.data = dst;
+  constexpr int COLS = kThreads / T;
+  const std::size_t smem = static_cast<std::size_t>(N) * COLS * sizeof(float2);
+  const dim3 grid((N + COLS - 1) / COLS, nb);
+  const auto launch = [&](auto kernel) {
+    ensure_smem(kernel);
+    kernel<<<grid, kThreads, smem, s>>>(a, tw);
+  };
+  switch (mode) {
+    case kScreen: launch(k_cols_reg<false, kScreen, T, V>); break;
+    case kPropagate: launch(k_cols_reg<true, kPropagate, T, V>); break;
+    case kScale: launch(k_cols_reg<false, kScale, T, V>); break;
+    default: launch(k_cols_reg<true, kSplit, T, V>); break;
+  }
+  check_launch("bpm cols");
 }
 
 // Spectrum of the unit envelope: n^2 at the zero bin of every plane.
@@ -334,6 +442,17 @@ std::size_t BpmPlan::device_bytes() const {
 void BpmPlan::fft2(const float2* src, float2* dst, bool forward, int nb, int mode, const void* args_v,
                    cudaStream_t s) {
   const int n = t_.n;
+  if (fft_reg_engine_enabled() && (n == 64 || n == 128 || n == 256)) {
+    const ColArgs& args = *static_cast<const ColArgs*>(args_v);
+    if (n == 64) {
+      fft2_reg<8, 8>(src, dst, forward, nb, mode, args, s);
+    } else if (n == 128) {
+      fft2_reg<8, 16>(src, dst, forward, nb, mode, args, s);
+    } else {
+      fft2_reg<16, 16>(src, dst, forward, nb, mode, args, s);
+    }
+    return;
+  }
   const FftLen& L = fft_len(n);
   const int c = rows_cols(n);
   const std::size_t rows = static_cast<std::size_t>(nb) * n;

@@ -693,6 +693,7 @@ void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
   require(n_outer >= 1 && n_outer <= 65535 && batch >= 1 && batch <= 65535,
           "fft: too many lines in the outer dimension");
+  if (axis_pass_reg(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s, batch, sb)) return;
   require(static_cast<std::size_t>(n) * 2 * sizeof(float2) <= 200 * 1024, "fft: transform length too large");
   const int cols = tuned_choice(axis_key(n_outer, so, n, sp, ni, forward, mode, batch), axis_default(n));
   axis_cols(cols, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s);
@@ -702,6 +703,7 @@ void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_
                     AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
   require(n_outer >= 1 && n_outer <= 65535 && batch >= 1 && batch <= 65535,
           "fft: too many lines in the outer dimension");
+  if (fft_reg_engine_enabled() && (n == 64 || n == 128 || n == 256 || n == 512)) return;  // no tile choice
   autotune(axis_key(n_outer, so, n, sp, ni, forward, mode, batch), axis_candidates(n), axis_default(n),
            [&](int c) { axis_cols(c, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); }, s);
 }
@@ -712,6 +714,7 @@ void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_
 
 void rows_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, cudaStream_t s) {
   require(nx >= 2 && nx % 2 == 0, "rfft: row length must be even");
+  if (rows_r2c_reg(x, e, rows, nx, clamp, s)) return;
   switch (nx / 2) {
 #define QHK_R2C(M)                                                \
   case M:                                                         \
@@ -733,6 +736,7 @@ void rows_r2c(const float* x, float2* e, std::size_t rows, int nx, bool clamp, c
 void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
               cudaStream_t s) {
   require(nx >= 2 && nx % 2 == 0, "irfft: row length must be even");
+  if (rows_c2r_reg(e, x, rows, nx, mode, nm2, inv_k02, s)) return;
   switch (nx / 2) {
 #define QHK_C2R(M)                                                          \
   case M:                                                                   \
@@ -753,6 +757,7 @@ void rows_c2r(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode,
 
 void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s) {
   require(nx >= 2 && nx % 2 == 0, "rfft: row length must be even");
+  if (rows_c2r_r2c_reg(e, rows, nx, s)) return;
   switch (nx / 2) {
 #define QHK_C2R_R2C(M)                                    \
   case M:                                                 \
@@ -774,6 +779,7 @@ void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s) {
 void rows_tv_final_r2c(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda, float momentum,
                        float* xprev, float2* e, cudaStream_t s) {
   require(nx >= 2 && nx % 2 == 0 && nz >= 1 && ny >= 1, "rfft: row length must be even");
+  if (rows_tv_final_r2c_reg(b, p, nz, ny, nx, lambda, momentum, xprev, e, s)) return;
   switch (nx / 2) {
 #define QHK_TVF_R2C(M)                                                                           \
   case M:                                                                                        \

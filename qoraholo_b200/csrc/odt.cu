@@ -56,28 +56,31 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 
 // Half-spectrum mapping, one warp per lateral column (ky, kx) of the half spectrum (kx <= n/2), kMapCols
 // columns per block, consecutive in the flattened (ky, kx) order, so that the block's output rows are
-// contiguous. Lane l owns the K axial bins [l K, l K + K) of its warp's column (32 K >= nz). The
-// column's Ewald targets are computed once each: lane l takes illuminations l, l + 32, ..., for the
-// column itself (side P) and for its mirror (-ky, -kx) (side N, whose bin kz lands on -kz here). They
-// are then broadcast with warp shuffles in illumination order, and the owner of the target bin adds
-// the mapped value to its registers -- every bin's sums in the CPU's order, no atomics. The block
-// stages a, hits of its columns in shared memory and writes them out coalesced.
-constexpr int kMapCols = 16;  // columns (warps) per block
-
-template <int K>
-__device__ __forceinline__ void accumulate_k(float (&re)[K], float (&im)[K], float (&w)[K], int slot, float vr,
-                                             float vi) {
-#pragma unroll
-  for (int i = 0; i < K; ++i) {
-    if (slot == i) {
-      re[i] = __fadd_rn(re[i], vr);
-      im[i] = __fadd_rn(im[i], vi);
-      w[i] = __fadd_rn(w[i], 1.0f);
+// contiguous. Each warp accumulates its column in shared memory: the sums and hit counts of side P (the
+// column itself) and side N (its mirror (-ky, -kx), whose bin kz lands on -kz here). Lane l computes the
+// targets of illuminations l, l + 32, ... once each and adds its own value; lanes of one round that hit
+// the same bin (found with __match_any_sync) add one after another in lane order, i.e. in illumination
+// order, so every bin's sum has the CPU's order and no atomics are used. Then the lanes turn the
+// column into half data a = (P + conj N) / 2 and hits, and the block writes its columns out coalesced.
+// Adds `value` to acc[bin] and one to cnt[bin] for every lane with `bin` >= 0, lanes with equal bins in
+// increasing lane order.
+__device__ __forceinline__ void ordered_add(float2* acc, std::uint16_t* cnt, int bin, float2 value, int lane) {
+  unsigned pend = __ballot_sync(0xffffffffu, bin >= 0);
+  const unsigned same = __match_any_sync(0xffffffffu, bin);
+  while (pend) {
+    const unsigned mine = same & pend;
+    const bool leader = ((pend >> lane) & 1u) && (__ffs(mine) - 1 == lane);
+    if (leader) {
+      const float2 a = acc[bin];
+      acc[bin] = make_float2(__fadd_rn(a.x, value.x), __fadd_rn(a.y, value.y));
+      cnt[bin] = static_cast<std::uint16_t>(cnt[bin] + 1);
     }
+    __syncwarp();
+    pend &= ~__ballot_sync(0xffffffffu, leader);
   }
 }
 
-template <int K>
+template <int kMapCols>  // columns (warps) per block
 __global__ void __launch_bounds__(32 * kMapCols)
     k_map_half(const float2* __restrict__ spectra, const float4* __restrict__ illum, int count, Grid g,
                float2* __restrict__ a, std::uint8_t* __restrict__ hits, unsigned long long* __restrict__ filled) {
@@ -92,74 +95,61 @@ __global__ void __launch_bounds__(32 * kMapCols)
     hits += v * nz * hplane;
     filled += v;
   }
-  auto* a_tile = reinterpret_cast<float2*>(map_smem);                    // [nz][kMapCols]
-  auto* h_tile = reinterpret_cast<std::uint8_t*>(a_tile + nz * kMapCols);  // [nz][kMapCols]
   const int lane = static_cast<int>(threadIdx.x) & 31;
   const int warp = static_cast<int>(threadIdx.x) >> 5;
+  // Shared memory: the block's output tile a_tile[nz][kMapCols], then per warp the column sums accP[nz],
+  // accN[nz]; then per warp the counts cntP[nz], cntN[nz]; then the tile's hits h_tile[nz][kMapCols].
+  auto* a_tile = reinterpret_cast<float2*>(map_smem);
+  float2* accP = a_tile + nz * kMapCols + 2 * warp * nz;
+  float2* accN = accP + nz;
+  auto* cnt0 = reinterpret_cast<std::uint16_t*>(a_tile + nz * kMapCols + 2 * kMapCols * nz);
+  std::uint16_t* cntP = cnt0 + 2 * warp * nz;
+  std::uint16_t* cntN = cntP + nz;
+  auto* h_tile = reinterpret_cast<std::uint8_t*>(cnt0 + 2 * kMapCols * nz);
   const std::size_t col0 = static_cast<std::size_t>(blockIdx.x) * kMapCols;
   const std::size_t col = col0 + warp;
   unsigned long long cnt = 0;
-  if (col < hplane) {
+  if (col < hplane) {  // warp-uniform
     const int ky = static_cast<int>(col / h);
     const int kx = static_cast<int>(col - static_cast<std::size_t>(ky) * h);
     const int myk = negative_bin(ky, n);
     const int mkx = negative_bin(kx, n);
-    const int k0 = lane * K;
-    float pre[K] = {}, pim[K] = {}, pw[K] = {};
-    float nre[K] = {}, nim[K] = {}, nw[K] = {};
+    for (int k = lane; k < nz; k += 32) {
+      accP[k] = make_float2(0.0f, 0.0f);
+      accN[k] = make_float2(0.0f, 0.0f);
+      cntP[k] = 0;
+      cntN[k] = 0;
+    }
+    __syncwarp();
     for (int base = 0; base < count; base += 32) {
       const int ai = base + lane;
-      int kp = -1, kn = -1;  // target bins of side P (own column) and N (mirror, already negated)
-      float pr = 0.0f, pi = 0.0f, qr = 0.0f, qi = 0.0f;
+      int kp = -1, kn = -1;  // target bins of side P and side N (already negated), -1: none
+      float2 vp = make_float2(0.0f, 0.0f), vn = make_float2(0.0f, 0.0f);
       if (ai < count) {
         const float4 il = __ldg(illum + ai);
         int kz;
         float nuz;
         if (ewald_target(g, ky, kx, il.x, il.y, il.z, kz, nuz)) {
-          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(ky) * n + kx], pr, pi);
+          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(ky) * n + kx], vp.x, vp.y);
           kp = kz;
         }
         if (ewald_target(g, myk, mkx, il.x, il.y, il.z, kz, nuz)) {
-          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(myk) * n + mkx], qr, qi);
+          mapped(g, nuz, kz, spectra[ai * plane + static_cast<std::size_t>(myk) * n + mkx], vn.x, vn.y);
           kn = negative_bin(kz, nz);
         }
       }
-      const unsigned has_p = __ballot_sync(0xffffffffu, kp >= 0);
-      const unsigned has_n = __ballot_sync(0xffffffffu, kn >= 0);
-      const int last = min(32, count - base);
-      for (int src = 0; src < last; ++src) {  // illumination base + src, in order
-        if ((has_p >> src) & 1u) {
-          const int kz = __shfl_sync(0xffffffffu, kp, src);
-          const float vr = __shfl_sync(0xffffffffu, pr, src);
-          const float vi = __shfl_sync(0xffffffffu, pi, src);
-          if (kz >= k0 && kz < k0 + K) accumulate_k<K>(pre, pim, pw, kz - k0, vr, vi);
-        }
-        if ((has_n >> src) & 1u) {
-          const int kz = __shfl_sync(0xffffffffu, kn, src);
-          const float vr = __shfl_sync(0xffffffffu, qr, src);
-          const float vi = __shfl_sync(0xffffffffu, qi, src);
-          if (kz >= k0 && kz < k0 + K) accumulate_k<K>(nre, nim, nw, kz - k0, vr, vi);
-        }
-      }
+      ordered_add(accP, cntP, kp, vp, lane);
+      ordered_add(accN, cntN, kn, vn, lane);
     }
     const bool mirror_is_full_only = kx >= 1 && kx <= n / 2 - 1;
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      const int kz = k0 + i;
-      if (kz < nz) {
-        float pr = pre[i], pi = pim[i], mr = nre[i], mi = nim[i];
-        if (pw[i] > 0.0f) {
-          pr = __fdiv_rn(pr, pw[i]);
-          pi = __fdiv_rn(pi, pw[i]);
-        }
-        if (nw[i] > 0.0f) {
-          mr = __fdiv_rn(mr, nw[i]);
-          mi = __fdiv_rn(mi, nw[i]);
-        }
-        a_tile[kz * kMapCols + warp] = make_float2(__fmul_rn(0.5f, __fadd_rn(pr, mr)), __fmul_rn(0.5f, __fsub_rn(pi, mi)));
-        h_tile[kz * kMapCols + warp] = static_cast<std::uint8_t>((pw[i] > 0.0f) + (nw[i] > 0.0f));
-        cnt += (pw[i] > 0.0f) + (mirror_is_full_only && nw[i] > 0.0f);
-      }
+    for (int kz = lane; kz < nz; kz += 32) {
+      float2 p = accP[kz], m = accN[kz];
+      const float pw = static_cast<float>(cntP[kz]), nw = static_cast<float>(cntN[kz]);
+      if (pw > 0.0f) p = make_float2(__fdiv_rn(p.x, pw), __fdiv_rn(p.y, pw));
+      if (nw > 0.0f) m = make_float2(__fdiv_rn(m.x, nw), __fdiv_rn(m.y, nw));
+      a_tile[kz * kMapCols + warp] = make_float2(__fmul_rn(0.5f, __fadd_rn(p.x, m.x)), __fmul_rn(0.5f, __fsub_rn(p.y, m.y)));
+      h_tile[kz * kMapCols + warp] = static_cast<std::uint8_t>((pw > 0.0f) + (nw > 0.0f));
+      cnt += (pw > 0.0f) + (mirror_is_full_only && nw > 0.0f);
     }
   }
   __syncthreads();
@@ -239,28 +229,22 @@ __global__ void __launch_bounds__(256)
 void map_half(const float2* spectra, const float4* illum, int count, const Grid& g, float2* a, std::uint8_t* hits,
               unsigned long long* filled, cudaStream_t s, int batch) {
   require(batch >= 1 && batch <= 65535, "ewald mapping: invalid batch");
-  require(g.nz >= 1 && g.nz <= 32 * 16, "ewald mapping: nz must be at most 512");
+  require(g.nz >= 1 && g.nz <= 1024, "ewald mapping: nz must be at most 1024");
+  require(count <= 65535, "ewald mapping: at most 65535 illuminations");
   const std::size_t columns = static_cast<std::size_t>(g.n) * (g.n / 2 + 1);
-  const dim3 grid(blocks_for(columns, kMapCols), batch);
-  const std::size_t smem = static_cast<std::size_t>(g.nz) * kMapCols * (sizeof(float2) + 1);
-  const int per_lane = (g.nz + 31) / 32;
-  const auto launch = [&](auto kernel) {
-    if (smem > 48 * 1024) {
-      check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-            "cudaFuncSetAttribute");
-    }
-    kernel<<<grid, 32 * kMapCols, smem, s>>>(spectra, illum, count, g, a, hits, filled);
+  const auto launch = [&](auto kernel, int cols) {
+    // Output tile, per-warp column sums and counts, tile hits, as laid out in k_map_half.
+    const std::size_t smem = static_cast<std::size_t>(g.nz) * cols * (3 * sizeof(float2) + 2 * sizeof(std::uint16_t) + 1);
+    ensure_smem(kernel);
+    kernel<<<dim3(blocks_for(columns, cols), batch), 32 * cols, smem, s>>>(spectra, illum, count, g, a, hits, filled);
   };
-  if (per_lane <= 2) {
-    launch(k_map_half<2>);
-  } else if (per_lane <= 4) {
-    launch(k_map_half<4>);
-  } else if (per_lane <= 8) {
-    launch(k_map_half<8>);
-  } else if (per_lane <= 12) {
-    launch(k_map_half<12>);
+  // About 59 KB of shared memory per block: three blocks per SM.
+  if (g.nz <= 256) {
+    launch(k_map_half<8>, 8);
+  } else if (g.nz <= 512) {
+    launch(k_map_half<4>, 4);
   } else {
-    launch(k_map_half<16>);
+    launch(k_map_half<2>, 2);
   }
   check_launch("ewald mapping");
 }

@@ -38,7 +38,8 @@ def test_fft2d_matches_numpy(cuda, qhk, n):
     assert rel_err(host(t), a) < 2e-6
 
 
-@pytest.mark.parametrize("shape", [(4, 6, 8), (16, 12, 20), (32, 32, 32), (34, 32, 32), (62, 60, 60), (24, 48, 62)])
+@pytest.mark.parametrize("shape", [(4, 6, 8), (16, 12, 20), (32, 32, 32), (34, 32, 32), (62, 60, 60), (24, 48, 62),
+                                   (64, 64, 64), (128, 256, 64), (256, 128, 32), (16, 512, 8)])
 def test_rfft3_and_irfft3_match_numpy(cuda, qhk, shape):
     nz, ny, nx = shape
     rng = np.random.default_rng(sum(shape))
