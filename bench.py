@@ -939,7 +939,9 @@ def kernel_case(name, reps, tv_form=0):
     """Small standalone launches of one kernel family for profiling (no JSON line): `c2` runs the C2
     reconstruction (the bench workload, device-resident) `reps` times after a warm-up run, each inside
     the NVTX range "c2_step"; `refcuda` the reference's CUDA Pipeline::run on the same workload (`reps`
-    runs); `unwrapbatch` the C4 batch of 512 uneven unwraps (`reps` runs, no graph); `fgp` runs the
+    runs); `unwrapbatch` the C4 batch of 512 uneven unwraps (`reps` runs, no graph); `bpmstep` one BPM
+    gradient (forward + backward, 256^2 x 128 slices, 49 views, checkpoint every 16 slices) after a warm-up,
+    inside the NVTX range "bpm_step"; `fgp` runs the
     TV proximal step at 256^3 on a 12-volume workspace (10 FGP steps in the tuned form + final primal
     per rep); `fft` a 256^3 rfft3 + irfft3
     per rep; `kspace` a 256^3 GP-4 solve from 49 random 256^2 fields per rep (the k-space step's
@@ -986,6 +988,24 @@ def kernel_case(name, reps, tv_form=0):
             torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         pipe.check_waits(stream)
+    elif name == "bpmstep":
+        import qoraholo_b200 as qh
+        from qoraholo_b200.autograd import BpmModel
+
+        geom = qh.Geometry(wavelength=WAVELENGTH, n_medium=N_MEDIUM, na=NA, pixel=BPM_PIXEL)
+        illum = circular_scan(BPM_VIEWS, 0.9)
+        model = BpmModel(BPM_NZ, BPM_N, illum, geom, checkpoint_every=BPM_EVERY)
+        x = torch.full((BPM_NZ, BPM_N, BPM_N), N_MEDIUM + 0.01, device="cuda", requires_grad=True)
+        g = torch.ones((BPM_VIEWS, BPM_N, BPM_N), dtype=torch.complex64, device="cuda")
+        model(x).backward(g)  # warm (plans, checkpoints)
+        torch.cuda.synchronize()
+        for _ in range(reps):  # ncu --nvtx --nvtx-include "bpm_step/" captures one gradient
+            torch.cuda.nvtx.range_push("bpm_step")
+            x.grad = None
+            model(x).backward(g)
+            torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        model.plan.close()
     elif name == "unwrapbatch":
         rng = np.random.default_rng(5)
         shapes = [(int(v), int(v)) for v in rng.choice(C4_SIDES, C4_UNWRAP)]
@@ -1039,7 +1059,7 @@ def kernel_case(name, reps, tv_form=0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel-case", choices=["fgp", "fft", "kspace", "pipeline", "c2", "refcuda", "unwrapbatch",
-                                              "serve", "bpm", "c4"],
+                                              "bpmstep", "serve", "bpm", "c4"],
                     default=None,
                     help="run only a small profiling case and exit")
     ap.add_argument("--reps", type=int, default=3)

@@ -137,6 +137,17 @@ int qhk_pinned_free(void* ptr);
  * the counter without waiting for work queued on other streams. */
 int qhk_wait_timeouts(uint64_t* count);
 
+/* Bounds checks of the debug build (compiled with QHK_DEBUG: `python qoraholo_b200/_build.py --debug`
+ * writes qoraholo_b200/debug/libqhk.so, the same ABI). Its tile loaders, work-queue items, line indices
+ * and shared-memory layouts check themselves and skip an access that would leave its buffer, recording
+ * it instead of faulting; a skipped tile load also ends its bounded wait (QHK_TIMEOUT). No counterpart
+ * in the reference, which has no device checks. qhk_debug_enabled: 1 in the debug build, else 0.
+ * qhk_debug_violations: failed checks since the last reset (reset != 0 clears them), after waiting
+ * for the device; when there were some, qhk_last_error names the source line of a first one. Always 0
+ * in the release build. */
+int qhk_debug_enabled(void);
+int qhk_debug_violations(uint64_t* count, int reset);
+
 /* Number of kernels this library has launched since it was loaded (for launch accounting). */
 uint64_t qhk_kernel_launches(void);
 

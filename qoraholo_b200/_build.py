@@ -5,8 +5,13 @@
   qoraholo_b200/_core*.so        pybind11 bindings with the reference's Python signatures
 
 nvcc cross-compiles without a GPU. Objects go to qoraholo_b200/_build/; a library is rebuilt
-when any of its sources or headers is newer. Usage: python qoraholo_b200/_build.py [--force]
+when any of its sources or headers is newer. Usage: python qoraholo_b200/_build.py [--force] [--debug]
 (run as a script: importing the package itself needs the built extension).
+
+--debug also builds qoraholo_b200/debug/libqhk.so, the same ABI with the device bounds checks of
+csrc/debug.cuh compiled in (QHK_DEBUG): the units that include debug.cuh are compiled again into
+qoraholo_b200/_build_debug/, the others are linked from the release objects. Load it in place of the
+release library with QHK_LIBRARY=qoraholo_b200/debug/libqhk.so (qoraholo_b200.capi).
 """
 
 from __future__ import annotations
@@ -15,6 +20,7 @@ import os
 import subprocess
 import sys
 import sysconfig
+import time
 from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
@@ -31,6 +37,8 @@ CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", f"-I{INCLUDE}", 
 
 LIB_QHK = PKG / "libqhk.so"
 LIB_HOST = PKG / "libqoraholo.so"
+BUILD_DEBUG = PKG / "_build_debug"
+LIB_QHK_DEBUG = PKG / "debug" / "libqhk.so"
 
 
 def _newest(paths):
@@ -60,9 +68,22 @@ def _run(cmd):
     return r
 
 
+def _compile(cmd):
+    """One compile job; an object whose source or headers changed while it compiled is dated back to the
+    start of the compile, so that the next build compiles it again."""
+    t0 = time.time()
+    _run(cmd)
+    obj = Path(cmd[cmd.index("-o") + 1])
+    dep = obj.with_suffix(".d")
+    if dep.exists():
+        files = [Path(t) for t in dep.read_text().replace("\\\n", " ").partition(":")[2].split()]
+        if any(f.exists() and f.stat().st_mtime > t0 for f in files):
+            os.utime(obj, (t0 - 1, t0 - 1))
+
+
 def _compile_many(jobs):
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
-        list(ex.map(_run, jobs))
+        list(ex.map(_compile, jobs))
 
 
 def build_qhk(force=False) -> Path:
@@ -78,6 +99,33 @@ def build_qhk(force=False) -> Path:
     if force or jobs or not LIB_QHK.exists() or LIB_QHK.stat().st_mtime < _newest(objs):
         _run([NVCC, *ARCH, "-shared", "-o", str(LIB_QHK), *map(str, objs)])
     return LIB_QHK
+
+
+def _uses_debug_checks(obj: Path) -> bool:
+    """True when the release object's dependency list names debug.cuh (its unit has bounds checks)."""
+    dep = obj.with_suffix(".d")
+    return dep.exists() and "debug.cuh" in dep.read_text()
+
+
+def build_qhk_debug(force=False) -> Path:
+    """The debug library: the release objects, with the units that include debug.cuh recompiled with
+    QHK_DEBUG."""
+    build_qhk(False)
+    BUILD_DEBUG.mkdir(exist_ok=True)
+    LIB_QHK_DEBUG.parent.mkdir(exist_ok=True)
+    jobs, objs = [], []
+    for src in sorted(CSRC.glob("*.cu")):
+        obj = BUILD / (src.stem + ".o")
+        if _uses_debug_checks(obj):
+            obj = BUILD_DEBUG / (src.stem + ".o")
+            if force or _stale(obj, src):
+                jobs.append([NVCC, *NVCC_FLAGS, "-DQHK_DEBUG", "-MD", "-MF", str(obj.with_suffix(".d")), "-c",
+                             str(src), "-o", str(obj)])
+        objs.append(obj)
+    _compile_many(jobs)
+    if force or jobs or not LIB_QHK_DEBUG.exists() or LIB_QHK_DEBUG.stat().st_mtime < _newest(objs):
+        _run([NVCC, *ARCH, "-shared", "-o", str(LIB_QHK_DEBUG), *map(str, objs)])
+    return LIB_QHK_DEBUG
 
 
 def build_host(force=False) -> Path | None:
@@ -113,12 +161,14 @@ def build_bindings(force=False) -> Path | None:
     return out
 
 
-def build(force=False):
+def build(force=False, debug=False):
     build_qhk(force)
     build_host(force)
     build_bindings(force)
+    if debug:
+        build_qhk_debug(force)
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv)
-    print("built", LIB_QHK)
+    build(force="--force" in sys.argv, debug="--debug" in sys.argv)
+    print("built", LIB_QHK, *([LIB_QHK_DEBUG] if "--debug" in sys.argv else []))

@@ -9,11 +9,13 @@ library has not been built (``python qoraholo_b200/_build.py``); there is no fal
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "libqhk.so"
+# QHK_LIBRARY selects another build of the same ABI, e.g. the debug build qoraholo_b200/debug/libqhk.so.
+LIB_PATH = Path(os.environ.get("QHK_LIBRARY") or Path(__file__).resolve().parent / "libqhk.so")
 
 OK, INVALID_ARGUMENT, CUDA_ERROR, LOGIC_ERROR, OUT_OF_MEMORY, TIMEOUT, INTERNAL = range(7)
 SOLVERS = {"gp": 0, "tv": 1}
@@ -86,6 +88,8 @@ _PROTOS = {
     "qhk_tv_prox_device": (_I, [_VP, _VP, _VP, _I, _I, _I, _F, _I, _VP]),
     "qhk_kernel_launches": (C.c_uint64, []),
     "qhk_wait_timeouts": (_I, [C.POINTER(C.c_uint64)]),
+    "qhk_debug_enabled": (_I, []),
+    "qhk_debug_violations": (_I, [C.POINTER(C.c_uint64), _I]),
     "qhk_pinned_alloc": (_I, [C.c_size_t, C.POINTER(_VP)]),
     "qhk_pinned_free": (_I, [_VP]),
     "qhk_tv_prox_workspace": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _F, _I, _VP]),
@@ -275,6 +279,20 @@ def wait_timeouts() -> int:
     n = C.c_uint64()
     check(lib().qhk_wait_timeouts(C.byref(n)))
     return n.value
+
+
+def debug_enabled() -> bool:
+    """True when the loaded library is the debug build (device bounds checks compiled in)."""
+    return bool(lib().qhk_debug_enabled())
+
+
+def debug_violations(reset: bool = False) -> tuple[int, str]:
+    """Failed device bounds checks of the debug build since the last reset, and where the first one
+    was (qhk_debug_violations); (0, "") in the release build."""
+    n = C.c_uint64()
+    check(lib().qhk_debug_violations(C.byref(n), int(bool(reset))))
+    where = lib().qhk_last_error().decode() if n.value else ""
+    return n.value, where
 
 
 def autotune_enable(enabled: bool = True):

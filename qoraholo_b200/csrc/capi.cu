@@ -15,6 +15,7 @@
 
 #include "autotune.hpp"
 #include "bpm.hpp"
+#include "debug.cuh"
 #include "field.hpp"
 #include "odt.hpp"
 #include "pipeline.hpp"
@@ -285,6 +286,18 @@ int qhk_wait_timeouts(uint64_t* count) {
   return guard([&] {
     qhk::require(count != nullptr, "wait_timeouts: null argument");
     *count = qhk::tv_wait_timeouts();
+  });
+}
+
+int qhk_debug_enabled(void) { return qhk::debug::enabled() ? 1 : 0; }
+
+int qhk_debug_violations(uint64_t* count, int reset) {
+  return guard([&] {
+    qhk::require(count != nullptr, "debug_violations: null argument");
+    if (qhk::debug::enabled()) qhk::check(cudaDeviceSynchronize(), "debug_violations");
+    std::string first;
+    *count = qhk::debug::violations(reset != 0, &first);
+    g_last_error = first.empty() ? std::string() : "first failed bounds check at " + first;
   });
 }
 

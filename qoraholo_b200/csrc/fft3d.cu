@@ -703,7 +703,7 @@ void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_
                     AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
   require(n_outer >= 1 && n_outer <= 65535 && batch >= 1 && batch <= 65535,
           "fft: too many lines in the outer dimension");
-  if (fft_reg_engine_enabled() && (n == 64 || n == 128 || n == 256 || n == 512)) return;  // no tile choice
+  if (fft_reg_engine_enabled() && (n == 64 || n == 128 || n == 192 || n == 256 || n == 512)) return;  // no tile choice
   autotune(axis_key(n_outer, so, n, sp, ni, forward, mode, batch), axis_candidates(n), axis_default(n),
            [&](int c) { axis_cols(c, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); }, s);
 }
@@ -779,7 +779,6 @@ void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s) {
 void rows_tv_final_r2c(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda, float momentum,
                        float* xprev, float2* e, cudaStream_t s) {
   require(nx >= 2 && nx % 2 == 0 && nz >= 1 && ny >= 1, "rfft: row length must be even");
-  if (rows_tv_final_r2c_reg(b, p, nz, ny, nx, lambda, momentum, xprev, e, s)) return;
   switch (nx / 2) {
 #define QHK_TVF_R2C(M)                                                                           \
   case M:                                                                                        \

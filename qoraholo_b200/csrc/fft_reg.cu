@@ -1,5 +1,5 @@
 // FFT axis passes on the register-resident engine (fft_reg.cuh) for the lengths it covers: 64, 128,
-// 256 and 512. A CTA takes COLS lines (consecutive inner columns) of one outer slice, T threads per
+// 192, 256 and 512. A CTA takes COLS lines (consecutive inner columns) of one outer slice, T threads per
 // line holding V = n / T values each; loads and stores are rows of COLS consecutive complex values.
 // The modes are those of the staged kernels (fft3d.cu k_axis): plain transform with a scale, the
 // k-space restore between a forward and an inverse transform (half-spectrum data or a mask), and an
@@ -26,6 +26,8 @@ __global__ void __launch_bounds__(kRegThreads)
   constexpr int kFrom = static_cast<int>(AxisMode::from_data);
   constexpr int kHalf = static_cast<int>(AxisMode::restore_half);
   constexpr int kMask = static_cast<int>(AxisMode::restore_mask);
+  constexpr std::size_t kSmem = (static_cast<std::size_t>(T) * V * COLS + (Mode == kHalf || Mode == kMask ? V * kRegThreads : 0)) * sizeof(float2);
+  if (!QHK_CHECK(kSmem <= debug::dynamic_smem_bytes() && blockDim.x == kRegThreads)) return;  // block-uniform
   const int c = static_cast<int>(threadIdx.x) % COLS;
   const int t = static_cast<int>(threadIdx.x) / COLS;
   const int col = static_cast<int>(blockIdx.x) * COLS + c;
@@ -125,10 +127,12 @@ void axis_reg_mode(float2* data, int n_outer, std::size_t so, std::size_t sp, in
 
 // ---- real rows <-> half spectra ---------------------------------------------------------------------
 // Rows of nx = 2M real values as M complex values (the pairs 2m, 2m + 1), a length-M transform on the
-// register engine, and the split / merge of the half spectrum with the same formulas as the staged row
+// register engine (the R2C, C2R and GP-step-boundary passes; the FISTA-TV final-primal pass stays on the
+// staged engine, whose flat loads of its seven operands measured faster), and the split / merge of the half spectrum with the same formulas as the staged row
 // kernels (fft3d.cu k_rows_*): e[k] = (Z[k] + conj Z[M-k]) / 2 + W_nx^k (Z[k] - conj Z[M-k]) / (2i),
 // k = 0..M. A CTA takes R = 256 / T rows, T threads per row (consecutive threads on consecutive
-// positions of a row). The exchange buffer has strides A, B of the row-tile layout (conflict-free in
+// positions of a row), for half lengths 64, 128, 192 and 256. The exchange buffer has strides A, B of
+// the row-tile layout (conflict-free in
 // both exchange phases); the split stages Z in natural order, rows kRowPitch(M) apart.
 
 using regfft::RowTile;
@@ -196,6 +200,7 @@ template <bool Clamp, int T, int V>
 __global__ void __launch_bounds__(kRegThreads)
     k_rows_r2c_reg(const float* __restrict__ x, float2* __restrict__ e, std::size_t rows,
                    const float2* __restrict__ tw, const float2* __restrict__ twn) {
+  if (!QHK_CHECK(row_smem<T, V>() <= debug::dynamic_smem_bytes() && blockDim.x == kRegThreads)) return;
   using Tile = RowTile<T>;
   constexpr int M = T * V, h = M + 1, P = row_pitch<M>();
   extern __shared__ float2 sm[];
@@ -221,6 +226,7 @@ template <int Mode, int T, int V>
 __global__ void __launch_bounds__(kRegThreads)
     k_rows_c2r_reg(const float2* __restrict__ e, float* __restrict__ x, std::size_t rows, const float2* __restrict__ tw,
                    const float2* __restrict__ twn, float nm2, float inv_k02) {
+  if (!QHK_CHECK(row_smem<T, V>() <= debug::dynamic_smem_bytes() && blockDim.x == kRegThreads)) return;
   using Tile = RowTile<T>;
   constexpr int M = T * V, h = M + 1;
   extern __shared__ float2 sm[];
@@ -248,6 +254,7 @@ template <int T, int V>
 __global__ void __launch_bounds__(kRegThreads)
     k_rows_c2r_r2c_reg(float2* __restrict__ e, std::size_t rows, const float2* __restrict__ tw,
                        const float2* __restrict__ twn) {
+  if (!QHK_CHECK(row_smem<T, V>() <= debug::dynamic_smem_bytes() && blockDim.x == kRegThreads)) return;
   using Tile = RowTile<T>;
   constexpr int M = T * V, h = M + 1, P = row_pitch<M>();
   extern __shared__ float2 sm[];
@@ -260,68 +267,6 @@ __global__ void __launch_bounds__(kRegThreads)
 #pragma unroll
   for (int j = 0; j < V; ++j) v[j] = live ? make_float2(fmaxf(v[j].x, 0.0f), fmaxf(v[j].y, 0.0f)) : make_float2(0.0f, 0.0f);
   __syncthreads();
-  regfft::line_fft<T, V, true>(v, t, sm + r, Tile::A, Tile::B, tw);
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < V; ++j) sm[r * P + t + T * j] = v[j];
-  __syncthreads();
-  if (live) split_store<T, V>(sm + r * P, t, twn, e + row * h);
-}
-
-// The end of one FISTA-TV iteration and the start of the next on rows (as fft3d.cu
-// k_rows_tv_final_r2c: the final primal x = max(b - lambda div p, 0) with the same additions in the
-// same order, y = x + m (x - xprev), xprev <- x, then the R2C of y's rows), y never written.
-template <int T, int V>
-__global__ void __launch_bounds__(kRegThreads)
-    k_rows_tv_final_r2c_reg(const float* __restrict__ b, const float* __restrict__ pz, const float* __restrict__ py,
-                            const float* __restrict__ px, int nz, int ny, float lambda, float momentum,
-                            float* __restrict__ xprev, float2* __restrict__ e, std::size_t rows,
-                            const float2* __restrict__ tw, const float2* __restrict__ twn) {
-  using Tile = RowTile<T>;
-  constexpr int M = T * V, h = M + 1, P = row_pitch<M>(), nx = 2 * M;
-  extern __shared__ float2 sm[];
-  const int t = static_cast<int>(threadIdx.x) % T, r = static_cast<int>(threadIdx.x) / T;
-  const std::size_t row = static_cast<std::size_t>(blockIdx.x) * Tile::R + r;
-  const bool live = row < rows;
-  const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
-  const int y = live ? static_cast<int>(row % static_cast<std::size_t>(ny)) : 0;
-  const int z = live ? static_cast<int>(row / static_cast<std::size_t>(ny)) : 0;
-  float2 v[V];
-#pragma unroll
-  for (int j = 0; j < V; ++j) {
-    const int m = t + T * j;
-    v[j] = make_float2(0.0f, 0.0f);
-    if (live) {
-      const std::size_t i0 = row * nx + 2 * m;
-      const float2 bv = *reinterpret_cast<const float2*>(b + i0);
-      const float2 cz = *reinterpret_cast<const float2*>(pz + i0);
-      const float2 cy = *reinterpret_cast<const float2*>(py + i0);
-      const float2 cx = *reinterpret_cast<const float2*>(px + i0);
-      const float2 pv = *reinterpret_cast<const float2*>(xprev + i0);
-      float2 bz = make_float2(0.0f, 0.0f), by = make_float2(0.0f, 0.0f);
-      if (z > 0) bz = *reinterpret_cast<const float2*>(pz + i0 - nxy);
-      if (y > 0) by = *reinterpret_cast<const float2*>(py + i0 - nx);
-      const float left = m > 0 ? px[i0 - 1] : 0.0f;
-      const float bb[2] = {bv.x, bv.y}, czz[2] = {cz.x, cz.y}, cyy[2] = {cy.x, cy.y}, cxx[2] = {cx.x, cx.y};
-      const float bzz[2] = {bz.x, bz.y}, byy[2] = {by.x, by.y}, pvv[2] = {pv.x, pv.y};
-      float xv[2], yv[2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int xx = 2 * m + i;
-        float sdiv = 0.0f;
-        if (z < nz - 1) sdiv = __fadd_rn(sdiv, czz[i]);
-        if (z > 0) sdiv = __fsub_rn(sdiv, bzz[i]);
-        if (y < ny - 1) sdiv = __fadd_rn(sdiv, cyy[i]);
-        if (y > 0) sdiv = __fsub_rn(sdiv, byy[i]);
-        if (xx < nx - 1) sdiv = __fadd_rn(sdiv, cxx[i]);
-        if (xx > 0) sdiv = __fsub_rn(sdiv, i == 0 ? left : cxx[0]);
-        xv[i] = tv_primal(bb[i], lambda, sdiv);
-        yv[i] = __fadd_rn(xv[i], __fmul_rn(momentum, __fsub_rn(xv[i], pvv[i])));
-      }
-      *reinterpret_cast<float2*>(xprev + i0) = make_float2(xv[0], xv[1]);
-      v[j] = make_float2(yv[0], yv[1]);
-    }
-  }
   regfft::line_fft<T, V, true>(v, t, sm + r, Tile::A, Tile::B, tw);
   __syncthreads();
 #pragma unroll
@@ -343,6 +288,7 @@ bool with_row_shape(int M, F&& f) {
   switch (M) {
     case 64: f.template operator()<8, 8>(); return true;
     case 128: f.template operator()<8, 16>(); return true;
+    case 192: f.template operator()<8, 24>(); return true;
     case 256: f.template operator()<16, 16>(); return true;
     default: return false;
   }
@@ -395,19 +341,6 @@ bool rows_c2r_r2c_reg(float2* e, std::size_t rows, int nx, cudaStream_t s) {
   });
 }
 
-bool rows_tv_final_r2c_reg(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda,
-                           float momentum, float* xprev, float2* e, cudaStream_t s) {
-  return with_row_shape(nx / 2, [&]<int T, int V>() {
-    const std::size_t rows = static_cast<std::size_t>(nz) * ny;
-    const std::size_t smem = row_smem<T, V>();
-    const unsigned grid = static_cast<unsigned>((rows + RowTile<T>::R - 1) / RowTile<T>::R);
-    row_smem_attr(k_rows_tv_final_r2c_reg<T, V>, smem);
-    k_rows_tv_final_r2c_reg<T, V><<<grid, kRegThreads, smem, s>>>(b, p[0], p[1], p[2], nz, ny, lambda, momentum, xprev,
-                                                                   e, rows, fft_len(T * V).tw, fft_len(nx).tw);
-    check_launch("rows tv final r2c");
-  });
-}
-
 bool fft_reg_engine_enabled() {
   // QHK_FFT_ENGINE=staged keeps every pass on the staged shared-memory engine (for comparisons).
   static const bool on = [] {
@@ -423,6 +356,7 @@ bool axis_pass_reg(float2* data, int n_outer, std::size_t so, int n, std::size_t
   switch (n) {
     case 64: axis_reg_mode<8, 8>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
     case 128: axis_reg_mode<8, 16>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
+    case 192: axis_reg_mode<8, 24>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
     case 256: axis_reg_mode<16, 16>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
     case 512: axis_reg_mode<16, 32>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
     default: return false;

@@ -19,6 +19,7 @@
 
 #include <cuda_runtime.h>
 
+#include "debug.cuh"
 #include "fft_engine.cuh"
 
 namespace qhk {
@@ -40,18 +41,32 @@ __device__ __forceinline__ float w32_re(int q) {
 }
 __device__ __forceinline__ float w32_im(int q) { return -w32_re(q + 24); }  // -sin(a) = cos(a + 3 pi / 2)
 
-// v * W_R^m, W_R = e^{-2 pi i / R} (its conjugate for the inverse), R a divisor of 32. Called with R
-// and m constant after unrolling, so the factors 1, -i, -1, i cost no multiplication and the others
-// are immediates.
+// cos(2 pi q / 24), q = 0..23, from the quarter wave (0, 15, ..., 90 degrees) by symmetry.
+__device__ __forceinline__ float w24_re(int q) {
+  constexpr float c[7] = {1.0f, 0.96592582628906828675f, 0.86602540378443864676f, 0.70710678118654752440f,
+                          0.5f, 0.25881904510252076235f, 0.0f};
+  q %= 24;
+  if (q <= 6) return c[q];
+  if (q <= 12) return -c[12 - q];
+  if (q <= 18) return -c[q - 12];
+  return c[24 - q];
+}
+__device__ __forceinline__ float w24_im(int q) { return -w24_re(q + 18); }  // -sin(a) = cos(a + 3 pi / 2)
+
+// v * W_R^m, W_R = e^{-2 pi i / R} (its conjugate for the inverse), R a divisor of 32 or of 24. Called
+// with R and m constant after unrolling, so the factors 1, -i, -1, i cost no multiplication and the
+// others are immediates.
 template <bool Fwd>
 __device__ __forceinline__ float2 wmul(float2 v, int R, int m) {
-  const int q = (m % R) * (32 / R);  // the same root as a power of W_32
+  const bool of32 = 32 % R == 0;
+  const int L = of32 ? 32 : 24;
+  const int q = (m % R) * (L / R);  // the same root as a power of W_L
   if (q == 0) return v;
-  if (q == 16) return make_float2(-v.x, -v.y);
-  if (q == 8) return Fwd ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
-  if (q == 24) return Fwd ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
-  const float c = w32_re(q);
-  const float s = Fwd ? w32_im(q) : -w32_im(q);
+  if (2 * q == L) return make_float2(-v.x, -v.y);
+  if (4 * q == L) return Fwd ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+  if (4 * q == 3 * L) return Fwd ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+  const float c = of32 ? w32_re(q) : w24_re(q);
+  const float s = (Fwd ? 1.0f : -1.0f) * (of32 ? w32_im(q) : w24_im(q));
   return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
 }
 
@@ -86,14 +101,18 @@ __device__ __forceinline__ void dft(float2* v) {
   if constexpr (R == 1) {
   } else if constexpr (R == 2) {
     fftdev::dft2<Fwd>(v);
+  } else if constexpr (R == 3) {
+    fftdev::dft3<Fwd>(v);
   } else if constexpr (R == 4) {
     fftdev::dft4<Fwd>(v[0], v[1], v[2], v[3]);
   } else if constexpr (R == 8) {
     fftdev::dft8<Fwd>(v);
   } else if constexpr (R == 16) {
     dft_split<4, 4, Fwd>(v);
+  } else if constexpr (R == 24) {
+    dft_split<3, 8, Fwd>(v);
   } else {
-    static_assert(R == 32, "register DFT lengths: 1, 2, 4, 8, 16, 32");
+    static_assert(R == 32, "register DFT lengths: 1, 2, 3, 4, 8, 16, 24, 32");
     dft_split<4, 8, Fwd>(v);
   }
 }
@@ -102,17 +121,18 @@ __device__ __forceinline__ void dft(float2* v) {
 // entry and X[t + T j] on return. `xs` is this line's exchange buffer: element (k1, s) -- bin k1 of
 // thread s -- at xs[k1 * A + s * B]; lines of a tile interleave (the caller offsets `xs` per line), and
 // A, B are chosen per tile shape so that the writes (k1 fixed) and the reads (s fixed) of a warp fall
-// on distinct banks. `tw` is the length-N table e^{-2 pi i k / N}. All threads of the CTA call it
-// together: it synchronises before the exchange reads, and the caller must synchronise before writing
-// `xs` again.
+// on distinct banks. tw[i * tws] is e^{-2 pi i i / N}, i < N (tws = 2 reads a length-2N table, whose
+// even entries are exactly those of the length-N one). All threads of the CTA call it together: it
+// synchronises before the exchange reads, and the caller must synchronise before writing `xs` again.
 template <int T, int V, bool Fwd>
-__device__ __forceinline__ void line_fft(float2 (&v)[V], int t, float2* xs, int A, int B, const float2* tw) {
+__device__ __forceinline__ void line_fft(float2 (&v)[V], int t, float2* xs, int A, int B, const float2* tw,
+                                         int tws = 1) {
   static_assert(V % T == 0, "register FFT: V must be a multiple of T");
   constexpr int N = T * V;
   dft<V, Fwd>(v);
 #pragma unroll
   for (int k1 = 1; k1 < V; ++k1) {
-    const float2 w = __ldg(tw + (t * k1) % N);
+    const float2 w = __ldg(tw + ((t * k1) % N) * tws);
     v[k1] = cmul(v[k1], Fwd ? w : make_float2(w.x, -w.y));
   }
 #pragma unroll
@@ -132,15 +152,17 @@ __device__ __forceinline__ void line_fft(float2 (&v)[V], int t, float2* xs, int 
 }
 
 // Exchange strides for tiles of rows: 256 threads, T per row (consecutive threads on consecutive positions
-// of a row), R = 256 / T rows. With T = 8 a warp spans 8 threads of 4 rows, with T = 16 16 threads of
-// 2 rows; B (per thread) and A (per bin) are chosen so that t * B + r and t * A + r cover the 16
-// two-bank slots of a 64-bit access evenly, in the writes and in the reads of the exchange.
+// of a row), R = 256 / T rows. With T = 4 a warp spans 4 threads of 8 rows, with T = 8 8 threads of 4
+// rows, with T = 16 16 threads of 2 rows; B (per thread) and A (per bin) are chosen so that t * B + r and
+// t * A + r cover the 16 two-bank slots of a 64-bit access evenly, in the writes and in the reads of the
+// exchange, and so that B >= R and A >= T * B (the (bin, thread, row) elements do not overlap).
 template <int T>
 struct RowTile {
-  static_assert(T == 8 || T == 16, "row tiles of 8 or 16 threads per row");
+  static_assert(T == 4 || T == 8 || T == 16, "row tiles of 4, 8 or 16 threads per row");
   static constexpr int R = 256 / T;
-  static constexpr int B = T == 8 ? 36 : 17;
-  static constexpr int A = T == 8 ? 8 * 36 + 4 : 16 * 17 + 1;
+  static constexpr int B = T == 4 ? 72 : T == 8 ? 36 : 17;
+  static constexpr int A = T == 4 ? 4 * 72 + 8 : T == 8 ? 8 * 36 + 4 : 16 * 17 + 1;
+  static_assert(B >= R && A >= T * B, "row tile exchange elements overlap");
 };
 
 }  // namespace regfft

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "autotune.hpp"
+#include "debug.cuh"
 #include "odt.hpp"
 #include "nvtx.hpp"
 
@@ -62,6 +63,10 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // the same bin (found with __match_any_sync) add one after another in lane order, i.e. in illumination
 // order, so every bin's sum has the CPU's order and no atomics are used. Then the lanes turn the
 // column into half data a = (P + conj N) / 2 and hits, and the block writes its columns out coalesced.
+// Row pitch (float2 elements) of a column of the mapping's output tile: at least nz, congruent to 4
+// modulo 16, so that 8 consecutive columns at 4 consecutive bins fill the 16 two-bank slots twice.
+__host__ __device__ constexpr int map_pitch(int nz) { return (nz + 15) / 16 * 16 + 4; }
+
 // Adds `value` to acc[bin] and one to cnt[bin] for every lane with `bin` >= 0, lanes with equal bins in
 // increasing lane order.
 __device__ __forceinline__ void ordered_add(float2* acc, std::uint16_t* cnt, int bin, float2 value, int lane) {
@@ -97,12 +102,20 @@ __global__ void __launch_bounds__(32 * kMapCols)
   }
   const int lane = static_cast<int>(threadIdx.x) & 31;
   const int warp = static_cast<int>(threadIdx.x) >> 5;
-  // Shared memory: the block's output tile a_tile[nz][kMapCols], then per warp the column sums accP[nz],
-  // accN[nz]; then per warp the counts cntP[nz], cntN[nz]; then the tile's hits h_tile[nz][kMapCols].
+  // Shared memory: the block's output tile, one padded row per column (a_tile[col][pitch]: a warp writes
+  // its own row, and the read-out, consecutive threads on consecutive columns, falls on distinct banks),
+  // then per warp the column sums accP[nz], accN[nz]; then per warp the counts cntP[nz], cntN[nz]; then
+  // the tile's hits h_tile[col][pitch].
+  const int pitch = map_pitch(nz);
+  // The layout must fit the launch's shared memory (block-uniform).
+  if (!QHK_CHECK(static_cast<std::size_t>(kMapCols) * (pitch * (sizeof(float2) + 1) + 2 * nz * (sizeof(float2) + 2)) <=
+                 debug::dynamic_smem_bytes())) {
+    return;
+  }
   auto* a_tile = reinterpret_cast<float2*>(map_smem);
-  float2* accP = a_tile + nz * kMapCols + 2 * warp * nz;
+  float2* accP = a_tile + pitch * kMapCols + 2 * warp * nz;
   float2* accN = accP + nz;
-  auto* cnt0 = reinterpret_cast<std::uint16_t*>(a_tile + nz * kMapCols + 2 * kMapCols * nz);
+  auto* cnt0 = reinterpret_cast<std::uint16_t*>(a_tile + pitch * kMapCols + 2 * kMapCols * nz);
   std::uint16_t* cntP = cnt0 + 2 * warp * nz;
   std::uint16_t* cntN = cntP + nz;
   auto* h_tile = reinterpret_cast<std::uint8_t*>(cnt0 + 2 * kMapCols * nz);
@@ -138,6 +151,7 @@ __global__ void __launch_bounds__(32 * kMapCols)
           kn = negative_bin(kz, nz);
         }
       }
+      if (!QHK_CHECK(kp < nz && kn < nz)) kp = kn = -1;  // a target bin outside the column
       ordered_add(accP, cntP, kp, vp, lane);
       ordered_add(accN, cntN, kn, vn, lane);
     }
@@ -147,8 +161,8 @@ __global__ void __launch_bounds__(32 * kMapCols)
       const float pw = static_cast<float>(cntP[kz]), nw = static_cast<float>(cntN[kz]);
       if (pw > 0.0f) p = make_float2(__fdiv_rn(p.x, pw), __fdiv_rn(p.y, pw));
       if (nw > 0.0f) m = make_float2(__fdiv_rn(m.x, nw), __fdiv_rn(m.y, nw));
-      a_tile[kz * kMapCols + warp] = make_float2(__fmul_rn(0.5f, __fadd_rn(p.x, m.x)), __fmul_rn(0.5f, __fsub_rn(p.y, m.y)));
-      h_tile[kz * kMapCols + warp] = static_cast<std::uint8_t>((pw > 0.0f) + (nw > 0.0f));
+      a_tile[warp * pitch + kz] = make_float2(__fmul_rn(0.5f, __fadd_rn(p.x, m.x)), __fmul_rn(0.5f, __fsub_rn(p.y, m.y)));
+      h_tile[warp * pitch + kz] = static_cast<std::uint8_t>((pw > 0.0f) + (nw > 0.0f));
       cnt += (pw > 0.0f) + (mirror_is_full_only && nw > 0.0f);
     }
   }
@@ -159,8 +173,8 @@ __global__ void __launch_bounds__(32 * kMapCols)
     const int kz = i / kMapCols, c = i - kz * kMapCols;
     if (c < ncols) {
       const std::size_t o = kz * hplane + col0 + c;
-      a[o] = a_tile[i];
-      hits[o] = h_tile[i];
+      a[o] = a_tile[c * pitch + kz];
+      hits[o] = h_tile[c * pitch + kz];
     }
   }
   cnt = warp_sum(cnt);
@@ -234,7 +248,8 @@ void map_half(const float2* spectra, const float4* illum, int count, const Grid&
   const std::size_t columns = static_cast<std::size_t>(g.n) * (g.n / 2 + 1);
   const auto launch = [&](auto kernel, int cols) {
     // Output tile, per-warp column sums and counts, tile hits, as laid out in k_map_half.
-    const std::size_t smem = static_cast<std::size_t>(g.nz) * cols * (3 * sizeof(float2) + 2 * sizeof(std::uint16_t) + 1);
+    const std::size_t smem = static_cast<std::size_t>(cols) *
+                             (map_pitch(g.nz) * (sizeof(float2) + 1) + g.nz * (2 * sizeof(float2) + 2 * sizeof(std::uint16_t)));
     ensure_smem(kernel);
     kernel<<<dim3(blocks_for(columns, cols), batch), 32 * cols, smem, s>>>(spectra, illum, count, g, a, hits, filled);
   };

@@ -38,8 +38,8 @@ std::size_t axis_smem_budget();
 // `batch` arrays of that layout, each sb elements after the previous (data and aux alike).
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch = 1, std::size_t sb = 0);
-// The same pass on the register-resident engine (fft_reg.cu) when it covers length n (64, 128, 256,
-// 512); false otherwise, or when QHK_FFT_ENGINE=staged. axis_pass calls it first.
+// The same pass on the register-resident engine (fft_reg.cu) when it covers length n (64, 128, 192,
+// 256, 512); false otherwise, or when QHK_FFT_ENGINE=staged. axis_pass calls it first.
 bool axis_pass_reg(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
                    AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb);
 bool fft_reg_engine_enabled();
@@ -65,14 +65,12 @@ void rows_c2r_r2c(float2* e, std::size_t rows, int nx, cudaStream_t s);
 // e <- R2C(x + momentum (x - xprev)). Volumes dense (nz, ny, nx), nx even, 8-byte aligned.
 void rows_tv_final_r2c(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda, float momentum,
                        float* xprev, float2* e, cudaStream_t s);
-// The row passes above on the register-resident engine (fft_reg.cu) when it covers the half length
-// nx / 2 (64, 128, 256); false otherwise. The staged functions call them first.
+// R2C, C2R and the GP step boundary on the register-resident engine (fft_reg.cu) when it covers the
+// half length nx / 2 (64, 128, 192, 256); false otherwise. The staged functions call them first.
 bool rows_r2c_reg(const float* x, float2* e, std::size_t rows, int nx, bool clamp, cudaStream_t s);
 bool rows_c2r_reg(const float2* e, float* x, std::size_t rows, int nx, C2rMode mode, float nm2, float inv_k02,
                   cudaStream_t s);
 bool rows_c2r_r2c_reg(float2* e, std::size_t rows, int nx, cudaStream_t s);
-bool rows_tv_final_r2c_reg(const float* b, const float* const p[3], int nz, int ny, int nx, float lambda,
-                           float momentum, float* xprev, float2* e, cudaStream_t s);
 
 // Complex rows of length nx (dense). Modes for the complex Gerchberg-Papoulis loop.
 enum class RowMode : int {

@@ -13,6 +13,8 @@
 
 #include <cstdint>
 
+#include "debug.cuh"
+
 namespace qhk {
 
 // Tensor map of the volume at `base` (dense nz x ny x nx floats, 16-byte aligned, nx % 4 == 0)
@@ -39,8 +41,10 @@ __device__ __forceinline__ void mbar_expect(std::uint64_t* bar, unsigned bytes) 
 // writes of TMA loads it issues next.
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-// Box at (x, y, z) of `map` into dst, completing on `bar`.
+// Box at (x, y, z) of `map` into dst, completing on `bar`. The debug build skips (and records) a box
+// whose x is not on a 16-byte boundary or whose destination or mbarrier is misaligned.
 __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, std::uint64_t* bar) {
+  if (!QHK_CHECK((x & 3) == 0 && (smem_addr(dst) & 127u) == 0 && (smem_addr(bar) & 7u) == 0)) return;
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
       "[%5];\n" ::"r"(smem_addr(dst)),

@@ -782,6 +782,11 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
       }
     }
   };
+  // The layout, mbarriers included, must fit the shared memory the launch was given (CTA-uniform).
+  if (!QHK_CHECK(static_cast<std::size_t>(OPK + 3 * R1P) * sizeof(float) + 4 * sizeof(std::uint64_t) <=
+                 debug::dynamic_smem_bytes())) {
+    return;
+  }
   if (linear == 0) {
     for (int i = 0; i < 4; ++i) tma::mbar_init(bars + i, 1);
   }
@@ -822,6 +827,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   for (long long u = units * blockIdx.x / gridDim.x; u < u_end;) {
     const int y0 = static_cast<int>(u / nz) * TY;
     const int z0 = static_cast<int>(u % nz);
+    if (!QHK_CHECK(y0 < ny && u < units)) break;  // CTA-uniform
     const int zend = static_cast<int>(min(static_cast<long long>(nz), z0 + (u_end - u)));
     u += zend - z0;
     const int zmax = min(zend + 1, nz - 1);  // last plane of r_k and b read
@@ -834,6 +840,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
     // z, rows y0-1 .. y0+TY, into the p_k slot on mbarrier 3. Rows outside the volume arrive as
     // zeros and are never read.
     const auto issue = [&](int z, int s, int comps, bool with_b) {
+      if (!QHK_CHECK(z >= 0 && z < nz && s >= 0 && s < 3)) return;
       tma::fence_async_shared();
       std::uint64_t* bar = bars + s;
       arm(s);
@@ -842,6 +849,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
       if (with_b) tma::load_3d(smem2 + OB + s * BP, &M.b, 0, y0 - 1, z, bar);
     };
     const auto issue_pk = [&](int z) {
+      if (!QHK_CHECK(z >= 0 && z < nz)) return;
       tma::fence_async_shared();
       arm(3);
       tma::mbar_expect(bars + 3, static_cast<unsigned>(3 * R1_ROWS * P * 4));

@@ -73,7 +73,9 @@ class UnwrapBatchPlan {
   DevBuf<float> d1_;
   DevBuf<double> partial_;
   DevBuf<float2> consts_;
-  Pass pass_[5];
+  // Passes 1-5 (staged tiles for passes 1-3), then passes 1-3 of the images whose lines run on the
+  // register engine: each has its own queue, so that each kernel holds only its own tiles' registers.
+  Pass pass_[8];
   CapturedWork graph_;
   bool warmed_ = false;
 };
