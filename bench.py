@@ -282,13 +282,14 @@ def fgp_form(capi, n):
     return False, 0
 
 
-def fgp_roofline(torch, capi, stream):
-    """Average duration of one launch of the FGP kernel the TV proximal step runs at 256^3 (CUDA
-    events, kernel timed alone, on a 12-volume workspace so that the tuned form can run) and its
-    algorithmic bytes: a launch reads b, r (3), p (3) and writes p (3), r (3) (13 volumes); the first
-    reads p as r and the last writes no r (10 volumes each). The one-step form (k_fgp) does one FGP
-    step per launch, the two-step form (k_fgp2) two, so a prox of TV_INNER steps takes TV_INNER or
-    TV_INNER / 2 launches."""
+def fgp_roofline(torch, capi, stream, live):
+    """Roofline of the FGP kernel the TV proximal step runs at 256^3. Its average launch duration is
+    `live` = (milliseconds, launches) of the proximal steps inside the timed reconstructions (CUDA events
+    the pipeline records on its stream around each step, Pipeline.time_prox); the same kernel timed alone
+    on random data (a 12-volume workspace, so that the tuned form runs) is reported beside it. Algorithmic
+    bytes: a launch reads b, r (3), p (3) and writes p (3), r (3) (13 volumes); the first reads p as r and
+    the last writes no r (10 volumes each). The one-step form (k_fgp) does one FGP step per launch, the
+    two-step form (k_fgp2) two, so a prox of TV_INNER steps takes TV_INNER or TV_INNER / 2 launches."""
     n = FIELD_N
     vol = n * n * n
     b = torch.rand((n, n, n), device="cuda")
@@ -309,7 +310,11 @@ def fgp_roofline(torch, capi, stream):
     t10, t0 = timed(TV_INNER), timed(0)
     two_step, rows = fgp_form(capi, n)
     launches = TV_INNER // 2 if two_step else TV_INNER
-    t_launch = (t10 - t0) / launches
+    t_alone = (t10 - t0) / launches
+    live_ms, live_launches = live
+    if live_launches % launches:
+        raise RuntimeError(f"proximal-step timing saw {live_launches} launches, not a multiple of {launches}")
+    t_launch = live_ms / live_launches
     volumes = (10 + 13 * (launches - 2) + 10) / launches
     alg = volumes * vol * 4
     peak, which = measured_peaks()
@@ -322,7 +327,11 @@ def fgp_roofline(torch, capi, stream):
             "traffic": FGP2_TRAFFIC_BYTES if two_step else FGP_TRAFFIC_BYTES,
             "traffic_source": "ncu capture of one middle launch (constant in bench.py)",
             "algorithmic_bytes_per_launch": alg, "avg_launch_ms": round(t_launch, 5),
-            "fgp_steps_per_launch": 2 if two_step else 1, "ms_per_fgp_step": round((t10 - t0) / TV_INNER, 5)}
+            "timing": f"CUDA events around the {live_launches} FGP launches of the timed reconstructions",
+            "fgp_steps_per_launch": 2 if two_step else 1,
+            "ms_per_fgp_step": round(t_launch / (2 if two_step else 1), 5),
+            "alone_avg_launch_ms": round(t_alone, 5),
+            "alone": "the same kernel timed alone on random data (b uniform in [0, 1)), L2 warm"}
 
 
 def reference_run(holo, bg, illum):
@@ -1142,6 +1151,7 @@ def main():
         dist.barrier()
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     launches0 = capi.kernel_launches()
+    pipe.time_prox(True)  # CUDA events around every TV proximal step of the timed runs (the roofline)
     with ClockSampler(physical_gpu_index(local)) as clocks:
         for s, e in events:
             flush.zero_()
@@ -1150,6 +1160,8 @@ def main():
             e.record()
         torch.cuda.synchronize()
     launches = capi.kernel_launches() - launches0
+    prox_live = pipe.prox_time()  # (ms, FGP launches) of the proximal steps inside the timed runs
+    pipe.time_prox(False)
     step_ms = [s.elapsed_time(e) for s, e in events]
     if dist:
         dist.barrier()
@@ -1180,7 +1192,7 @@ def main():
     stream_equals_run = bool(all(np.array_equal(rs[i], ri) for i in range(e2e_steps)))
     del rs, stream_in, api
 
-    roof = fgp_roofline(torch, capi, stream)
+    roof = fgp_roofline(torch, capi, stream, prox_live)
 
     bpm = None
     if rank == 0 and world == 1 and not args.no_bpm:

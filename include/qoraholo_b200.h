@@ -314,10 +314,18 @@ int qhk_pipeline_check_waits(qhk_pipeline* pipeline, void* stream);
  * the pipeline's own stream; returns QHK_TIMEOUT as a run whose wait ran out does. No load is in
  * flight, so the pipeline stays usable. */
 int qhk_pipeline_wait_probe(qhk_pipeline* pipeline, int polls);
+/* Device time of the FISTA-TV proximal steps inside the pipeline's runs (no counterpart in the
+ * reference; for measurement): after qhk_pipeline_time_prox(pipeline, 1), runs launched directly (not
+ * under stream capture) record CUDA events on their stream around the proximal step of every outer
+ * iteration but the last; qhk_pipeline_prox_time waits for them and returns their total milliseconds
+ * and the kernel launches inside them (the FGP launches), and starts a new count. */
+int qhk_pipeline_time_prox(qhk_pipeline* pipeline, int enable);
+int qhk_pipeline_prox_time(qhk_pipeline* pipeline, double* ms, uint64_t* launches);
 int qhk_pipeline_shape(const qhk_pipeline* pipeline, int* nz, int* ny, int* nx);
 /* Batched pipeline (no counterpart in the reference): `batch` requests of this geometry per run, each
- * pass one launch for all of them. Input (batch * count, N, N), output (batch, nz, m, m); the
- * background holograms stay one stack (count, N, N). Supports the GP solver and plain Rytov ODT. */
+ * pass one launch for all of them (FISTA-TV: the k-space passes span the batch, the TV proximal steps
+ * run volume by volume). Input (batch * count, N, N), output (batch, nz, m, m); the background
+ * holograms stay one stack (count, N, N). Every solver; each volume bitwise its single run. */
 int qhk_pipeline_create_batched(qhk_pipeline** pipeline, const qhk_pipeline_options* options, const float* illum_fyfx,
                                 const qhk_geometry* geometry, int batch);
 /* process_device replayed as one CUDA graph (the first call for a pair of buffers runs directly). */

@@ -107,6 +107,8 @@ _PROTOS = {
     "qhk_pipeline_filled": (_I, [_VP, _VP, C.POINTER(C.c_double)]),
     "qhk_pipeline_check_waits": (_I, [_VP, _VP]),
     "qhk_pipeline_wait_probe": (_I, [_VP, _I]),
+    "qhk_pipeline_time_prox": (_I, [_VP, _I]),
+    "qhk_pipeline_prox_time": (_I, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "qhk_pipeline_shape": (_I, [_VP, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "qhk_pipeline_device_bytes": (C.c_size_t, [_VP]),
     "qhk_pipeline_destroy": (_I, [_VP]),
@@ -481,6 +483,17 @@ class Pipeline:
         """Waits for `stream`; raises QhkError (TIMEOUT) if a bounded device wait of this pipeline ran
         out since the last check (device-form runs cannot report it themselves)."""
         check(lib().qhk_pipeline_check_waits(self._h, _VP(stream)))
+
+    def time_prox(self, enable=True):
+        """Record CUDA events around the TV proximal steps of the following direct runs
+        (qhk_pipeline_time_prox)."""
+        check(lib().qhk_pipeline_time_prox(self._h, int(bool(enable))))
+
+    def prox_time(self):
+        """(milliseconds, FGP launches) of the proximal steps recorded since time_prox or the last call."""
+        ms, n = C.c_double(), C.c_uint64()
+        check(lib().qhk_pipeline_prox_time(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def wait_probe(self, polls=1000):
         """Test hook of the timeout path: one bounded wait that nothing completes, counted in this

@@ -484,7 +484,6 @@ int qhk_pipeline_create_batched(qhk_pipeline** pipeline, const qhk_pipeline_opti
     qhk::require(n >= 4 && n % 2 == 0, "Pipeline: hologram_size must be even");
     const qhk::CropPlan crop = qhk::make_crop(n, o->center_y, o->center_x, o->radius, o->output_size);
     qhk::OdtConfig c = odt_config(crop.out, o->count, illum_fyfx, geometry, &o->odt);
-    qhk::require(batch == 1 || !c.tv, "Pipeline: batches need the GP solver or plain Rytov ODT");
     c.batch = batch;
     qhk::require(o->upload_chunks >= 1 && o->upload_chunks <= o->count * batch,
                  "Pipeline: upload_chunks must be between 1 and count * batch");
@@ -577,6 +576,22 @@ int qhk_pipeline_check_waits(qhk_pipeline* p, void* stream) {
   return guard([&] {
     qhk::require(p != nullptr, "Pipeline: null pipeline");
     p->plan.check_device_waits(as_stream(stream));
+  });
+}
+
+int qhk_pipeline_time_prox(qhk_pipeline* p, int enable) {
+  return guard([&] {
+    qhk::require(p != nullptr, "Pipeline: null pipeline");
+    p->plan.odt().enable_prox_timing(enable != 0);
+  });
+}
+
+int qhk_pipeline_prox_time(qhk_pipeline* p, double* ms, uint64_t* launches) {
+  return guard([&] {
+    qhk::require(p && ms && launches, "Pipeline: null argument");
+    const auto [t, n] = p->plan.odt().prox_timing();
+    *ms = t;
+    *launches = n;
   });
 }
 

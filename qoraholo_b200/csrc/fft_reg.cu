@@ -16,8 +16,14 @@ namespace {
 
 constexpr int kRegThreads = 256;
 
+// The restore modes hold two transforms' state: two CTAs per SM (at most 128 registers) keep their loads
+// overlapping each other's transforms.
+constexpr bool restore_mode(int mode) {
+  return mode == static_cast<int>(AxisMode::restore_half) || mode == static_cast<int>(AxisMode::restore_mask);
+}
+
 template <bool Fwd, int Mode, int T, int V>
-__global__ void __launch_bounds__(kRegThreads)
+__global__ void __launch_bounds__(kRegThreads, restore_mode(Mode) ? 2 : 1)
     k_axis_reg(float2* __restrict__ data, std::size_t so, std::size_t sp, int ni, const float2* __restrict__ tw,
                float scale, const float2* __restrict__ aux_a, const std::uint8_t* __restrict__ aux_h,
                std::size_t sb) {

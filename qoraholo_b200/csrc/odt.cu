@@ -301,9 +301,8 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
   const int n = g.n, nz = g.nz, h = n / 2 + 1;
   require(n >= 4 && n % 2 == 0 && nz >= 2 && nz % 2 == 0, "odt: invalid grid");
   require(cfg_.count >= 1, "odt: need at least one field");
-  require(cfg_.batch >= 1 && cfg_.batch <= 65535 && (cfg_.batch == 1 || !cfg_.tv) &&
-              static_cast<long long>(cfg_.batch) * nz <= 65535,
-          "odt: batches of reconstructions need the GP solver and batch * nz <= 65535");
+  require(cfg_.batch >= 1 && cfg_.batch <= 65535 && static_cast<long long>(cfg_.batch) * nz <= 65535,
+          "odt: batches of reconstructions need batch * nz <= 65535");
   real_ = cfg_.iterations > 0 && (cfg_.tv || cfg_.r2c);
   half_ = static_cast<std::size_t>(nz) * n * h;
   vol_ = static_cast<std::size_t>(nz) * n * n;
@@ -314,17 +313,22 @@ OdtPlan::OdtPlan(const OdtConfig& cfg, const float* illum_fyfx) : cfg_(cfg) {
   filled_.reset(b);
   waits_.reset(1);
   check(cudaMemset(waits_.get(), 0, waits_.bytes()), "cudaMemset");
-  tv_.wait_status = waits_.get();
   if (real_) {
     a_.reset(b * half_);
     hits_.reset(b * half_);
     e_.reset(b * half_);
     if (cfg_.tv) {  // GP keeps its real rows on chip (rows_c2r_r2c)
+      // Per volume: the real volume, x_prev and four dual triplets (the proximal step runs volume by
+      // volume; the k-space passes span the batch).
       x_.reset(b * vol_);
-      xprev_.reset(vol_);
-      dual_.reset(12 * vol_);
-      for (int i = 0; i < 4; ++i)
-        for (int c = 0; c < 3; ++c) tv_.v[i][c] = dual_.get() + (3 * i + c) * vol_;
+      xprev_.reset(b * vol_);
+      dual_.reset(12 * b * vol_);
+      tv_.resize(b);
+      for (std::size_t v = 0; v < b; ++v) {
+        tv_[v].wait_status = waits_.get();
+        for (int i = 0; i < 4; ++i)
+          for (int c = 0; c < 3; ++c) tv_[v].v[i][c] = dual_.get() + (12 * v + 3 * i + c) * vol_;
+      }
     }
   } else {
     pot_.reset(b * vol_);
@@ -361,7 +365,7 @@ void OdtPlan::tune() {
     }
     tune_axis_pass(scratch, n, h, nz, nh, h, false, AxisMode::from_data, 1.0f, aux, s, b, half_);
     tune_axis_pass(scratch, n, h, nz, nh, h, true, AxisMode::restore_half, 1.0f, aux, s, b, half_);
-    if (cfg_.tv) tune_tv(x_.get(), tv_, nz, n, n, cfg_.lambda, s);
+    if (cfg_.tv) tune_tv(x_.get(), tv_[0], nz, n, n, cfg_.lambda, s);
   } else {
     for (const bool fwd : {true, false}) {
       tune_axis_pass(scratch, b * nz, nn, n, static_cast<std::size_t>(n), n, fwd, AxisMode::plain, 1.0f, AxisAux{},
@@ -455,11 +459,14 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
     axis_pass(e, b * nz, nh, n, h, h, false, AxisMode::plain, 1.0f, AxisAux{}, s);
     rows_c2r(e, out, rows, n, mode, cfg_.nm2, cfg_.inv_k02, s);
   };
-  // FISTA-TV: y lives in x_ (it is also b, the C2R output), x_prev in xprev_, the dual in dual_.
+  // FISTA-TV: y lives in x_ (it is also b, the C2R output), x_prev in xprev_, the dual in dual_; volume v
+  // of a batch at offset v * vol_ of x_, xprev_ and the index, its half spectrum at v * half_ of E.
   const std::size_t vbytes = vol_ * sizeof(float);
-  check(cudaMemcpyAsync(xprev_.get(), x_.get(), vbytes, cudaMemcpyDeviceToDevice, s), "copy x");
-  check(cudaMemsetAsync(dual_.get(), 0, 3 * vbytes, s), "cudaMemset");
-  tv_.p_index = 0;
+  check(cudaMemcpyAsync(xprev_.get(), x_.get(), b * vbytes, cudaMemcpyDeviceToDevice, s), "copy x");
+  for (int v = 0; v < b; ++v) {
+    check(cudaMemsetAsync(tv_[v].v[0][0], 0, 3 * vbytes, s), "cudaMemset");
+    tv_[v].p_index = 0;
+  }
   float t = 1.0f;
   // Between iterations the final primal, the momentum point y and y's R2C run as one row pass
   // (rows_tv_final_r2c), so y is never written: the next k-space step starts from its spectra.
@@ -478,16 +485,57 @@ void OdtPlan::solve_real(float* index, float inv, cudaStream_t s) {
     const float tn = fista_t(t);
     const float m = (t - 1.0f) / tn;
     const NvtxRange r("qhk:tv_prox");
-    if (last) {
-      tv_prox(x_.get(), tv_, nz, n, n, cfg_.lambda, cfg_.tv_inner, TvFinal::index, m, xprev_.get(), index,
-              cfg_.nm2, cfg_.inv_k02, s);
-    } else {
-      tv_prox(x_.get(), tv_, nz, n, n, cfg_.lambda, cfg_.tv_inner, TvFinal::none, m, xprev_.get(), x_.get(),
-              cfg_.nm2, cfg_.inv_k02, s);
-      rows_tv_final_r2c(x_.get(), tv_.v[tv_.p_index], nz, n, n, cfg_.lambda, m, xprev_.get(), e, s);
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    check(cudaStreamIsCapturing(s, &capturing), "cudaStreamIsCapturing");
+    const bool timed = prox_timing_ && !last && capturing == cudaStreamCaptureStatusNone;
+    const std::uint64_t launches0 = g_launches.load(std::memory_order_relaxed);
+    if (timed) {
+      prox_events_.emplace_back();
+      check(cudaEventRecord(prox_events_.back().start(), s), "cudaEventRecord");
+    }
+    for (int v = 0; v < b; ++v) {
+      float* xv = x_.get() + v * vol_;
+      float* pv = xprev_.get() + v * vol_;
+      if (last) {
+        tv_prox(xv, tv_[v], nz, n, n, cfg_.lambda, cfg_.tv_inner, TvFinal::index, m, pv, index + v * vol_, cfg_.nm2,
+                cfg_.inv_k02, s);
+      } else {
+        tv_prox(xv, tv_[v], nz, n, n, cfg_.lambda, cfg_.tv_inner, TvFinal::none, m, pv, xv, cfg_.nm2, cfg_.inv_k02,
+                s);
+      }
+    }
+    if (timed) {  // the proximal steps only: the fused row passes below are not FGP work
+      check(cudaEventRecord(prox_events_.back().end(), s), "cudaEventRecord");
+      prox_launches_ += g_launches.load(std::memory_order_relaxed) - launches0;
+    }
+    if (!last) {
+      for (int v = 0; v < b; ++v) {
+        const TvBuffers& tb = tv_[v];
+        rows_tv_final_r2c(x_.get() + v * vol_, tb.v[tb.p_index], nz, n, n, cfg_.lambda, m, xprev_.get() + v * vol_,
+                          e + v * half_, s);
+      }
     }
     t = tn;
   }
+}
+
+void OdtPlan::enable_prox_timing(bool on) {
+  prox_timing_ = on && cfg_.tv;
+  prox_timing();  // drops what an earlier count recorded
+}
+
+std::pair<double, std::uint64_t> OdtPlan::prox_timing() {
+  double ms = 0.0;
+  for (const EventPair& e : prox_events_) {
+    float t = 0.0f;
+    check(cudaEventSynchronize(e.end()), "cudaEventSynchronize");
+    check(cudaEventElapsedTime(&t, e.start(), e.end()), "cudaEventElapsedTime");
+    ms += t;
+  }
+  prox_events_.clear();
+  const std::uint64_t n = prox_launches_;
+  prox_launches_ = 0;
+  return {ms, n};
 }
 
 // Full complex spectra (src/cpu/odt.cpp:208-240): plain Rytov ODT, or GP with the C2C transforms.

@@ -2,6 +2,7 @@
 // runs fields -> index on a stream.
 #pragma once
 
+#include <utility>
 #include <vector>
 
 #include "qhk_internal.hpp"
@@ -47,6 +48,32 @@ struct OdtConfig {
   int batch = 1;       // independent reconstructions of this geometry per run (not with TV)
 };
 
+// Two CUDA events owned together (start and end of a timed span); destroyed with their owner.
+class EventPair {
+ public:
+  EventPair() {
+    check(cudaEventCreate(&a_), "cudaEventCreate");
+    check(cudaEventCreate(&b_), "cudaEventCreate");
+  }
+  ~EventPair() {
+    if (a_) cudaEventDestroy(a_);
+    if (b_) cudaEventDestroy(b_);
+  }
+  EventPair(EventPair&& o) noexcept : a_(std::exchange(o.a_, nullptr)), b_(std::exchange(o.b_, nullptr)) {}
+  EventPair& operator=(EventPair&& o) noexcept {
+    std::swap(a_, o.a_);
+    std::swap(b_, o.b_);
+    return *this;
+  }
+  EventPair(const EventPair&) = delete;
+  EventPair& operator=(const EventPair&) = delete;
+  [[nodiscard]] cudaEvent_t start() const { return a_; }
+  [[nodiscard]] cudaEvent_t end() const { return b_; }
+
+ private:
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+};
+
 class OdtPlan {
  public:
   // Stage marks recorded by run() when a clock is given, in this order.
@@ -73,6 +100,13 @@ class OdtPlan {
   [[nodiscard]] std::size_t device_bytes() const;
   [[nodiscard]] const OdtConfig& config() const { return cfg_; }
 
+  // Device time of the FISTA-TV proximal steps inside runs (every outer iteration's but the last, which
+  // also writes the index): CUDA events on the run's stream around each step, from enable_prox_timing(true)
+  // on, in runs launched directly (not under stream capture). prox_timing() waits for the events and returns
+  // the milliseconds and the kernel launches they cover, and starts a new count.
+  void enable_prox_timing(bool on);
+  std::pair<double, std::uint64_t> prox_timing();
+
  private:
   void mark(StageClock* clock, int m, cudaStream_t s) const;
   void tune();
@@ -93,7 +127,10 @@ class OdtPlan {
   DevBuf<float> x_;
   DevBuf<float> xprev_;
   DevBuf<float> dual_;
-  TvBuffers tv_;
+  std::vector<TvBuffers> tv_;  // per volume of a batch (FISTA-TV)
+  bool prox_timing_ = false;
+  std::vector<EventPair> prox_events_;
+  std::uint64_t prox_launches_ = 0;
   DevBuf<float2> pot_;
   DevBuf<std::uint8_t> mask_;
   DevBuf<float2> measured_;

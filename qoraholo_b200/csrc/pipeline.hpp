@@ -78,6 +78,7 @@ class PipelinePlan {
   [[nodiscard]] std::size_t device_bytes() const;
   [[nodiscard]] bool has_background() const { return has_background_; }
   [[nodiscard]] const OdtPlan& odt() const { return odt_; }
+  OdtPlan& odt() { return odt_; }
   [[nodiscard]] const CropPlan& crop() const { return crop_; }
   [[nodiscard]] int count() const { return count_; }
   // Requests of this geometry per run (OdtConfig::batch): inputs, fields and volumes are that many

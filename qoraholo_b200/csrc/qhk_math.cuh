@@ -33,10 +33,22 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 
-// p - 2 pi floor((p + pi) / 2 pi) in the host's operation order.
+// p - 2 pi floor((p + pi) / 2 pi) in the host's operation order. For x = p + pi in (-3, 12) -- every
+// difference of two phases in [-pi, pi] -- the floor of the correctly rounded quotient x / 2pi is -1, 0
+// or 1, and since that quotient is monotonic in x it is decided by comparisons: it is 1 exactly from
+// x = 2pi on (x just below 2pi gives a quotient one or two units below 1 in the last place, which rounds
+// below 1), and below 0 exactly for x < 0 (x is then at least 2^-23 in magnitude, p and pi being floats
+// near pi, so the quotient does not round to -0). Outside that range the division runs. Either way the
+// result is bitwise that of the division.
 __device__ __forceinline__ float wrap_phase(float p) {
   const float two_pi = __fmul_rn(2.0f, kPiF);
-  const float f = floorf(__fdiv_rn(__fadd_rn(p, kPiF), two_pi));
+  const float x = __fadd_rn(p, kPiF);
+  float f;
+  if (x > -3.0f && x < 12.0f) {
+    f = x < 0.0f ? -1.0f : (x >= two_pi ? 1.0f : 0.0f);
+  } else {
+    f = floorf(__fdiv_rn(x, two_pi));
+  }
   return __fsub_rn(p, __fmul_rn(two_pi, f));
 }
 

@@ -13,6 +13,7 @@
 // shift of the Rytov phase.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <map>
 #include <numbers>
 #include <vector>
@@ -300,6 +301,24 @@ __host__ __device__ constexpr std::size_t reg_cols_smem() {
   return static_cast<std::size_t>(T * V + 1) * (kThreads / T) * sizeof(float2);
 }
 
+// Four consecutive floats of global memory: one 16-byte access when `vec` (the address 16-byte aligned),
+// else four 4-byte ones -- the images of an uneven batch are packed densely, so their rows need not be
+// aligned. ldg4 reads through the read-only cache (data the kernel does not write).
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<std::uintptr_t>(p) & 15u) == 0; }
+__device__ __forceinline__ float4 ld4(const float* p, bool vec) {
+  return vec ? *reinterpret_cast<const float4*>(p) : make_float4(p[0], p[1], p[2], p[3]);
+}
+__device__ __forceinline__ float4 ldg4(const float* p, bool vec) {
+  return vec ? __ldg(reinterpret_cast<const float4*>(p)) : make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3));
+}
+__device__ __forceinline__ void st4(float* p, float4 v, bool vec) {
+  if (vec) {
+    *reinterpret_cast<float4*>(p) = v;
+  } else {
+    p[0] = v.x, p[1] = v.y, p[2] = v.z, p[3] = v.w;
+  }
+}
+
 // Pass 1: rows y0 .. y0 + R - 1 (R = 256 / T) of one image of width n = 2 T V. The rows y0 - 1 .. y0 + R
 // of psi come in coalesced; the divergence of the wrapped differences is formed in natural order in shared
 // memory and read by the transform in the half-length DCT's order; the DCT rows leave coalesced.
@@ -318,11 +337,11 @@ __device__ __forceinline__ void div_dctx_tile_reg(const float* __restrict__ psi,
   const int t = tid % T, r = tid / T;
   float* rows = reinterpret_cast<float*>(sm + reg_rows_area<T, V>());
   float* dv = reinterpret_cast<float*>(sm);
+  const bool vec = aligned16(psi) && aligned16(d1);  // n is a multiple of 4: every row alike
   for (int i = tid; i < (R + 2) * Q; i += kThreads) {  // rows outside the image are never read
     const int rr = i / Q, yy = y0 - 1 + rr;
     if (yy >= 0 && yy < ny) {
-      reinterpret_cast<float4*>(rows)[i] =
-          __ldg(reinterpret_cast<const float4*>(psi + static_cast<std::size_t>(yy) * n) + (i - rr * Q));
+      reinterpret_cast<float4*>(rows)[i] = ldg4(psi + static_cast<std::size_t>(yy) * n + 4 * (i - rr * Q), vec);
     }
   }
   __syncthreads();
@@ -367,8 +386,8 @@ __device__ __forceinline__ void div_dctx_tile_reg(const float* __restrict__ psi,
   for (int i = tid; i < R * Q; i += kThreads) {
     const int rr = i / Q, yy = y0 + rr;
     if (yy < ny) {
-      reinterpret_cast<float4*>(d1 + static_cast<std::size_t>(yy) * n)[i - rr * Q] =
-          reinterpret_cast<const float4*>(rows + rr * OP)[i - rr * Q];
+      st4(d1 + static_cast<std::size_t>(yy) * n + 4 * (i - rr * Q),
+          reinterpret_cast<const float4*>(rows + rr * OP)[i - rr * Q], vec);
     }
   }
 }
@@ -454,9 +473,10 @@ __device__ __forceinline__ void idctx_tile_reg(float* __restrict__ phi, const fl
   const int tid = static_cast<int>(threadIdx.x), nth = static_cast<int>(blockDim.x);
   const int t = tid % T, r = tid / T;
   float* rows = reinterpret_cast<float*>(sm + reg_rows_area<T, V>());
+  const bool vec = aligned16(phi) && aligned16(psi);  // n is a multiple of 4: every row alike
   for (int i = tid; i < R * Q; i += kThreads) {
     const int rr = i / Q, yy = y0 + rr;
-    const float4 a = yy < ny ? __ldg(reinterpret_cast<const float4*>(phi + static_cast<std::size_t>(yy) * n) + (i - rr * Q))
+    const float4 a = yy < ny ? ld4(phi + static_cast<std::size_t>(yy) * n + 4 * (i - rr * Q), vec)
                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     reinterpret_cast<float4*>(rows + rr * IP)[i - rr * Q] = a;
   }
@@ -489,8 +509,8 @@ __device__ __forceinline__ void idctx_tile_reg(float* __restrict__ phi, const fl
     const float2 od = *reinterpret_cast<const float2*>(qr + n - 2 - x0 / 2);  // x0 + 3, x0 + 1
     const float4 val = make_float4(ev.x, od.y, ev.y, od.x);
     const std::size_t g = static_cast<std::size_t>(yy) * n + x0;
-    *reinterpret_cast<float4*>(phi + g) = val;
-    const float4 ps = __ldg(reinterpret_cast<const float4*>(psi + g));
+    st4(phi + g, val, vec);
+    const float4 ps = ldg4(psi + g, vec);
     const float d[4] = {__fsub_rn(ps.x, val.x), __fsub_rn(ps.y, val.y), __fsub_rn(ps.z, val.z),
                         __fsub_rn(ps.w, val.w)};
 #pragma unroll
