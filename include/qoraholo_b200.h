@@ -203,6 +203,16 @@ int qhk_unwrap_noalloc(const float* d_wrapped, float* d_unwrapped, int count, in
  * per (device, shape) for the process; results are bitwise the same for every shape. On by default
  * (environment QHK_AUTOTUNE=0 turns it off). */
 int qhk_autotune_enable(int enabled);
+/* Also time the FFT decomposition of the axis passes (the register engine's variants T x V and the
+ * staged radix engine) when plans are built, and keep the fastest. Off by default (environment
+ * QHK_AUTOTUNE_RADIX=1 turns it on): the decompositions round differently, so with it on results stay
+ * within the oracle's tolerance but depend on which variant won -- runs are no longer bitwise
+ * reproducible across processes, nor batches bitwise equal to single requests. */
+int qhk_autotune_radix(int enabled);
+/* Forces the FFT decomposition of the axis passes the register engine covers, for tests and comparisons:
+ * 0 the staged radix engine, 1 and 2 the register variants (2 where the length has one: 64, 128, 256);
+ * -1 (the default) the tuned or default choice. */
+int qhk_fft_axis_engine(int engine);
 /* FGP step form of tv_prox (bitwise the same results): 0 the tuned one, 1 the extrapolated point
  * stored between steps (13 volumes of traffic per step), 2 recomputed from the two previous duals
  * (10 volumes), 3 two steps per pass (13 volumes per two steps; needs rows of a multiple of 4

@@ -124,6 +124,8 @@ _PROTOS = {
     "qhk_synthesize_holograms_device": (_I, [_VP, _I, _I, _VP, C.c_double, C.c_double, C.c_double, C.c_double, _F,
                                              C.c_uint64, _VP, _VP]),
     "qhk_autotune_enable": (_I, [_I]),
+    "qhk_autotune_radix": (_I, [_I]),
+    "qhk_fft_axis_engine": (_I, [_I]),
     "qhk_tv_form": (_I, [_I]),
     "qhk_autotune_report": (C.c_size_t, [_VP, C.c_size_t]),
     "qhk_server_create": (_I, [C.POINTER(_VP), C.c_size_t, _I, _I]),
@@ -300,6 +302,18 @@ def debug_violations(reset: bool = False) -> tuple[int, str]:
 def autotune_enable(enabled: bool = True):
     """Plans built from now on time their launch shapes (on by default)."""
     check(lib().qhk_autotune_enable(int(bool(enabled))))
+
+
+def autotune_radix(enabled: bool = True):
+    """Plans built from now on also time the FFT decomposition of their axis passes (off by default: the
+    variants round differently, so results then depend on which one won)."""
+    check(lib().qhk_autotune_radix(int(bool(enabled))))
+
+
+def fft_axis_engine(engine: int = -1):
+    """Force the FFT decomposition of the register-covered axis passes (0 staged, 1 or 2 register
+    variants; -1 tuned / default). For tests and comparisons."""
+    check(lib().qhk_fft_axis_engine(int(engine)))
 
 
 def synthesize_holograms_device(d_ratio, count, n, illuminations, pixel, carrier=(5.0, 5.0), reference_amplitude=1.0,

@@ -26,7 +26,13 @@ int initial_enabled() {
 }
 std::atomic<int> g_enabled{initial_enabled()};
 
-const char* family_name(TuneFamily f) { return f == TuneFamily::axis ? "axis_cols" : "fgp_rows"; }
+const char* family_name(TuneFamily f) {
+  switch (f) {
+    case TuneFamily::axis: return "axis_cols";
+    case TuneFamily::fgp: return "fgp_rows";
+    default: return "axis_engine";
+  }
+}
 
 // Optional table of choices shared between runs (QHK_AUTOTUNE_FILE): one line per key, "family s0 ..
 // s5 choice". Keys found there are not timed again; new choices are appended. A profiled run can so
@@ -48,7 +54,7 @@ void load_table(int device) {
   while (in >> fam) {
     TuneKey k;
     k.device = device;
-    k.family = fam == "fgp_rows" ? TuneFamily::fgp : TuneFamily::axis;
+    k.family = fam == "fgp_rows" ? TuneFamily::fgp : fam == "axis_engine" ? TuneFamily::axis_engine : TuneFamily::axis;
     for (long long& v : k.shape) in >> v;
     Entry e;
     in >> e.choice;

@@ -6,9 +6,11 @@
 // the candidate with the smallest time wins. Kernels then read their shape from the table, falling
 // back to a fixed heuristic when a shape was never tuned (or tuning is off: QHK_AUTOTUNE=0). With
 // QHK_AUTOTUNE_FILE set, choices are also read from and appended to that file, so that another run
-// (a profiled one, say) uses the same shapes without timing them again. The
-// choices only change how work is tiled, never the arithmetic of any output element, so results
-// are bitwise the same whichever shape wins.
+// (a profiled one, say) uses the same shapes without timing them again. The tile-shape choices only
+// change how work is tiled, never the arithmetic of any output element, so results are bitwise the same
+// whichever shape wins. The FFT decomposition of the axis passes (family axis_engine) does change the
+// rounding, so it is timed only when radix tuning is switched on (QHK_AUTOTUNE_RADIX=1,
+// qhk_autotune_radix): results then stay within the oracle's tolerance but depend on which variant won.
 #pragma once
 
 #include <array>
@@ -21,8 +23,9 @@
 namespace qhk {
 
 enum class TuneFamily : int {
-  axis = 0,  // FFT axis pass: columns per CTA
-  fgp = 1,   // FGP step: rows per CTA
+  axis = 0,         // FFT axis pass: columns per CTA
+  fgp = 1,          // FGP step: rows per CTA
+  axis_engine = 2,  // FFT axis pass: decomposition (register variants, staged engine); opt-in
 };
 
 struct TuneKey {

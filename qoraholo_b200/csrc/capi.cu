@@ -801,6 +801,17 @@ int qhk_autotune_enable(int enabled) {
   return guard([&] { qhk::set_autotune_enabled(enabled != 0); });
 }
 
+int qhk_autotune_radix(int enabled) {
+  return guard([&] { qhk::set_radix_tuning(enabled != 0); });
+}
+
+int qhk_fft_axis_engine(int engine) {
+  return guard([&] {
+    qhk::require(engine >= -1 && engine <= 2, "fft_axis_engine: -1, 0, 1 or 2");
+    qhk::force_axis_engine(engine);
+  });
+}
+
 size_t qhk_autotune_report(char* buf, size_t size) {
   const std::string r = qhk::autotune_report();
   if (buf && size > 0) {

@@ -9,8 +9,10 @@
 //     value) with the split / merge step in shared memory;
 //   * complex rows, with the clamp of the complex GP loop between its inverse and forward row
 //     transforms, or the refractive index as the epilogue of the last inverse.
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -689,11 +691,50 @@ TuneKey axis_key(int n_outer, std::size_t so, int n, std::size_t sp, int ni, boo
 
 }  // namespace
 
+namespace {
+
+// Engine of an axis pass (FFT decomposition): 1 and 2 the register engine's variants, 0 the staged
+// engine with its own tile width.
+TuneKey engine_key(int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward, AxisMode mode,
+                   int batch) {
+  return tune_key(TuneFamily::axis_engine,
+                  {n, ni, n_outer, static_cast<long long>(so), static_cast<long long>(sp),
+                   2 * static_cast<long long>(mode) + (forward ? 1 : 0) + 16LL * batch});
+}
+
+std::atomic<int> g_radix_tuning{-1};  // -1: from the environment
+std::atomic<int> g_axis_engine{-1};   // -1: the tuned or default decomposition; else forced
+
+}  // namespace
+
+void force_axis_engine(int engine) { g_axis_engine.store(engine, std::memory_order_relaxed); }
+
+bool radix_tuning_enabled() {
+  int v = g_radix_tuning.load(std::memory_order_relaxed);
+  if (v < 0) {
+    const char* e = std::getenv("QHK_AUTOTUNE_RADIX");
+    v = e && std::strcmp(e, "1") == 0 ? 1 : 0;
+    g_radix_tuning.store(v, std::memory_order_relaxed);
+  }
+  return v == 1;
+}
+
+void set_radix_tuning(bool on) { g_radix_tuning.store(on ? 1 : 0, std::memory_order_relaxed); }
+
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
   require(n_outer >= 1 && n_outer <= 65535 && batch >= 1 && batch <= 65535,
           "fft: too many lines in the outer dimension");
-  if (axis_pass_reg(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s, batch, sb)) return;
+  const int forced = g_axis_engine.load(std::memory_order_relaxed);
+  int engine = 1;
+  if (forced >= 0 && forced <= axis_reg_variants(n)) {
+    engine = forced;
+  } else if (axis_reg_variants(n) > 0 && radix_tuning_enabled()) {
+    engine = tuned_choice(engine_key(n_outer, so, n, sp, ni, forward, mode, batch), 1);
+  }
+  if (engine != 0 && axis_pass_reg(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s, batch, sb, engine)) {
+    return;
+  }
   require(static_cast<std::size_t>(n) * 2 * sizeof(float2) <= 200 * 1024, "fft: transform length too large");
   const int cols = tuned_choice(axis_key(n_outer, so, n, sp, ni, forward, mode, batch), axis_default(n));
   axis_cols(cols, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s);
@@ -703,7 +744,24 @@ void tune_axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_
                     AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
   require(n_outer >= 1 && n_outer <= 65535 && batch >= 1 && batch <= 65535,
           "fft: too many lines in the outer dimension");
-  if (fft_reg_engine_enabled() && (n == 64 || n == 128 || n == 192 || n == 256 || n == 512)) return;  // no tile choice
+  if (const int variants = axis_reg_variants(n); variants > 0) {
+    // The register engine covers n: its decomposition is fixed unless radix tuning is on, in which case
+    // its variants and the staged engine (at its default tile width) are timed against each other.
+    if (!radix_tuning_enabled()) return;
+    std::vector<int> candidates{1};
+    if (variants > 1) candidates.push_back(2);
+    if (static_cast<std::size_t>(n) * 2 * sizeof(float2) <= 200 * 1024) candidates.push_back(0);
+    autotune(engine_key(n_outer, so, n, sp, ni, forward, mode, batch), candidates, 1,
+             [&](int c) {
+               if (c == 0) {
+                 axis_cols(axis_default(n), data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s);
+               } else {
+                 axis_pass_reg(data, n_outer, so, n, sp, ni, forward, mode, scale, aux, s, batch, sb, c);
+               }
+             },
+             s);
+    return;
+  }
   autotune(axis_key(n_outer, so, n, sp, ni, forward, mode, batch), axis_candidates(n), axis_default(n),
            [&](int c) { axis_cols(c, data, n_outer, so, n, sp, ni, forward, mode, scale, aux, batch, sb, s); }, s);
 }

@@ -356,14 +356,45 @@ bool fft_reg_engine_enabled() {
   return on;
 }
 
-bool axis_pass_reg(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-                   AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb) {
-  if (!fft_reg_engine_enabled()) return false;
+int axis_reg_variants(int n) {
+  if (!fft_reg_engine_enabled()) return 0;
   switch (n) {
-    case 64: axis_reg_mode<8, 8>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
-    case 128: axis_reg_mode<8, 16>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
+    case 64: case 128: case 256: return 2;
+    case 192: case 512: return 1;
+    default: return 0;
+  }
+}
+
+// Variant 1 (the default) and variant 2 (fewer threads per line, longer per-thread DFTs) of the register
+// engine's decomposition N = T V for each length it covers.
+bool axis_pass_reg(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
+                   AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb,
+                   int variant) {
+  if (variant < 1 || variant > axis_reg_variants(n)) return false;
+  const bool alt = variant == 2;
+  switch (n) {
+    case 64:
+      if (alt) {
+        axis_reg_mode<4, 16>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s);
+      } else {
+        axis_reg_mode<8, 8>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s);
+      }
+      return true;
+    case 128:
+      if (alt) {
+        axis_reg_mode<4, 32>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s);
+      } else {
+        axis_reg_mode<8, 16>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s);
+      }
+      return true;
     case 192: axis_reg_mode<8, 24>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
-    case 256: axis_reg_mode<16, 16>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
+    case 256:
+      if (alt) {
+        axis_reg_mode<8, 32>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s);
+      } else {
+        axis_reg_mode<16, 16>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s);
+      }
+      return true;
     case 512: axis_reg_mode<16, 32>(data, n_outer, so, sp, ni, forward, mode, scale, aux, batch, sb, s); return true;
     default: return false;
   }

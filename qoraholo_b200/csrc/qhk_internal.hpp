@@ -39,9 +39,21 @@ std::size_t axis_smem_budget();
 void axis_pass(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
                AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch = 1, std::size_t sb = 0);
 // The same pass on the register-resident engine (fft_reg.cu) when it covers length n (64, 128, 192,
-// 256, 512); false otherwise, or when QHK_FFT_ENGINE=staged. axis_pass calls it first.
+// 256, 512) in decomposition `variant` (1: the default; 2: fewer threads per line with longer
+// per-thread DFTs, for 64, 128, 256); false otherwise, or when QHK_FFT_ENGINE=staged.
 bool axis_pass_reg(float2* data, int n_outer, std::size_t so, int n, std::size_t sp, int ni, bool forward,
-                   AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb);
+                   AxisMode mode, float scale, const AxisAux& aux, cudaStream_t s, int batch, std::size_t sb,
+                   int variant = 1);
+// Register-engine decompositions of length n (0: not covered).
+int axis_reg_variants(int n);
+// Whether plans also time the FFT decomposition of their axis passes (register variants against the
+// staged engine): off by default, since the decompositions round differently and the choice would make
+// results depend on timing (QHK_AUTOTUNE_RADIX=1 or qhk_autotune_radix(1)).
+bool radix_tuning_enabled();
+void set_radix_tuning(bool on);
+// Forces the decomposition of every axis pass the register engine covers (0: staged engine; 1, 2: the
+// register variants, where the length has them); -1 restores the tuned or default one. For tests.
+void force_axis_engine(int engine);
 bool fft_reg_engine_enabled();
 
 // Times the tile widths of this axis pass on `data` (scratch: it is overwritten) and keeps the

@@ -689,14 +689,9 @@ __device__ __forceinline__ void fgp_dual_pair(float2 c, float2 cz, float2 cy, fl
     q[a] = add2(r[a], mul2(st, g[a], nz));
     norm2 = add2(norm2, mul2(q[a], q[a], nz));
   }
-  // 1 / sqrt(norm2) where a point leaves the unit ball, as tv_dual_step; a warp none of whose points
-  // leaves it skips the correctly rounded square roots and reciprocals altogether.
-  float2 scale = make_float2(1.0f, 1.0f);
-  const bool out_x = norm2.x > 1.0f, out_y = norm2.y > 1.0f;
-  if (__any_sync(__activemask(), out_x || out_y)) {
-    if (out_x) scale.x = __frcp_rn(__fsqrt_rn(norm2.x));
-    if (out_y) scale.y = __frcp_rn(__fsqrt_rn(norm2.y));
-  }
+  // 1 / sqrt(norm2) per point, as tv_dual_step.
+  const float2 scale = make_float2(norm2.x > 1.0f ? __frcp_rn(__fsqrt_rn(norm2.x)) : 1.0f,
+                                   norm2.y > 1.0f ? __frcp_rn(__fsqrt_rn(norm2.y)) : 1.0f);
   const float2 m = make_float2(momentum, momentum);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
