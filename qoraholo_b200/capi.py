@@ -126,6 +126,7 @@ _PROTOS = {
     "qhk_autotune_enable": (_I, [_I]),
     "qhk_autotune_radix": (_I, [_I]),
     "qhk_fft_axis_engine": (_I, [_I]),
+    "qhk_selftest_rcp_sqrt": (_I, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "qhk_tv_form": (_I, [_I]),
     "qhk_autotune_report": (C.c_size_t, [_VP, C.c_size_t]),
     "qhk_server_create": (_I, [C.POINTER(_VP), C.c_size_t, _I, _I]),
@@ -314,6 +315,14 @@ def fft_axis_engine(engine: int = -1):
     """Force the FFT decomposition of the register-covered axis passes (0 staged, 1 or 2 register
     variants; -1 tuned / default). For tests and comparisons."""
     check(lib().qhk_fft_axis_engine(int(engine)))
+
+
+def selftest_rcp_sqrt():
+    """(mismatches, first mismatching input bits) of the projection factor against the IEEE operations
+    over every float in (1, 2^126) (qhk_selftest_rcp_sqrt)."""
+    n, b = C.c_uint64(), C.c_uint32()
+    check(lib().qhk_selftest_rcp_sqrt(C.byref(n), C.byref(b)))
+    return n.value, b.value
 
 
 def synthesize_holograms_device(d_ratio, count, n, illuminations, pixel, carrier=(5.0, 5.0), reference_amplitude=1.0,

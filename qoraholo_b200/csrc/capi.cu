@@ -805,6 +805,17 @@ int qhk_autotune_radix(int enabled) {
   return guard([&] { qhk::set_radix_tuning(enabled != 0); });
 }
 
+int qhk_selftest_rcp_sqrt(uint64_t* mismatches, uint32_t* first_bad) {
+  return guard([&] {
+    qhk::require(mismatches && first_bad, "selftest_rcp_sqrt: null argument");
+    unsigned long long n = 0;
+    unsigned b = 0;
+    qhk::selftest_rcp_sqrt(&n, &b);
+    *mismatches = n;
+    *first_bad = b;
+  });
+}
+
 int qhk_fft_axis_engine(int engine) {
   return guard([&] {
     qhk::require(engine >= -1 && engine <= 2, "fft_axis_engine: -1, 0, 1 or 2");

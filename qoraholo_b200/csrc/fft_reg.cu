@@ -16,14 +16,16 @@ namespace {
 
 constexpr int kRegThreads = 256;
 
-// The restore modes hold two transforms' state: two CTAs per SM (at most 128 registers) keep their loads
-// overlapping each other's transforms.
+// Resident CTAs per SM, so that their loads overlap each other's transforms: for V <= 16 values per
+// thread, three for one transform (at most 85 registers) and two for the restore modes, which hold two
+// transforms' state (at most 128); longer per-thread DFTs keep the registers they need (no bound).
 constexpr bool restore_mode(int mode) {
   return mode == static_cast<int>(AxisMode::restore_half) || mode == static_cast<int>(AxisMode::restore_mask);
 }
+constexpr int axis_min_blocks(int mode, int V) { return V >= 24 ? 1 : restore_mode(mode) ? 2 : 3; }
 
 template <bool Fwd, int Mode, int T, int V>
-__global__ void __launch_bounds__(kRegThreads, restore_mode(Mode) ? 2 : 1)
+__global__ void __launch_bounds__(kRegThreads, axis_min_blocks(Mode, V))
     k_axis_reg(float2* __restrict__ data, std::size_t so, std::size_t sp, int ni, const float2* __restrict__ tw,
                float scale, const float2* __restrict__ aux_a, const std::uint8_t* __restrict__ aux_h,
                std::size_t sb) {

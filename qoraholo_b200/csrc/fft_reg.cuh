@@ -152,17 +152,33 @@ __device__ __forceinline__ void line_fft(float2 (&v)[V], int t, float2* xs, int 
 }
 
 // Exchange strides for tiles of rows: 256 threads, T per row (consecutive threads on consecutive positions
-// of a row), R = 256 / T rows. With T = 4 a warp spans 4 threads of 8 rows, with T = 8 8 threads of 4
-// rows, with T = 16 16 threads of 2 rows; B (per thread) and A (per bin) are chosen so that t * B + r and
-// t * A + r cover the 16 two-bank slots of a 64-bit access evenly, in the writes and in the reads of the
-// exchange, and so that B >= R and A >= T * B (the (bin, thread, row) elements do not overlap).
+// of a row), R = 256 / T rows. A 64-bit shared-memory access is served per half-warp, 16 threads over the
+// 16 two-bank slots: with T = 4 a half-warp spans 4 threads of 4 rows, with T = 8 8 threads of 2 rows,
+// with T = 16 16 threads of one row. B (per thread) and A (per bin) are chosen so that t * B + r and
+// t * A + r fall on 16 distinct slots within every half-warp, in the writes and in the reads of the
+// exchange (B and A congruent to 16 / T times an odd number modulo 16, rows r0 .. r0 + 16 / T - 1 with r0 a
+// multiple of 16 / T), and so that B >= R and A >= T * B (the (bin, thread, row) elements do not overlap).
+// True when t * S + r lands on 16 distinct two-bank slots over one half-warp: T threads of 16 / T rows.
+constexpr bool half_warp_distinct(int T, int S) {
+  bool seen[16] = {};
+  for (int t = 0; t < T; ++t) {
+    for (int r = 0; r < 16 / T; ++r) {
+      const int slot = (t * S + r) % 16;
+      if (seen[slot]) return false;
+      seen[slot] = true;
+    }
+  }
+  return true;
+}
+
 template <int T>
 struct RowTile {
   static_assert(T == 4 || T == 8 || T == 16, "row tiles of 4, 8 or 16 threads per row");
   static constexpr int R = 256 / T;
-  static constexpr int B = T == 4 ? 72 : T == 8 ? 36 : 17;
-  static constexpr int A = T == 4 ? 4 * 72 + 8 : T == 8 ? 8 * 36 + 4 : 16 * 17 + 1;
+  static constexpr int B = T == 4 ? 68 : T == 8 ? 34 : 17;
+  static constexpr int A = T == 4 ? 4 * 68 + 4 : T == 8 ? 8 * 34 + 2 : 16 * 17 + 1;
   static_assert(B >= R && A >= T * B, "row tile exchange elements overlap");
+  static_assert(half_warp_distinct(T, B) && half_warp_distinct(T, A), "row tile exchange has bank conflicts");
 };
 
 }  // namespace regfft

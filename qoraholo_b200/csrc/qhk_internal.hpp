@@ -54,6 +54,11 @@ void set_radix_tuning(bool on);
 // Forces the decomposition of every axis pass the register engine covers (0: staged engine; 1, 2: the
 // register variants, where the length has them); -1 restores the tuned or default one. For tests.
 void force_axis_engine(int engine);
+
+// Runs rcp_sqrt_rn (qhk_math.cuh) against __frcp_rn(__fsqrt_rn(x)) for every float x in (1, 2^126) on
+// the current device: the number of mismatches and the bits of the smallest mismatching x (all ones
+// when there is none). Synchronous.
+void selftest_rcp_sqrt(unsigned long long* mismatches, unsigned* first_bad);
 bool fft_reg_engine_enabled();
 
 // Times the tile widths of this axis pass on `data` (scratch: it is overwritten) and keeps the

@@ -690,8 +690,8 @@ __device__ __forceinline__ void fgp_dual_pair(float2 c, float2 cz, float2 cy, fl
     norm2 = add2(norm2, mul2(q[a], q[a], nz));
   }
   // 1 / sqrt(norm2) per point, as tv_dual_step.
-  const float2 scale = make_float2(norm2.x > 1.0f ? __frcp_rn(__fsqrt_rn(norm2.x)) : 1.0f,
-                                   norm2.y > 1.0f ? __frcp_rn(__fsqrt_rn(norm2.y)) : 1.0f);
+  const float2 scale = make_float2(norm2.x > 1.0f ? rcp_sqrt_rn(norm2.x) : 1.0f,
+                                   norm2.y > 1.0f ? rcp_sqrt_rn(norm2.y) : 1.0f);
   const float2 m = make_float2(momentum, momentum);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
