@@ -232,6 +232,269 @@ void fft2_reg(const float2* src, float2* dst, bool forward, int nb, int mode, co
   check_launch("bpm cols");
 }
 
+// One slice of the forward sweep as two passes on the register engine, each keeping a line of every
+// plane on chip across a transform, the pointwise step and the opposite transform:
+//   column pass (kPropInv): the forward column transform of the row-transformed envelope completes its
+//     2D FFT W; S = c (q W + (1 - q) S) (as the kPropagate epilogue) is stored; the inverse column
+//     transform of S starts the next inverse 2D FFT. kInvOnly applies only the inverse column transform to
+//     S (the first slice of a recomputed segment).
+//   row pass (kScreenFwd): the inverse row transform completes IFFT(S); x 1/n^2, store the envelope, times
+//     the screen (as the kScreen epilogue), then the forward row transform of the next slice's FFT.
+//     kScaleOut ends the sweep: inverse rows and x 1/n^2 only.
+// The inverse 2D FFT thus runs columns first and the forward one rows first; the recomputed segments use
+// the same two passes, so their envelopes are bitwise the forward sweep's.
+enum SliceMode : int { kPropInv = 0, kInvOnly = 1, kScreenFwd = 2, kScaleOut = 3, kSplitInv = 4 };
+
+template <int Mode, int T, int V>
+__global__ void __launch_bounds__(kThreads) k_slice_cols(ColArgs a, const float2* tw) {
+  constexpr int N = T * V, COLS = kThreads / T;
+  extern __shared__ float2 sm[];
+  const int c = static_cast<int>(threadIdx.x) % COLS, t = static_cast<int>(threadIdx.x) / COLS;
+  const int col = static_cast<int>(blockIdx.x) * COLS + c;
+  const bool live = col < N;
+  const std::size_t base = static_cast<std::size_t>(blockIdx.y) * N * N + (live ? col : 0);
+  float2 v[V];
+  if constexpr (Mode == kPropInv) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) v[j] = live ? a.data[base + static_cast<std::size_t>(t + T * j) * N] : make_float2(0.f, 0.f);
+    regfft::line_fft<T, V, true>(v, t, sm + c, T * COLS, COLS, tw);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      if (!live) continue;
+      const std::size_t g = base + static_cast<std::size_t>(t + T * j) * N;
+      const float2 vv = v[j];
+      const float2 cc = a.coef[g];
+      const float q = a.q[g];
+      const float2 sv = a.s[g];
+      const float tre = q * vv.x + (1.0f - q) * sv.x;
+      const float tim = q * vv.y + (1.0f - q) * sv.y;
+      v[j] = make_float2(cc.x * tre - cc.y * tim, cc.x * tim + cc.y * tre);
+      a.s[g] = v[j];
+    }
+    __syncthreads();  // the inverse transform reuses the exchange buffer
+  } else if constexpr (Mode == kSplitInv) {
+    // Adjoint: the forward column transform completes FFT(w); U = conj(c)(g + back) (as the kSplit
+    // epilogue), g = (1 - q) U is stored, b = q U goes on to the inverse column transform.
+#pragma unroll
+    for (int j = 0; j < V; ++j) v[j] = live ? a.data[base + static_cast<std::size_t>(t + T * j) * N] : make_float2(0.f, 0.f);
+    regfft::line_fft<T, V, true>(v, t, sm + c, T * COLS, COLS, tw);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      if (!live) continue;
+      const std::size_t g = base + static_cast<std::size_t>(t + T * j) * N;
+      const float2 vv = v[j];
+      float2 gi = a.s[g];
+      if (a.has_back) gi = cadd(gi, vv);
+      else gi = vv;
+      const float2 cc = a.coef[g];
+      const float q = a.q[g];
+      const float ure = cc.x * gi.x + cc.y * gi.y;
+      const float uim = cc.x * gi.y - cc.y * gi.x;
+      v[j] = make_float2(q * ure, q * uim);
+      a.s[g] = make_float2((1.0f - q) * ure, (1.0f - q) * uim);
+    }
+    __syncthreads();
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) v[j] = live ? a.s[base + static_cast<std::size_t>(t + T * j) * N] : make_float2(0.f, 0.f);
+  }
+  regfft::line_fft<T, V, false>(v, t, sm + c, T * COLS, COLS, tw);
+  if (!live) return;
+#pragma unroll
+  for (int j = 0; j < V; ++j) a.data[base + static_cast<std::size_t>(t + T * j) * N] = v[j];
+}
+
+template <int Mode, int T, int V>
+__global__ void __launch_bounds__(kThreads) k_slice_rows(ColArgs a, std::size_t rows, const float2* tw) {
+  using Tile = regfft::RowTile<T>;
+  constexpr int N = T * V;
+  extern __shared__ float2 sm[];
+  const int t = static_cast<int>(threadIdx.x) % T, r = static_cast<int>(threadIdx.x) / T;
+  const std::size_t row = static_cast<std::size_t>(blockIdx.x) * Tile::R + r;
+  const bool live = row < rows;
+  const std::size_t y = row % N;
+  float2 v[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) v[j] = live ? a.data[row * N + t + T * j] : make_float2(0.f, 0.f);
+  regfft::line_fft<T, V, false>(v, t, sm + r, Tile::A, Tile::B, tw);
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    const int pos = t + T * j;
+    float2 w = cscale(v[j], a.inv);
+    if constexpr (Mode == kScreenFwd) {
+      if (live && a.store) a.store[row * N + pos] = w;
+      float sn, cs;
+      sincosf(a.phase * a.x[y * N + pos], &sn, &cs);
+      w = cmul(make_float2(cs, sn), w);
+    }
+    v[j] = w;
+  }
+  if constexpr (Mode == kScreenFwd) {
+    __syncthreads();  // the forward transform reuses the exchange buffer
+    regfft::line_fft<T, V, true>(v, t, sm + r, Tile::A, Tile::B, tw);
+  }
+  if (!live) return;
+#pragma unroll
+  for (int j = 0; j < V; ++j) a.data[row * N + t + T * j] = v[j];
+}
+
+// Adjoint row pass of slice k for image row y (blockIdx.x) of one group of R = 256 / T illuminations
+// (blockIdx.y), one row each: the inverse row transform completes IFFT(b); x 1/n^2; each view's term of the
+// gradient, Im(conj(t w_k) b) with t = e^{i phase x_k}, goes to shared memory, and one thread per pixel adds
+// the group's terms in view order into part[group, y, :]; b <- conj(t) b, then (kForward) the forward row
+// transform of the next slice's FFT. k_gradient_groups adds the groups in order into the gradient.
+template <bool kForward, int T, int V>
+__global__ void __launch_bounds__(kThreads)
+    k_slice_gradient(float2* __restrict__ data, const float2* __restrict__ env, const float* __restrict__ x,
+                     float phase, float inv, int nb, float* __restrict__ part, const float2* tw) {
+  using Tile = regfft::RowTile<T>;
+  constexpr int N = T * V, R = Tile::R;
+  extern __shared__ float2 sm[];
+  float* terms = reinterpret_cast<float*>(sm + static_cast<std::size_t>(V) * Tile::A);  // R views x N pixels
+  float2* screen = reinterpret_cast<float2*>(terms + R * N);                            // (cos, sin) of row y
+  const int tid = static_cast<int>(threadIdx.x);
+  const int t = tid % T, r = tid / T;
+  const int y = static_cast<int>(blockIdx.x);
+  const int v0 = static_cast<int>(blockIdx.y) * R;
+  if (tid < N) {  // the screen of row y, the same for every view
+    float sn, cs;
+    sincosf(phase * x[static_cast<std::size_t>(y) * N + tid], &sn, &cs);
+    screen[tid] = make_float2(cs, sn);
+  }
+  const int view = v0 + r;
+  const bool live = view < nb;
+  const std::size_t row = (static_cast<std::size_t>(live ? view : 0) * N + y) * N;
+  float2 v[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) v[j] = live ? data[row + t + T * j] : make_float2(0.f, 0.f);
+  regfft::line_fft<T, V, false>(v, t, sm + r, Tile::A, Tile::B, tw);  // its barrier also publishes `screen`
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    const int pos = t + T * j;
+    const float cs = screen[pos].x, sn = screen[pos].y;
+    const float2 bv = cscale(v[j], inv);
+    float term = 0.0f;
+    if (live) {
+      const float2 w = cmul(make_float2(cs, sn), env[row + pos]);
+      term = w.x * bv.y - w.y * bv.x;
+    }
+    terms[r * N + pos] = term;
+    v[j] = cmul(make_float2(cs, -sn), bv);
+  }
+  __syncthreads();
+  if (tid < N) {
+    float acc = 0.0f;
+    for (int i = 0; i < R && v0 + i < nb; ++i) acc += terms[i * N + tid];
+    part[(static_cast<std::size_t>(blockIdx.y) * N + y) * N + tid] = acc;
+  }
+  if constexpr (kForward) regfft::line_fft<T, V, true>(v, t, sm + r, Tile::A, Tile::B, tw);
+  if (!live) return;
+#pragma unroll
+  for (int j = 0; j < V; ++j) data[row + t + T * j] = v[j];
+}
+
+// grad += gscale phase (part[0] + part[1] + ...), the groups added in order, per pixel.
+__global__ void k_gradient_groups(const float* __restrict__ part, int groups, std::size_t plane, float gscale,
+                                  float phase, float* __restrict__ grad) {
+  for (std::size_t p = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; p < plane;
+       p += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+    float acc = part[p];
+    for (int g = 1; g < groups; ++g) acc += part[g * plane + p];
+    grad[p] += gscale * phase * acc;
+  }
+}
+
+// Calls f.template operator()<T, V>() for the plane sides the slice passes cover; false otherwise.
+template <class F>
+bool with_slice_shape(int n, F&& f) {
+  if (!fft_reg_engine_enabled()) return false;
+  switch (n) {
+    case 64: f.template operator()<8, 8>(); return true;
+    case 128: f.template operator()<8, 16>(); return true;
+    case 256: f.template operator()<16, 16>(); return true;
+    default: return false;
+  }
+}
+
+template <int T, int V>
+void slice_cols(int mode, const ColArgs& a, int nb, cudaStream_t s) {
+  constexpr int N = T * V, COLS = kThreads / T;
+  const std::size_t smem = static_cast<std::size_t>(N) * COLS * sizeof(float2);
+  const dim3 grid((N + COLS - 1) / COLS, nb);
+  const float2* tw = fft_len(N).tw;
+  const auto launch = [&](auto kernel) {
+    ensure_smem(kernel);
+    kernel<<<grid, kThreads, smem, s>>>(a, tw);
+  };
+  if (mode == kPropInv) {
+    launch(k_slice_cols<kPropInv, T, V>);
+  } else if (mode == kSplitInv) {
+    launch(k_slice_cols<kSplitInv, T, V>);
+  } else {
+    launch(k_slice_cols<kInvOnly, T, V>);
+  }
+  check_launch("bpm slice columns");
+}
+
+template <int T, int V>
+void slice_rows(int mode, const ColArgs& a, int nb, cudaStream_t s) {
+  using Tile = regfft::RowTile<T>;
+  constexpr int N = T * V;
+  const std::size_t rows = static_cast<std::size_t>(nb) * N;
+  const std::size_t smem = static_cast<std::size_t>(V) * Tile::A * sizeof(float2);
+  const unsigned grid = static_cast<unsigned>((rows + Tile::R - 1) / Tile::R);
+  const float2* tw = fft_len(N).tw;
+  const auto launch = [&](auto kernel) {
+    ensure_smem(kernel);
+    kernel<<<grid, kThreads, smem, s>>>(a, rows, tw);
+  };
+  if (mode == kScreenFwd) {
+    launch(k_slice_rows<kScreenFwd, T, V>);
+  } else {
+    launch(k_slice_rows<kScaleOut, T, V>);
+  }
+  check_launch("bpm slice rows");
+}
+
+template <int T, int V>
+void slice_gradient(bool forward, float2* data, const float2* env, const float* x, float phase, float inv, int nb,
+                    float gscale, float* part, float* grad, cudaStream_t s) {
+  using Tile = regfft::RowTile<T>;
+  constexpr int N = T * V;
+  const int groups = (nb + Tile::R - 1) / Tile::R;
+  const std::size_t smem = static_cast<std::size_t>(V) * Tile::A * sizeof(float2) +
+                           static_cast<std::size_t>(Tile::R) * N * sizeof(float) + static_cast<std::size_t>(N) * sizeof(float2);
+  const float2* tw = fft_len(N).tw;
+  const dim3 grid(N, groups);
+  const auto launch = [&](auto kernel) {
+    ensure_smem(kernel);
+    kernel<<<grid, kThreads, smem, s>>>(data, env, x, phase, inv, nb, part, tw);
+  };
+  if (forward) {
+    launch(k_slice_gradient<true, T, V>);
+  } else {
+    launch(k_slice_gradient<false, T, V>);
+  }
+  check_launch("bpm slice gradient");
+  const std::size_t plane = static_cast<std::size_t>(N) * N;
+  k_gradient_groups<<<static_cast<unsigned>((plane + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+      part, groups, plane, gscale, phase, grad);
+  check_launch("bpm gradient groups");
+}
+
+// Forward rows only (the envelope of the first slice entering the sweep).
+template <int T, int V>
+void rows_forward(float2* data, int nb, cudaStream_t s) {
+  using Tile = regfft::RowTile<T>;
+  constexpr int N = T * V;
+  const std::size_t rows = static_cast<std::size_t>(nb) * N;
+  const std::size_t smem = static_cast<std::size_t>(V) * Tile::A * sizeof(float2);
+  const unsigned grid = static_cast<unsigned>((rows + Tile::R - 1) / Tile::R);
+  ensure_smem(k_rows_reg<true, T, V>);
+  k_rows_reg<true, T, V><<<grid, kThreads, smem, s>>>(data, data, rows, fft_len(N).tw);
+  check_launch("bpm rows");
+}
+
 // Spectrum of the unit envelope: n^2 at the zero bin of every plane.
 __global__ void k_unit_spectrum(float2* s, std::size_t plane, std::size_t total) {
   for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < total;
@@ -432,11 +695,12 @@ BpmPlan::BpmPlan(const BpmTablesHost& t, int chunk, bool store, int checkpoint_e
     rw_.reset(plane_ * chunk);
   }
   partial_.reset(4096);
+  gpart_.reset(plane_ * ((chunk + 15) / 16));  // per-group gradient sums (groups of at least 16 views)
 }
 
 std::size_t BpmPlan::device_bytes() const {
   return step_.bytes() + last_.bytes() + q_.bytes() + s_.bytes() + w_.bytes() + stored_.bytes() + partial_.bytes() +
-         ckpt_.bytes() + env_.bytes() + rs_.bytes() + rw_.bytes();
+         ckpt_.bytes() + env_.bytes() + rs_.bytes() + rw_.bytes() + gpart_.bytes();
 }
 
 void BpmPlan::fft2(const float2* src, float2* dst, bool forward, int nb, int mode, const void* args_v,
@@ -514,6 +778,36 @@ void BpmPlan::forward(const float* x, int first, int nb, cudaStream_t s) {
   k_first_screen<<<grid_for(total), kThreads, 0, s>>>(w_.get(), store_on_ ? stored_.get() : nullptr, x, t_.phase,
                                                       plane_, total);
   check_launch("bpm start");
+  // Two passes per slice on the register engine (k_slice_cols / k_slice_rows).
+  if (with_slice_shape(t_.n, [&]<int T, int V>() {
+        rows_forward<T, V>(w_.get(), nb, s);
+        for (int k = 0; k < nz; ++k) {
+          if (every_ > 0 && k % every_ == 0) {
+            float2* ck = ckpt_.get() + (static_cast<std::size_t>(k / every_) * t_.count + first) * plane_;
+            check(cudaMemcpyAsync(ck, s_.get(), total * sizeof(float2), cudaMemcpyDeviceToDevice, s),
+                  "bpm checkpoint");
+          }
+          ColArgs c{};
+          c.data = w_.get();
+          c.s = s_.get();
+          c.coef = (k == nz - 1 ? last_.get() : step_.get()) + off;
+          c.q = q_.get() + off;
+          slice_cols<T, V>(kPropInv, c, nb, s);
+          ColArgs w{};
+          w.data = w_.get();
+          w.inv = inv;
+          if (k + 1 < nz) {
+            w.store = store_on_ ? stored_.get() + (k + 1) * total : nullptr;
+            w.x = x + (k + 1) * plane_;
+            w.phase = t_.phase;
+            slice_rows<T, V>(kScreenFwd, w, nb, s);
+          } else {
+            slice_rows<T, V>(kScaleOut, w, nb, s);  // envelopes at z = 0 in w
+          }
+        }
+      })) {
+    return;
+  }
   for (int k = 0; k < nz; ++k) {
     if (every_ > 0 && k % every_ == 0) {
       // Spectrum entering slice k of illuminations first .. first + nb - 1.
@@ -551,22 +845,46 @@ void BpmPlan::adjoint(const float* x, const float2* residual_or_null, int first,
     check(cudaMemcpyAsync(w_.get(), residual_or_null, total * sizeof(float2), cudaMemcpyDeviceToDevice, s),
           "copy residual");
   }
+  require(store_on_ || every_ > 0, "bpm: the plan keeps no envelopes for an adjoint");
+  const auto envelope = [&](int k) -> const float2* {
+    if (every_ > 0) {
+      const int k0 = (k / every_) * every_;
+      if (k == nz - 1 || k % every_ == every_ - 1) recompute(x, first, nb, k0, std::min(k0 + every_, nz), s);
+      return env_.get() + (k - k0) * total;
+    }
+    return stored_.get() + k * total;
+  };
+  // Two passes per slice on the register engine: k_slice_gradient (inverse rows, gradient, conj(screen),
+  // forward rows) and k_slice_cols<kSplitInv> (forward columns, split, inverse columns).
+  if (with_slice_shape(t_.n, [&]<int T, int V>() {
+        const auto split = [&](const float2* coef, int has_back) {
+          ColArgs c{};
+          c.data = w_.get();
+          c.s = s_.get();
+          c.coef = coef + off;
+          c.q = q_.get() + off;
+          c.has_back = has_back;
+          slice_cols<T, V>(kSplitInv, c, nb, s);
+        };
+        rows_forward<T, V>(w_.get(), nb, s);
+        split(last_.get(), 0);
+        for (int k = nz - 1; k >= 0; --k) {
+          const float2* env = envelope(k);
+          slice_gradient<T, V>(k > 0, w_.get(), env, x + k * plane_, t_.phase, inv, nb, gscale, gpart_.get(),
+                               grad + k * plane_, s);
+          if (k > 0) split(step_.get(), 1);
+        }
+      })) {
+    return;
+  }
   ColArgs a{};
   a.s = s_.get();
   a.coef = last_.get() + off;
   a.q = q_.get() + off;
   a.has_back = 0;
   fft2(w_.get(), w_.get(), true, nb, kSplit, &a, s);
-  require(store_on_ || every_ > 0, "bpm: the plan keeps no envelopes for an adjoint");
   for (int k = nz - 1; k >= 0; --k) {
-    const float2* env = nullptr;
-    if (every_ > 0) {
-      const int k0 = (k / every_) * every_;
-      if (k == nz - 1 || k % every_ == every_ - 1) recompute(x, first, nb, k0, std::min(k0 + every_, nz), s);
-      env = env_.get() + (k - k0) * total;
-    } else {
-      env = stored_.get() + k * total;
-    }
+    const float2* env = envelope(k);
     ColArgs b{};
     b.inv = inv;
     fft2(w_.get(), w_.get(), false, nb, kScale, &b, s);
@@ -590,6 +908,40 @@ void BpmPlan::recompute(const float* x, int first, int nb, int k0, int k1, cudaS
   const float inv = 1.0f / static_cast<float>(plane_);
   const float2* ck = ckpt_.get() + (static_cast<std::size_t>(k0 / every_) * t_.count + first) * plane_;
   check(cudaMemcpyAsync(rs_.get(), ck, total * sizeof(float2), cudaMemcpyDeviceToDevice, s), "bpm restore");
+  // The forward sweep's two passes per slice (register engine), so the envelopes are bitwise its own.
+  if (with_slice_shape(t_.n, [&]<int T, int V>() {
+        const auto screen = [&](int k) {  // rw_ holds C^-1(S) of slice k: envelope k, then its row FFT
+          ColArgs w{};
+          w.data = rw_.get();
+          w.inv = inv;
+          w.store = env_.get() + (k - k0) * total;
+          w.x = x + k * plane_;
+          w.phase = t_.phase;
+          slice_rows<T, V>(kScreenFwd, w, nb, s);
+        };
+        if (k0 == 0) {
+          k_first_screen<<<grid_for(total), kThreads, 0, s>>>(rw_.get(), env_.get(), x, t_.phase, plane_, total);
+          check_launch("bpm recompute");
+          rows_forward<T, V>(rw_.get(), nb, s);
+        } else {
+          ColArgs c{};
+          c.data = rw_.get();
+          c.s = rs_.get();
+          slice_cols<T, V>(kInvOnly, c, nb, s);
+          screen(k0);
+        }
+        for (int k = k0; k + 1 < k1; ++k) {  // the spectrum entering k + 1, then envelope k + 1
+          ColArgs c{};
+          c.data = rw_.get();
+          c.s = rs_.get();
+          c.coef = step_.get() + off;
+          c.q = q_.get() + off;
+          slice_cols<T, V>(kPropInv, c, nb, s);
+          screen(k + 1);
+        }
+      })) {
+    return;
+  }
   for (int k = k0; k < k1; ++k) {
     float2* env = env_.get() + (k - k0) * total;
     if (k == 0) {

@@ -58,6 +58,7 @@ class BpmPlan {
   DevBuf<double> partial_;
   int every_ = 0;
   DevBuf<float2> ckpt_, env_, rs_, rw_;  // checkpoint mode
+  DevBuf<float> gpart_;                   // gradient sums per group of views (adjoint, register engine)
 };
 
 // x = ri - n_medium (optionally clamped at 0), and back.
