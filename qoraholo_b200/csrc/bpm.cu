@@ -3,15 +3,18 @@
 // and follows the CPU form (src/cpu/bpm.cpp:18-243) and the tables of src/bpm.cpp:10-60.
 //
 // A pass of the model processes a chunk of nb illuminations at once, all planes (nb, n, n). Each
-// slice is two 2D FFTs, each split into a row pass and a column pass; the pointwise work of the
-// slice is folded into the column pass epilogues:
-//   forward:  IFFT(S) -> [x (1/n^2), store envelope, times the screen e^{i phase x_k}] ->
-//             FFT -> [S = c (q V + (1 - q) S)]                          (4 launches per slice)
-//   adjoint:  IFFT(b) -> [x 1/n^2] -> gradient kernel (one thread per pixel, sums the nb
-//             illuminations in order, writes conj(screen) b) -> FFT -> [U = conj(c)(g + back),
-//             b = q U, g = (1 - q) U]                                   (5 launches per slice)
-// The gradient has one writer per voxel and a fixed summation order; the data term is summed in
-// double per CTA and reduced in order.
+// slice is two 2D FFTs. For n = 64, 128, 256 (the register-resident engine) a slice is two passes, each
+// keeping a line of every plane on chip across a transform, the pointwise step and the opposite transform:
+//   forward:  columns [FFT (completing FFT(w)), S = c (q W + (1 - q) S), IFFT] ->
+//             rows [IFFT (completing IFFT(S)), x 1/n^2, store envelope, times the screen e^{i phase x_k},
+//             FFT]                                                        (2 launches per slice)
+//   adjoint:  rows [IFFT, x 1/n^2, gradient terms summed per pixel in view order within groups of views,
+//             conj(screen) b, FFT] + the groups' sums in order -> columns [FFT, U = conj(c)(g + back),
+//             g = (1 - q) U, b = q U, IFFT]                               (3 launches per slice)
+// Other sides use the staged engine with the pointwise work folded into the column pass epilogues
+// (4 launches per forward slice, 5 per adjoint slice: a separate gradient kernel with one thread per
+// pixel summing the views in order). The gradient has a fixed summation order; the data term is summed
+// in double per CTA and reduced in order.
 #include <algorithm>
 #include <cmath>
 #include <complex>
