@@ -307,28 +307,36 @@ __global__ void __launch_bounds__(kThreads) k_slice_cols(ColArgs a, const float2
   for (int j = 0; j < V; ++j) a.data[base + static_cast<std::size_t>(t + T * j) * N] = v[j];
 }
 
+// Row pass for image row y (blockIdx.x) of one group of R = 256 / T illuminations (blockIdx.y), one row
+// each, so that the group shares the screen factors of row y (computed once, in shared memory).
 template <int Mode, int T, int V>
-__global__ void __launch_bounds__(kThreads) k_slice_rows(ColArgs a, std::size_t rows, const float2* tw) {
+__global__ void __launch_bounds__(kThreads) k_slice_rows(ColArgs a, int nb, const float2* tw) {
   using Tile = regfft::RowTile<T>;
-  constexpr int N = T * V;
+  constexpr int N = T * V, R = Tile::R;
   extern __shared__ float2 sm[];
-  const int t = static_cast<int>(threadIdx.x) % T, r = static_cast<int>(threadIdx.x) / T;
-  const std::size_t row = static_cast<std::size_t>(blockIdx.x) * Tile::R + r;
-  const bool live = row < rows;
-  const std::size_t y = row % N;
+  float2* screen = sm + static_cast<std::size_t>(V) * Tile::A;  // (cos, sin) of row y
+  const int tid = static_cast<int>(threadIdx.x);
+  const int t = tid % T, r = tid / T;
+  const int y = static_cast<int>(blockIdx.x);
+  const int view = static_cast<int>(blockIdx.y) * R + r;
+  const bool live = view < nb;
+  const std::size_t row = (static_cast<std::size_t>(live ? view : 0) * N + y) * N;
+  if (Mode == kScreenFwd && tid < N) {
+    float sn, cs;
+    sincosf(a.phase * a.x[static_cast<std::size_t>(y) * N + tid], &sn, &cs);
+    screen[tid] = make_float2(cs, sn);
+  }
   float2 v[V];
 #pragma unroll
-  for (int j = 0; j < V; ++j) v[j] = live ? a.data[row * N + t + T * j] : make_float2(0.f, 0.f);
-  regfft::line_fft<T, V, false>(v, t, sm + r, Tile::A, Tile::B, tw);
+  for (int j = 0; j < V; ++j) v[j] = live ? a.data[row + t + T * j] : make_float2(0.f, 0.f);
+  regfft::line_fft<T, V, false>(v, t, sm + r, Tile::A, Tile::B, tw);  // its barrier also publishes `screen`
 #pragma unroll
   for (int j = 0; j < V; ++j) {
     const int pos = t + T * j;
     float2 w = cscale(v[j], a.inv);
     if constexpr (Mode == kScreenFwd) {
-      if (live && a.store) a.store[row * N + pos] = w;
-      float sn, cs;
-      sincosf(a.phase * a.x[y * N + pos], &sn, &cs);
-      w = cmul(make_float2(cs, sn), w);
+      if (live && a.store) a.store[row + pos] = w;
+      w = cmul(screen[pos], w);
     }
     v[j] = w;
   }
@@ -338,7 +346,7 @@ __global__ void __launch_bounds__(kThreads) k_slice_rows(ColArgs a, std::size_t 
   }
   if (!live) return;
 #pragma unroll
-  for (int j = 0; j < V; ++j) a.data[row * N + t + T * j] = v[j];
+  for (int j = 0; j < V; ++j) a.data[row + t + T * j] = v[j];
 }
 
 // Adjoint row pass of slice k for image row y (blockIdx.x) of one group of R = 256 / T illuminations
@@ -443,13 +451,12 @@ template <int T, int V>
 void slice_rows(int mode, const ColArgs& a, int nb, cudaStream_t s) {
   using Tile = regfft::RowTile<T>;
   constexpr int N = T * V;
-  const std::size_t rows = static_cast<std::size_t>(nb) * N;
-  const std::size_t smem = static_cast<std::size_t>(V) * Tile::A * sizeof(float2);
-  const unsigned grid = static_cast<unsigned>((rows + Tile::R - 1) / Tile::R);
+  const std::size_t smem = static_cast<std::size_t>(V) * Tile::A * sizeof(float2) + static_cast<std::size_t>(N) * sizeof(float2);
+  const dim3 grid(N, (nb + Tile::R - 1) / Tile::R);
   const float2* tw = fft_len(N).tw;
   const auto launch = [&](auto kernel) {
     ensure_smem(kernel);
-    kernel<<<grid, kThreads, smem, s>>>(a, rows, tw);
+    kernel<<<grid, kThreads, smem, s>>>(a, nb, tw);
   };
   if (mode == kScreenFwd) {
     launch(k_slice_rows<kScreenFwd, T, V>);
