@@ -217,7 +217,7 @@ int qhk_fft_axis_engine(int engine);
 /* Self-check of the FGP dual projection's factor 1 / sqrt(x) (no counterpart in the reference): the
  * library computes it from approximate hardware results refined with fused multiply-adds, and this runs
  * it against the IEEE square root and reciprocal (the reference's 1.0f / std::sqrt) for every float in
- * (1, 2^126) on the current device. `mismatches` receives their number (0 when the two agree
+ * [1, 2^126) on the current device. `mismatches` receives their number (0 when the two agree
  * everywhere), `first_bad` the bits of the smallest mismatching input. Synchronous. */
 int qhk_selftest_rcp_sqrt(uint64_t* mismatches, uint32_t* first_bad);
 /* FGP step form of tv_prox (bitwise the same results): 0 the tuned one, 1 the extrapolated point

@@ -319,7 +319,7 @@ def fft_axis_engine(engine: int = -1):
 
 def selftest_rcp_sqrt():
     """(mismatches, first mismatching input bits) of the projection factor against the IEEE operations
-    over every float in (1, 2^126) (qhk_selftest_rcp_sqrt)."""
+    over every float in [1, 2^126) (qhk_selftest_rcp_sqrt)."""
     n, b = C.c_uint64(), C.c_uint32()
     check(lib().qhk_selftest_rcp_sqrt(C.byref(n), C.byref(b)))
     return n.value, b.value

@@ -55,7 +55,7 @@ void set_radix_tuning(bool on);
 // register variants, where the length has them); -1 restores the tuned or default one. For tests.
 void force_axis_engine(int engine);
 
-// Runs rcp_sqrt_rn (qhk_math.cuh) against __frcp_rn(__fsqrt_rn(x)) for every float x in (1, 2^126) on
+// Runs rcp_sqrt_rn (qhk_math.cuh) against __frcp_rn(__fsqrt_rn(x)) for every float x in [1, 2^126) on
 // the current device: the number of mismatches and the bits of the smallest mismatching x (all ones
 // when there is none). Synchronous.
 void selftest_rcp_sqrt(unsigned long long* mismatches, unsigned* first_bad);

@@ -80,11 +80,11 @@ __device__ __forceinline__ bool ewald_target(const Grid& g, int ky, int kx, floa
 }
 
 // 1 / sqrt(x) with the two roundings of the host's 1.0f / std::sqrt(x) -- RN(1 / RN(sqrt(x))) -- for
-// x > 1 (the dual projection's factor), from the hardware's approximate reciprocal square root and
+// x >= 1 (the dual projection's factor), from the hardware's approximate reciprocal square root and
 // reciprocal refined with fused multiply-adds after Markstein (P. Markstein, "IA-64 and Elementary
 // Functions", 2000, the Newton-Raphson refinements with an exactly computed residual): the root as g = x y
 // from y ~ 1 / sqrt(x), corrected by the residual x - g^2 times y / 2; its reciprocal from z ~ 1 / s
-// refined once by z + z (1 - s z). Equal to __frcp_rn(__fsqrt_rn(x)) for every float in (1, 2^126),
+// refined once by z + z (1 - s z). Equal to __frcp_rn(__fsqrt_rn(x)) for every float in [1, 2^126),
 // checked exhaustively on the device (qhk_selftest_rcp_sqrt); above that, and for NaN, the IEEE intrinsics
 // run. (Further refinements of y and z were checked exhaustively too; none changes a single result.)
 __device__ __forceinline__ float rcp_sqrt_rn(float x) {
@@ -110,8 +110,9 @@ __device__ __forceinline__ void tv_dual_step(const float g[3], float step, float
     q[a] = __fadd_rn(r[a], __fmul_rn(step, g[a]));
     norm2 = __fadd_rn(norm2, __fmul_rn(q[a], q[a]));
   }
-  // 1 / sqrt(norm2) with two roundings as the host's 1.0f / std::sqrt(norm2) (rcp_sqrt_rn).
-  const float scale = norm2 > 1.0f ? rcp_sqrt_rn(norm2) : 1.0f;
+  // 1 / sqrt(norm2) with two roundings as the host's 1.0f / std::sqrt(norm2) where norm2 > 1, else 1:
+  // rcp_sqrt_rn(max(norm2, 1)), without a branch (exactly 1 at 1; max(NaN, 1) = 1).
+  const float scale = rcp_sqrt_rn(fmaxf(norm2, 1.0f));
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const float next = __fmul_rn(q[a], scale);
@@ -129,8 +130,9 @@ __device__ __forceinline__ void tv_dual_project(const float g[3], float step, co
     q[a] = __fadd_rn(r[a], __fmul_rn(step, g[a]));
     norm2 = __fadd_rn(norm2, __fmul_rn(q[a], q[a]));
   }
-  // 1 / sqrt(norm2) with two roundings as the host's 1.0f / std::sqrt(norm2) (rcp_sqrt_rn).
-  const float scale = norm2 > 1.0f ? rcp_sqrt_rn(norm2) : 1.0f;
+  // 1 / sqrt(norm2) with two roundings as the host's 1.0f / std::sqrt(norm2) where norm2 > 1, else 1:
+  // rcp_sqrt_rn(max(norm2, 1)), without a branch (exactly 1 at 1; max(NaN, 1) = 1).
+  const float scale = rcp_sqrt_rn(fmaxf(norm2, 1.0f));
 #pragma unroll
   for (int a = 0; a < 3; ++a) p[a] = __fmul_rn(q[a], scale);
 }

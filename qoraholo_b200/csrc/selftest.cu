@@ -30,8 +30,8 @@ void selftest_rcp_sqrt(unsigned long long* mismatches, unsigned* first_bad) {
   DevBuf<unsigned> first(1);
   check(cudaMemset(bad.get(), 0, sizeof(unsigned long long)), "cudaMemset");
   check(cudaMemset(first.get(), 0xff, sizeof(unsigned)), "cudaMemset");
-  // Every float in (1, 2^126): the helper's fast domain.
-  const std::uint32_t lo = 0x3f800001u, hi = 0x7e800000u;
+  // Every float in [1, 2^126): the helper's fast domain (1 itself for the branch-free projection).
+  const std::uint32_t lo = 0x3f800000u, hi = 0x7e800000u;
   int sms = 0;
   check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0), "cudaDeviceGetAttribute");
   k_check_rcp_sqrt<<<sms * 8, 256>>>(lo, hi, bad.get(), first.get());

@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 
 def test_projection_factor_equals_ieee_sqrt_and_reciprocal_everywhere(cuda):
     """The FGP projection's 1 / sqrt(x), from approximate hardware results refined with FMAs, equals
-    RN(1 / RN(sqrt(x))) -- the reference's 1.0f / std::sqrt(x) -- for every float in (1, 2^126)."""
+    RN(1 / RN(sqrt(x))) -- the reference's 1.0f / std::sqrt(x) -- for every float in [1, 2^126)."""
     from qoraholo_b200 import capi
 
     mismatches, first = capi.selftest_rcp_sqrt()
