@@ -74,6 +74,12 @@ struct ColArgs {
   float phase;          // screen phase per unit contrast
   float inv;            // 1 / n^2
   int has_back;         // kSplit: add data (the back-propagated screen term) to g
+  // kSplitInv: also finish the previous slice's gradient (the first plane's blocks, one pixel per thread
+  // position): grad += gscale phase (part[0] + part[1] + ...), when grad is set.
+  const float* part;
+  int groups;
+  float gscale;
+  float* grad;
 };
 
 template <bool Fwd, int Mode, int COLS>
@@ -278,6 +284,16 @@ __global__ void __launch_bounds__(kThreads) k_slice_cols(ColArgs a, const float2
   } else if constexpr (Mode == kSplitInv) {
     // Adjoint: the forward column transform completes FFT(w); U = conj(c)(g + back) (as the kSplit
     // epilogue), g = (1 - q) U is stored, b = q U goes on to the inverse column transform.
+    if (a.grad && blockIdx.y == 0 && live) {  // the previous slice's per-group sums, in group order
+      constexpr std::size_t plane = static_cast<std::size_t>(N) * N;
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        const std::size_t p = static_cast<std::size_t>(t + T * j) * N + col;
+        float acc = a.part[p];
+        for (int g = 1; g < a.groups; ++g) acc += a.part[g * plane + p];
+        a.grad[p] += a.gscale * a.phase * acc;
+      }
+    }
 #pragma unroll
     for (int j = 0; j < V; ++j) v[j] = live ? a.data[base + static_cast<std::size_t>(t + T * j) * N] : make_float2(0.f, 0.f);
     regfft::line_fft<T, V, true>(v, t, sm + c, T * COLS, COLS, tw);
@@ -486,10 +502,12 @@ void slice_gradient(bool forward, float2* data, const float2* env, const float* 
     launch(k_slice_gradient<false, T, V>);
   }
   check_launch("bpm slice gradient");
-  const std::size_t plane = static_cast<std::size_t>(N) * N;
-  k_gradient_groups<<<static_cast<unsigned>((plane + kThreads - 1) / kThreads), kThreads, 0, s>>>(
-      part, groups, plane, gscale, phase, grad);
-  check_launch("bpm gradient groups");
+  if (grad) {  // else the next column pass adds the groups (ColArgs::grad)
+    const std::size_t plane = static_cast<std::size_t>(N) * N;
+    k_gradient_groups<<<static_cast<unsigned>((plane + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+        part, groups, plane, gscale, phase, grad);
+    check_launch("bpm gradient groups");
+  }
 }
 
 // Forward rows only (the envelope of the first slice entering the sweep).
@@ -867,22 +885,29 @@ void BpmPlan::adjoint(const float* x, const float2* residual_or_null, int first,
   // Two passes per slice on the register engine: k_slice_gradient (inverse rows, gradient, conj(screen),
   // forward rows) and k_slice_cols<kSplitInv> (forward columns, split, inverse columns).
   if (with_slice_shape(t_.n, [&]<int T, int V>() {
-        const auto split = [&](const float2* coef, int has_back) {
+        const int groups = (nb + regfft::RowTile<T>::R - 1) / regfft::RowTile<T>::R;
+        const auto split = [&](const float2* coef, int has_back, float* slice_grad) {
           ColArgs c{};
           c.data = w_.get();
           c.s = s_.get();
           c.coef = coef + off;
           c.q = q_.get() + off;
           c.has_back = has_back;
+          c.part = gpart_.get();
+          c.groups = groups;
+          c.gscale = gscale;
+          c.phase = t_.phase;
+          c.grad = slice_grad;
           slice_cols<T, V>(kSplitInv, c, nb, s);
         };
         rows_forward<T, V>(w_.get(), nb, s);
-        split(last_.get(), 0);
+        split(last_.get(), 0, nullptr);
         for (int k = nz - 1; k >= 0; --k) {
           const float2* env = envelope(k);
+          // Slice k's gradient groups are added by the next column pass, or here for the last slice.
           slice_gradient<T, V>(k > 0, w_.get(), env, x + k * plane_, t_.phase, inv, nb, gscale, gpart_.get(),
-                               grad + k * plane_, s);
-          if (k > 0) split(step_.get(), 1);
+                               k > 0 ? nullptr : grad, s);
+          if (k > 0) split(step_.get(), 1, grad + k * plane_);
         }
       })) {
     return;
