@@ -23,6 +23,7 @@
 
 #include "autotune.hpp"
 #include "qhk_internal.hpp"
+#include "rcp_sqrt2.cuh"
 #include "tma.cuh"
 
 namespace qhk {
@@ -692,7 +693,7 @@ __device__ __forceinline__ void fgp_dual_pair(float2 c, float2 cz, float2 cy, fl
   // 1 / sqrt(norm2) per point where norm2 > 1, else 1, as tv_dual_step: computed for every point, without
   // a branch, as rcp_sqrt_rn(max(norm2, 1)) -- exactly 1 at 1 (the self-check covers [1, 2^126)), and
   // max(NaN, 1) = 1 as the host's comparison gives.
-  const float2 scale = make_float2(rcp_sqrt_rn(fmaxf(norm2.x, 1.0f)), rcp_sqrt_rn(fmaxf(norm2.y, 1.0f)));
+  const float2 scale = rcp_sqrt_rn2(make_float2(fmaxf(norm2.x, 1.0f), fmaxf(norm2.y, 1.0f)), nz);
   const float2 m = make_float2(momentum, momentum);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
