@@ -23,6 +23,14 @@ __device__ __forceinline__ float2 rsq2_fma(float2 a, float2 b, float2 c) {
   return rsq2_unpack(d);
 }
 
+// -a on both lanes as one packed subtraction from -0: (-0) - a = -a for every a, signed zeros included
+// ((-0) - (+0) = -0, (-0) - (-0) = +0), where negating each lane on its own costs an instruction per lane.
+__device__ __forceinline__ float2 rsq2_neg(float2 a, float2 neg_zero) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(rsq2_pack(neg_zero)), "l"(rsq2_pack(a)));
+  return rsq2_unpack(d);
+}
+
 // Both lanes in [1, 2^126) take the packed path; otherwise each lane runs the scalar form.
 __device__ __forceinline__ float2 rcp_sqrt_rn2(float2 x, float2 neg_zero) {
   if (!(x.x < 0x1p126f && x.y < 0x1p126f)) return make_float2(rcp_sqrt_rn(x.x), rcp_sqrt_rn(x.y));
@@ -30,13 +38,13 @@ __device__ __forceinline__ float2 rcp_sqrt_rn2(float2 x, float2 neg_zero) {
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y.x) : "f"(x.x));
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y.y) : "f"(x.y));
   const float2 g = rsq2_fma(x, y, neg_zero);                                   // x y
-  const float2 r = rsq2_fma(make_float2(-g.x, -g.y), g, x);                    // x - g^2
+  const float2 r = rsq2_fma(rsq2_neg(g, neg_zero), g, x);                      // x - g^2
   const float2 h = rsq2_fma(make_float2(0.5f, 0.5f), y, neg_zero);             // y / 2
   const float2 s = rsq2_fma(r, h, g);
   float2 z;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(z.x) : "f"(s.x));
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(z.y) : "f"(s.y));
-  const float2 e = rsq2_fma(make_float2(-s.x, -s.y), z, make_float2(1.0f, 1.0f));  // 1 - s z
+  const float2 e = rsq2_fma(rsq2_neg(s, neg_zero), z, make_float2(1.0f, 1.0f));  // 1 - s z
   return rsq2_fma(e, z, z);
 }
 

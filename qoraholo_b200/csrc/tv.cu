@@ -709,29 +709,33 @@ constexpr std::size_t fgp2_rows(int ty) { return 20 * static_cast<std::size_t>(t
 // Threads per CTA the two-step kernel is compiled for (nx / 4 x TY must stay within it).
 constexpr int fgp2_threads(int ty) { return ty == 8 ? 512 : 256; }
 
-template <int TY, bool FIRST, bool LAST>
+// CUBE > 0: compiled for a CUBE^3 volume (the sizes, the pitch and the block shape are constants, so
+// shared-memory and global addresses fold into immediate offsets); 0: any size, from the arguments.
+template <int TY, bool FIRST, bool LAST, int CUBE = 0>
 __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const __grid_constant__ Fgp2Maps M) {
   extern __shared__ __align__(128) float smem2[];
   constexpr int VEC = 4;
   constexpr int RK_ROWS = TY + 4, B_ROWS = TY + 3, R1_ROWS = TY + 2, Z1_ROWS = TY + 1;
   constexpr int HALO = (8 + TY - 1) / TY;  // halo pair slots per thread: 2 nx over nx / 4 * TY threads
-  const int nx = A.nx, ny = A.ny, nz = A.nz;
+  constexpr bool kFullWarps = CUBE > 0 && (CUBE / VEC * TY) % 32 == 0;
+  const int nx = CUBE > 0 ? CUBE : A.nx, ny = CUBE > 0 ? CUBE : A.ny, nz = CUBE > 0 ? CUBE : A.nz;
+  const int bx = CUBE > 0 ? CUBE / VEC : static_cast<int>(blockDim.x);
   const int tx = static_cast<int>(threadIdx.x);
   const int ty = static_cast<int>(threadIdx.y);
   const int x0 = tx * VEC;
-  const int nthreads = static_cast<int>(blockDim.x) * TY;
-  const int linear = ty * static_cast<int>(blockDim.x) + tx;
+  const int nthreads = bx * TY;
+  const int linear = ty * bx + tx;
   const int lane = linear & 31;
-  const int warp_threads = min(32, nthreads - (linear & ~31));
+  const int warp_threads = kFullWarps ? 32 : min(32, nthreads - (linear & ~31));
   const unsigned lanes = warp_threads >= 32 ? 0xffffffffu : ((1u << warp_threads) - 1u);
   const std::size_t nxy = static_cast<std::size_t>(nx) * ny;
-  // Shared memory in floats, rows of P = A.pitch floats (nx rounded up to 128 bytes; the columns
+  // Shared memory in floats, rows of P floats (A.pitch: nx rounded up to 128 bytes; the columns
   // from nx on hold the zeros the box loads fill in): slot strides and buffer bases (32-bit offsets
   // from smem2), then the mbarriers. r_{k+1} keeps in shared memory only what other threads read:
   // its y component (rows y0-1 .. y0+TY), its z component of row y0+TY for two planes, its x
   // component of row y0+TY, and each thread's last own x value (the left neighbour of the next
   // thread's first point); the rest the z_{k+1} phase takes from the registers of its own thread.
-  const int P = A.pitch;
+  const int P = CUBE > 0 ? (CUBE + 31) / 32 * 32 : A.pitch;
   const int RKP = RK_ROWS * P, BP = B_ROWS * P, R1P = R1_ROWS * P, Z1P = Z1_ROWS * P;
   const int EDGE_ROWS = (nthreads + P - 1) / P;
   const int OB = 9 * RKP, OZ = OB + 3 * BP, ORY = OZ + 2 * BP, ORZH = ORY + R1P, ORXH = ORZH + 2 * P,
@@ -752,36 +756,52 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   const auto primal4 = [&](int z, int yy, const float* vz, const float* vzb, const float* vy, const float* vym,
                            const float* vx, float left, const float* vb, float* out) {
     const bool zhi = z < nz - 1, zlo = z > 0, yhi = yy < ny - 1, ylo = yy > 0;
-    const float2 o0 = fgp_primal_pair(zhi, zlo, yhi, ylo, x_first, false, f2(vz[0], vz[1]), f2(vzb[0], vzb[1]),
-                                      f2(vy[0], vy[1]), f2(vym[0], vym[1]), f2(vx[0], vx[1]), f2(left, vx[0]),
-                                      f2(vb[0], vb[1]), A.lambda, nzero);
-    const float2 o1 = fgp_primal_pair(zhi, zlo, yhi, ylo, false, x_last, f2(vz[2], vz[3]), f2(vzb[2], vzb[3]),
-                                      f2(vy[2], vy[3]), f2(vym[2], vym[3]), f2(vx[2], vx[3]), f2(vx[1], vx[2]),
-                                      f2(vb[2], vb[3]), A.lambda, nzero);
-    out[0] = o0.x, out[1] = o0.y, out[2] = o1.x, out[3] = o1.y;
+    const auto pairs = [&](bool zh, bool zl, bool yh, bool yl) {
+      const float2 o0 = fgp_primal_pair(zh, zl, yh, yl, x_first, false, f2(vz[0], vz[1]), f2(vzb[0], vzb[1]),
+                                        f2(vy[0], vy[1]), f2(vym[0], vym[1]), f2(vx[0], vx[1]), f2(left, vx[0]),
+                                        f2(vb[0], vb[1]), A.lambda, nzero);
+      const float2 o1 = fgp_primal_pair(zh, zl, yh, yl, false, x_last, f2(vz[2], vz[3]), f2(vzb[2], vzb[3]),
+                                        f2(vy[2], vy[3]), f2(vym[2], vym[3]), f2(vx[2], vx[3]), f2(vx[1], vx[2]),
+                                        f2(vb[2], vb[3]), A.lambda, nzero);
+      out[0] = o0.x, out[1] = o0.y, out[2] = o1.x, out[3] = o1.y;
+    };
+    // Interior rows (warp-uniform: a warp holds part of one row of one plane) with the guards as
+    // constants, so that the pair code has no branches; the boundary rows with the guards.
+    if (zhi && zlo && yhi && ylo) {
+      pairs(true, true, true, true);
+    } else {
+      pairs(zhi, zlo, yhi, ylo);
+    }
   };
   // Dual steps of the own points (row yy) of plane z from primal values c, +z (cz), +y (cy) and the
   // primal value right of the last point; p and r updated in place.
   const auto dual4 = [&](int z, int yy, const float* c, const float* cz, const float* cy, float right,
                          float momentum, float (*pv)[VEC], float (*rv)[VEC]) {
     const bool zhi = z < nz - 1, yhi = yy < ny - 1;
+    const auto pairs = [&](bool zh, bool yh) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int k0 = 2 * h;
-      float2 pp[3], rr[3];
+      for (int h = 0; h < 2; ++h) {
+        const int k0 = 2 * h;
+        float2 pp[3], rr[3];
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        pp[cc] = f2(pv[cc][k0], pv[cc][k0 + 1]);
-        rr[cc] = f2(rv[cc][k0], rv[cc][k0 + 1]);
+        for (int cc = 0; cc < 3; ++cc) {
+          pp[cc] = f2(pv[cc][k0], pv[cc][k0 + 1]);
+          rr[cc] = f2(rv[cc][k0], rv[cc][k0 + 1]);
+        }
+        fgp_dual_pair(f2(c[k0], c[k0 + 1]), f2(cz[k0], cz[k0 + 1]), f2(cy[k0], cy[k0 + 1]),
+                      f2(c[k0 + 1], h == 0 ? c[2] : right), zh, yh, h == 1 && x_last, A.step, momentum, pp, rr,
+                      nzero);
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          pv[cc][k0] = pp[cc].x, pv[cc][k0 + 1] = pp[cc].y;
+          rv[cc][k0] = rr[cc].x, rv[cc][k0 + 1] = rr[cc].y;
+        }
       }
-      fgp_dual_pair(f2(c[k0], c[k0 + 1]), f2(cz[k0], cz[k0 + 1]), f2(cy[k0], cy[k0 + 1]),
-                    f2(c[k0 + 1], h == 0 ? c[2] : right), zhi, yhi, h == 1 && x_last, A.step, momentum, pp, rr,
-                    nzero);
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        pv[cc][k0] = pp[cc].x, pv[cc][k0 + 1] = pp[cc].y;
-        rv[cc][k0] = rr[cc].x, rv[cc][k0 + 1] = rr[cc].y;
-      }
+    };
+    if (zhi && yhi) {  // interior rows: guards as constants, as in primal4
+      pairs(true, true);
+    } else {
+      pairs(zhi, yhi);
     }
   };
   // The layout, mbarriers included, must fit the shared memory the launch was given (CTA-uniform).
@@ -824,7 +844,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
   const auto ld2 = [](const float* p) { return *reinterpret_cast<const float2*>(p); };
   const auto st2 = [](float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; };
 
-  const long long units = static_cast<long long>(A.ytiles) * nz;
+  const long long units = static_cast<long long>(CUBE > 0 ? (CUBE + TY - 1) / TY : A.ytiles) * nz;
   const long long u_end = units * (blockIdx.x + 1) / gridDim.x;
   for (long long u = units * blockIdx.x / gridDim.x; u < u_end;) {
     const int y0 = static_cast<int>(u / nz) * TY;
@@ -1240,9 +1260,9 @@ void launch_fgp_p(const FgpPArgs& a, const FgpShape& sh, cudaStream_t s) {
   check_launch("fgp step");
 }
 
-template <int TY, bool FIRST, bool LAST>
+template <int TY, bool FIRST, bool LAST, int CUBE>
 void launch_fgp2_t(const Fgp2Args& a, const float* const rin[3], const float* b, int grid, cudaStream_t s) {
-  auto kernel = k_fgp2<TY, FIRST, LAST>;
+  auto kernel = k_fgp2<TY, FIRST, LAST, CUBE>;
   ensure_smem(kernel);
   Fgp2Maps maps;
   for (int c = 0; c < 3; ++c) maps.r[c] = volume_tensor_map(rin[c], a.nx, a.ny, a.nz, a.pitch, TY + 4);
@@ -1252,17 +1272,17 @@ void launch_fgp2_t(const Fgp2Args& a, const float* const rin[3], const float* b,
   check_launch("fgp two steps");
 }
 
-template <int TY>
+template <int TY, int CUBE = 0>
 void launch_fgp2_rows(bool first, bool last, const Fgp2Args& a, const float* const rin[3], const float* b, int grid,
                       cudaStream_t s) {
   if (first && last) {
-    launch_fgp2_t<TY, true, true>(a, rin, b, grid, s);
+    launch_fgp2_t<TY, true, true, CUBE>(a, rin, b, grid, s);
   } else if (first) {
-    launch_fgp2_t<TY, true, false>(a, rin, b, grid, s);
+    launch_fgp2_t<TY, true, false, CUBE>(a, rin, b, grid, s);
   } else if (last) {
-    launch_fgp2_t<TY, false, true>(a, rin, b, grid, s);
+    launch_fgp2_t<TY, false, true, CUBE>(a, rin, b, grid, s);
   } else {
-    launch_fgp2_t<TY, false, false>(a, rin, b, grid, s);
+    launch_fgp2_t<TY, false, false, CUBE>(a, rin, b, grid, s);
   }
 }
 
@@ -1272,7 +1292,9 @@ void launch_fgp2(bool first, bool last, Fgp2Args a, const float* const rin[3], c
   require(fgp2_fits(a.nx, sh.ty), "tv: two-step FGP shape out of range");
   a.pitch = fgp2_pitch(a.nx);
   a.neg_zero = -0.0f;
-  if (sh.ty == 8) {
+  if (sh.ty == 8 && a.nx == 256 && a.ny == 256 && a.nz == 256) {  // the 256^3 volumes, sizes compiled in
+    launch_fgp2_rows<8, 256>(first, last, a, rin, b, sh.grid, s);
+  } else if (sh.ty == 8) {
     launch_fgp2_rows<8>(first, last, a, rin, b, sh.grid, s);
   } else if (sh.ty == 4) {
     launch_fgp2_rows<4>(first, last, a, rin, b, sh.grid, s);

@@ -177,7 +177,9 @@ def test_odt_plan_runs_are_deterministic(cuda, qhk):
 def test_two_step_fgp_equals_one_step_at_full_size(cuda, qhk, shape):
     """At the bench's 256^3 (and a ragged 130 x 250 x 256) every CTA of the two-step kernel marches
     through several tiles and z segments; its prox must still equal the one-step kernel's (which
-    the tests above pin to the oracle) bit for bit, dual included."""
+    the tests above pin to the oracle) bit for bit, dual included. At 256^3 the two-step kernel is the
+    instantiation with the volume's sizes compiled in (k_fgp2<8, ., ., 256>), which no other test
+    reaches."""
     rng = np.random.default_rng(21)
     b = dev(cuda, rng.uniform(-0.2, 1.0, shape).astype(np.float32))
     p0 = (rng.uniform(-0.6, 0.6, (3,) + shape) * (rng.uniform(size=(3,) + shape) > 0.3)).astype(np.float32)
