@@ -407,6 +407,10 @@ __global__ void __launch_bounds__(kThreads)
   const int nr = static_cast<int>(min(static_cast<std::size_t>(COLS), rows - r0));
   const int tid = static_cast<int>(threadIdx.x);
   const int nth = static_cast<int>(blockDim.x);
+  // Plane and image row of the tile's first volume row, by one division; those of the others by
+  // counting on from it (a 64-bit division per loaded item cost more than the item's arithmetic).
+  const int y_first = static_cast<int>(r0 % static_cast<std::size_t>(ny));
+  const int z_first = static_cast<int>(r0 / static_cast<std::size_t>(ny));
 
   for (int idx = tid; idx < M * COLS; idx += nth) {
     const int row = idx / M;
@@ -414,8 +418,8 @@ __global__ void __launch_bounds__(kThreads)
     float2 v = make_float2(0.0f, 0.0f);
     if (row < nr) {
       const std::size_t r = r0 + row;
-      const int y = static_cast<int>(r % static_cast<std::size_t>(ny));
-      const int z = static_cast<int>(r / static_cast<std::size_t>(ny));
+      int y = y_first + row, z = z_first;
+      while (y >= ny) y -= ny, ++z;  // row < COLS: at most ceil(COLS / ny) steps
       const std::size_t i0 = r * nx + 2 * m;
       const float2 bv = *reinterpret_cast<const float2*>(b + i0);
       const float2 cz = *reinterpret_cast<const float2*>(pz + i0);
