@@ -90,9 +90,10 @@ class PipelinePlan {
   static constexpr int kOutParts = 8;
   // chunked_upload: the holograms come from input_ in chunks on the copy stream, each first
   // copied there from `host_src` when that is given (or transferred straight from it when it is
-  // page-locked).
+  // page-locked). solve_slot >= 0 (process_stream's volume slot, without marks): the reconstruction
+  // from the fields runs as that slot's CUDA graph, directly on the slot's first use.
   void compute(const float* d_holo, bool chunked_upload, const float2* bg, float* d_index, cudaStream_t s,
-               bool marks, const float* host_src = nullptr, bool host_src_locked = false);
+               bool marks, const float* host_src = nullptr, bool host_src_locked = false, int solve_slot = -1);
 
   CropPlan crop_;
   int count_;
@@ -125,6 +126,8 @@ class PipelinePlan {
   StageClock clock_;
   CapturedWork graph_;
   bool graph_warm_ = false;
+  CapturedWork solve_graph_[2];  // process_stream: the solve into volume slot k, replayed
+  bool solve_warm_[2] = {false, false};
   PipelineTimes timings_;
   double filled_ = 0;
   bool has_background_ = false;

@@ -166,7 +166,9 @@ def test_stream_equals_runs(cuda, odt, items, chunks):
     """qhk_pipeline_run_stream over `items` different stacks gives, volume by volume, bitwise what
     qhk_pipeline_run gives for each stack (the two device volumes alternate, the transfers overlap
     the solves), into a new array or a caller array that is not page aligned; filled is the last
-    stack's; a single run afterwards is unaffected."""
+    stack's; a single run afterwards is unaffected. From a volume slot's second use on, its solve is
+    replayed as a CUDA graph (captured on the third stack, or in the second call), so items = 5 and
+    the second call cover capture and replay."""
     from qoraholo_b200 import capi
 
     il, bg, stacks = _stacks(items, seed=11)
