@@ -312,8 +312,10 @@ int qhk_pipeline_run(qhk_pipeline* pipeline, const float* holograms, float* inde
  * Pipeline::run): holograms (items, count, N, N) -> index (items, nz, m, m), host memory as for
  * qhk_pipeline_run, synchronous. The upload of stack i + 1 and the download of volume i - 1 overlap
  * the solve of stack i, so a stream costs about the device time of its stacks rather than that plus
- * the transfers; each volume is bitwise what qhk_pipeline_run gives for its stack. Afterwards
- * `filled` is that of the last stack and the timings hold only `total`. One more device volume. */
+ * the transfers; each volume is bitwise what qhk_pipeline_run gives for its stack. From each of the
+ * two device volumes' second use on (within a call or across calls), the solve into it is replayed
+ * as a captured CUDA graph instead of being launched kernel by kernel. Afterwards `filled` is that of
+ * the last stack and the timings hold only `total`. One more device volume, and two graphs. */
 int qhk_pipeline_run_stream(qhk_pipeline* pipeline, const float* holograms, int items, float* index);
 /* Device-resident variant: d_holo (count, N, N) and d_index (nz, m, m) on the device, asynchronous on
  * `stream`, no host copies (for serving loops and benchmarks). */
