@@ -916,6 +916,11 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
       // Slot m0 held plane q, last read one iteration ago: plane q+3 streams in for a whole plane.
       if (linear == 0 && q + 3 <= zmax) issue(q + 3, m0, 3, true);
 
+      // z_k of plane a2 that this thread computes and the dual step k below reads again: own row, halo pairs.
+      float zk_own[VEC] = {};
+      float2 hz_own[HALO];
+#pragma unroll
+      for (int j = 0; j < HALO; ++j) hz_own[j] = f2(0.0f, 0.0f);
       if (do_a) {
         const int a = a2;
         const float* Rz = smem2 + (m2 * 3 + 0) * RKP;
@@ -934,9 +939,8 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           Vec<VEC>::load(B + own_b, vb);
           const float from_lane = __shfl_up_sync(lanes, vx[3], 1);
           const float left = (x0 > 0 && lane == 0) ? Rx[own_rk - 1] : from_lane;
-          float out[VEC] = {};
-          if (own) primal4(a, y, vz, vzb, vy, vym, vx, left, vb, out);
-          Vec<VEC>::store(Z + own_b, out);
+          if (own) primal4(a, y, vz, vzb, vy, vym, vx, left, vb, zk_own);
+          Vec<VEC>::store(Z + own_b, zk_own);
         }
 #pragma unroll
         for (int j = 0; j < HALO; ++j) {
@@ -951,6 +955,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
                                              ld2(Rz + i), ld2(Rzb + i), ld2(Ry + i), ld2(Ry + i - P), vx,
                                              f2(x > 0 ? Rx[i - 1] : 0.0f, vx.x), ld2(B + zi * P + x), A.lambda, nzero);
             st2(Z + zi * P + x, o);
+            hz_own[j] = o;
           }
         }
       }
@@ -962,7 +967,6 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
       if (do_b) {
         const int a = a1;
         const float* Zc = smem2 + OZ + (par ^ 1) * BP;
-        const float* Zn = smem2 + OZ + par * BP;  // plane a+1; read only below plane nz-1
         const float* R = smem2 + (m1 * 3) * RKP;
         float* Ry1 = smem2 + ORY;
         float* RzH = smem2 + ORZH + (par ^ 1) * P;  // z component of row y0+TY, plane a1
@@ -971,7 +975,8 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           float zc[VEC], zy[VEC], zz[VEC];
           Vec<VEC>::load(Zc + own_b, zc);
           Vec<VEC>::load(Zc + own_b + P, zy);
-          Vec<VEC>::load(Zn + own_b, zz);
+#pragma unroll
+          for (int k = 0; k < VEC; ++k) zz[k] = zk_own[k];
           const float from_lane = __shfl_down_sync(lanes, zc[0], 1);
           const float right =
               (x0 + VEC < nx && (lane == 31 || lane == warp_threads - 1)) ? Zc[own_b + VEC] : from_lane;
@@ -1005,7 +1010,7 @@ __global__ void __launch_bounds__(fgp2_threads(TY), 1) k_fgp2(Fgp2Args A, const 
           if ((side == 0 || side == 1) && yy >= 0 && yy < ny) {
             const int i = zi * P + x;
             const float2 c0 = ld2(Zc + i);
-            const float2 cz = a < nz - 1 ? ld2(Zn + i) : f2(0.0f, 0.0f);
+            const float2 cz = a < nz - 1 ? hz_own[h] : f2(0.0f, 0.0f);  // this thread's write above
             const float2 cy = yy < ny - 1 ? ld2(Zc + i + P) : f2(0.0f, 0.0f);
             const float2 cx = f2(c0.y, x + 2 < nx ? Zc[i + 2] : 0.0f);
             float2 p[3], r[3];
