@@ -268,7 +268,7 @@ def measured_peaks():
 # kernel at 256^3 with 8-row tiles, from one ncu capture of `python bench.py --kernel-case fgp`
 # (profiles/k_fgp2_256cubed.txt, which gives the command). A constant, not a live measurement: no
 # DRAM counter is readable from inside an unprofiled run. Update it with the profile.
-FGP2_TRAFFIC_BYTES = 1036946432.0
+FGP2_TRAFFIC_BYTES = 1037607168.0
 FGP_TRAFFIC_BYTES = None  # the one-step kernel (not the tuned form at 256^3) has no capture here
 
 
