@@ -12,6 +12,12 @@
 // L2). Per step the HBM traffic is b, r_in (3), p (3) read and p (3), r_out (3) written -- 13
 // volumes; the first step reads p as r (10 volumes) and the last writes no r (10 volumes).
 //
+// Two steps per pass (k_fgp2, for float4 rows of at most 256 x values): a CTA also computes the first
+// step's primal and dual on the rows beyond its tile that the second step reads, so one pass moves 13
+// volumes for two steps. r, b and p arrive as TMA box loads counted on mbarriers (bounded waits), the
+// arithmetic runs on pairs of x points with the packed FP32 instructions, and 256^3 volumes run an
+// instantiation with the sizes compiled in.
+//
 // All arithmetic uses the round-to-nearest intrinsics in the reference's operation order, so the
 // device iterates are bit-identical to the CPU's.
 #include <algorithm>
